@@ -1,0 +1,735 @@
+"""CPU oracle for the real-space Kohn-Sham SCF hot path (TEST INFRASTRUCTURE).
+
+This module is the checker, never the product.  Only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline legs of ``bench.py`` may import
+it.  The product path (``parsec_python_b200``) runs on the GPU through
+``libpsc.so`` and never calls into this file.
+
+It restates, in NumPy/SciPy, the algorithm of PARSEC.py's CPU path
+(zeyizhang-berkeley/parsec_python, ``src/``).  Each function cites the
+reference file:line it follows.  Where the reference has a quirk that changes
+numbers (the aliased first search direction in ``pcg``, the beta rescale in
+``lancz_uppbnd``, the zero-padded tridiagonal in the same routine) the quirk is
+kept, because parity means "the same numbers as the reference".
+
+The restatement deliberately builds the same CSR Hamiltonian as the reference
+(``0.5*A + V_nl + diag(pot)`` with ``A = (1/h^2) * fd3d``) and makes the same
+``numpy.random`` calls in the same order, so that with the same global seed the
+oracle reproduces the reference's SCF trajectory to rounding.  It is pinned
+against fixtures generated by running the reference itself
+(``tests/golden/make_golden.py``).
+"""
+from __future__ import annotations
+
+import math
+from pathlib import Path
+
+import numpy as np
+import scipy.linalg
+import scipy.sparse as sp
+
+A0_ANG = 0.529177210903     # rsdft_models.py:14
+RY_EV = 13.605698066        # rsdft_models.py:15
+
+_DATA = Path(__file__).resolve().parents[1] / "parsec_python_b200" / "data"
+
+
+# ----------------------------------------------------------------------------
+# data tables
+# ----------------------------------------------------------------------------
+def load_elements(path: Path | None = None) -> dict:
+    """Element defaults; columns as in rsdft_input.py:23-31."""
+    path = Path(path or _DATA / "elements.csv")
+    out = {}
+    for order, line in enumerate(path.read_text().splitlines()):
+        if not line.strip():
+            continue
+        f = line.split(",")
+        out[f[0]] = {"order": order, "AtomicNumber": int(f[1]), "Z": int(f[2]),
+                     "Zvalue": float(f[3]), "h": float(f[4]), "r": float(f[5]),
+                     "R": float(f[6])}
+    return out
+
+
+def load_tables(path: Path | None = None) -> dict:
+    """Radial tables (radius, charge, hartree, pot_P, pot_S, wfn_P, wfn_S);
+    V_ion/splineData.py:5-37."""
+    with np.load(path or _DATA / "pseudo_tables.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+# ----------------------------------------------------------------------------
+# splines (Splines/fspline.py, Splines/fsplevalIO.py, Splines/trid.py,
+# V_ion/preProcess.py)
+# ----------------------------------------------------------------------------
+def prune_knots(v: np.ndarray) -> np.ndarray:
+    """Keep knot 0, every knot whose value moved by more than 1e-5 from the
+    previous raw knot, and the last knot.  V_ion/preProcess.py:4-26."""
+    v = np.asarray(v)
+    keep = np.abs(v[1:-1] - v[:-2]) > 10e-6
+    return np.concatenate([[0], np.nonzero(keep)[0] + 1, [len(v) - 1]])
+
+
+def spline_coeffs(xi: np.ndarray, yi: np.ndarray):
+    """Natural cubic spline in the (z, c, d) form of Splines/fspline.py:5-45,
+    tridiagonal solve by Splines/trid.py:3-32 (sequential Thomas sweep)."""
+    xi = np.asarray(xi, dtype=np.float64).ravel()
+    yi = np.asarray(yi, dtype=np.float64).ravel()
+    n = len(xi) - 1
+    h = xi[1:] - xi[:-1]
+    r = (yi[1:] - yi[:-1]) / h
+    r = (r[1:n] - r[0:n - 1]).tolist()
+    a = h[0:n - 1].tolist()
+    c = h[1:n].tolist()
+    d = (2 * (h[0:n - 1] + h[1:n])).tolist()
+    m = len(d)
+    for k in range(1, m):
+        piv = a[k] / d[k - 1]
+        d[k] = d[k] - piv * c[k - 1]
+        r[k] = r[k] - piv * r[k - 1]
+    r[m - 1] = r[m - 1] / d[m - 1]
+    for j in range(m - 2, -1, -1):
+        r[j] = (r[j] - c[j] * r[j + 1]) / d[j]
+    z = np.concatenate([[0.0], np.array(r), [0.0]])
+    cc = (yi[0:n] / h) - (z[0:n] * h)
+    dd = (yi[1:] / h) - (z[1:] * h)
+    return z, cc, dd
+
+
+class Spline:
+    """Knots + coefficients with the evaluation rule of Splines/fsplevalIO.py:2-65:
+    clamp x to [xi[0], xi[-1]], pick the interval [xi[j], xi[j+1]] containing x
+    (binary search convention: largest j with xi[j] <= x, at most n-2), then
+    y = t1*(z_j*t1*t1/h_j + c_j) + t2*(z_{j+1}*t2*t2/h_j + d_j).
+
+    The reference warm-starts the search from the previous point's interval;
+    that can only pick a different (adjacent) interval when x equals a knot
+    exactly, where both intervals give the same value up to rounding."""
+
+    def __init__(self, xi, yi):
+        self.xi = np.asarray(xi, dtype=np.float64)
+        self.z, self.c, self.d = spline_coeffs(self.xi, yi)
+
+    def __call__(self, x):
+        xi = self.xi
+        x = np.clip(np.asarray(x, dtype=np.float64), xi[0], xi[-1])
+        j = np.searchsorted(xi, x, side="right") - 1
+        j = np.clip(j, 0, len(xi) - 2)
+        t1 = xi[j + 1] - x
+        t2 = x - xi[j]
+        hj = xi[j + 1] - xi[j]
+        return t1 * (self.z[j] * t1 * t1 / hj + self.c[j]) + t2 * (self.z[j + 1] * t2 * t2 / hj + self.d[j])
+
+
+def pruned_spline(r, y) -> Spline:
+    idx = prune_knots(y)
+    return Spline(r[idx], y[idx])
+
+
+# ----------------------------------------------------------------------------
+# grid, Laplacian
+# ----------------------------------------------------------------------------
+def fd_stencil(order: int):
+    """Centre weight and per-offset weights of -h^2 * d2/dx2 summed over the
+    three axes; Laplacian/fd3d.py:49-94 (orders <=2, <=4, <=6, else 8)."""
+    if order <= 2:
+        return 6.0, (-1.0,)
+    if order <= 4:
+        return 15 / 2, (-4 / 3, 1 / 12)
+    if order <= 6:
+        return 49 / 6, (-3 / 2, 3 / 20, -1 / 90)
+    return 205 / 24, (-8 / 5, 1 / 5, -8 / 315, 1 / 560)
+
+
+def fd3d(nx: int, ny: int, nz: int, order: int) -> sp.csr_matrix:
+    """Sparse -h^2*Laplacian with zero Dirichlet values outside the cube,
+    flat index p = i + nx*(j + ny*k).  Same entries as Laplacian/fd3d.py:34-106
+    (duplicate diagonals of tiny grids summed)."""
+    c0, cs = fd_stencil(order)
+    n = nx * ny * nz
+    p = np.arange(n)
+    i = p % nx
+    j = (p // nx) % ny
+    k = p // (nx * ny)
+    rows, cols, vals = [p], [p], [np.full(n, c0)]
+    for d, cd in enumerate(cs, start=1):
+        for coord, ext, stride in ((i, nx, 1), (j, ny, nx), (k, nz, nx * ny)):
+            ok = coord + d < ext
+            a = p[ok]
+            b = a + d * stride
+            rows += [a, b]
+            cols += [b, a]
+            vals += [np.full(a.size, cd), np.full(a.size, cd)]
+    m = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    return m.tocsr()
+
+
+def laplacian(domain: dict, order: int) -> sp.csr_matrix:
+    """A = (1/h^2) * fd3d, rsdft_solver.py:186."""
+    h = domain["h"]
+    return ((1.0 / (h * h)) * fd3d(domain["nx"], domain["ny"], domain["nz"], order)).tocsr()
+
+
+# ----------------------------------------------------------------------------
+# ionic setup
+# ----------------------------------------------------------------------------
+def pseudo_diag(domain: dict, atoms: list, elements: dict, tables: dict):
+    """Superposition of atomic densities (SAD), local pseudopotential and the
+    SAD Hartree potential.  V_ion/pseudoDiag.py:44-421.
+
+    Per atom, in species then atom order, and per grid point:
+    ppot += S_potS(r), rho0 += max(0, S_charge(r) * h^3 / (4 pi)),
+    hpot0 += S_hartree(r), with r^2 = (dz^2 + dy^2) + dx^2 (pseudoDiag.py:203-212);
+    finally rho0 <- Z_sum * rho0 / sum(rho0) (pseudoDiag.py:293-297).
+    Returns (rho0, hpot0, ppot, info)."""
+    nx, ny, nz, h, rad = domain["nx"], domain["ny"], domain["nz"], domain["h"], domain["radius"]
+    n = nx * ny * nz
+    pot = np.zeros(n)
+    rho0 = np.zeros(n)
+    hpot0 = np.zeros(n)
+    z_sum = 0.0
+    for species in atoms:
+        typ, xyz = species["typ"], np.asarray(species["coord"], dtype=np.float64)
+        z_sum += elements[typ]["Z"] * xyz.shape[0]
+        data = tables[typ]
+        s_chg = pruned_spline(data[:, 0], data[:, 1])
+        s_pot = pruned_spline(data[:, 0], data[:, 4])
+        s_hrt = pruned_spline(data[:, 0], data[:, 2])
+        for a in range(xyz.shape[0]):
+            dz = (np.arange(nz) * h - rad - xyz[a, 2]) ** 2
+            dy = (np.arange(ny) * h - rad - xyz[a, 1]) ** 2
+            dx = (np.arange(nx) * h - rad - xyz[a, 0]) ** 2
+            r = np.sqrt((dz[:, None, None] + dy[None, :, None]) + dx[None, None, :]).ravel()
+            pot += s_pot(r)
+            rho0 += np.maximum(0, s_chg(r) * (h ** 3) / (4 * np.pi))
+            hpot0 += s_hrt(r)
+    rho0_sum = np.sum(rho0)
+    info = {"electron_count_initial": float(rho0_sum)}
+    rho0 = z_sum * rho0 / rho0_sum
+    info["electron_count_normalized"] = float(np.sum(rho0))
+    info["electron_target"] = float(z_sum)
+    return rho0, hpot0, pot, info
+
+
+def projectors(domain: dict, atoms: list, elements: dict, tables: dict) -> list:
+    """Kleinman-Bylander p-channel projectors in factored form.
+    V_ion/pseudoNL_original.py:9-208.
+
+    For each atom: window of grid points [i0-span, i0+span] (1-based, clipped)
+    with i0 = round((x + rad)/h + 1), span = round(R/h) (Python half-even
+    rounding), points with 0 < |r| < R (|r|^2 = (dx^2 + dy^2) + dz^2), and
+    u_m = (r_m/|r|) * wfn_P(|r|) * (pot_P - pot_S)(|r|), m = x, y, z.
+    V_nl = sum_atoms sum_m u_m u_m^T / xint with xint = Zvalue / h^3.
+    Returns a list of dicts {idx (0-based flat), u (3, n_a), xint}."""
+    nx, ny, nz, h, rad = domain["nx"], domain["ny"], domain["nz"], domain["h"], domain["radius"]
+    out = []
+    for species in atoms:
+        typ, xyz = species["typ"], np.asarray(species["coord"], dtype=np.float64)
+        data = tables[typ]
+        xi = data[:, 0]
+        pot_ps = data[:, 3] - data[:, 4]
+        wfn_p = data[:, 5]
+        s_wfn = pruned_spline(xi, wfn_p)
+        s_pps = pruned_spline(xi, pot_ps)
+        xint = elements[typ]["Zvalue"] / (h ** 3)
+        r0 = elements[typ]["R"]
+        for a in range(xyz.shape[0]):
+            xxa, yya, zza = float(xyz[a, 0]), float(xyz[a, 1]), float(xyz[a, 2])
+            i0 = int(round((xxa + rad) / h + 1))
+            j0 = int(round((yya + rad) / h + 1))
+            k0 = int(round((zza + rad) / h + 1))
+            span = int(round(r0 / h))
+            imin, imax = max(1, i0 - span), min(nx, i0 + span)
+            jmin, jmax = max(1, j0 - span), min(ny, j0 + span)
+            kmin, kmax = max(1, k0 - span), min(nz, k0 + span)
+            if imin > imax or jmin > jmax or kmin > kmax:
+                continue
+            kk, jj, ii = np.meshgrid(np.arange(kmin, kmax + 1), np.arange(jmin, jmax + 1),
+                                     np.arange(imin, imax + 1), indexing="ij")
+            kk, jj, ii = kk.ravel(), jj.ravel(), ii.ravel()
+            xxx = (ii - 1) * h - rad - xxa
+            yyy = (jj - 1) * h - rad - yya
+            zzz = (kk - 1) * h - rad - zza
+            dd = np.sqrt(xxx ** 2 + yyy ** 2 + zzz ** 2)
+            m = (dd > 0) & (dd < r0)
+            if not np.any(m):
+                continue
+            xxx, yyy, zzz, dd = xxx[m], yyy[m], zzz[m], dd[m]
+            idx = (ii[m] - 1) + nx * ((jj[m] - 1) + (kk[m] - 1) * ny)
+            vspp = s_pps(dd)
+            wavpp = s_wfn(dd)
+            u = np.stack([xxx / dd * wavpp * vspp, yyy / dd * wavpp * vspp, zzz / dd * wavpp * vspp])
+            out.append({"idx": idx.astype(np.int64), "u": u, "xint": float(xint), "typ": typ})
+    return out
+
+
+def nonlocal_csr(projs: list, n: int) -> sp.csr_matrix:
+    """Assemble V_nl as the reference does (dense per-atom blocks
+    outer(ux,ux)/xint + outer(uy,uy)/xint + outer(uz,uz)/xint summed over
+    atoms), pseudoNL_original.py:187-206."""
+    vnl = sp.csr_matrix((n, n))
+    for pr in projs:
+        ux, uy, uz = pr["u"]
+        xint = pr["xint"]
+        total = np.outer(ux, ux) / xint + np.outer(uy, uy) / xint + np.outer(uz, uz) / xint
+        idx = pr["idx"]
+        r = np.repeat(idx, idx.size)
+        c = np.tile(idx, idx.size)
+        vnl = vnl + sp.coo_matrix((total.ravel(), (r, c)), shape=(n, n)).tocsr()
+    return vnl.tocsr()
+
+
+def nonlocal_apply(projs: list, x: np.ndarray) -> np.ndarray:
+    """Factored V_nl @ x = sum_a sum_m u_m (u_m . x[idx]) / xint."""
+    y = np.zeros_like(x)
+    for pr in projs:
+        idx, u = pr["idx"], pr["u"]
+        proj = u @ x[idx]                      # (3, k)
+        y[idx] += (u.T @ proj) / pr["xint"]
+    return y
+
+
+def nuclear(atoms: list, elements: dict) -> float:
+    """E_nuc = 2 * sum_{i<j} Z_i Z_j / R_ij (Ry), Laplacian/nuclear.py:26-91."""
+    xs, zs = [], []
+    for species in atoms:
+        xyz = np.asarray(species["coord"], dtype=np.float64)
+        for a in range(xyz.shape[0]):
+            xs.append(xyz[a])
+            zs.append(elements[species["typ"]]["Z"])
+    e = 0
+    for i in range(len(xs)):
+        for j in range(i + 1, len(xs)):
+            d2 = (xs[i][0] - xs[j][0]) ** 2 + (xs[i][1] - xs[j][1]) ** 2 + (xs[i][2] - xs[j][2]) ** 2
+            e += zs[i] * zs[j] / np.sqrt(d2)
+    return float(e * 2)
+
+
+def nelectrons(atoms: list, elements: dict) -> int:
+    """V_ion/nelectrons.py:1-23."""
+    return sum(len(s["coord"]) * elements[s["typ"]]["Z"] for s in atoms)
+
+
+# ----------------------------------------------------------------------------
+# exchange-correlation
+# ----------------------------------------------------------------------------
+def exc_nspn(h: float, rho: np.ndarray):
+    """Ceperley-Alder / Perdew-Zunger LDA, V_xc/exc_nspn.py:8-103.
+    Returns (vxc [Ry], exc [Ry] = h^3 * sum(0.75 rho v_x + rho eps_c))."""
+    g, b1, b2 = -0.2846, 1.0529, 0.3334
+    c1, c2, c3, c4, c5 = 0.0622, 0.096, 0.004, 0.0232, 0.0192
+    third = 1.0 / 3.0
+    a0 = (4.0 / (9.0 * np.pi)) ** third
+    twovpia0 = 2.0 / (np.pi * a0)
+    p75vpi = 0.75 / np.pi
+    rho = np.asarray(rho, dtype=np.float64)
+    vxc = np.zeros_like(rho)
+    pos = rho > 0
+    rv = rho[pos]
+    rs = (p75vpi / rv) ** third
+    vx = -twovpia0 / rs
+    ec = np.empty_like(rs)
+    vc = np.empty_like(rs)
+    hi = rs >= 1.0
+    sq = np.sqrt(rs[hi])
+    ec[hi] = g / (1.0 + b1 * sq + b2 * rs[hi])
+    vc[hi] = (ec[hi] ** 2) * (1.0 + 3.5 * b1 * sq * third + 4.0 * b2 * rs[hi] * third) / g
+    lo = ~hi
+    al = np.log(rs[lo])
+    ec[lo] = c1 * al - c2 + (c3 * al - c4) * rs[lo]
+    vc[lo] = ec[lo] - (c1 + (c3 * al - c5) * rs[lo]) * third
+    vxc[pos] = vx + vc
+    exc = float(np.sum(0.75 * rv * vx + rv * ec)) * h ** 3
+    return vxc, exc
+
+
+# ----------------------------------------------------------------------------
+# eigensolver pieces (Eigensolvers/)
+# ----------------------------------------------------------------------------
+def _gram_upper(vin: np.ndarray, w: np.ndarray) -> np.ndarray:
+    """G[i,j] = Vin_i . W_j for i <= j, mirrored (first_filt.py:53-57,
+    chefsi1.py:51-54)."""
+    m = vin.T @ w
+    return np.triu(m) + np.triu(m, 1).T
+
+
+def lancz_uppbnd(n: int, A, k: int = 6):
+    """Eigensolvers/lancz_uppbnd.py:4-75, including the beta *= 10 rescale that
+    feeds the next step and the zero-padded (j+1)x(j+1) tridiagonal."""
+    k = min(max(k, 6), 10)
+    T = np.zeros((k, k))
+    v = np.random.rand(n, 1)
+    v = v / np.linalg.norm(v)
+    tol = 2.5e-16
+    upperb = np.zeros((3, k))
+    f = A @ v
+    alpha = np.vdot(v, f)
+    f = f - alpha * v
+    T[0, 0] = alpha
+    beta = np.linalg.norm(f)
+    upperb[:, 0] = alpha + beta
+    ritzv = None
+    X = None
+    j = 1
+    for j in range(2, k + 1):
+        if beta > tol:
+            v0 = v
+            v = f / beta
+            f = A @ v
+            f = f - beta * v0
+            alpha = np.vdot(v, f)
+            f = f - alpha * v
+            T[j - 1, j - 2] = beta
+            T[j - 2, j - 1] = beta
+            T[j - 1, j - 1] = alpha
+        else:
+            break
+        beta = np.linalg.norm(f)
+        ritzv, X = scipy.linalg.eigh(T[0:j + 1, 0:j + 1])
+        if beta < 1e-2:
+            beta = beta * 10
+        upperb[0, j - 1] = ritzv[-1] + beta
+        upperb[1, j - 1] = ritzv[-1] + abs(X[-1, -1]) * beta
+        upperb[2, j - 1] = ritzv[-1] + max(abs(X[-1, :])) * beta
+    uppbnd = (upperb[0, j - 1] + upperb[1, j - 1]) / 2
+    uppbnd = (upperb[2, j - 1] + uppbnd) / 2
+    return uppbnd, ritzv
+
+
+def lanczos_bound(B, v) -> float:
+    """Six-step Lanczos bound max|theta| + beta_6;
+    Eigensolvers/lanczosForChefsi1.py:5-99 with nev = m = 6, tol = 0."""
+    m = 6
+    n = B.shape[0]
+    v = v / np.linalg.norm(v)
+    v1 = v
+    v0 = np.zeros((n, 1))
+    bet = 0
+    T = np.zeros((m + 1, m + 1))
+    for kk in range(1, m + 1):
+        v = B @ v1 - bet * v0
+        alp = np.vdot(v1, v)
+        v = v - alp * v1
+        bet = np.linalg.norm(v)
+        v0 = v1
+        v1 = v / bet
+        T[kk - 1, kk - 1] = alp
+        T[kk, kk - 1] = bet
+        T[kk - 1, kk] = bet
+    rr = np.sort(scipy.linalg.eigh(T[:m, :m], eigvals_only=True))
+    return float(max(np.abs(rr)) + bet)
+
+
+def cheb_filter_slim(H, x, polm, low, high):
+    """Unscaled Chebyshev filter, Eigensolvers/first_filt.py:78-103."""
+    e = (high - low) / 2
+    center = (high + low) / 2
+    y = H @ x
+    y = (-y + center * x) / e
+    for _ in range(2, polm + 1):
+        ynew = H @ y
+        ynew = (-ynew + center * y) * 2 / e - x
+        x = y
+        y = ynew
+    return y
+
+
+def ch_filter(A, x, deg, lam1, low, high):
+    """Scaled Chebyshev filter, Eigensolvers/ch_filter.py:4-81."""
+    e = (high - low) / 2
+    c = (high + low) / 2
+    sigma1 = e / (lam1 - c)
+    sigma = sigma1
+    y = (A @ x - c * x) * (sigma1 / e)
+    two_over_s1 = 2.0 / sigma1
+    inv_e = 1.0 / e
+    for _ in range(2, deg + 1):
+        sigma_new = 1.0 / (two_over_s1 - sigma)
+        t1 = 2.0 * sigma_new * inv_e
+        t2 = sigma * sigma_new
+        ynew = (A @ y - c * y) * t1 - t2 * x
+        x = y
+        y = ynew
+        sigma = sigma_new
+    return y
+
+
+def first_filt(nev: int, H, polm: int = 10):
+    """First SCF step: random block + filter + RR rounds,
+    Eigensolvers/first_filt.py:6-75."""
+    energ_tol = 0.08
+    if polm < 10 or polm > 15:
+        polm = 10
+    max_iter = max(min(int(60 / polm), 5), 3)
+    n = H.shape[0]
+    upperb, ritzv = lancz_uppbnd(n, H)
+    lowerb = 0.8 * ritzv[0] + 0.2 * ritzv[-2]
+    W = np.random.rand(n, nev)
+    tr0 = 0.0
+    for it in range(1, max_iter + 1):
+        W = cheb_filter_slim(H, W, polm, lowerb, upperb)
+        W, _ = scipy.linalg.qr(W, mode="economic", pivoting=False)
+        Vin = H @ W
+        G = _gram_upper(Vin, W)
+        ritzv_raw, Q = scipy.linalg.eigh(G)
+        order = np.argsort(ritzv_raw)
+        ritzv = ritzv_raw[order]
+        lowerb = ritzv[-1]
+        W = W @ Q[:, order]
+        if it == 1:
+            tr0 = np.sum(ritzv[:nev])
+        else:
+            tr1 = np.sum(ritzv[:nev])
+            if abs(tr1 - tr0) <= energ_tol * abs(tr0):
+                break
+            tr0 = tr1
+    return W, ritzv
+
+
+def chefsi1(Vin, ritzv, deg, nev, H):
+    """One Chebyshev-filtered subspace step, Eigensolvers/chefsi1.py:10-69."""
+    n, n2 = Vin.shape
+    if nev >= n2:
+        raise ValueError("Vin should have more than nev columns")
+    upperb = lanczos_bound(H, np.random.randn(n, 1))
+    lowerb = np.max(ritzv)
+    lam1 = np.min(ritzv)
+    if lowerb > upperb:
+        raise ValueError("Bounds are incorrect")
+    W = ch_filter(H, Vin, deg, lam1, lowerb, upperb)
+    W, _ = scipy.linalg.qr(W, mode="economic", pivoting=False)
+    V = H @ W
+    G = _gram_upper(V, W)
+    ritzv_raw, Q = scipy.linalg.eigh(G)
+    order = np.argsort(ritzv_raw)
+    return W @ Q[:, order], ritzv_raw[order]
+
+
+def fermi_dirac(lam, ef, temp, nelec):
+    """Eigensolvers/FermiDirac.py:3-31 (kT = T * 6.33327186e-06, spin 1)."""
+    kT = temp * 6.33327186e-06
+    logits = (lam - ef) / kT
+    e = np.exp(-np.abs(logits))
+    occ = np.where(logits >= 0, e / (1.0 + e), 1.0 / (1.0 + e))
+    return np.sum(occ) - nelec / 2, occ
+
+
+def occupations(lam, temp, nelec, tol):
+    """Bisection for the Fermi level, Eigensolvers/occupations.py:5-56."""
+    lam = np.asarray(lam, dtype=np.float64)
+    its = 0
+    a = np.min(lam) - 1
+    fa, _ = fermi_dirac(lam, a, temp, nelec)
+    lmax = min(max(1, int(np.ceil(nelec / 2)) + 1), len(lam))
+    b = lam[lmax - 1] + 1
+    fb, _ = fermi_dirac(lam, b, temp, nelec)
+    c = (b + a) / 2
+    fc, occ = fermi_dirac(lam, c, temp, nelec)
+    error = 2 * np.sum(occ) - nelec
+    if fa * fb > tol:
+        return b, np.ones(len(lam))
+    while abs(error) > tol and its < 200:
+        its += 1
+        c = (b + a) / 2
+        fc, occ = fermi_dirac(lam, c, temp, nelec)
+        error = 2 * np.sum(occ) - nelec
+        if fc * fb < 0:
+            a = c
+        else:
+            b = c
+            fb = fc
+    return c, occ
+
+
+def pcg(A, rhs, x0, m, tol):
+    """Unpreconditioned CG, Eigensolvers/pcg.py:7-85.  In the reference the
+    first search direction p aliases the residual array r (z = r; p = z), so
+    the in-place update r -= alp*Ap also moves p, and the first direction
+    update gives p = (1 + beta) * r_1.  That is kept here."""
+    x = np.array(x0, dtype=np.float64)
+    r = rhs - A.dot(x)
+    ro1 = np.dot(r, r)
+    tol1 = tol * tol * ro1
+    its = 0
+    p = None
+    while its < m and ro1 > tol1:
+        its += 1
+        ro = ro1
+        ap = A.dot(r if p is None else p)
+        alp = ro / np.dot(ap, r if p is None else p)
+        x += alp * (r if p is None else p)
+        r = r - alp * ap
+        ro1 = np.dot(r, r)
+        bet = ro1 / ro
+        p = r + bet * r if p is None else r + bet * p
+    return x, its
+
+
+# ----------------------------------------------------------------------------
+# mixer (Mixer/msecant1.py with Mixer/includemix.py parameters)
+# ----------------------------------------------------------------------------
+def qinv(A, tol=np.finfo(float).eps):
+    """Quasi-inverse by pivoted QR, Mixer/qinv.py:5-62."""
+    m, n = A.shape
+    if m < n:
+        return qinv(A.T, tol).T
+    tol = tol * np.linalg.norm(A, np.inf)
+    Q, R, P = scipy.linalg.qr(A, mode="economic", pivoting=True)
+    r = n
+    for i in range(n):
+        if abs(R[i, i]) < tol:
+            r = i
+            break
+    S = np.zeros((r, r))
+    for j in range(r - 1, -1, -1):
+        S[j, j] = 1 / R[j, j]
+        for i in range(j - 1, -1, -1):
+            t = 0
+            for kk in range(i + 1, r):
+                t += R[i, kk] * S[kk, j]
+            S[i, j] = -t / R[i, i]
+    B = np.zeros((n, m))
+    B[:r, :] = S @ Q[:, :r].T
+    q = np.zeros(n, dtype=int)
+    for i in range(n):
+        q[P[i]] = i
+    return B[q, :]
+
+
+class MSecant1:
+    """Multisecant Type-I (Broyden-1 with group_size 1, mix 0.5, restart
+    factor 0.1), Mixer/msecant1.py:6-175 with Mixer/includemix.py:21-49."""
+
+    def __init__(self, mix=0.5, group_size=1, restart_factor=0.1):
+        self.mix, self.sz, self.rf = mix, group_size, restart_factor
+        self.tol = np.finfo(float).eps
+        self.DX = None
+        self.DF = None
+        self.N = None
+
+    def __call__(self, x1, f1):
+        mix, sz = self.mix, self.sz
+        x1 = np.asarray(x1, dtype=np.float64).ravel()
+        f1 = np.asarray(f1, dtype=np.float64).ravel()
+        m = 0 if self.DX is None else self.DX.shape[1]
+        if m == 0:
+            self.DX = x1[:, None].copy()
+            self.DF = f1[:, None].copy()
+            return x1 + mix * f1, 0
+        if m >= 2:
+            if np.linalg.norm(self.DF[:, m - 1]) < self.rf * np.linalg.norm(f1):
+                xr = self.DX[:, m - 1].copy()
+                fr = self.DF[:, m - 1].copy()
+                self.DX = xr[:, None]
+                self.DF = fr[:, None]
+                self.N = None
+                return xr + mix * fr, 0
+        res = (m + sz - 1) % sz + 1
+        ngroup = (m - res) // sz
+        self.DX[:, m - 1] = x1 - self.DX[:, m - 1]
+        self.DF[:, m - 1] = f1 - self.DF[:, m - 1]
+        dx = self.DX[:, m - 1].copy()
+        self.DX[:, m - 1] = self.DX[:, m - 1] + mix * self.DF[:, m - 1]
+        for i in range(1, ngroup + 1):
+            s, e = (i - 1) * sz, i * sz
+            self.DX[:, m - 1] = self.DX[:, m - 1] - self.DX[:, s:e] @ (self.DF[:, s:e].T @ self.DF[:, m - 1])
+        x_new = x1 + mix * f1
+        for i in range(1, ngroup + 1):
+            s, e = (i - 1) * sz, i * sz
+            x_new = x_new - self.DX[:, s:e] @ (self.DF[:, s:e].T @ f1)
+        if self.N is None or self.N.shape[1] < res:
+            self.N = np.zeros((x1.size, sz))
+        self.N[:, res - 1] = -mix * dx
+        for i in range(1, ngroup + 1):
+            s, e = (i - 1) * sz, i * sz
+            self.N[:, res - 1] = self.N[:, res - 1] + self.DF[:, s:e] @ (self.DX[:, s:e].T @ dx)
+        M = self.N[:, :res].T @ self.DF[:, m - res:m]
+        C = qinv(M, self.tol)
+        if res == sz:
+            self.DF[:, m - sz:m] = self.N[:, :sz] @ C.T
+            x_new = x_new - self.DX[:, m - res:m] @ (self.DF[:, m - res:m].T @ f1)
+        else:
+            x_new = x_new - self.DX[:, m - res:m] @ ((C @ self.N[:, :res].T) @ f1)
+        self.DX = np.hstack([self.DX, x1[:, None]])
+        self.DF = np.hstack([self.DF, f1[:, None]])
+        return x_new, m
+
+
+# ----------------------------------------------------------------------------
+# energies and the SCF loop (rsdft_solver.py)
+# ----------------------------------------------------------------------------
+def energy_components(rho, hpot, hpot0, vxc, exc, lam, occ, nev, e_nuc, h):
+    """rsdft_solver.py:128-153 (Rydberg)."""
+    esum = float(np.sum(lam[:nev] * occ[:nev]))
+    eig = 4.0 * esum
+    eh = float(np.sum(rho * (hpot + hpot0)) * h ** 3)
+    vxc_sum = float(np.sum(rho * vxc) * h ** 3)
+    total = eig - eh + float(exc) - vxc_sum + float(e_nuc)
+    return {"eigen_sum_ry": eig, "hartree_ry": eh, "xc_ry": float(exc), "ion_ry": float(e_nuc),
+            "total_ry": total}
+
+
+def build_system(atoms: list, *, h: float, radius: float, elements: dict | None = None):
+    """Domain for a given spacing and sphere radius (bohr), as
+    rsdft_setup.estimate_radius_and_grid (rsdft_setup.py:133-150) does with a
+    radius override."""
+    nx = int(2 * radius / h) + 1
+    nx = 2 * ((nx + 1) // 2)
+    rad = 0.5 * h * (nx - 1)
+    return {"radius": rad, "nx": nx, "ny": nx, "nz": nx, "h": h}
+
+
+def run_scf(domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
+            maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, seed: int | None = None,
+            z_charge: float = 0.0, elements=None, tables=None, log=None) -> dict:
+    """The SCF loop of rsdft_solver.run_rsdft_calculation (rsdft_solver.py:156-462)
+    for density_method = sad, diagmeth = 3, adaptive_scheme = 0, cg_prec = 0."""
+    elements = elements or load_elements()
+    tables = tables or load_tables()
+    if seed is not None:
+        np.random.seed(seed)
+    h = domain["h"]
+    A = laplacian(domain, fd_order)
+    n = A.shape[0]
+    Hpot = np.zeros(n)
+    err = 10.0 + tol
+    e_nuc = nuclear(atoms, elements)
+    rho0, hpot0, ppot, info = pseudo_diag(domain, atoms, elements, tables)
+    projs = projectors(domain, atoms, elements, tables)
+    vnl = nonlocal_csr(projs, n)
+    rhoxc = rho0 / h ** 3
+    xcpot, exc = exc_nspn(h, rhoxc)
+    nelec = nelectrons(atoms, elements) - z_charge
+    pot = ppot + hpot0 + 0.5 * xcpot
+    mixer = MSecant1()
+    half_a_plus_vnl = 0.5 * A + vnl
+    W = lam = None
+    history = []
+    its = 0
+    rho = np.zeros(n)
+    XCpot = xcpot
+    while err > tol and its < maxits:
+        its += 1
+        B = (half_a_plus_vnl + sp.diags(pot, 0, shape=(n, n))).tocsr()
+        if its == 1:
+            W, lam = first_filt(nev + 15, B, poldeg)
+        else:
+            W, lam = chefsi1(W, lam, poldeg, nev, B)
+        _, occ = occupations(lam[:nev], fermi_temp, nelec, 1e-6)
+        rho = (W[:, :nev] ** 2) @ (2 * occ)
+        hrhs = (4 * np.pi / h ** 3) * (rho - rho0)
+        rho = rho / h ** 3
+        Hpot, cg_its = pcg(A, hrhs, Hpot, 200, 1e-5)
+        XCpot, exc = exc_nspn(h, rho)
+        pot_new = ppot + 0.5 * XCpot + Hpot + hpot0
+        err = float(np.linalg.norm(pot_new - pot) / np.linalg.norm(pot_new))
+        en = energy_components(rho, Hpot, hpot0, XCpot, exc, lam, occ, nev, e_nuc, h)
+        history.append({"iter": its, "err": err, "lam": lam.copy(), "occ": np.asarray(occ).copy(),
+                        "cg_its": cg_its, **en})
+        if log:
+            log(f"iter {its} err {err:.3e} E {en['total_ry']:.10f}")
+        pot, _ = mixer(pot, pot_new - pot)
+    return {"rho": rho, "hpot": Hpot, "xc_potential": XCpot, "exc": float(exc), "potential": pot,
+            "W": W, "eigenvalues": lam, "occupations": occ, "iterations": its, "error": err,
+            "converged": err <= tol, "e_nuc0": e_nuc, "hpot0": hpot0, "rho0": rho0, "ppot": ppot,
+            "history": history, "energies": history[-1] if history else None, "diag_info": info}
