@@ -1,0 +1,430 @@
+"""Benchmark: SCF time-to-solution of the C10H8 configuration on the GPU.
+
+One step = one complete SCF solve (SAD setup, projector setup, first filter,
+Chebyshev-filtered subspace iterations, Hartree CG, LDA XC, mixing) of the
+planar naphthalene molecule (sphere radius 7 A, spacing 0.18 A -> 78^3 =
+474,552 grid points, nev 40 -> 55 subspace columns, poldeg 12, tol 1e-6),
+started from the atom coordinates with the pseudopotential tables already in
+device memory.  The step's device work is timed with CUDA events on the
+launching stream; the SCF working set (two 474,552 x 55 FP64 blocks = 418 MB
+plus the mixer history) is larger than the 126 MB L2, so no flush is needed.
+
+Extra keys: `e2e` times the public entry (input file -> .out log + density
+.npy files on the host) with host<->device copies inside; `roofline` times
+the fused H.X stencil (one Chebyshev step, FP64, k = 55) against the
+measured HBM copy bandwidth; `cpu_baseline` times the CPU oracle on a bounded
+sample (setup, first filter step, two more SCF iterations; extrapolated to
+the run's iteration count).
+
+--impl reference times that CPU implementation of the path alone (the
+reference is pure Python and does not run on the GPU box; its port, the
+oracle, does), one SCF iteration per step.  Multi-GPU runs are independent
+replicas (the SCF of one molecule does not shard in this implementation).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CFG_NAME = "c10h8"
+METRIC = "SCF time-to-1e-5 Ha (C10H8, FP64 GPU SCF); H.X GB/s"
+
+
+def workload_config(precision: str) -> dict:
+    return {"workload": "C10H8 naphthalene SCF: sphere radius 7 A, h 0.18 A, 78^3 = 474,552 points, nev 40 "
+                        "(k = 55), poldeg 12, fd_order 8, tol 1e-6, LDA, SAD init, msecant1 mixing",
+            "precision": precision, "init": "sad", "global_batch": 1, "parallelism": "replicas",
+            "l2": "working set (2 x 209 MB subspace blocks + mixer history) > 126 MB L2; no flush"}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if _cuda() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return rank, local, world
+
+
+def _cuda() -> bool:
+    import torch
+
+    return torch.cuda.is_available()
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def allmax(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if _cuda() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in self.path.read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def gpu_problem(precision: str, seed: int, name: str = CFG_NAME):
+    from parsec_python_b200 import workloads
+    from parsec_python_b200.inputs import ElementTable
+    from parsec_python_b200.models import SolverSettings
+    from parsec_python_b200.system import system_from_atoms
+
+    cfg = workloads.config_system(name)
+    s = SolverSettings(tol=cfg["tol"], poldeg=cfg["poldeg"], maxits=60, precision=precision, seed=seed)
+    s.normalize()
+    elem = ElementTable()
+    prob = system_from_atoms(cfg["atoms"], h=cfg["h"], radius=cfg["radius"], nev=cfg["nev"], settings=s, elem=elem)
+    return prob, elem, s
+
+
+def reference_energy(name: str = CFG_NAME):
+    f = ROOT / "tests" / "golden" / f"ref_{name}.json"
+    if f.exists():
+        m = json.loads(f.read_text())
+        return m["total_ry"], m["iterations"]
+    return None, None
+
+
+def solve_once(precision: str, seed: int):
+    from parsec_python_b200.backend import select_solver_backend
+    from parsec_python_b200.solver import run_rsdft_calculation
+
+    prob, elem, s = gpu_problem(precision, seed)
+    backend = select_solver_backend(s)
+    return run_rsdft_calculation(prob, elem, len(elem), backend, verbose=False)
+
+
+def stencil_roofline(reps: int = 40) -> dict:
+    """Time the fused stencil (one Chebyshev step Out = a H In + b In + g Prev,
+    FP64, k = 55, no projectors so that only the stencil kernel launches) on
+    the C10H8 grid; algorithmic bytes = read In + read Prev + write Out + read
+    pot = (3 k + 1) n 8."""
+    import torch
+
+    from parsec_python_b200 import gpu
+    from parsec_python_b200._lib import F64
+
+    prob, _, _ = gpu_problem("fp64", 0)
+    ctx = gpu.GridContext(prob.domain, 8)
+    n, k = ctx.n, prob.nev + 15
+    pot = torch.randn(n, dtype=torch.float64, device="cuda")
+    gpu.Hamiltonian(ctx, pot)
+    X = torch.randn(k, n, dtype=torch.float64, device="cuda")
+    Y = torch.randn(k, n, dtype=torch.float64, device="cuda")
+    st = gpu._stream()
+
+    def step(a, b):
+        ctx.call("psc_apply_h_axpby", F64, gpu._p(a), n, gpu._p(b), n, gpu._p(b), n, k, 0.1, -0.3, -0.5, st)
+
+    for _ in range(5):
+        step(X, Y)
+        step(Y, X)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(reps):
+        step(X, Y) if i % 2 == 0 else step(Y, X)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1000.0 / reps
+    bytes_ = (3 * k + 1) * n * 8
+    flops = n * k * (2 * (3 * 8 + 1) + 2 + 4)
+    return {"seconds": t, "bytes": bytes_, "gbs": bytes_ / t / 1e9, "gflops": flops / t / 1e9, "n": n, "k": k}
+
+
+def measured_peak() -> tuple[float, str]:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def stencil_traffic():
+    f = ROOT / "profiles" / "stencil_traffic.json"
+    if f.exists():
+        try:
+            return json.loads(f.read_text()).get("dram_bytes_per_launch_c10h8")
+        except Exception:
+            return None
+    return None
+
+
+E2E_INPUT = """$system
+{atoms}
+$system
+
+$settings
+unit = Angstrom
+density_method = sad
+grid_spacing = 0.180000
+sphere_radius = 7.000000
+tol = 1e-06
+Fermi_temp = 500
+maxits = 60
+fd_order = 8
+poldeg = 12
+diagmeth = 3
+nev = 40
+recenter_atoms = 0
+precision = {precision}
+$settings
+"""
+
+
+def e2e_once(precision: str, workdir: Path) -> tuple[float, int, int]:
+    """Public entry: write an input file, run it, read the outputs from disk."""
+    import torch
+
+    from parsec_python_b200 import __main__ as cli
+    from parsec_python_b200 import workloads
+
+    atoms = workloads.CONFIGS[CFG_NAME]["atoms"]()
+    lines = "\n".join(f"{a['typ']} {x:.8f} {y:.8f} {z:.8f}" for a in atoms for x, y, z in a["coord"])
+    inp = workdir / "c10h8.in"
+    inp.write_text(E2E_INPUT.format(atoms=lines, precision=precision))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = cli.main([str(inp)])
+    rho = np.load(workdir / "c10h8_conv_rho_grid.npy")
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    n = rho.size
+    k = 55
+    # host->device: species tables (5 splines x 4 arrays per species) + atoms + potential-free setup
+    from parsec_python_b200.inputs import pseudo_tables
+
+    tabs = pseudo_tables()
+    h2d = sum(5 * 4 * tabs[s].shape[0] * 8 for s in ("C", "H")) + 18 * (3 * 8 + 4) * 2
+    # device->host: init/conv densities (n doubles each), per-iteration log block, CG/mixer scalars
+    d2h = 2 * n * 8 + res.iterations * ((2 * k + 8) * 8 + 16 * 8)
+    return dt, h2d, d2h
+
+
+def cpu_sample(n_extra: int = 2, steps_total: int | None = None) -> dict:
+    """Oracle SCF on the host cores: setup, first iteration, n_extra more."""
+    from oracle import oracle as O
+    from parsec_python_b200 import workloads
+
+    cfg = workloads.config_system(CFG_NAME)
+    atoms = cfg["atoms"]
+    dom = O.build_system(atoms, h=cfg["h"], radius=cfg["radius"])
+    np.random.seed(0)
+    scf = O.OracleSCF(dom, atoms, nev=cfg["nev"], poldeg=cfg["poldeg"], tol=cfg["tol"], maxits=60)
+    scf.setup()
+    t_first = scf.step()["wall"]
+    walls = [scf.step()["wall"] for _ in range(n_extra)]
+    return {"t_setup": scf.t_setup, "t_first": t_first, "t_iter": float(np.mean(walls)), "walls": walls,
+            "scf": scf}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle as Orc
+    from parsec_python_b200 import workloads
+
+    _, ref_its = reference_energy()
+    cfg = workloads.config_system(CFG_NAME)
+    atoms = cfg["atoms"]
+    dom = Orc.build_system(atoms, h=cfg["h"], radius=cfg["radius"])
+    np.random.seed(0)
+    scf = Orc.OracleSCF(dom, atoms, nev=cfg["nev"], poldeg=cfg["poldeg"], tol=cfg["tol"], maxits=60)
+    scf.setup()
+    t_first = scf.step()["wall"]
+    for _ in range(args.warmup):
+        scf.step()
+    walls = [scf.step()["wall"] for _ in range(args.steps)]
+    its = ref_its or 23
+    value = scf.t_setup + t_first + (its - 1) * float(np.mean(walls))
+    cores = os.cpu_count()
+    sample = (f"oracle (NumPy/SciPy port of the reference CPU path) on {cores} host threads: setup "
+              f"{scf.t_setup:.1f}s + first SCF iteration {t_first:.1f}s + {args.steps} timed SCF iterations "
+              f"(mean {np.mean(walls):.2f}s) extrapolated to {its} iterations")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(walls)) * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic C10H8 geometry; the reference's pseudopotential tables",
+            "config": workload_config("fp64"),
+            "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu_arm(args, rank, local, world):
+    import torch
+
+    from parsec_python_b200 import _lib
+
+    torch.cuda.set_device(local)
+    lib = _lib.load()
+    prec = args.precision
+    e_ref, ref_its = reference_energy()
+    for w in range(args.warmup):
+        solve_once(prec, seed=100 + w)
+    torch.cuda.synchronize()
+    barrier(world)
+    times, energies, iters = [], [], []
+    launches0 = lib.psc_launch_count()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier(world)
+        for s in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = solve_once(prec, seed=1000 * rank + s)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1000.0)
+            energies.append(res.history[-1]["total_ry"])
+            iters.append(res.iterations)
+        torch.cuda.synchronize()
+        barrier(world)
+    launches = (lib.psc_launch_count() - launches0) // max(1, args.steps)
+    clocks = clk.summary()
+    t_step = allmax(float(np.mean(times)), world)
+    roof = stencil_roofline()
+    peak, peak_kind = measured_peak()
+    err_ha = None if e_ref is None else max(abs(e - e_ref) for e in energies) / 2.0
+    e2e_t = h2d = d2h = None
+    if rank == 0:
+        with tempfile.TemporaryDirectory() as td:
+            e2e_once(prec, Path(td))  # warm the public path once
+            e2e_t, h2d, d2h = e2e_once(prec, Path(td))
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cs = cpu_sample(2)
+        its = int(np.median(iters))
+        v = cs["t_setup"] + cs["t_first"] + (its - 1) * cs["t_iter"]
+        cpu = {"value": v, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"oracle on {os.cpu_count()} host threads: setup {cs['t_setup']:.1f}s + first SCF "
+                         f"iteration {cs['t_first']:.1f}s + 2 iterations (mean {cs['t_iter']:.2f}s), extrapolated "
+                         f"to the GPU run's {its} iterations"}
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32+f64",
+            "data": "synthetic C10H8 geometry; the reference's pseudopotential tables",
+            "config": workload_config(prec),
+            "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": roof["gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": roof["gbs"] / peak, "traffic": stencil_traffic(),
+                         "kernel": "k_stencil<double,4,2> (one Chebyshev step, k=55)",
+                         "peak_kind": peak_kind, "launch_s": roof["seconds"],
+                         "algorithmic_bytes": roof["bytes"]},
+            "hx_gbs": roof["gbs"], "hx_gflops": roof["gflops"],
+            "cpu_baseline": cpu, "clocks": clocks,
+            "iterations": int(np.median(iters)), "energy_error_ha_vs_reference": err_ha,
+            "reference_iterations": ref_its, "step_times_s": times}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, local, world = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, rank, world)
+        else:
+            run_gpu_arm(args, rank, local, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

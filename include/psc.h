@@ -1,0 +1,163 @@
+/*
+ * libpsc -- C ABI of the B200 (sm_100a) real-space Kohn-Sham SCF hot path.
+ *
+ * Plain pointers and sizes only.  Vectors are device pointers; a block of k
+ * vectors is column-major with leading dimension ld >= n = nx*ny*nz, grid
+ * index p = i + nx*(j + ny*k) (x fastest), zero Dirichlet values outside the
+ * cube.  `stream` is a cudaStream_t passed as void*.  Every function returns
+ * 0 on success, 2 for an invalid argument and 1 for a CUDA error; the message
+ * is available from psc_last_error().  Units follow the reference: bohr,
+ * Hartree for the Hamiltonian, Rydberg for XC potentials and energies.
+ *
+ * Each declaration names the part of PARSEC.py (zeyizhang-berkeley/
+ * parsec_python, src/) whose behaviour it reproduces.  In the reference these
+ * steps sit behind rsdft_backend.select_solver_backend (rsdft_backend.py:80)
+ * and the SolverBackend bundle (rsdft_models.py:179-217); XC, mixing and the
+ * Laplacian are direct imports in rsdft_solver.py:20-26.
+ */
+#ifndef PSC_H
+#define PSC_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSC_ABI_VERSION 1
+
+typedef struct psc_ctx psc_ctx;
+
+/* element types of vector blocks */
+#define PSC_DTYPE_F64 0
+#define PSC_DTYPE_F32 1
+
+int psc_version(void);
+/* Number of kernels this library has launched in the process so far. */
+long long psc_launch_count(void);
+const char* psc_last_error(const psc_ctx* ctx);
+
+/* Grid context: nx*ny*nz cube, spacing h (bohr), finite-difference order
+ * (orders <= 2, <= 4, <= 6, else 8 as Laplacian/fd3d.py:49-94).
+ * Replaces the construction A = (1/h^2) fd3d(...) at rsdft_solver.py:186. */
+int psc_ctx_create(int nx, int ny, int nz, double h, int fd_order, psc_ctx** out);
+int psc_ctx_destroy(psc_ctx* ctx);
+/* out[8] = nx, ny, nz, n, projector atoms, projector points, touched points, stencil radius */
+int psc_ctx_info(const psc_ctx* ctx, long* out);
+/* host flags[8] of device-side checks (1: filter bounds inverted, 2: Cholesky
+ * pivot <= 0 at column flags[1]-1, 3: Jacobi not converged); clear != 0 resets */
+int psc_status(psc_ctx* ctx, int* host_flags, int clear, void* stream);
+
+/* ---- ionic setup ------------------------------------------------------ */
+/* Radial tables of one species: row-major nknots x 7 (radius, charge,
+ * hartree, pot_P, pot_S, wfn_P, wfn_S) as V_ion/splineData.py:5-37; knots
+ * pruned by V_ion/preProcess.py:4-26, natural cubic splines by
+ * Splines/fspline.py:5-45.  zvalue/rcut: the Zvalue and R element columns. */
+int psc_set_species(psc_ctx* ctx, int species_id, int nknots, const double* table, double zvalue, double rcut);
+/* The host spline construction alone (pruning + coefficients), for checks. */
+int psc_spline_coeffs(int nknots, const double* x, const double* y, int* nkeep, double* xk, double* z,
+                      double* c, double* d);
+/* SAD density, local pseudopotential and SAD Hartree potential:
+ * V_ion/pseudoDiag.py:44-421 (backend.pseudo_diag, rsdft_solver.py:87).
+ * species/xyz (host): natoms entries in species-major order, bohr.
+ * h3 = h**3, fourpi = 4*pi, z_sum = sum of valence charges.
+ * info[2] (host) = electron count before / after normalisation. */
+int psc_sad_setup(psc_ctx* ctx, int natoms, const int* species, const double* xyz, double radius, double h3,
+                  double fourpi, double z_sum, double* rho0, double* hpot0, double* ppot, double* info,
+                  void* stream);
+/* Kleinman-Bylander projector tables (factored V_nl):
+ * V_ion/pseudoNL_original.py:9-208 (backend.pseudo_nl, rsdft_solver.py:116). */
+int psc_projector_setup(psc_ctx* ctx, int natoms, const int* species, const double* xyz, double radius,
+                        void* stream);
+/* Host copies of the projector tables (atom_off[atoms+1], idx[points],
+ * u[3*points], w[atoms]); any pointer may be NULL. */
+int psc_projector_export(psc_ctx* ctx, int* atom_off, int* idx, double* u, double* w);
+/* np.sum order (pairwise) of a device vector, result on the device. */
+int psc_numpy_sum(psc_ctx* ctx, const double* x, long n, double* out_dev, void* stream);
+
+/* ---- Hamiltonian ------------------------------------------------------ */
+/* Diagonal potential (Hartree, device, n): B = 0.5A + V_nl + diag(pot) at
+ * rsdft_solver.py:285 without assembling B. */
+int psc_set_potential(psc_ctx* ctx, const double* pot, void* stream);
+/* Y = H X for k columns (the SpMM `H @ X` in the Eigensolvers package). */
+int psc_apply_h(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long ldy, int k, void* stream);
+/* Y = alpha H X + beta X + gamma P (P may be NULL or alias Y). */
+int psc_apply_h_axpby(psc_ctx* ctx, int dtype, const void* X, long ldx, const void* P, long ldp, void* Y, long ldy,
+                      int k, double alpha, double beta, double gamma, void* stream);
+/* Y = A X with A = -Lap_h (Laplacian/fd3d.py:34-106 scaled by 1/h^2). */
+int psc_laplacian_apply(psc_ctx* ctx, const double* x, double* y, int k, long ld, void* stream);
+
+/* ---- eigensolver pieces ------------------------------------------------ */
+/* Chebyshev filter of degree deg, bounds_dev = [lam1, low, high] on the
+ * device.  mode 0: scaled filter Eigensolvers/ch_filter.py:4-81; mode 1:
+ * cheb_filter_slim Eigensolvers/first_filt.py:78-103.  X holds the input and
+ * is overwritten; *which = 0 if the result is in X, 1 if in Y. */
+int psc_cheb_filter(psc_ctx* ctx, int dtype, int mode, int deg, const double* bounds_dev, void* X, void* Y,
+                    long ld, int k, int* which, void* stream);
+/* Six-step Lanczos bound.  mode 0: Eigensolvers/lancz_uppbnd.py:4-75,
+ * out = [uppbnd, ritz_0..ritz_5]; mode 1: Eigensolvers/lanczosForChefsi1.py:5-99,
+ * out = [bound].  The start vector is drawn from `seed`. */
+int psc_lanczos_bound(psc_ctx* ctx, int mode, unsigned long long seed, double* out_dev, void* stream);
+/* Filter interval from device values: mode 0 chefsi1.py:29-38
+ * ([min ritz, max ritz, upper]); mode 1 first_filt.py:28-29; mode 2 first_filt.py:62. */
+int psc_filter_bounds(psc_ctx* ctx, int mode, const double* ritz_dev, int k, const double* upper_dev,
+                      double* bounds_dev, void* stream);
+/* Orthonormalise k columns by CholeskyQR applied `passes` times (replaces
+ * scipy.linalg.qr at Eigensolvers/chefsi1.py:43 and first_filt.py:43). */
+int psc_orthonormalize(psc_ctx* ctx, int dtype, void* W, void* T, long ld, int k, int passes, int* which,
+                       void* stream);
+/* Rayleigh-Ritz (chefsi1.py:46-67, first_filt.py:44-63): V = H W,
+ * G = W^T H W (upper triangle mirrored), ascending eigenpairs, result W Q
+ * written to V, Ritz values to ritz_dev. */
+int psc_rayleigh_ritz(psc_ctx* ctx, int dtype, const void* W, void* V, long ld, int k, double* ritz_dev,
+                      void* stream);
+/* Building blocks: G = A^T B (mode 0 plain, 1 upper mirrored, 2 symmetrised),
+ * Out = W Q, symmetric eigensolver (ascending, FP64, one CTA, k <= 1023). */
+int psc_gram(psc_ctx* ctx, int dtype, const void* A, long lda, const void* B, long ldb, int k, int mode,
+             double* out_dev, void* stream);
+int psc_gemm_nn(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Q, int kout, void* out,
+                long ldo, void* stream);
+int psc_syev(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, void* stream);
+/* Fermi level and occupations by bisection: Eigensolvers/occupations.py:5-56
+ * with Eigensolvers/FermiDirac.py:3-31 (backend.occupations, rsdft_solver.py:319). */
+int psc_occupations(psc_ctx* ctx, const double* lam_dev, int n, double temp, double nelec, double tol,
+                    double* ef_dev, double* occ_dev, void* stream);
+/* rho = sum_i W_i^2 (2 f_i) / h^3 and hrhs = fourpi_h3 (h^3 rho - rho0)
+ * (rsdft_solver.py:324-328); hrhs may be NULL. */
+int psc_density(psc_ctx* ctx, int dtype, const void* W, long ld, int nev, const double* occ_dev,
+                const double* rho0, double fourpi_h3, double h3, double* rho, double* hrhs, void* stream);
+
+/* ---- Hartree, XC, update, mixing ---------------------------------------- */
+/* CG on A x = rhs, warm start in x (Eigensolvers/pcg.py:7-85, backend.pcg at
+ * rsdft_solver.py:345). *its_out = iterations. */
+int psc_pcg_poisson(psc_ctx* ctx, const double* rhs, double* x, int maxit, double tol, int* its_out, void* stream);
+/* LDA (Ceperley-Alder / Perdew-Zunger), V_xc/exc_nspn.py:8-103.
+ * out_dev = [exc, max rho, min rho]. */
+int psc_lda_xc(psc_ctx* ctx, const double* rho, double* vxc, double h3, double* out_dev, void* stream);
+/* pot_new = ppot + 0.5 vxc + hpot + hpot0, f = pot_new - pot (may be NULL),
+ * out_dev = [|f|^2, |pot_new|^2, sum rho(hpot+hpot0), sum rho vxc]
+ * (rsdft_solver.py:351-352 and :141-146). */
+int psc_scf_update(psc_ctx* ctx, const double* ppot, const double* vxc, const double* hpot, const double* hpot0,
+                   const double* rho, const double* pot, double* pot_new, double* f, double* out_dev, void* stream);
+/* Multisecant Type-I mixer, group size 1: Mixer/mixer.py:169-217 and
+ * Mixer/msecant1.py:40-175.  reset clears the history (capacity columns). */
+int psc_mixer_reset(psc_ctx* ctx, int capacity);
+int psc_mixer_step(psc_ctx* ctx, const double* x1, const double* f1, double mix, double restart_factor,
+                   double* x_new, int* m_used, void* stream);
+int psc_mixer_history(psc_ctx* ctx, int* m_out);
+
+/* ---- utilities ---------------------------------------------------------- */
+/* Counter-based random block: dist 0 uniform [0,1) (np.random.rand in
+ * first_filt.py:37 and lancz_uppbnd.py:21), dist 1 standard normal
+ * (np.random.randn in chefsi1.py:29). */
+int psc_random(psc_ctx* ctx, int dtype, int dist, unsigned long long seed, void* out, long ld, long rows, int cols,
+               void* stream);
+int psc_cast(psc_ctx* ctx, int to_dtype, const void* src, void* dst, long n, void* stream);
+/* out = a x + b y (y may be NULL), n doubles. */
+int psc_axpby(psc_ctx* ctx, const double* x, const double* y, double a, double b, double* out, long n, void* stream);
+/* Deterministic dot product, result on the device. */
+int psc_dot(psc_ctx* ctx, const double* a, const double* b, long n, double* out_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSC_H */

@@ -679,57 +679,98 @@ def build_system(atoms: list, *, h: float, radius: float, elements: dict | None 
     return {"radius": rad, "nx": nx, "ny": nx, "nz": nx, "h": h}
 
 
+class OracleSCF:
+    """The SCF of rsdft_solver.run_rsdft_calculation (rsdft_solver.py:156-462)
+    for density_method = sad, diagmeth = 3, adaptive_scheme = 0, cg_prec = 0,
+    split into setup() and step() so that a bounded number of iterations can
+    be timed.  Wall times (s) are kept in t_setup and in each history entry."""
+
+    def __init__(self, domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
+                 maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, z_charge: float = 0.0,
+                 elements=None, tables=None):
+        self.domain, self.atoms, self.nev, self.poldeg, self.tol = domain, atoms, nev, poldeg, tol
+        self.maxits, self.fd_order, self.fermi_temp, self.z_charge = maxits, fd_order, fermi_temp, z_charge
+        self.elements = elements or load_elements()
+        self.tables = tables or load_tables()
+        self.history: list = []
+        self.its = 0
+        self.t_setup = None
+
+    def setup(self) -> None:
+        import time
+
+        t0 = time.perf_counter()
+        d, h = self.domain, self.domain["h"]
+        self.A = laplacian(d, self.fd_order)
+        n = self.n = self.A.shape[0]
+        self.Hpot = np.zeros(n)
+        self.err = 10.0 + self.tol
+        self.e_nuc = nuclear(self.atoms, self.elements)
+        self.rho0, self.hpot0, self.ppot, self.info = pseudo_diag(d, self.atoms, self.elements, self.tables)
+        projs = projectors(d, self.atoms, self.elements, self.tables)
+        vnl = nonlocal_csr(projs, n)
+        xcpot, self.exc = exc_nspn(h, self.rho0 / h ** 3)
+        self.XCpot = xcpot
+        self.nelec = nelectrons(self.atoms, self.elements) - self.z_charge
+        self.pot = self.ppot + self.hpot0 + 0.5 * xcpot
+        self.mixer = MSecant1()
+        self.half_a_plus_vnl = 0.5 * self.A + vnl
+        self.W = self.lam = None
+        self.rho = np.zeros(n)
+        self.t_setup = time.perf_counter() - t0
+
+    def done(self) -> bool:
+        return not (self.err > self.tol and self.its < self.maxits)
+
+    def step(self) -> dict:
+        import time
+
+        t0 = time.perf_counter()
+        n, h, nev = self.n, self.domain["h"], self.nev
+        self.its += 1
+        B = (self.half_a_plus_vnl + sp.diags(self.pot, 0, shape=(n, n))).tocsr()
+        if self.its == 1:
+            self.W, self.lam = first_filt(nev + 15, B, self.poldeg)
+        else:
+            self.W, self.lam = chefsi1(self.W, self.lam, self.poldeg, nev, B)
+        _, occ = occupations(self.lam[:nev], self.fermi_temp, self.nelec, 1e-6)
+        rho = (self.W[:, :nev] ** 2) @ (2 * occ)
+        hrhs = (4 * np.pi / h ** 3) * (rho - self.rho0)
+        self.rho = rho / h ** 3
+        self.Hpot, cg_its = pcg(self.A, hrhs, self.Hpot, 200, 1e-5)
+        self.XCpot, self.exc = exc_nspn(h, self.rho)
+        pot_new = self.ppot + 0.5 * self.XCpot + self.Hpot + self.hpot0
+        self.err = float(np.linalg.norm(pot_new - self.pot) / np.linalg.norm(pot_new))
+        en = energy_components(self.rho, self.Hpot, self.hpot0, self.XCpot, self.exc, self.lam, occ, nev,
+                               self.e_nuc, h)
+        self.occ = occ
+        self.pot, _ = self.mixer(self.pot, pot_new - self.pot)
+        rec = {"iter": self.its, "err": self.err, "lam": self.lam.copy(), "occ": np.asarray(occ).copy(),
+               "cg_its": cg_its, "wall": time.perf_counter() - t0, **en}
+        self.history.append(rec)
+        return rec
+
+    def result(self) -> dict:
+        return {"rho": self.rho, "hpot": self.Hpot, "xc_potential": self.XCpot, "exc": float(self.exc),
+                "potential": self.pot, "W": self.W, "eigenvalues": self.lam, "occupations": self.occ,
+                "iterations": self.its, "error": self.err, "converged": self.err <= self.tol,
+                "e_nuc0": self.e_nuc, "hpot0": self.hpot0, "rho0": self.rho0, "ppot": self.ppot,
+                "history": self.history, "energies": self.history[-1] if self.history else None,
+                "diag_info": self.info, "t_setup": self.t_setup}
+
+
 def run_scf(domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
             maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, seed: int | None = None,
             z_charge: float = 0.0, elements=None, tables=None, log=None) -> dict:
-    """The SCF loop of rsdft_solver.run_rsdft_calculation (rsdft_solver.py:156-462)
-    for density_method = sad, diagmeth = 3, adaptive_scheme = 0, cg_prec = 0."""
-    elements = elements or load_elements()
-    tables = tables or load_tables()
+    """Run OracleSCF to convergence; with a seed, numpy's global generator is
+    seeded first so the random draws match a reference run with that seed."""
     if seed is not None:
         np.random.seed(seed)
-    h = domain["h"]
-    A = laplacian(domain, fd_order)
-    n = A.shape[0]
-    Hpot = np.zeros(n)
-    err = 10.0 + tol
-    e_nuc = nuclear(atoms, elements)
-    rho0, hpot0, ppot, info = pseudo_diag(domain, atoms, elements, tables)
-    projs = projectors(domain, atoms, elements, tables)
-    vnl = nonlocal_csr(projs, n)
-    rhoxc = rho0 / h ** 3
-    xcpot, exc = exc_nspn(h, rhoxc)
-    nelec = nelectrons(atoms, elements) - z_charge
-    pot = ppot + hpot0 + 0.5 * xcpot
-    mixer = MSecant1()
-    half_a_plus_vnl = 0.5 * A + vnl
-    W = lam = None
-    history = []
-    its = 0
-    rho = np.zeros(n)
-    XCpot = xcpot
-    while err > tol and its < maxits:
-        its += 1
-        B = (half_a_plus_vnl + sp.diags(pot, 0, shape=(n, n))).tocsr()
-        if its == 1:
-            W, lam = first_filt(nev + 15, B, poldeg)
-        else:
-            W, lam = chefsi1(W, lam, poldeg, nev, B)
-        _, occ = occupations(lam[:nev], fermi_temp, nelec, 1e-6)
-        rho = (W[:, :nev] ** 2) @ (2 * occ)
-        hrhs = (4 * np.pi / h ** 3) * (rho - rho0)
-        rho = rho / h ** 3
-        Hpot, cg_its = pcg(A, hrhs, Hpot, 200, 1e-5)
-        XCpot, exc = exc_nspn(h, rho)
-        pot_new = ppot + 0.5 * XCpot + Hpot + hpot0
-        err = float(np.linalg.norm(pot_new - pot) / np.linalg.norm(pot_new))
-        en = energy_components(rho, Hpot, hpot0, XCpot, exc, lam, occ, nev, e_nuc, h)
-        history.append({"iter": its, "err": err, "lam": lam.copy(), "occ": np.asarray(occ).copy(),
-                        "cg_its": cg_its, **en})
+    scf = OracleSCF(domain, atoms, nev=nev, poldeg=poldeg, tol=tol, maxits=maxits, fd_order=fd_order,
+                    fermi_temp=fermi_temp, z_charge=z_charge, elements=elements, tables=tables)
+    scf.setup()
+    while not scf.done():
+        rec = scf.step()
         if log:
-            log(f"iter {its} err {err:.3e} E {en['total_ry']:.10f}")
-        pot, _ = mixer(pot, pot_new - pot)
-    return {"rho": rho, "hpot": Hpot, "xc_potential": XCpot, "exc": float(exc), "potential": pot,
-            "W": W, "eigenvalues": lam, "occupations": occ, "iterations": its, "error": err,
-            "converged": err <= tol, "e_nuc0": e_nuc, "hpot0": hpot0, "rho0": rho0, "ppot": ppot,
-            "history": history, "energies": history[-1] if history else None, "diag_info": info}
+            log(f"iter {rec['iter']} err {rec['err']:.3e} E {rec['total_ry']:.10f}")
+    return scf.result()

@@ -1,0 +1,71 @@
+"""Backend selection: the GPU bundle behind the reference's entry points.
+
+``select_solver_backend(settings)`` returns a ``SolverBackend`` with the
+callables PARSEC.py's rsdft_backend.select_solver_backend
+(rsdft_backend.py:80-137) provides for ``use_gpu = 1`` -- pseudo_diag,
+pseudo_nl, first_filt, chefsi1, lanczos, chsubsp, occupations, pcg -- with
+the same argument meaning.  They run on libpsc.so; there is no CPU path, and
+as in the reference a GPU that cannot be used ends the run with SystemExit.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import gpu
+from .inputs import pseudo_tables
+from .models import SolverBackend, SolverSettings
+
+
+class GpuRuntime:
+    """Per-run device state: one grid context per domain, precision, seeds."""
+
+    def __init__(self, settings: SolverSettings):
+        self.settings = settings
+        self.block_dtype = torch.float32 if settings.precision == "mixed" else torch.float64
+        self.ctx: gpu.GridContext | None = None
+
+    def context(self, domain: dict) -> gpu.GridContext:
+        if self.ctx is None or not self.ctx.matches(domain, self.settings.fd_order):
+            self.ctx = gpu.GridContext(domain, self.settings.fd_order, seed=self.settings.seed)
+        return self.ctx
+
+    # -- reference entry points ------------------------------------------------
+    def pseudo_diag(self, domain, atoms, elem, n_elements=None, return_info=False):
+        ctx = self.context(domain)
+        rho0, hpot0, ppot, info = gpu.sad_setup(ctx, atoms, elem, pseudo_tables())
+        return (rho0, hpot0, ppot, info) if return_info else (rho0, hpot0, ppot)
+
+    def pseudo_nl(self, domain, atoms, elem, n_elements=None):
+        return gpu.projector_setup(self.context(domain), atoms, elem, pseudo_tables())
+
+    def first_filt(self, nev, H, polm=10):
+        return gpu.first_filt(nev, H, polm, dtype=self.block_dtype)
+
+    def chefsi1(self, W, ritzv, deg, nev, H):
+        return gpu.chefsi1(W, ritzv, deg, nev, H)
+
+    def lanczos(self, *args, **kwargs):
+        raise NotImplementedError("diagmeth 0/1 (full Lanczos, Eigensolvers/lanczos.py) is not implemented; "
+                                  "use diagmeth = 3")
+
+    def chsubsp(self, *args, **kwargs):
+        raise NotImplementedError("diagmeth 2 (Eigensolvers/chsubsp.py) is not implemented; use diagmeth = 3")
+
+    def occupations(self, lam, temp, nelec, tol):
+        return gpu.occupations(self.ctx, lam, temp, nelec, tol)
+
+    def pcg(self, A, rhs, x0, maxit, tol, *prec):
+        return gpu.pcg(A, rhs, x0, maxit, tol, *prec)
+
+
+def select_solver_backend(settings: SolverSettings) -> SolverBackend:
+    if not settings.use_gpu:
+        raise SystemExit("this implementation has only the GPU backend (use_gpu = 1)")
+    try:
+        gpu.require_cuda()
+    except Exception as exc:  # same contract as the reference: no usable GPU -> SystemExit
+        raise SystemExit(f"GPU backend requested but unavailable: {exc}") from exc
+    rt = GpuRuntime(settings)
+    return SolverBackend(label="gpu", pseudo_diag=rt.pseudo_diag, pseudo_nl=rt.pseudo_nl, first_filt=rt.first_filt,
+                         chefsi1=rt.chefsi1, lanczos=rt.lanczos, chsubsp=rt.chsubsp, occupations=rt.occupations,
+                         pcg=rt.pcg, array_module=torch, cupy_module=None, runtime=rt)

@@ -1,0 +1,405 @@
+// Subspace linear algebra: Gram products W^T V (n x k -> k x k), block
+// products W*Q, Cholesky, triangular inverse and a one-CTA cyclic Jacobi
+// symmetric eigensolver, plus the two subspace drivers built from them:
+// CholeskyQR2 orthonormalisation (replaces the Householder QR at
+// Eigensolvers/chefsi1.py:43 and first_filt.py:43) and Rayleigh-Ritz
+// (chefsi1.py:46-67, first_filt.py:44-63).  Small k x k work is FP64.
+#include "psc_internal.cuh"
+#include "../../include/psc.h"
+
+#include <algorithm>
+#include <cmath>
+
+// ---------------------------------------------------------------------------
+// Gram partials: partial[chunk] (k1 x k2, column-major) = A[rows]^T B[rows]
+// ---------------------------------------------------------------------------
+constexpr int GT = 64;  // output tile edge
+constexpr int GR = 32;  // rows staged per step
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_gram_partial(const T* __restrict__ A, long lda, int k1, const T* __restrict__ B, long ldb, int k2, long n,
+               long chunk, int tiles_j, int upper_only, double* __restrict__ partial) {
+  __shared__ double As[GR][GT + 1];
+  __shared__ double Bs[GR][GT + 1];
+  const int ti = blockIdx.y / tiles_j, tj = blockIdx.y % tiles_j;
+  if (upper_only && ti > tj) return;
+  const long r0 = (long)blockIdx.x * chunk;
+  const long r1 = min(n, r0 + chunk);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (long rb = r0; rb < r1; rb += GR) {
+    for (int e = threadIdx.x; e < GR * GT; e += 256) {
+      const int r = e % GR, c = e / GR;
+      const long row = rb + r;
+      const int ca = ti * GT + c, cb = tj * GT + c;
+      As[r][c] = (row < r1 && ca < k1) ? (double)A[row + (long)ca * lda] : 0.0;
+      Bs[r][c] = (row < r1 && cb < k2) ? (double)B[row + (long)cb * ldb] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int r = 0; r < GR; ++r) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[r][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[r][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+    }
+    __syncthreads();
+  }
+  double* out = partial + (long)blockIdx.x * k1 * k2;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gi = ti * GT + ty + 16 * i, gj = tj * GT + tx + 16 * j;
+      if (gi < k1 && gj < k2) out[gi + (long)gj * k1] = acc[i][j];
+    }
+}
+
+// out = sum over chunks (fixed order); mode 0: plain, 1: mirror the upper
+// triangle (G[i,j] = M[i,j] for i <= j, as the reference's dot loop), 2: 0.5(M+M^T)
+__global__ void k_gram_final(const double* __restrict__ partial, int nchunk, int k1, int k2, int mode,
+                             double* __restrict__ out) {
+  const long kk = (long)k1 * k2;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < kk; e += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % k1), j = (int)(e / k1);
+    long src = e;
+    if (mode == 1 && i > j) src = j + (long)i * k1;
+    double s = 0.0;
+    for (int c = 0; c < nchunk; ++c) s += partial[(long)c * kk + src];
+    if (mode == 2) {
+      double t = 0.0;
+      const long tr = j + (long)i * k1;
+      for (int c = 0; c < nchunk; ++c) t += partial[(long)c * kk + tr];
+      s = 0.5 * (s + t);
+    }
+    out[e] = s;
+  }
+}
+
+int psc_ensure_dense(psc_ctx* ctx, int k) {
+  PSC_REQUIRE(ctx, k >= 1 && k <= PSC_MAX_K, "subspace width out of range");
+  if (k <= ctx->dense_cap) return 0;
+  cudaFree(ctx->gram); cudaFree(ctx->gram2); cudaFree(ctx->evec); cudaFree(ctx->tri); cudaFree(ctx->gram_partial);
+  const int cap = std::max(k, 64);
+  const size_t kk = (size_t)cap * cap;
+  PSC_CUDA(ctx, cudaMalloc(&ctx->gram, kk * sizeof(double)));
+  PSC_CUDA(ctx, cudaMalloc(&ctx->gram2, kk * sizeof(double)));
+  PSC_CUDA(ctx, cudaMalloc(&ctx->evec, kk * sizeof(double)));
+  PSC_CUDA(ctx, cudaMalloc(&ctx->tri, kk * sizeof(double)));
+  ctx->gram_blocks = 296;
+  PSC_CUDA(ctx, cudaMalloc(&ctx->gram_partial, (size_t)ctx->gram_blocks * kk * sizeof(double)));
+  ctx->dense_cap = cap;
+  return 0;
+}
+
+int psc_gram_impl(psc_ctx* ctx, int dtype, const void* A, long lda, const void* B, long ldb, int k, double* out,
+                  int mode, cudaStream_t st) {
+  if (psc_ensure_dense(ctx, k)) return 1;
+  const long n = ctx->n;
+  const int tiles = (k + GT - 1) / GT;
+  const int ntile = tiles * tiles;
+  int nchunk = std::max(1, std::min(ctx->gram_blocks, (148 * 4 + ntile - 1) / ntile));
+  nchunk = (int)std::min<long>(nchunk, std::max<long>(1, n / GR));
+  const long chunk = ((n + nchunk - 1) / nchunk + GR - 1) / GR * GR;
+  nchunk = (int)((n + chunk - 1) / chunk);
+  dim3 grid(nchunk, ntile);
+  const int upper = (mode == 1) ? 1 : 0;
+  if (dtype == PSC_F64)
+    k_gram_partial<double><<<grid, 256, 0, st>>>((const double*)A, lda, k, (const double*)B, ldb, k, n, chunk,
+                                                  tiles, upper, ctx->gram_partial);
+  else
+    k_gram_partial<float><<<grid, 256, 0, st>>>((const float*)A, lda, k, (const float*)B, ldb, k, n, chunk, tiles,
+                                                 upper, ctx->gram_partial);
+  PSC_LAUNCH_CHECK(ctx);
+  const long kk = (long)k * k;
+  k_gram_final<<<std::max(1, (int)std::min<long>(592, (kk + 255) / 256)), 256, 0, st>>>(ctx->gram_partial, nchunk, k,
+                                                                                    k, mode, out);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
+
+extern "C" int psc_gram(psc_ctx* ctx, int dtype, const void* A, long lda, const void* B, long ldb, int k,
+                        int mode, double* out_dev, void* stream) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, lda >= ctx->n && ldb >= ctx->n, "gram: ld < n");
+  return psc_gram_impl(ctx, dtype, A, lda, B, ldb, k, out_dev, mode, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Out (n x kout) = W (n x k) * Q (k x kout, FP64, column-major)
+// ---------------------------------------------------------------------------
+constexpr int MM_J = 32;   // output columns per CTA
+constexpr int MM_I = 128;  // Q rows staged per step
+
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_gemm_nn(const T* __restrict__ W, long ldw, int k, const double* __restrict__ Q, int kout, T* __restrict__ O,
+          long ldo, long n) {
+  __shared__ double Qs[MM_I][MM_J];
+  const long row = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int j0 = blockIdx.y * MM_J;
+  const int nj = min(MM_J, kout - j0);
+  double acc[MM_J];
+#pragma unroll
+  for (int j = 0; j < MM_J; ++j) acc[j] = 0.0;
+  for (int i0 = 0; i0 < k; i0 += MM_I) {
+    const int ni = min(MM_I, k - i0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < MM_I * MM_J; e += blockDim.x) {
+      const int i = e / MM_J, j = e % MM_J;
+      Qs[i][j] = (i < ni && j < nj) ? Q[(i0 + i) + (long)(j0 + j) * k] : 0.0;
+    }
+    __syncthreads();
+    if (row < n) {
+      for (int i = 0; i < ni; ++i) {
+        const double w = (double)W[row + (long)(i0 + i) * ldw];
+#pragma unroll
+        for (int j = 0; j < MM_J; ++j) acc[j] += w * Qs[i][j];
+      }
+    }
+  }
+  if (row < n) {
+#pragma unroll
+    for (int j = 0; j < MM_J; ++j)
+      if (j < nj) O[row + (long)(j0 + j) * ldo] = (T)acc[j];
+  }
+}
+
+int psc_gemm_nn_impl(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Q, int kout, void* out,
+                     long ldo, cudaStream_t st) {
+  PSC_REQUIRE(ctx, W != out, "gemm: output must not alias input");
+  dim3 grid(psc_div_up(ctx->n, 128), psc_div_up(kout, MM_J));
+  if (dtype == PSC_F64)
+    k_gemm_nn<double><<<grid, 128, 0, st>>>((const double*)W, ldw, k, Q, kout, (double*)out, ldo, ctx->n);
+  else
+    k_gemm_nn<float><<<grid, 128, 0, st>>>((const float*)W, ldw, k, Q, kout, (float*)out, ldo, ctx->n);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
+
+extern "C" int psc_gemm_nn(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Q, int kout,
+                           void* out, long ldo, void* stream) {
+  if (!ctx) return 2;
+  return psc_gemm_nn_impl(ctx, dtype, W, ldw, k, Q, kout, out, ldo, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Cholesky (upper, G = R^T R, in place, one CTA) and upper-triangular inverse
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_cholesky(double* A, int k, int* status) {
+  for (int j = 0; j < k; ++j) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const double d = A[j + (long)j * k];
+      if (!(d > 0.0)) status[1] = j + 1;  // not positive definite
+      A[j + (long)j * k] = d > 0.0 ? sqrt(d) : 1.0;
+    }
+    __syncthreads();
+    const double rjj = A[j + (long)j * k];
+    for (int c = j + 1 + threadIdx.x; c < k; c += blockDim.x) A[j + (long)c * k] /= rjj;
+    __syncthreads();
+    const int m = k - j - 1;
+    for (long e = threadIdx.x; e < (long)m * m; e += blockDim.x) {
+      const int r = j + 1 + (int)(e % m), c = j + 1 + (int)(e / m);
+      if (r <= c) A[r + (long)c * k] -= A[j + (long)r * k] * A[j + (long)c * k];
+    }
+  }
+  __syncthreads();
+  for (long e = threadIdx.x; e < (long)k * k; e += blockDim.x) {
+    const int r = (int)(e % k), c = (int)(e / k);
+    if (r > c) A[e] = 0.0;
+  }
+}
+
+__global__ void k_triu_inv(const double* __restrict__ R, int k, double* __restrict__ X) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x) {
+    double* xj = X + (long)j * k;
+    for (int i = j + 1; i < k; ++i) xj[i] = 0.0;
+    xj[j] = 1.0 / R[j + (long)j * k];
+    for (int i = j - 1; i >= 0; --i) {
+      double s = 0.0;
+      for (int l = i + 1; l <= j; ++l) s += R[i + (long)l * k] * xj[l];
+      xj[i] = -s / R[i + (long)i * k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cyclic Jacobi eigensolver, one CTA.  Round-robin pairing (circle method):
+// every round rotates k/2 disjoint (p,q) planes -- columns of A and V first,
+// then rows of A -- so each sweep annihilates every off-diagonal pair once.
+// Converged when off(A) <= 1e-15 * ||A||_F or after 40 sweeps.  Eigenvalues
+// ascending, eigenvectors permuted to match.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024)
+k_jacobi(double* __restrict__ Ag, int k, double* __restrict__ evals, double* __restrict__ Vout, int use_smem,
+         double* __restrict__ Vg, int* status) {
+  extern __shared__ double sm[];
+  __shared__ double red[32];
+  __shared__ int rp[512], rq[512];
+  __shared__ double rc[512], rs[512];
+  __shared__ int done;
+  double* A = use_smem ? sm : Ag;
+  double* V = use_smem ? sm + (long)k * k : Vg;
+  const long kk = (long)k * k;
+  if (use_smem)
+    for (long e = threadIdx.x; e < kk; e += blockDim.x) A[e] = Ag[e];
+  for (long e = threadIdx.x; e < kk; e += blockDim.x) V[e] = ((e % k) == (e / k)) ? 1.0 : 0.0;
+  const int m = k + (k & 1);
+  const int half = m / 2;
+  if (threadIdx.x == 0) done = 0;
+  __syncthreads();
+  for (int sweep = 0; sweep < 40 && k > 1; ++sweep) {
+    // convergence test
+    double off = 0.0, tot = 0.0;
+    for (long e = threadIdx.x; e < kk; e += blockDim.x) {
+      const double v = A[e] * A[e];
+      tot += v;
+      if ((e % k) != (e / k)) off += v;
+    }
+    off = psc_block_sum<double, 1024>(off, red);
+    __syncthreads();
+    tot = psc_block_sum<double, 1024>(tot, red);
+    if (threadIdx.x == 0) done = (off <= 1e-30 * tot) ? 1 : 0;
+    __syncthreads();
+    if (done) break;
+    for (int r = 0; r < m - 1; ++r) {
+      for (int i = threadIdx.x; i < half; i += blockDim.x) {
+        const int a = (i == 0) ? 0 : ((i - 1 + r) % (m - 1)) + 1;
+        const int b = ((m - 1 - i - 1 + r) % (m - 1)) + 1;
+        const int p = min(a, b), q = max(a, b);
+        double c = 1.0, s = 0.0;
+        if (q < k) {
+          const double apq = A[p + (long)q * k];
+          if (apq != 0.0) {
+            const double app = A[p + (long)p * k], aqq = A[q + (long)q * k];
+            const double theta = (aqq - app) / (2.0 * apq);
+            double t;
+            if (fabs(theta) > 1e150) t = 0.5 / theta;
+            else t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            c = 1.0 / sqrt(t * t + 1.0);
+            s = t * c;
+          }
+        }
+        rp[i] = p; rq[i] = q; rc[i] = c; rs[i] = s;
+      }
+      __syncthreads();
+      // columns: A <- A P, V <- V P
+      for (long e = threadIdx.x; e < (long)half * k; e += blockDim.x) {
+        const int i = (int)(e / k), row = (int)(e % k);
+        if (rq[i] >= k || rs[i] == 0.0) continue;
+        const int p = rp[i], q = rq[i];
+        const double c = rc[i], s = rs[i];
+        double* ap = A + (long)p * k;
+        double* aq = A + (long)q * k;
+        const double x = ap[row], y = aq[row];
+        ap[row] = c * x - s * y;
+        aq[row] = s * x + c * y;
+        double* vp = V + (long)p * k;
+        double* vq = V + (long)q * k;
+        const double vx = vp[row], vy = vq[row];
+        vp[row] = c * vx - s * vy;
+        vq[row] = s * vx + c * vy;
+      }
+      __syncthreads();
+      // rows: A <- P^T A
+      for (long e = threadIdx.x; e < (long)half * k; e += blockDim.x) {
+        const int i = (int)(e / k), col = (int)(e % k);
+        if (rq[i] >= k || rs[i] == 0.0) continue;
+        const int p = rp[i], q = rq[i];
+        const double c = rc[i], s = rs[i];
+        const double x = A[p + (long)col * k], y = A[q + (long)col * k];
+        A[p + (long)col * k] = c * x - s * y;
+        A[q + (long)col * k] = s * x + c * y;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0 && sweep == 39) status[2] = 1;  // did not converge
+  }
+  __syncthreads();
+  // sort ascending (stable by index) and permute eigenvectors
+  for (int i = threadIdx.x; i < k; i += blockDim.x) {
+    const double li = A[i + (long)i * k];
+    int rank = 0;
+    for (int j = 0; j < k; ++j) {
+      const double lj = A[j + (long)j * k];
+      rank += (lj < li) || (lj == li && j < i);
+    }
+    evals[rank] = li;
+    for (int r = 0; r < k; ++r) Vout[r + (long)rank * k] = V[r + (long)i * k];
+  }
+}
+
+int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, cudaStream_t st) {
+  PSC_REQUIRE(ctx, k >= 1 && k <= 1023, "syev: k out of range");
+  if (psc_ensure_dense(ctx, k)) return 1;
+  const size_t smem = 2 * (size_t)k * k * sizeof(double);
+  const int use_smem = smem <= 200 * 1024;
+  if (use_smem && smem > 48 * 1024)
+    PSC_CUDA(ctx, cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // V scratch in global memory when the matrices do not fit on chip
+  double* vg = use_smem ? nullptr : ctx->gram2;
+  PSC_REQUIRE(ctx, use_smem || (A != ctx->gram2 && evecs != ctx->gram2), "syev: scratch aliasing");
+  k_jacobi<<<1, 1024, use_smem ? smem : 0, st>>>(A, k, evals, evecs, use_smem, vg, ctx->dev_status);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
+
+extern "C" int psc_syev(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, void* stream) {
+  if (!ctx) return 2;
+  return psc_syev_impl(ctx, A, k, evals, evecs, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// subspace drivers
+// ---------------------------------------------------------------------------
+// CholeskyQR applied `passes` times: W <- W R^{-1} with W^T W = R^T R.  Uses
+// T (same shape) as the second buffer; *which = 0 if the result is in W.
+extern "C" int psc_orthonormalize(psc_ctx* ctx, int dtype, void* W, void* T, long ld, int k, int passes,
+                                  int* which, void* stream) {
+  if (!ctx) return 2;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (psc_ensure_dense(ctx, k)) return 1;
+  void* buf[2] = {W, T};
+  int cur = 0;
+  for (int p = 0; p < passes; ++p) {
+    int rc = psc_gram_impl(ctx, dtype, buf[cur], ld, buf[cur], ld, k, ctx->gram, 2, st);
+    if (rc) return rc;
+    k_cholesky<<<1, 1024, 0, st>>>(ctx->gram, k, ctx->dev_status);
+    PSC_LAUNCH_CHECK(ctx);
+    k_triu_inv<<<psc_div_up(k, 128), 128, 0, st>>>(ctx->gram, k, ctx->tri);
+    PSC_LAUNCH_CHECK(ctx);
+    rc = psc_gemm_nn_impl(ctx, dtype, buf[cur], ld, k, ctx->tri, k, buf[cur ^ 1], ld, st);
+    if (rc) return rc;
+    cur ^= 1;
+  }
+  if (which) *which = cur;
+  return 0;
+}
+
+// Rayleigh-Ritz on an orthonormal W: V = H W, G = W^T H W (upper triangle
+// mirrored, as the reference's dot loop), G = Q diag(ritz) Q^T, result W Q is
+// written to V.  ritz_dev receives the k Ritz values in ascending order.
+extern "C" int psc_rayleigh_ritz(psc_ctx* ctx, int dtype, const void* W, void* V, long ld, int k, double* ritz_dev,
+                                 void* stream) {
+  if (!ctx) return 2;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (psc_ensure_dense(ctx, k)) return 1;
+  int rc = psc_apply_h_impl(ctx, dtype, W, ld, V, ld, nullptr, 0, k, nullptr, 1.0, 0.0, 0.0, st);
+  if (rc) return rc;
+  rc = psc_gram_impl(ctx, dtype, V, ld, W, ld, k, ctx->gram, 1, st);
+  if (rc) return rc;
+  rc = psc_syev_impl(ctx, ctx->gram, k, ritz_dev, ctx->evec, st);
+  if (rc) return rc;
+  return psc_gemm_nn_impl(ctx, dtype, W, ld, k, ctx->evec, k, V, ld, st);
+}

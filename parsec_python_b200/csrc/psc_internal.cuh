@@ -1,0 +1,208 @@
+// Internal definitions shared by the libpsc translation units.
+//
+// libpsc is the device side of the real-space Kohn-Sham SCF hot path:
+// matrix-free Hamiltonian H = -0.5*Lap_h + V_nl + diag(pot) on an
+// nx*ny*nz cube (x fastest, zero Dirichlet outside), Chebyshev filtering,
+// subspace orthonormalisation and Rayleigh-Ritz, Hartree CG, LDA XC,
+// multisecant mixing and the SAD/projector setup.  All vectors live in device
+// memory owned by the caller; blocks of k vectors are column-major with a
+// leading dimension ld.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#define PSC_MAX_DEG 64        // highest Chebyshev degree accepted per filter call
+#define PSC_MAX_K 1024        // widest subspace block accepted
+#define PSC_RED_BLOCKS 592    // fixed partial-sum count of the deterministic reductions (4 x 148 SMs)
+#define PSC_RED_SLOTS 16      // simultaneous dot products per reduction launch
+
+enum { PSC_F64 = 0, PSC_F32 = 1 };
+
+struct psc_species {
+  // Five natural cubic splines on pruned knots: 0 charge, 1 hartree, 2 pot_S,
+  // 3 wfn_P, 4 pot_P - pot_S.  Device arrays x, z, c, d per spline.
+  int nk[5] = {0, 0, 0, 0, 0};
+  double* x[5] = {nullptr};
+  double* z[5] = {nullptr};
+  double* c[5] = {nullptr};
+  double* d[5] = {nullptr};
+  double zvalue = 0.0;  // KB denominator (Zvalue column of the element table)
+  double rcut = 0.0;    // projector radius R
+  int valid = 0;
+};
+
+struct psc_spline_dev {  // flat view handed to kernels
+  const double* x;
+  const double* z;
+  const double* c;
+  const double* d;
+  int n;
+};
+
+struct psc_ctx {
+  int device = 0;
+  int nx = 0, ny = 0, nz = 0;
+  long n = 0;
+  double h = 0.0;
+  int fd_order = 8;
+  int radius = 4;            // stencil half-width (fd_order/2, capped at 4)
+  double lap_c0 = 0.0;       // centre weight of A = -Lap_h (1/h^2 folded in)
+  double lap_c[4] = {0, 0, 0, 0};
+  double ham_c0 = 0.0;       // 0.5 * A weights, as 0.5*(c*(1/(h*h)))
+  double ham_c[4] = {0, 0, 0, 0};
+
+  // potential (both precisions)
+  double* pot64 = nullptr;
+  float* pot32 = nullptr;
+
+  // species tables
+  std::vector<psc_species> species;
+
+  // projector tables: n_atoms_nl atoms, compacted ball points
+  int nl_atoms = 0;
+  long nl_points = 0;
+  int* nl_atom_off = nullptr;    // [nl_atoms+1] offsets into the point arrays
+  int* nl_idx = nullptr;         // [nl_points] grid index of each ball point
+  double* nl_u64 = nullptr;      // [3][nl_points]
+  float* nl_u32 = nullptr;       // [3][nl_points]
+  double* nl_w = nullptr;        // [nl_atoms] 1/xint = h^3 / Zvalue
+  long nl_touched = 0;           // unique grid points covered by any ball
+  int* nl_t_idx = nullptr;       // [nl_touched] grid index
+  int* nl_t_off = nullptr;       // [nl_touched+1] offsets into nl_t_ent
+  int* nl_t_ent = nullptr;       // [nl_points] ball-point ids (atom order)
+  int* nl_point_atom = nullptr;  // [nl_points] owning atom of each ball point
+  void* nl_proj = nullptr;       // [nl_atoms][3][k] projections (double; reused for float)
+  size_t nl_proj_bytes = 0;
+
+  // Chebyshev per-step coefficients (alpha, beta, gamma) on the device
+  double* cheb_coef = nullptr;   // [PSC_MAX_DEG+1][3]
+
+  // deterministic reductions
+  double* red_partial = nullptr;  // [PSC_RED_SLOTS][PSC_RED_BLOCKS]
+  double* scalars = nullptr;      // general device scalar scratch [256]
+  double* host_scalars = nullptr; // pinned host mirror [256]
+
+  // small dense work (k x k)
+  int dense_cap = 0;
+  double* gram = nullptr;        // [cap*cap]
+  double* gram2 = nullptr;       // [cap*cap]
+  double* evec = nullptr;        // [cap*cap]
+  double* tri = nullptr;         // [cap*cap]
+  double* gram_partial = nullptr;// [gram_blocks][cap*cap] Gram partial sums
+  int gram_blocks = 0;
+  int* dev_status = nullptr;     // device-side error flags [8]
+
+  // Lanczos vectors (double)
+  double* lz_v = nullptr;        // [3][n]
+
+  // PCG vectors (double)
+  double* cg_r = nullptr;
+  double* cg_p = nullptr;
+  double* cg_ap = nullptr;
+  double* cg_part = nullptr;     // [2][cg_part_cap] per-CTA partial sums
+  int cg_part_cap = 0;
+
+  // mixer history
+  int mix_cap = 0;
+  int mix_m = 0;                 // columns in DX/DF
+  double* mix_dx = nullptr;      // [cap][n]
+  double* mix_df = nullptr;      // [cap][n]
+  double* mix_nv = nullptr;      // [n]  (group vector N for group size 1)
+  double* mix_tmp = nullptr;     // [n]
+  double* mix_coef = nullptr;    // [3*cap + 8] dot products and scalars
+  double* mix_partial = nullptr; // [3*cap + 2][PSC_RED_BLOCKS]
+  double mix_last_fnorm = -1.0;
+
+  std::string last_error;
+};
+
+// ---------------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------------
+void psc_set_error(psc_ctx* ctx, const std::string& msg);
+
+#define PSC_CUDA(ctx, call)                                                            \
+  do {                                                                                 \
+    cudaError_t _e = (call);                                                           \
+    if (_e != cudaSuccess) {                                                           \
+      psc_set_error((ctx), std::string(#call) + ": " + cudaGetErrorString(_e));        \
+      return 1;                                                                        \
+    }                                                                                  \
+  } while (0)
+
+// Every kernel launch site is followed by exactly one PSC_LAUNCH_CHECK, which
+// also counts the launch (psc_launch_count).
+void psc_note_launch();
+#define PSC_LAUNCH_CHECK(ctx)                                                          \
+  do {                                                                                 \
+    psc_note_launch();                                                                 \
+    cudaError_t _e = cudaGetLastError();                                               \
+    if (_e != cudaSuccess) {                                                           \
+      psc_set_error((ctx), std::string("kernel launch: ") + cudaGetErrorString(_e) +   \
+                               " at " + __FILE__ + ":" + std::to_string(__LINE__));    \
+      return 1;                                                                        \
+    }                                                                                  \
+  } while (0)
+
+#define PSC_REQUIRE(ctx, cond, msg)                                                    \
+  do {                                                                                 \
+    if (!(cond)) {                                                                     \
+      psc_set_error((ctx), std::string(msg));                                          \
+      return 2;                                                                        \
+    }                                                                                  \
+  } while (0)
+
+static inline int psc_div_up(long a, long b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T psc_warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum of one value per thread; result valid in thread 0.  The
+// combine order is fixed, so the result is reproducible run to run.
+template <typename T, int NT>
+__device__ __forceinline__ T psc_block_sum(T v, T* sh /* >= NT/32 */) {
+  v = psc_warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  T r = T(0);
+  if (w == 0) {
+    r = (l < NT / 32) ? sh[l] : T(0);
+    r = psc_warp_sum(r);
+  }
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// cross-unit host entry points used internally
+// ---------------------------------------------------------------------------
+// Deterministic multi-dot: out[s] = sum_i a_s[i]*b_s[i] for s < nslots (device result).
+int psc_dots(psc_ctx* ctx, int nslots, const double* const* a, const double* const* b, long n,
+             double* out_dev, cudaStream_t st);
+int psc_ensure_dense(psc_ctx* ctx, int k);
+int psc_ensure_proj(psc_ctx* ctx, int k);
+int psc_apply_h_impl(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long ldy,
+                     const void* P, long ldp, int k, const double* coef_dev, double a, double b,
+                     double g, cudaStream_t st);
+int psc_gram_impl(psc_ctx* ctx, int dtype, const void* A, long lda, const void* B, long ldb, int k,
+                  double* out, int symmetrize, cudaStream_t st);
+int psc_gemm_nn_impl(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Q,
+                     int kout, void* out, long ldo, cudaStream_t st);
+int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, cudaStream_t st);
+int psc_stencil_blocks(psc_ctx* ctx, int k);
+int psc_laplacian_fused(psc_ctx* ctx, const double* x, const double* prev, double* y, double a, double b,
+                        double g, double* dot_partial, int* nblocks, cudaStream_t st);
+int psc_random_impl(psc_ctx* ctx, int dtype, int dist, unsigned long long seed, void* out, long ld,
+                    long rows, int cols, cudaStream_t st);

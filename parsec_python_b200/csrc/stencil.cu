@@ -1,0 +1,319 @@
+// Matrix-free Hamiltonian / Laplacian application and the Chebyshev filter.
+//
+// One launch computes, for a block of k column vectors,
+//   Out = alpha * (W * In) + beta * In + gamma * Prev
+// where W is either the Hamiltonian's local part 0.5*A + diag(pot) or the
+// Laplacian A = -Lap_h alone (pot == NULL).  The Kleinman-Bylander term is
+// added by nonlocal.cu (project before, scatter after).
+//
+// Kernel shape (B200): each CTA owns a contiguous slab of S = 256*PPT flat xy
+// points of one column and marches in z over a chunk of planes.  The 2R+1
+// z-neighbours of each owned point are kept in a register queue; the current
+// plane (owned points + R rows of y halo on each side) is staged in shared
+// memory, double buffered, so x and y neighbours come from shared memory and
+// every global load is a coalesced row segment.  HBM traffic per step is one
+// read of In, one read of Prev and one write of Out per point and column.
+#include "psc_internal.cuh"
+#include "../../include/psc.h"
+
+template <typename T>
+struct StencilW {
+  T c0;      // centre weight
+  T c[4];    // offset weights
+};
+
+template <typename T, int R, int PPT>
+__global__ void __launch_bounds__(256)
+k_stencil(const T* __restrict__ X, long ldx, const T* Pv, long ldp, T* Y, long ldy,
+          const T* __restrict__ pot, int nx, int ny, int nz, int zchunk, StencilW<T> w,
+          const double* __restrict__ coef, double ha, double hb, double hg,
+          double* __restrict__ dot_partial) {
+  constexpr int NT = 256;
+  constexpr int S = NT * PPT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* plane = reinterpret_cast<T*>(smem_raw);
+  const int nxy = nx * ny;
+  const int halo = R * nx;
+  const int win = S + 2 * halo;           // window length per buffer
+  const int slab0 = blockIdx.x * S;
+  const int seff = min(S, nxy - slab0);   // owned points in this slab
+  const int z0 = blockIdx.y * zchunk;
+  const int z1 = min(nz, z0 + zchunk);
+  const long col = blockIdx.z;
+  const T* Xc = X + col * ldx;
+  const T* Pc = Pv ? Pv + col * ldp : nullptr;
+  T* Yc = Y + col * ldy;
+
+  T a, b, g;
+  if (coef) { a = (T)coef[0]; b = (T)coef[1]; g = (T)coef[2]; }
+  else { a = (T)ha; b = (T)hb; g = (T)hg; }
+
+  int q[PPT], xi[PPT], yi[PPT];
+  bool own[PPT];
+#pragma unroll
+  for (int v = 0; v < PPT; ++v) {
+    const int loc = threadIdx.x + NT * v;
+    own[v] = loc < seff;
+    q[v] = slab0 + loc;
+    xi[v] = own[v] ? q[v] % nx : 0;
+    yi[v] = own[v] ? q[v] / nx : 0;
+  }
+
+  // z queue: zq[v][i] holds plane z - R + i of owned point v.
+  T zq[PPT][2 * R + 1];
+#pragma unroll
+  for (int v = 0; v < PPT; ++v)
+#pragma unroll
+    for (int i = 0; i < 2 * R; ++i) {
+      const int zz = z0 - R + i;
+      zq[v][i] = (own[v] && zz >= 0 && zz < nz) ? Xc[(long)zz * nxy + q[v]] : T(0);
+    }
+
+  double dacc = 0.0;
+  int buf = 0;
+  const int hcount = win - seff;          // non-owned window positions
+  for (int z = z0; z < z1; ++z) {
+    T* pl = plane + buf * win;
+    const long zoff = (long)z * nxy;
+#pragma unroll
+    for (int v = 0; v < PPT; ++v) {
+      const int zz = z + R;
+      zq[v][2 * R] = (own[v] && zz < nz) ? Xc[(long)zz * nxy + q[v]] : T(0);
+      if (own[v]) pl[halo + threadIdx.x + NT * v] = zq[v][R];
+    }
+    for (int j = threadIdx.x; j < hcount; j += NT) {
+      const int pos = j < halo ? j : j + seff;
+      const int fq = slab0 - halo + pos;
+      pl[pos] = (fq >= 0 && fq < nxy) ? Xc[zoff + fq] : T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < PPT; ++v) {
+      if (!own[v]) continue;
+      const int s = halo + threadIdx.x + NT * v;
+      const T xc = zq[v][R];
+      T acc = w.c0 * xc;
+#pragma unroll
+      for (int d = 1; d <= R; ++d) {
+        const T cd = w.c[d - 1];
+        T sx = T(0), sy = T(0), sz = T(0);
+        if (xi[v] - d >= 0) sx += pl[s - d];
+        if (xi[v] + d < nx) sx += pl[s + d];
+        if (yi[v] - d >= 0) sy += pl[s - d * nx];
+        if (yi[v] + d < ny) sy += pl[s + d * nx];
+        sz = zq[v][R - d] + zq[v][R + d];
+        acc += cd * (sx + sy + sz);
+      }
+      if (pot) acc += pot[zoff + q[v]] * xc;
+      T out = a * acc + b * xc;
+      if (Pc) out += g * Pc[zoff + q[v]];
+      Yc[zoff + q[v]] = out;
+      if (dot_partial) dacc += (double)out * (double)xc;
+    }
+#pragma unroll
+    for (int v = 0; v < PPT; ++v)
+#pragma unroll
+      for (int i = 0; i < 2 * R; ++i) zq[v][i] = zq[v][i + 1];
+    buf ^= 1;
+  }
+  if (dot_partial) {
+    __shared__ double sh[NT / 32];
+    dacc = psc_block_sum<double, NT>(dacc, sh);
+    if (threadIdx.x == 0)
+      dot_partial[((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = dacc;
+  }
+}
+
+struct StencilPlan {
+  int ppt, zchunk;
+  dim3 grid;
+  size_t smem;
+};
+
+// Choose points-per-thread and z-chunk so that the grid holds a few CTAs per
+// SM even for a single column, with long z runs when there are many columns.
+static StencilPlan plan_stencil(const psc_ctx* ctx, int k, size_t elem) {
+  StencilPlan p;
+  const int nxy = ctx->nx * ctx->ny;
+  p.ppt = (nxy >= 2048) ? 2 : 1;
+  const int S = 256 * p.ppt;
+  const int nslab = (nxy + S - 1) / S;
+  const long target = 148L * 6;
+  long per_col = (target + k - 1) / k;
+  int nzc = (int)std::max<long>(1, std::min<long>(ctx->nz, (per_col + nslab - 1) / nslab));
+  int zchunk = (ctx->nz + nzc - 1) / nzc;
+  if (zchunk < 4) zchunk = std::min(ctx->nz, 4);
+  nzc = (ctx->nz + zchunk - 1) / zchunk;
+  p.zchunk = zchunk;
+  p.grid = dim3(nslab, nzc, k);
+  p.smem = 2 * (size_t)(S + 2 * ctx->radius * ctx->nx) * elem;
+  return p;
+}
+
+template <typename T, int R, int PPT>
+static int launch_stencil_t(psc_ctx* ctx, const StencilPlan& p, const T* X, long ldx, const T* P,
+                            long ldp, T* Y, long ldy, const T* pot, StencilW<T> w, const double* coef,
+                            double a, double b, double g, double* dot_partial, cudaStream_t st) {
+  auto kern = k_stencil<T, R, PPT>;
+  if (p.smem > 48 * 1024) {
+    PSC_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem));
+  }
+  kern<<<p.grid, 256, p.smem, st>>>(X, ldx, P, ldp, Y, ldy, pot, ctx->nx, ctx->ny, ctx->nz, p.zchunk, w,
+                                    coef, a, b, g, dot_partial);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
+
+template <typename T>
+static int launch_stencil(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy,
+                          const T* pot, const double* c0c, const double* coef, double a, double b,
+                          double g, double* dot_partial, int* nblocks_out, cudaStream_t st) {
+  StencilPlan p = plan_stencil(ctx, k, sizeof(T));
+  if (nblocks_out) *nblocks_out = (int)(p.grid.x * p.grid.y * p.grid.z);
+  StencilW<T> w;
+  w.c0 = (T)c0c[0];
+  for (int i = 0; i < 4; ++i) w.c[i] = (T)c0c[1 + i];
+  const int R = ctx->radius;
+#define PSC_DISPATCH(RR)                                                                           \
+  if (R == RR) {                                                                                   \
+    if (p.ppt == 2)                                                                                \
+      return launch_stencil_t<T, RR, 2>(ctx, p, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g,     \
+                                        dot_partial, st);                                         \
+    return launch_stencil_t<T, RR, 1>(ctx, p, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g,       \
+                                      dot_partial, st);                                           \
+  }
+  PSC_DISPATCH(1) PSC_DISPATCH(2) PSC_DISPATCH(3) PSC_DISPATCH(4)
+#undef PSC_DISPATCH
+  PSC_REQUIRE(ctx, false, "stencil radius must be 1..4");
+}
+
+int psc_stencil_blocks(psc_ctx* ctx, int k) {
+  StencilPlan p = plan_stencil(ctx, k, sizeof(double));
+  return (int)(p.grid.x * p.grid.y * p.grid.z);
+}
+
+// Laplacian (k = 1, double) with an optional fused per-block partial of Out.In.
+int psc_laplacian_fused(psc_ctx* ctx, const double* x, const double* prev, double* y, double a, double b,
+                        double g, double* dot_partial, int* nblocks, cudaStream_t st) {
+  double w[5] = {ctx->lap_c0, ctx->lap_c[0], ctx->lap_c[1], ctx->lap_c[2], ctx->lap_c[3]};
+  return launch_stencil<double>(ctx, 1, x, ctx->n, prev, ctx->n, y, ctx->n, nullptr, w, nullptr, a, b, g,
+                                dot_partial, nblocks, st);
+}
+
+// nonlocal.cu
+int psc_nl_project(psc_ctx* ctx, int dtype, const void* X, long ldx, int k, cudaStream_t st);
+int psc_nl_scatter(psc_ctx* ctx, int dtype, void* Y, long ldy, int k, const double* coef, double a,
+                   cudaStream_t st);
+
+int psc_apply_h_impl(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long ldy, const void* P,
+                     long ldp, int k, const double* coef_dev, double a, double b, double g,
+                     cudaStream_t st) {
+  PSC_REQUIRE(ctx, k >= 1 && k <= 65535, "apply_h: k out of range");
+  PSC_REQUIRE(ctx, ldx >= ctx->n && ldy >= ctx->n && (!P || ldp >= ctx->n), "apply_h: ld < n");
+  PSC_REQUIRE(ctx, X != Y, "apply_h: input and output must differ");
+  if (ctx->nl_atoms > 0) {
+    int rc = psc_nl_project(ctx, dtype, X, ldx, k, st);
+    if (rc) return rc;
+  }
+  double w[5] = {ctx->ham_c0, ctx->ham_c[0], ctx->ham_c[1], ctx->ham_c[2], ctx->ham_c[3]};
+  int rc;
+  if (dtype == PSC_F64)
+    rc = launch_stencil<double>(ctx, k, (const double*)X, ldx, (const double*)P, ldp, (double*)Y, ldy,
+                                ctx->pot64, w, coef_dev, a, b, g, nullptr, nullptr, st);
+  else
+    rc = launch_stencil<float>(ctx, k, (const float*)X, ldx, (const float*)P, ldp, (float*)Y, ldy,
+                               ctx->pot32, w, coef_dev, a, b, g, nullptr, nullptr, st);
+  if (rc) return rc;
+  if (ctx->nl_atoms > 0) return psc_nl_scatter(ctx, dtype, Y, ldy, k, coef_dev, a, st);
+  return 0;
+}
+
+extern "C" int psc_apply_h(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long ldy, int k,
+                           void* stream) {
+  if (!ctx) return 2;
+  return psc_apply_h_impl(ctx, dtype, X, ldx, Y, ldy, nullptr, 0, k, nullptr, 1.0, 0.0, 0.0,
+                          (cudaStream_t)stream);
+}
+
+extern "C" int psc_apply_h_axpby(psc_ctx* ctx, int dtype, const void* X, long ldx, const void* P, long ldp,
+                                 void* Y, long ldy, int k, double alpha, double beta, double gamma,
+                                 void* stream) {
+  if (!ctx) return 2;
+  return psc_apply_h_impl(ctx, dtype, X, ldx, Y, ldy, P, ldp, k, nullptr, alpha, beta, gamma,
+                          (cudaStream_t)stream);
+}
+
+extern "C" int psc_laplacian_apply(psc_ctx* ctx, const double* x, double* y, int k, long ld, void* stream) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, x != y && ld >= ctx->n, "laplacian_apply: bad arguments");
+  double w[5] = {ctx->lap_c0, ctx->lap_c[0], ctx->lap_c[1], ctx->lap_c[2], ctx->lap_c[3]};
+  return launch_stencil<double>(ctx, k, x, ld, nullptr, 0, y, ld, nullptr, w, nullptr, 1.0, 0.0, 0.0,
+                                nullptr, nullptr, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Chebyshev filter coefficients computed on the device from device bounds.
+// mode 0 = scaled filter (Eigensolvers/ch_filter.py:4-81),
+// mode 1 = slim filter  (Eigensolvers/first_filt.py:78-103).
+// bounds = [lam1, low, high].  coef[j] = (alpha, beta, gamma) of step j.
+// ---------------------------------------------------------------------------
+__global__ void k_cheb_coef(int mode, int deg, const double* bounds, double* coef, int* status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double lam1 = bounds[0], lo = bounds[1], hi = bounds[2];
+  const double e = (hi - lo) / 2;
+  const double c = (hi + lo) / 2;
+  if (!(hi > lo)) status[0] = 1;  // bounds are incorrect (chefsi1.py:37-38)
+  if (mode == 0) {
+    const double s1 = e / (lam1 - c);
+    double s = s1;
+    coef[0] = s1 / e;
+    coef[1] = -c * (s1 / e);
+    coef[2] = 0.0;
+    const double two_s1 = 2.0 / s1;
+    const double inv_e = 1.0 / e;
+    for (int j = 1; j < deg; ++j) {
+      const double sn = 1.0 / (two_s1 - s);
+      const double t1 = 2.0 * sn * inv_e;
+      const double t2 = s * sn;
+      coef[3 * j + 0] = t1;
+      coef[3 * j + 1] = -c * t1;
+      coef[3 * j + 2] = -t2;
+      s = sn;
+    }
+  } else {
+    coef[0] = -1.0 / e;
+    coef[1] = c / e;
+    coef[2] = 0.0;
+    for (int j = 1; j < deg; ++j) {
+      coef[3 * j + 0] = -2.0 / e;
+      coef[3 * j + 1] = 2.0 * c / e;
+      coef[3 * j + 2] = -1.0;
+    }
+  }
+}
+
+// Filter X (k columns) to degree deg.  X holds Y_0 on entry and is reused as
+// storage, Y is the second buffer; *which = 0 if the result is in X, 1 if in Y.
+extern "C" int psc_cheb_filter(psc_ctx* ctx, int dtype, int mode, int deg, const double* bounds_dev,
+                               void* X, void* Y, long ld, int k, int* which, void* stream) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, deg >= 1 && deg <= PSC_MAX_DEG, "cheb_filter: degree out of range");
+  PSC_REQUIRE(ctx, mode == 0 || mode == 1, "cheb_filter: mode must be 0 (scaled) or 1 (slim)");
+  cudaStream_t st = (cudaStream_t)stream;
+  k_cheb_coef<<<1, 32, 0, st>>>(mode, deg, bounds_dev, ctx->cheb_coef, ctx->dev_status);
+  PSC_LAUNCH_CHECK(ctx);
+  void* buf[2] = {X, Y};
+  // step 0: Y = a*H X + b*X
+  int rc = psc_apply_h_impl(ctx, dtype, X, ld, Y, ld, nullptr, 0, k, ctx->cheb_coef, 0, 0, 0, st);
+  if (rc) return rc;
+  int cur = 1;  // buffer holding Y_j
+  for (int j = 1; j < deg; ++j) {
+    // Y_{j+1} = a*H Y_j + b*Y_j + g*Y_{j-1}, written over Y_{j-1}
+    rc = psc_apply_h_impl(ctx, dtype, buf[cur], ld, buf[cur ^ 1], ld, buf[cur ^ 1], ld, k,
+                          ctx->cheb_coef + 3 * j, 0, 0, 0, st);
+    if (rc) return rc;
+    cur ^= 1;
+  }
+  if (which) *which = cur;
+  return 0;
+}

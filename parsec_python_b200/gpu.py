@@ -1,0 +1,384 @@
+"""Device-side objects and solver stages over libpsc.
+
+Vectors are torch CUDA tensors used only as device memory; every
+computation is a libpsc kernel.  A block of k vectors is a (k, n) tensor,
+i.e. an n x k column-major matrix with leading dimension n, which is the
+layout the C ABI expects.
+
+The stages mirror the reference's backend functions
+(PARSEC.py src/Eigensolvers, src/V_ion, src/V_xc, src/Mixer) with the same
+argument meaning; results stay on the device (as the reference's CuPy path
+returns CuPy arrays) and the caller converts what it logs.
+"""
+from __future__ import annotations
+
+import ctypes
+import itertools
+import math
+from ctypes import byref, c_int, c_long, c_void_p
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import F32, F64, PscError, call
+
+_DT = {F64: torch.float64, F32: torch.float32}
+
+
+def _p(t: torch.Tensor | None) -> c_void_p:
+    return c_void_p(t.data_ptr() if t is not None else None)
+
+
+def _stream() -> c_void_p:
+    return c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def require_cuda() -> torch.device:
+    if not torch.cuda.is_available():
+        raise PscError("the GPU backend needs a CUDA device (no CPU fallback exists)")
+    _lib.load()
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+class GridContext:
+    """libpsc context of one cube domain and finite-difference order."""
+
+    def __init__(self, domain: dict, fd_order: int = 8, seed: int = 0):
+        self.device = require_cuda()
+        self.nx, self.ny, self.nz = int(domain["nx"]), int(domain["ny"]), int(domain["nz"])
+        self.h = float(domain["h"])
+        self.radius = float(domain["radius"])
+        self.fd_order = int(fd_order)
+        self.n = self.nx * self.ny * self.nz
+        ptr = c_void_p()
+        call("psc_ctx_create", self.nx, self.ny, self.nz, self.h, self.fd_order, byref(ptr))
+        self.ptr = ptr
+        self.species: dict[str, int] = {}
+        self._seed = itertools.count(int(seed) * 1_000_003 + 17)
+        self.projectors = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "ptr", None) and self.ptr.value:
+                _lib.load().psc_ctx_destroy(self.ptr)
+                self.ptr = c_void_p()
+        except Exception:
+            pass
+
+    def matches(self, domain: dict, fd_order: int) -> bool:
+        return (self.nx, self.ny, self.nz, self.h, self.radius, self.fd_order) == (
+            int(domain["nx"]), int(domain["ny"]), int(domain["nz"]), float(domain["h"]), float(domain["radius"]),
+            int(fd_order))
+
+    def call(self, name: str, *args) -> None:
+        call(name, self.ptr, *args, ctx=self.ptr)
+
+    def next_seed(self) -> int:
+        return next(self._seed)
+
+    def empty(self, *shape, dtype=torch.float64) -> torch.Tensor:
+        return torch.empty(*shape, dtype=dtype, device=self.device)
+
+    def zeros(self, *shape, dtype=torch.float64) -> torch.Tensor:
+        return torch.zeros(*shape, dtype=dtype, device=self.device)
+
+    def register_species(self, symbol: str, elem, tables) -> int:
+        if symbol in self.species:
+            return self.species[symbol]
+        sid = len(self.species)
+        tab = np.ascontiguousarray(tables[symbol], dtype=np.float64)
+        row = elem[symbol]
+        self.call("psc_set_species", sid, tab.shape[0], tab.ctypes.data_as(c_void_p), float(row["Zvalue"]),
+                  float(row["R"]))
+        self.species[symbol] = sid
+        return sid
+
+    def atom_arrays(self, atoms, elem, tables):
+        sp, xyz = [], []
+        for a in atoms:
+            sid = self.register_species(a["typ"], elem, tables)
+            c = np.asarray(a["coord"], dtype=np.float64).reshape(-1, 3)
+            for row in c:
+                sp.append(sid)
+                xyz.append(row)
+        return (np.ascontiguousarray(sp, dtype=np.int32), np.ascontiguousarray(np.array(xyz, dtype=np.float64)))
+
+    def status(self, clear: bool = True) -> list[int]:
+        flags = (c_int * 8)()
+        self.call("psc_status", flags, int(clear), _stream())
+        return list(flags)
+
+    def check_status(self) -> None:
+        f = self.status(clear=True)
+        if f[0]:
+            raise ValueError("Bounds are incorrect")
+        if f[1]:
+            raise PscError(f"Cholesky of the overlap matrix failed at column {f[1] - 1} (subspace rank deficient)")
+        if f[2]:
+            raise PscError("Jacobi eigensolver did not converge")
+
+    def info(self) -> dict:
+        out = (c_long * 8)()
+        self.call("psc_ctx_info", out)
+        keys = ("nx", "ny", "nz", "n", "nl_atoms", "nl_points", "nl_touched", "stencil_radius")
+        return dict(zip(keys, list(out)))
+
+
+class NonlocalProjectors:
+    """Factored Kleinman-Bylander term held by the context (what the
+    reference's pseudoNL returns as an n x n sparse matrix)."""
+
+    def __init__(self, ctx: GridContext):
+        self.ctx = ctx
+        self.shape = (ctx.n, ctx.n)
+        i = ctx.info()
+        self.n_atoms, self.n_points, self.n_touched = i["nl_atoms"], i["nl_points"], i["nl_touched"]
+
+    def tables(self):
+        """(atom_off, idx, u[3, points], w) on the host."""
+        na, npt = self.n_atoms, self.n_points
+        off = np.zeros(na + 1, dtype=np.int32)
+        idx = np.zeros(npt, dtype=np.int32)
+        u = np.zeros(3 * npt, dtype=np.float64)
+        w = np.zeros(na, dtype=np.float64)
+        if na:
+            self.ctx.call("psc_projector_export", off.ctypes.data_as(c_void_p), idx.ctypes.data_as(c_void_p),
+                          u.ctypes.data_as(c_void_p), w.ctypes.data_as(c_void_p))
+        return off, idx, u.reshape(3, npt), w
+
+
+class Laplacian:
+    """A = -Lap_h (rsdft_solver.py:186), applied by the stencil kernel."""
+
+    def __init__(self, ctx: GridContext):
+        self.ctx = ctx
+        self.shape = (ctx.n, ctx.n)
+
+    def __matmul__(self, x: torch.Tensor) -> torch.Tensor:
+        x = x.contiguous()
+        k = 1 if x.dim() == 1 else x.shape[0]
+        y = torch.empty_like(x)
+        self.ctx.call("psc_laplacian_apply", _p(x), _p(y), k, self.ctx.n, _stream())
+        return y
+
+
+class Hamiltonian:
+    """H = 0.5 A + V_nl + diag(pot) (rsdft_solver.py:263,285), matrix-free.
+    `dtype` selects the precision of H.X (F64 or F32 blocks)."""
+
+    def __init__(self, ctx: GridContext, pot: torch.Tensor, dtype: int = F64):
+        self.ctx = ctx
+        self.shape = (ctx.n, ctx.n)
+        self.dtype = dtype
+        self.set_potential(pot)
+
+    def set_potential(self, pot: torch.Tensor) -> None:
+        self.pot = pot
+        self.ctx.call("psc_set_potential", _p(pot), _stream())
+
+    def __matmul__(self, X: torch.Tensor) -> torch.Tensor:
+        X = X.contiguous()
+        k = 1 if X.dim() == 1 else X.shape[0]
+        dt = F32 if X.dtype == torch.float32 else F64
+        Y = torch.empty_like(X)
+        self.ctx.call("psc_apply_h", dt, _p(X), self.ctx.n, _p(Y), self.ctx.n, k, _stream())
+        return Y
+
+
+def _dtype_code(t: torch.Tensor) -> int:
+    return F32 if t.dtype == torch.float32 else F64
+
+
+# ---------------------------------------------------------------------------
+# eigensolver stages
+# ---------------------------------------------------------------------------
+def cheb_filter(H: Hamiltonian, W: torch.Tensor, T: torch.Tensor, deg: int, bounds: torch.Tensor, mode: int):
+    """Filter W in place of (W, T); returns (result, other)."""
+    which = c_int()
+    H.ctx.call("psc_cheb_filter", _dtype_code(W), mode, deg, _p(bounds), _p(W), _p(T), H.ctx.n, W.shape[0],
+               byref(which), _stream())
+    return (T, W) if which.value else (W, T)
+
+
+def orthonormalize(ctx: GridContext, W: torch.Tensor, T: torch.Tensor, passes: int = 2):
+    which = c_int()
+    ctx.call("psc_orthonormalize", _dtype_code(W), _p(W), _p(T), ctx.n, W.shape[0], passes, byref(which), _stream())
+    return (T, W) if which.value else (W, T)
+
+
+def rayleigh_ritz(ctx: GridContext, W: torch.Tensor, V: torch.Tensor, ritz: torch.Tensor):
+    ctx.call("psc_rayleigh_ritz", _dtype_code(W), _p(W), _p(V), ctx.n, W.shape[0], _p(ritz), _stream())
+    return V, W
+
+
+def lanczos_bound(ctx: GridContext, mode: int) -> torch.Tensor:
+    out = ctx.empty(8)
+    ctx.call("psc_lanczos_bound", mode, ctx.next_seed(), _p(out), _stream())
+    return out
+
+
+def first_filt(nev: int, H: Hamiltonian, polm: int = 10, dtype=torch.float64, log_trace=None):
+    """First SCF step (Eigensolvers/first_filt.py:6-75): Lanczos bounds,
+    random block, up to max_iter rounds of slim filter + orthonormalisation +
+    Rayleigh-Ritz, stop when the Ritz trace moves by <= 8%."""
+    ctx = H.ctx
+    if polm < 10 or polm > 15:
+        polm = 10
+    max_iter = max(min(int(60 / polm), 5), 3)
+    lz = lanczos_bound(ctx, 0)                       # [uppbnd, ritz_0..5]
+    bounds = ctx.empty(3)
+    ctx.call("psc_filter_bounds", 1, _p(lz[1:7]), 6, _p(lz[0:1]), _p(bounds), _stream())
+    W = ctx.empty(nev, ctx.n, dtype=dtype)
+    ctx.call("psc_random", _dtype_code(W), 0, ctx.next_seed(), _p(W), ctx.n, ctx.n, nev, _stream())
+    T = torch.empty_like(W)
+    ritz = ctx.empty(nev)
+    tr0 = None
+    for it in range(1, max_iter + 1):
+        W, T = cheb_filter(H, W, T, polm, bounds, mode=1)
+        W, T = orthonormalize(ctx, W, T)
+        W, T = rayleigh_ritz(ctx, W, T, ritz)
+        ctx.call("psc_filter_bounds", 2, _p(ritz), nev, _p(lz[0:1]), _p(bounds), _stream())
+        tr = float(np.sum(ritz.cpu().numpy()))
+        if log_trace:
+            log_trace(it, tr)
+        if it == 1:
+            tr0 = tr
+        else:
+            if abs(tr - tr0) <= 0.08 * abs(tr0):
+                break
+            tr0 = tr
+    ctx.check_status()
+    return W, ritz
+
+
+def chefsi1(W: torch.Tensor, ritzv: torch.Tensor, deg: int, nev: int, H: Hamiltonian):
+    """One Chebyshev-filtered subspace step (Eigensolvers/chefsi1.py:10-69)."""
+    ctx = H.ctx
+    k = W.shape[0]
+    if nev >= k:
+        raise ValueError("Vin should have more than nev columns")
+    lz = lanczos_bound(ctx, 1)
+    bounds = ctx.empty(3)
+    ctx.call("psc_filter_bounds", 0, _p(ritzv), k, _p(lz[0:1]), _p(bounds), _stream())
+    T = torch.empty_like(W)
+    W, T = cheb_filter(H, W, T, deg, bounds, mode=0)
+    W, T = orthonormalize(ctx, W, T)
+    ritz = ctx.empty(k)
+    W, T = rayleigh_ritz(ctx, W, T, ritz)
+    return W, ritz
+
+
+def occupations(ctx: GridContext, lam: torch.Tensor, temp: float, nelec: float, tol: float):
+    """Fermi level and occupations (Eigensolvers/occupations.py:5-56)."""
+    lam = lam.contiguous()
+    ef = ctx.empty(1)
+    occ = ctx.empty(lam.shape[0])
+    ctx.call("psc_occupations", _p(lam), lam.shape[0], float(temp), float(nelec), float(tol), _p(ef), _p(occ),
+             _stream())
+    return ef, occ
+
+
+def density(ctx: GridContext, W: torch.Tensor, nev: int, occ: torch.Tensor, rho0: torch.Tensor):
+    """(rho [e/bohr^3], hrhs) from the first nev columns (rsdft_solver.py:324-328)."""
+    h = ctx.h
+    rho = ctx.empty(ctx.n)
+    hrhs = ctx.empty(ctx.n)
+    ctx.call("psc_density", _dtype_code(W), _p(W), ctx.n, nev, _p(occ), _p(rho0), 4 * np.pi / h ** 3, h ** 3,
+             _p(rho), _p(hrhs), _stream())
+    return rho, hrhs
+
+
+def pcg(A: Laplacian, rhs: torch.Tensor, x0: torch.Tensor, maxit: int, tol: float, *prec):
+    """CG on A x = rhs from x0 (Eigensolvers/pcg.py:7-85); x0 is not modified."""
+    if prec:
+        raise NotImplementedError("the ILU-preconditioned Hartree solve (cg_prec = 1) is not implemented")
+    x = x0.clone()
+    its = c_int()
+    A.ctx.call("psc_pcg_poisson", _p(rhs), _p(x), int(maxit), float(tol), byref(its), _stream())
+    return x, its.value
+
+
+def lda_xc(ctx: GridContext, rho: torch.Tensor):
+    """LDA XC (V_xc/exc_nspn.py:8-103): (vxc [Ry], out=[exc, max rho, min rho]) on the device."""
+    vxc = ctx.empty(ctx.n)
+    out = ctx.empty(3)
+    ctx.call("psc_lda_xc", _p(rho), _p(vxc), ctx.h ** 3, _p(out), _stream())
+    return vxc, out
+
+
+class Mixer:
+    """msecant1 mixer with its history in device memory (Mixer/msecant1.py)."""
+
+    def __init__(self, ctx: GridContext, capacity: int, mix: float = 0.5, restart_factor: float = 0.1):
+        self.ctx, self.mix, self.rf = ctx, mix, restart_factor
+        ctx.call("psc_mixer_reset", int(capacity))
+
+    def __call__(self, x1: torch.Tensor, f1: torch.Tensor):
+        out = torch.empty_like(x1)
+        m = c_int()
+        self.ctx.call("psc_mixer_step", _p(x1), _p(f1), self.mix, self.rf, _p(out), byref(m), _stream())
+        return out, m.value
+
+
+def sad_setup(ctx: GridContext, atoms, elem, tables):
+    """SAD density, local and SAD Hartree potentials (V_ion/pseudoDiag.py)."""
+    sp, xyz = ctx.atom_arrays(atoms, elem, tables)
+    z_sum = 0.0
+    for a in atoms:
+        z_sum += elem[a["typ"]]["Z"] * np.asarray(a["coord"]).reshape(-1, 3).shape[0]
+    rho0, hpot0, ppot = ctx.empty(ctx.n), ctx.empty(ctx.n), ctx.empty(ctx.n)
+    info = (ctypes.c_double * 2)()
+    h = ctx.h
+    ctx.call("psc_sad_setup", len(sp), sp.ctypes.data_as(c_void_p), xyz.ctypes.data_as(c_void_p), ctx.radius,
+             h ** 3, 4 * np.pi, float(z_sum), _p(rho0), _p(hpot0), _p(ppot), info, _stream())
+    diag_info = {"electron_count_initial": info[0], "electron_count_normalized": info[1],
+                 "electron_target": float(z_sum)}
+    return rho0, hpot0, ppot, diag_info
+
+
+def projector_setup(ctx: GridContext, atoms, elem, tables) -> NonlocalProjectors:
+    sp, xyz = ctx.atom_arrays(atoms, elem, tables)
+    ctx.call("psc_projector_setup", len(sp), sp.ctypes.data_as(c_void_p), xyz.ctypes.data_as(c_void_p),
+             ctx.radius, _stream())
+    ctx.projectors = NonlocalProjectors(ctx)
+    return ctx.projectors
+
+
+def scf_update(ctx, ppot, vxc, hpot, hpot0, rho, pot):
+    """pot_new, f = pot_new - pot and [|f|^2, |pot_new|^2, sum rho(hpot+hpot0), sum rho vxc]."""
+    pot_new, f, sums = ctx.empty(ctx.n), ctx.empty(ctx.n), ctx.empty(4)
+    ctx.call("psc_scf_update", _p(ppot), _p(vxc), _p(hpot), _p(hpot0), _p(rho), _p(pot), _p(pot_new), _p(f),
+             _p(sums), _stream())
+    return pot_new, f, sums
+
+
+def axpby(ctx, x, y, a, b):
+    out = ctx.empty(ctx.n)
+    ctx.call("psc_axpby", _p(x), _p(y), float(a), float(b), _p(out), ctx.n, _stream())
+    return out
+
+
+def numpy_sum(ctx, x) -> torch.Tensor:
+    out = ctx.empty(1)
+    ctx.call("psc_numpy_sum", _p(x), x.numel(), _p(out), _stream())
+    return out
+
+
+def nuclear(atoms, elem) -> float:
+    """E_nuc = 2 sum_{i<j} Z_i Z_j / R_ij in Ry (Laplacian/nuclear.py:26-91)."""
+    pts, zs = [], []
+    for a in atoms:
+        for row in np.asarray(a["coord"], dtype=float).reshape(-1, 3):
+            pts.append(row)
+            zs.append(elem[a["typ"]]["Z"])
+    e = 0
+    for i in range(len(pts)):
+        for j in range(i + 1, len(pts)):
+            d2 = (pts[i][0] - pts[j][0]) ** 2 + (pts[i][1] - pts[j][1]) ** 2 + (pts[i][2] - pts[j][2]) ** 2
+            e += zs[i] * zs[j] / math.sqrt(d2)
+    return float(e * 2)
+
+
+def nelectrons(atoms, elem) -> int:
+    return int(sum(elem[a["typ"]]["Z"] * np.asarray(a["coord"]).reshape(-1, 3).shape[0] for a in atoms))

@@ -1,0 +1,211 @@
+"""The SCF driver: same stages, stopping rule and outputs as PARSEC.py's
+rsdft_solver.run_rsdft_calculation (rsdft_solver.py:156-462), with the
+Hamiltonian matrix-free on the GPU and every vector resident in HBM.
+
+Per SCF iteration the host reads back one small block (eigenvalues,
+occupations, the error and energy sums); the Hartree CG and the mixer's
+restart test read one scalar each.  Timings in the log are CUDA-event times
+of the device work.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import torch
+
+from . import gpu, output
+from .models import RY_EV, EnergyComponents, PreparedSystem, SCFResult, SolverBackend
+
+
+def _scaled_poldeg(poldeg: int, modifier: float) -> int:
+    return max(1, int(round(poldeg * modifier)))
+
+
+def energy_components(lam, occ, nev, sums, exc, e_nuc, h) -> EnergyComponents:
+    """rsdft_solver.py:128-153: E = 4 sum(lam f) - E_H + E_xc - int(rho V_xc) + E_nuc (Ry)."""
+    eig = 4.0 * float(np.sum(lam[:nev] * occ[:nev]))
+    eh = float(sums[2]) * h ** 3
+    vxc = float(sums[3]) * h ** 3
+    return EnergyComponents(eigen_sum_ry=eig, hartree_ry=eh, xc_ry=float(exc), ion_ry=float(e_nuc),
+                            total_ry=eig - eh + float(exc) - vxc + float(e_nuc))
+
+
+class _Events:
+    def __init__(self):
+        self.ev: dict[str, torch.cuda.Event] = {}
+
+    def mark(self, name: str) -> None:
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.ev[name] = e
+
+    def seconds(self, a: str, b: str) -> float:
+        return self.ev[a].elapsed_time(self.ev[b]) / 1000.0
+
+
+def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: SolverBackend, *,
+                          init_density=None, verbose: bool = True, on_iteration=None) -> SCFResult:
+    """Run one SCF to convergence (or maxits).
+
+    init_density: optional callable (ctx, rho0, hpot0, ppot, A) -> (rho1, hpot1)
+    replacing the SAD starting density and its Hartree potential (the
+    contract of V_ion/pseudoDiag_ML4Den_poisson.py); None keeps SAD.
+    on_iteration: optional callable(dict) receiving each iteration's record.
+    """
+    say = print if verbose else (lambda *a, **k: None)
+    rt = backend.runtime
+    s = problem.settings
+    dom = problem.domain
+    h = float(dom["h"])
+    out = problem.paths.output_file
+    atoms = problem.input_data.atoms
+    n_atoms = sum(np.asarray(a["coord"]).reshape(-1, 3).shape[0] for a in atoms)
+    timings: dict[str, float] = {}
+    setup_log: list[tuple[str, float]] = []
+
+    def stage(label, t0):
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        setup_log.append((label, dt))
+        timings[label] = dt
+
+    t_start = time.perf_counter()
+    t0 = time.perf_counter()
+    ctx = rt.context(dom)
+    A = gpu.Laplacian(ctx)
+    stage("Laplacian construction", t0)
+    n = ctx.n
+
+    t0 = time.perf_counter()
+    e_nuc0 = gpu.nuclear(atoms, elem)
+    stage("Ion-ion repulsion setup", t0)
+
+    t0 = time.perf_counter()
+    rho0, hpot0, ppot, diag_info = backend.pseudo_diag(dom, atoms, elem, n_elements, return_info=True)
+    if init_density is not None:
+        rho0, hpot0 = init_density(ctx, rho0, hpot0, ppot, A)
+    stage("Diagonal ionic potential setup", t0)
+    output.write_diag_info(out, diag_info)
+    if problem.input_data.z_charge != 0:
+        scale = problem.ztest / problem.zelec
+        rho0 = gpu.axpby(ctx, rho0, None, scale, 0.0)
+        hpot0 = gpu.axpby(ctx, hpot0, None, scale, 0.0)
+    if problem.paths.initial_density_base:
+        output.save_density_variants(rho0.cpu().numpy(), dom, problem.paths.initial_density_base)
+
+    rhoxc = gpu.axpby(ctx, rho0, None, 1.0 / h ** 3, 0.0)
+    t0 = time.perf_counter()
+    backend.pseudo_nl(dom, atoms, elem, n_elements)
+    stage("Nonlocal ionic potential setup", t0)
+
+    t0 = time.perf_counter()
+    xcpot, xc0 = gpu.lda_xc(ctx, rhoxc)
+    stage("Exchange-correlation setup", t0)
+    zero = ctx.zeros(n)
+    pot, _, init_sums = gpu.scf_update(ctx, ppot, xcpot, zero, hpot0, zero, zero)
+    if out:
+        hps = gpu.numpy_sum(ctx, rho0 * hpot0).item() * RY_EV
+        x0 = xc0.cpu().numpy()
+        output.write_initial_density_diagnostics(out, x0[1], x0[2], hps, x0[0])
+        output.write_timings(out, setup_log)
+        with open(out, "a", encoding="utf-8") as fh:
+            fh.write("\n----------------------------------\n\n")
+    timings["setup_total"] = time.perf_counter() - t_start
+
+    nelec = gpu.nelectrons(atoms, elem) - problem.input_data.z_charge
+    mixer = gpu.Mixer(ctx, capacity=s.maxits + 2)
+    H = gpu.Hamiltonian(ctx, pot)
+    if s.adaptive_scheme != 0 and sum(problem.input_data.n_atom) <= 2:
+        deg_mod = 0.75
+    else:
+        deg_mod = 1.0
+    nev = problem.nev
+    k = nev + 15
+    W = lam = occ = None
+    Hpot = ctx.zeros(n)
+    rho = ctx.zeros(n)
+    XCpot = xcpot
+    err = 10.0 + s.tol
+    its = 0
+    lam_h = occ_h = None
+    energies = None
+    history = []
+    exc = float(xc0[0].item())
+    host = torch.empty(2 * k + 8, dtype=torch.float64, pin_memory=True)
+    t_loop = time.perf_counter()
+    while err > s.tol and its < s.maxits:
+        its += 1
+        say(f"  Working ... SCF iter # {its} ... ")
+        ev = _Events()
+        H.set_potential(pot)
+        ev.mark("d0")
+        deg = _scaled_poldeg(s.poldeg, deg_mod)
+        if its == 1 and s.diagmeth == 3:
+            label = f"first_filt_{backend.label} (diagmeth={s.diagmeth})"
+            W, lam = backend.first_filt(k, H, deg)
+        elif its == 1 and s.diagmeth == 2:
+            label = f"chsubsp_{backend.label} (diagmeth={s.diagmeth})"
+            W, lam = backend.chsubsp(deg, k, H)
+        elif s.diagmeth == 1 or (its == 1 and s.diagmeth == 0):
+            label = f"lanczos_{backend.label} (diagmeth={s.diagmeth})"
+            W, lam = backend.lanczos(H, k)
+        else:
+            label = f"chebsf_{backend.label} (diagmeth={s.diagmeth})"
+            W, lam = backend.chefsi1(W, lam, deg, nev, H)
+        ev.mark("d1")
+        _, occ = backend.occupations(lam[:nev], s.fermi_temp, nelec, 1e-6)
+        rho, hrhs = gpu.density(ctx, W, nev, occ, rho0)
+        ev.mark("h0")
+        Hpot, cg_its = backend.pcg(A, hrhs, Hpot, 200, 1e-5)
+        ev.mark("h1")
+        XCpot, xcv = gpu.lda_xc(ctx, rho)
+        pot_new, f, sums = gpu.scf_update(ctx, ppot, XCpot, Hpot, hpot0, rho, pot)
+        host[:k].copy_(lam, non_blocking=True)
+        host[k:k + nev].copy_(occ, non_blocking=True)
+        host[2 * k:2 * k + 4].copy_(sums, non_blocking=True)
+        host[2 * k + 4:2 * k + 7].copy_(xcv, non_blocking=True)
+        ev.mark("end")
+        torch.cuda.current_stream().synchronize()
+        ctx.check_status()
+        hv = host.numpy()
+        lam_h = hv[:k].copy()
+        occ_h = hv[k:k + nev].copy()
+        sm = hv[2 * k:2 * k + 4].copy()
+        exc = float(hv[2 * k + 4])
+        err_new = float(np.sqrt(sm[0]) / np.sqrt(sm[1]))
+        if s.adaptive_scheme == 0 or err_new > 1 or err_new > 2 * err:
+            deg_mod = 1.0
+        elif err_new > err:
+            deg_mod = min(1.1, deg_mod + 0.2)
+        elif 3 * err_new < err:
+            deg_mod = max(0.5, deg_mod - 0.1)
+        err = err_new
+        energies = energy_components(lam_h, occ_h, nev, sm, exc, e_nuc0, h)
+        diag_t, hart_t = ev.seconds("d0", "d1"), ev.seconds("h0", "h1")
+        rec = {"iter": its, "err": err, "total_ry": energies.total_ry, "eigen_sum_ry": energies.eigen_sum_ry,
+               "hartree_ry": energies.hartree_ry, "xc_ry": energies.xc_ry, "lam": lam_h, "occ": occ_h,
+               "cg_its": cg_its, "diag_s": diag_t, "hartree_s": hart_t, "iter_s": ev.seconds("d0", "end")}
+        history.append(rec)
+        if on_iteration:
+            on_iteration(rec)
+        if out:
+            output.write_density_range(out, float(hv[2 * k + 5]), float(hv[2 * k + 6]))
+            output.write_scf_iteration(out, its, label, diag_t, nev, lam_h, occ_h, 1e-5, "no prec", hart_t, err,
+                                       energies, n_atoms)
+        say(f"   ... SCF error = {err:10.2e}\n")
+        pot, _ = mixer(pot, f)
+    timings["scf_loop"] = time.perf_counter() - t_loop
+    timings["total"] = time.perf_counter() - t_start
+    converged = err <= s.tol
+    say("SCF loop completed." + (" CONVERGED SOLUTION!!" if converged else " !!THE SYSTEM DID NOT CONVERGE!!"))
+    if problem.paths.converged_density_base:
+        output.save_density_variants((rho * h ** 3).cpu().numpy(), dom, problem.paths.converged_density_base)
+    if out and energies is not None:
+        output.write_total_energy_summary(out, energies, n_atoms)
+    if s.save_wfn and problem.paths.wfn_file:
+        output.save_wavefunction(problem.paths.wfn_file, dom, pot.cpu().numpy(), rho.cpu().numpy(),
+                                 W.double().t().cpu().numpy(), nev, problem.n_types, atoms)
+    return SCFResult(rho=rho, hpot=Hpot, xc_potential=XCpot, exc=exc, potential=pot, wavefunctions=W,
+                     eigenvalues=lam_h, occupations=occ_h, iterations=its, error=err, converged=converged,
+                     e_nuc0=e_nuc0, hpot0=hpot0, n_atoms=n_atoms, timings=timings, history=history)

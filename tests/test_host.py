@@ -1,0 +1,124 @@
+"""Host-side logic (no GPU): input parsing, units, system preparation,
+settings overrides, output formats, benchmark geometries."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from parsec_python_b200 import workloads
+from parsec_python_b200.inputs import ElementTable, load_atomic_data_from_file, prepare_input_data
+from parsec_python_b200.models import SolverSettings
+from parsec_python_b200 import output
+from parsec_python_b200.system import prepare_system
+
+SAMPLE_IN = """$system
+O  -3.56626  1.77639  0.00000
+H  -2.59626  1.77639  0.00000
+H  -3.88959  1.36040 -0.81444
+$system
+
+$settings
+unit = Angstrom
+Z_charge = 0
+density_method = sad
+grid_spacing = 0.200000
+sphere_radius = 5.000000
+tol = 2.000000e-04
+Fermi_temp = 500
+maxits = 50
+fd_order = 8
+poldeg = 10
+diagmeth = 3
+save_wfn = 0
+use_gpu = 0
+recenter_atoms = 1
+$settings
+"""
+
+
+def test_sample_input_prepares_the_reference_domain(tmp_path):
+    f = tmp_path / "H2O_sad_diagmeth3_5A_0p2A.in"
+    f.write_text(SAMPLE_IN)
+    s = SolverSettings()
+    data = prepare_input_data(s, str(f))
+    s.apply_overrides(data.settings_overrides)
+    assert (s.tol, s.maxits, s.poldeg, s.fd_order, s.diagmeth) == (2e-4, 50, 10, 8, 3)
+    elem = ElementTable()
+    p = prepare_system(data, s, elem)
+    # values printed in the shipped samples/h2o/*.out
+    assert p.domain["nx"] == 52 and p.nev == 16
+    assert f"{p.domain['radius']:10.5f}" == "   9.63760"
+    assert f"{p.h:10.5f}" == "   0.37795"
+    c = np.vstack([a["coord"] for a in p.input_data.atoms])
+    assert f"{c[0, 0]:12.6f}" == "   -0.407343" and f"{c[2, 2]:12.6f}" == "   -1.026046"
+    assert p.paths.output_file.endswith("H2O_sad_diagmeth3_5A_0p2A.out")
+
+
+def test_settings_override_rules():
+    s = SolverSettings()
+    ap = s.apply_overrides({"TOL": "6", "Fermi_temp": "300", "adaptiveScheme": "1", "unknown": 3, "write_wfn": "yes"})
+    assert s.tol == 1e-6 and s.fermi_temp == 300.0 and s.adaptive_scheme == 1 and s.save_wfn == 1
+    assert "unknown" not in ap
+    s.apply_overrides({"diagmeth": 7})
+    assert s.diagmeth == 3
+
+
+def test_json_and_txt_inputs(tmp_path):
+    j = tmp_path / "h.json"
+    j.write_text('{"atoms": [{"typ": "H", "coord": [[0.0, 0.0, 0.0]]}], "charge": 0.0, '
+                 '"settings": {"unit": "bohr", "maxits": 1, "nev": 1}}')
+    d = load_atomic_data_from_file(str(j))
+    assert d.atoms[0]["typ"] == "H" and d.settings_overrides["nev"] == 1 and d.settings_overrides["unit"] == "bohr"
+    t = tmp_path / "x.txt"
+    t.write_text("C 0 0 0\nH 1 0 0\nC 2 0 0\n")
+    d = load_atomic_data_from_file(str(t))
+    assert [a["typ"] for a in d.atoms] == ["C", "H"] and d.n_atom == [2, 1]
+    with pytest.raises(ValueError):
+        t.write_text("C 0 0\n")
+        load_atomic_data_from_file(str(t))
+
+
+def test_scf_iteration_block_format(tmp_path):
+    from parsec_python_b200.models import EnergyComponents
+
+    out = tmp_path / "a.out"
+    output.initialize_output_file(str(out), "gpu", "sad")
+    e = EnergyComponents(-10.78258, 45.85619, -8.79420, 13.76119, -40.14373)
+    output.write_scf_iteration(str(out), 1, "first_filt_gpu (diagmeth=3)", 0.5, 2, np.array([-1.09310376, -0.65923964]),
+                               np.array([1.0, 1.0]), 1e-5, "no prec", 0.1, 0.328, e, 3)
+    text = out.read_text()
+    assert "    1     -2.1862075200" in text
+    assert "   ... SCF error =   3.28e-01" in text
+    assert "     Total electronic energy = -546.18347  eV   =  -40.14373  Ry  " in text
+
+
+def test_density_npy_variants(tmp_path):
+    dom = {"nx": 4, "ny": 4, "nz": 4, "h": 0.5, "radius": 0.75}
+    g = np.arange(64, dtype=float)
+    output.save_density_variants(g, dom, str(tmp_path / "r"))
+    a = np.load(tmp_path / "r_grid.npy")
+    assert a.shape == (4, 4, 4) and a[1, 0, 0] == 1.0 and a[0, 1, 0] == 4.0
+    np.testing.assert_allclose(np.load(tmp_path / "r_bohr3.npy"), a / 0.125)
+
+
+def test_benchmark_geometries():
+    c = workloads.count
+    assert c(workloads.naphthalene()) == {"C": 10, "H": 8}
+    assert c(workloads.sih_cluster(4)) == {"Si": 35, "H": 36}
+    assert c(workloads.sih_cluster(7)) == {"Si": 87, "H": 76}
+    for seed in (0, 5, 511):
+        w = workloads.water_cluster(seed)
+        n = c(w)["O"]
+        assert 2 <= n <= 8 and c(w)["H"] == 2 * n
+        o = w[0]["coord"]
+        d = np.linalg.norm(o[:, None] - o[None], axis=-1) + np.eye(n) * 10
+        assert d.min() >= 2.6 and np.linalg.norm(o, axis=1).max() <= 6.0
+
+
+def test_oracle_and_product_grid_rules_agree():
+    s = SolverSettings()
+    elem = ElementTable()
+    from parsec_python_b200.system import cube_for_radius
+
+    for h, r in ((0.378, 9.45), (0.34, 13.2), (0.4724, 17.0)):
+        assert cube_for_radius(r, h) == O.build_system([], h=h, radius=r)
+    assert s.precision == "fp64" and len(elem) == 18
