@@ -82,6 +82,9 @@ int psc_apply_h(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long 
 /* Y = alpha H X + beta X + gamma P (P may be NULL or alias Y). */
 int psc_apply_h_axpby(psc_ctx* ctx, int dtype, const void* X, long ldx, const void* P, long ldp, void* Y, long ldy,
                       int k, double alpha, double beta, double gamma, void* stream);
+/* Stencil implementation: 0 = TMA-fed pipeline where the bulk-copy alignment
+ * rules hold (default), 1 = register-queue kernel everywhere. */
+int psc_set_stencil_impl(psc_ctx* ctx, int impl);
 /* Y = A X with A = -Lap_h (Laplacian/fd3d.py:34-106 scaled by 1/h^2). */
 int psc_laplacian_apply(psc_ctx* ctx, const double* x, double* y, int k, long ld, void* stream);
 
@@ -129,6 +132,9 @@ int psc_density(psc_ctx* ctx, int dtype, const void* W, long ld, int nev, const 
 /* CG on A x = rhs, warm start in x (Eigensolvers/pcg.py:7-85, backend.pcg at
  * rsdft_solver.py:345). *its_out = iterations. */
 int psc_pcg_poisson(psc_ctx* ctx, const double* rhs, double* x, int maxit, double tol, int* its_out, void* stream);
+/* 1 (default): replay captured CUDA graphs for the CG iterations; 0: launch
+ * each kernel from the host. */
+int psc_set_use_graphs(psc_ctx* ctx, int on);
 /* LDA (Ceperley-Alder / Perdew-Zunger), V_xc/exc_nspn.py:8-103.
  * out_dev = [exc, max rho, min rho]. */
 int psc_lda_xc(psc_ctx* ctx, const double* rho, double* vxc, double h3, double* out_dev, void* stream);

@@ -34,6 +34,7 @@ _SIGS = {
     "psc_apply_h": ([_P, c_int, _P, c_long, _P, c_long, c_int, _P], c_int),
     "psc_apply_h_axpby": ([_P, c_int, _P, c_long, _P, c_long, _P, c_long, c_int, c_double, c_double, c_double, _P],
                           c_int),
+    "psc_set_stencil_impl": ([_P, c_int], c_int),
     "psc_laplacian_apply": ([_P, _P, _P, c_int, c_long, _P], c_int),
     "psc_cheb_filter": ([_P, c_int, c_int, c_int, _P, _P, _P, c_long, c_int, POINTER(c_int), _P], c_int),
     "psc_lanczos_bound": ([_P, c_int, c_ulonglong, _P, _P], c_int),
@@ -46,6 +47,7 @@ _SIGS = {
     "psc_occupations": ([_P, _P, c_int, c_double, c_double, c_double, _P, _P, _P], c_int),
     "psc_density": ([_P, c_int, _P, c_long, c_int, _P, _P, c_double, c_double, _P, _P, _P], c_int),
     "psc_pcg_poisson": ([_P, _P, _P, c_int, c_double, POINTER(c_int), _P], c_int),
+    "psc_set_use_graphs": ([_P, c_int], c_int),
     "psc_lda_xc": ([_P, _P, _P, c_double, _P, _P], c_int),
     "psc_scf_update": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], c_int),
     "psc_mixer_reset": ([_P, c_int], c_int),

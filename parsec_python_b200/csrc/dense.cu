@@ -345,7 +345,8 @@ int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, 
   if (psc_ensure_dense(ctx, k)) return 1;
   const size_t smem = 2 * (size_t)k * k * sizeof(double);
   const int use_smem = smem <= 200 * 1024;
-  if (use_smem && smem > 48 * 1024)
+  // the opt-in limit covers dynamic + static shared memory (~12.5 KB static here)
+  if (use_smem)
     PSC_CUDA(ctx, cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // V scratch in global memory when the matrices do not fit on chip
   double* vg = use_smem ? nullptr : ctx->gram2;

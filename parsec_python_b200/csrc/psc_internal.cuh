@@ -50,6 +50,7 @@ struct psc_ctx {
   double h = 0.0;
   int fd_order = 8;
   int radius = 4;            // stencil half-width (fd_order/2, capped at 4)
+  int stencil_impl = 0;      // 0: TMA pipeline where it applies, 1: register-queue kernel only
   double lap_c0 = 0.0;       // centre weight of A = -Lap_h (1/h^2 folded in)
   double lap_c[4] = {0, 0, 0, 0};
   double ham_c0 = 0.0;       // 0.5 * A weights, as 0.5*(c*(1/(h*h)))
@@ -105,6 +106,10 @@ struct psc_ctx {
   double* cg_ap = nullptr;
   double* cg_part = nullptr;     // [2][cg_part_cap] per-CTA partial sums
   int cg_part_cap = 0;
+  double* cg_x = nullptr;        // solution buffer the captured CG graph works on
+  cudaGraphExec_t cg_exec = nullptr;
+  cudaStream_t cap_stream = nullptr;  // private stream used only for graph capture
+  int use_graphs = 1;
 
   // mixer history
   int mix_cap = 0;

@@ -155,7 +155,7 @@ static int launch_stencil_t(psc_ctx* ctx, const StencilPlan& p, const T* X, long
                             long ldp, T* Y, long ldy, const T* pot, StencilW<T> w, const double* coef,
                             double a, double b, double g, double* dot_partial, cudaStream_t st) {
   auto kern = k_stencil<T, R, PPT>;
-  if (p.smem > 48 * 1024) {
+  if (p.smem > 40 * 1024) {
     PSC_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem));
   }
   kern<<<p.grid, 256, p.smem, st>>>(X, ldx, P, ldp, Y, ldy, pot, ctx->nx, ctx->ny, ctx->nz, p.zchunk, w,
@@ -165,9 +165,19 @@ static int launch_stencil_t(psc_ctx* ctx, const StencilPlan& p, const T* X, long
 }
 
 template <typename T>
+int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy, const T* pot,
+                    const double* w, const double* coef, double a, double b, double g, cudaStream_t st);
+
+template <typename T>
 static int launch_stencil(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy,
                           const T* pot, const double* c0c, const double* coef, double a, double b,
                           double g, double* dot_partial, int* nblocks_out, cudaStream_t st) {
+  // the TMA pipeline serves every launch that needs no fused dot product and
+  // meets the bulk-copy alignment rules; the register-queue kernel the rest
+  if (!dot_partial && ctx->stencil_impl == 0) {
+    const int rc = psc_stencil_tma<T>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, c0c, coef, a, b, g, st);
+    if (rc >= 0) return rc;
+  }
   StencilPlan p = plan_stencil(ctx, k, sizeof(T));
   if (nblocks_out) *nblocks_out = (int)(p.grid.x * p.grid.y * p.grid.z);
   StencilW<T> w;
@@ -315,5 +325,13 @@ extern "C" int psc_cheb_filter(psc_ctx* ctx, int dtype, int mode, int deg, const
     cur ^= 1;
   }
   if (which) *which = cur;
+  return 0;
+}
+
+// 0: TMA pipeline wherever it applies (default), 1: register-queue kernel only.
+extern "C" int psc_set_stencil_impl(psc_ctx* ctx, int impl) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, impl == 0 || impl == 1, "stencil impl must be 0 or 1");
+  ctx->stencil_impl = impl;
   return 0;
 }

@@ -162,7 +162,8 @@ def test_dense_building_blocks():
         W = rng.standard_normal((ctx.n, k))
         V = rng.standard_normal((ctx.n, k))
         g = ctx.empty(k, k)
-        ctx.call("psc_gram", F64, gpu._p(block(V)), ctx.n, gpu._p(block(W)), ctx.n, k, 0, gpu._p(g), gpu._stream())
+        Vd, Wd = block(V), block(W)  # keep the device buffers alive across the call
+        ctx.call("psc_gram", F64, gpu._p(Vd), ctx.n, gpu._p(Wd), ctx.n, k, 0, gpu._p(g), gpu._stream())
         G = g.cpu().numpy().T
         assert rel(G, V.T @ W) < 1e-13
         # symmetric eigensolver (k x k FP64, one CTA)
@@ -188,7 +189,7 @@ def test_dense_building_blocks():
         Qm = rng.standard_normal((k, k))
         out = ctx.empty(k, ctx.n)
         Qd = torch.from_numpy(Qm.ravel(order="F").copy()).to(DEV)
-        ctx.call("psc_gemm_nn", F64, gpu._p(block(W)), ctx.n, k, gpu._p(Qd), k, gpu._p(out), ctx.n, gpu._stream())
+        ctx.call("psc_gemm_nn", F64, gpu._p(Wd), ctx.n, k, gpu._p(Qd), k, gpu._p(out), ctx.n, gpu._stream())
         assert rel(host(out), W @ Qm) < 1e-13
 
 
@@ -245,3 +246,48 @@ def test_lanczos_bounds_bracket_the_spectrum(h2o_box, golden_dir):
     assert abs(b0[0] - float(ev["uppbnd"])) < 0.05 * abs(float(ev["uppbnd"]))
     assert abs(b1[0] - float(ev["bound"])) < 0.05 * abs(float(ev["bound"]))
     assert np.all(np.diff(b0[1:7]) >= 0)
+
+
+@pytest.mark.parametrize("shape,order", [((78, 78, 78), 8), ((24, 24, 24), 8), ((20, 16, 12), 6), ((12, 10, 8), 4),
+                                         ((10, 12, 14), 2), ((90, 90, 90), 8)])
+@pytest.mark.parametrize("dt", ["f64", "f32"])
+def test_tma_stencil_matches_register_kernel(shape, order, dt):
+    nx, ny, nz = shape
+    dom = {"nx": nx, "ny": ny, "nz": nz, "h": 0.34, "radius": 0.17 * (nx - 1)}
+    ctx = gpu.GridContext(dom, order)
+    n = ctx.n
+    k = 55 if nx >= 78 else 5
+    tdt = torch.float64 if dt == "f64" else torch.float32
+    code = F64 if dt == "f64" else F32
+    g = torch.Generator(device="cuda").manual_seed(7)
+    gpu.Hamiltonian(ctx, torch.randn(n, dtype=torch.float64, device=DEV, generator=g))
+    X = torch.randn(k, n, dtype=tdt, device=DEV, generator=g)
+    P = torch.randn(k, n, dtype=tdt, device=DEV, generator=g)
+    outs = []
+    for impl in (0, 1):
+        ctx.call("psc_set_stencil_impl", impl)
+        Y = P.clone()
+        ctx.call("psc_apply_h_axpby", code, gpu._p(X), n, gpu._p(Y), n, gpu._p(Y), n, k, 0.7, -0.2, -0.9,
+                 gpu._stream())
+        outs.append(Y.double().cpu().numpy())
+    tol = 1e-14 if dt == "f64" else 2e-6
+    assert rel(outs[0], outs[1]) < tol
+
+
+def test_pcg_graph_equals_direct_launches():
+    dom = {"nx": 40, "ny": 40, "nz": 40, "h": 0.4, "radius": 7.8}
+    ctx = gpu.GridContext(dom, 8)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    rhs = torch.randn(ctx.n, dtype=torch.float64, device=DEV, generator=g)
+    x0 = torch.randn(ctx.n, dtype=torch.float64, device=DEV, generator=g) * 0.1
+    A = gpu.Laplacian(ctx)
+    res = []
+    for on in (1, 0):
+        ctx.call("psc_set_use_graphs", on)
+        res.append(gpu.pcg(A, rhs, x0, 200, 1e-5))
+    assert res[0][1] == res[1][1]
+    assert torch.equal(res[0][0], res[1][0])
+    # the oracle's CG on the same system
+    xo, its = O.pcg(O.laplacian(dom, 8), rhs.cpu().numpy(), x0.cpu().numpy(), 200, 1e-5)
+    assert abs(its - res[0][1]) <= 1
+    assert rel(res[0][0].cpu().numpy(), xo) < 1e-8
