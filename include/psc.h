@@ -112,6 +112,11 @@ int psc_orthonormalize(psc_ctx* ctx, int dtype, void* W, void* T, long ld, int k
  * written to V, Ritz values to ritz_dev. */
 int psc_rayleigh_ritz(psc_ctx* ctx, int dtype, const void* W, void* V, long ld, int k, double* ritz_dev,
                       void* stream);
+/* Rayleigh-Ritz of a filtered, not necessarily orthonormal block W in one
+ * pass: V = H W, S = W^T W = R^T R, K = W^T V, eigenpairs of R^{-T} K R^{-1},
+ * result W R^{-1} Y written to V (same Ritz pairs as QR followed by
+ * Rayleigh-Ritz, chefsi1.py:43-67 / first_filt.py:43-63). */
+int psc_subspace_rr(psc_ctx* ctx, int dtype, const void* W, void* V, long ld, int k, double* ritz_dev, void* stream);
 /* Building blocks: G = A^T B (mode 0 plain, 1 upper mirrored, 2 symmetrised),
  * Out = W Q, symmetric eigensolver (ascending, FP64, one CTA, k <= 1023). */
 int psc_gram(psc_ctx* ctx, int dtype, const void* A, long lda, const void* B, long ldb, int k, int mode,

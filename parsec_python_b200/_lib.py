@@ -41,6 +41,7 @@ _SIGS = {
     "psc_filter_bounds": ([_P, c_int, _P, c_int, _P, _P, _P], c_int),
     "psc_orthonormalize": ([_P, c_int, _P, _P, c_long, c_int, c_int, POINTER(c_int), _P], c_int),
     "psc_rayleigh_ritz": ([_P, c_int, _P, _P, c_long, c_int, _P, _P], c_int),
+    "psc_subspace_rr": ([_P, c_int, _P, _P, c_long, c_int, _P, _P], c_int),
     "psc_gram": ([_P, c_int, _P, c_long, _P, c_long, c_int, c_int, _P, _P], c_int),
     "psc_gemm_nn": ([_P, c_int, _P, c_long, c_int, _P, c_int, _P, c_long, _P], c_int),
     "psc_syev": ([_P, _P, c_int, _P, _P, _P], c_int),

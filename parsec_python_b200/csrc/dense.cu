@@ -90,8 +90,10 @@ int psc_ensure_dense(psc_ctx* ctx, int k) {
   PSC_REQUIRE(ctx, k >= 1 && k <= PSC_MAX_K, "subspace width out of range");
   if (k <= ctx->dense_cap) return 0;
   cudaFree(ctx->gram); cudaFree(ctx->gram2); cudaFree(ctx->evec); cudaFree(ctx->tri); cudaFree(ctx->gram_partial);
+  cudaFree(ctx->jac_v);
   const int cap = std::max(k, 64);
   const size_t kk = (size_t)cap * cap;
+  PSC_CUDA(ctx, cudaMalloc(&ctx->jac_v, kk * sizeof(double)));
   PSC_CUDA(ctx, cudaMalloc(&ctx->gram, kk * sizeof(double)));
   PSC_CUDA(ctx, cudaMalloc(&ctx->gram2, kk * sizeof(double)));
   PSC_CUDA(ctx, cudaMalloc(&ctx->evec, kk * sizeof(double)));
@@ -136,55 +138,15 @@ extern "C" int psc_gram(psc_ctx* ctx, int dtype, const void* A, long lda, const 
 }
 
 // ---------------------------------------------------------------------------
-// Out (n x kout) = W (n x k) * Q (k x kout, FP64, column-major)
+// Out (n x kout) = W (n x k) * Q (k x kout, FP64, column-major): k_gemm_tall
+// in subspace.cu
 // ---------------------------------------------------------------------------
-constexpr int MM_J = 32;   // output columns per CTA
-constexpr int MM_I = 128;  // Q rows staged per step
-
-template <typename T>
-__global__ void __launch_bounds__(128)
-k_gemm_nn(const T* __restrict__ W, long ldw, int k, const double* __restrict__ Q, int kout, T* __restrict__ O,
-          long ldo, long n) {
-  __shared__ double Qs[MM_I][MM_J];
-  const long row = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const int j0 = blockIdx.y * MM_J;
-  const int nj = min(MM_J, kout - j0);
-  double acc[MM_J];
-#pragma unroll
-  for (int j = 0; j < MM_J; ++j) acc[j] = 0.0;
-  for (int i0 = 0; i0 < k; i0 += MM_I) {
-    const int ni = min(MM_I, k - i0);
-    __syncthreads();
-    for (int e = threadIdx.x; e < MM_I * MM_J; e += blockDim.x) {
-      const int i = e / MM_J, j = e % MM_J;
-      Qs[i][j] = (i < ni && j < nj) ? Q[(i0 + i) + (long)(j0 + j) * k] : 0.0;
-    }
-    __syncthreads();
-    if (row < n) {
-      for (int i = 0; i < ni; ++i) {
-        const double w = (double)W[row + (long)(i0 + i) * ldw];
-#pragma unroll
-        for (int j = 0; j < MM_J; ++j) acc[j] += w * Qs[i][j];
-      }
-    }
-  }
-  if (row < n) {
-#pragma unroll
-    for (int j = 0; j < MM_J; ++j)
-      if (j < nj) O[row + (long)(j0 + j) * ldo] = (T)acc[j];
-  }
-}
+int psc_gemm_tall(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Tm, int kout, void* O,
+                  long ldo, cudaStream_t st);
 
 int psc_gemm_nn_impl(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Q, int kout, void* out,
                      long ldo, cudaStream_t st) {
-  PSC_REQUIRE(ctx, W != out, "gemm: output must not alias input");
-  dim3 grid(psc_div_up(ctx->n, 128), psc_div_up(kout, MM_J));
-  if (dtype == PSC_F64)
-    k_gemm_nn<double><<<grid, 128, 0, st>>>((const double*)W, ldw, k, Q, kout, (double*)out, ldo, ctx->n);
-  else
-    k_gemm_nn<float><<<grid, 128, 0, st>>>((const float*)W, ldw, k, Q, kout, (float*)out, ldo, ctx->n);
-  PSC_LAUNCH_CHECK(ctx);
-  return 0;
+  return psc_gemm_tall(ctx, dtype, W, ldw, k, Q, kout, out, ldo, st);
 }
 
 extern "C" int psc_gemm_nn(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Q, int kout,
@@ -238,41 +200,41 @@ __global__ void k_triu_inv(const double* __restrict__ R, int k, double* __restri
 // Cyclic Jacobi eigensolver, one CTA.  Round-robin pairing (circle method):
 // every round rotates k/2 disjoint (p,q) planes -- columns of A and V first,
 // then rows of A -- so each sweep annihilates every off-diagonal pair once.
-// Converged when off(A) <= 1e-15 * ||A||_F or after 40 sweeps.  Eigenvalues
-// ascending, eigenvectors permuted to match.
+// The input is symmetrised first.  A pair is rotated only while
+// |a_pq| > 1e-17 (|a_pp| + |a_qq|); the solver has converged when a whole
+// sweep rotates nothing (at most 40 sweeps).  Eigenvalues ascending,
+// eigenvectors permuted to match.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024)
+template <int NT>
+__global__ void __launch_bounds__(NT)
 k_jacobi(double* __restrict__ Ag, int k, double* __restrict__ evals, double* __restrict__ Vout, int use_smem,
          double* __restrict__ Vg, int* status) {
   extern __shared__ double sm[];
-  __shared__ double red[32];
   __shared__ int rp[512], rq[512];
   __shared__ double rc[512], rs[512];
-  __shared__ int done;
+  __shared__ int nrot;
   double* A = use_smem ? sm : Ag;
   double* V = use_smem ? sm + (long)k * k : Vg;
   const long kk = (long)k * k;
   if (use_smem)
     for (long e = threadIdx.x; e < kk; e += blockDim.x) A[e] = Ag[e];
   for (long e = threadIdx.x; e < kk; e += blockDim.x) V[e] = ((e % k) == (e / k)) ? 1.0 : 0.0;
+  __syncthreads();
+  // symmetrise: callers may pass a matrix that is symmetric only to rounding
+  for (long e = threadIdx.x; e < kk; e += blockDim.x) {
+    const int i = (int)(e % k), j = (int)(e / k);
+    if (i < j) {
+      const double v = 0.5 * (A[i + (long)j * k] + A[j + (long)i * k]);
+      A[i + (long)j * k] = v;
+      A[j + (long)i * k] = v;
+    }
+  }
   const int m = k + (k & 1);
   const int half = m / 2;
-  if (threadIdx.x == 0) done = 0;
   __syncthreads();
   for (int sweep = 0; sweep < 40 && k > 1; ++sweep) {
-    // convergence test
-    double off = 0.0, tot = 0.0;
-    for (long e = threadIdx.x; e < kk; e += blockDim.x) {
-      const double v = A[e] * A[e];
-      tot += v;
-      if ((e % k) != (e / k)) off += v;
-    }
-    off = psc_block_sum<double, 1024>(off, red);
+    if (threadIdx.x == 0) nrot = 0;
     __syncthreads();
-    tot = psc_block_sum<double, 1024>(tot, red);
-    if (threadIdx.x == 0) done = (off <= 1e-30 * tot) ? 1 : 0;
-    __syncthreads();
-    if (done) break;
     for (int r = 0; r < m - 1; ++r) {
       for (int i = threadIdx.x; i < half; i += blockDim.x) {
         const int a = (i == 0) ? 0 : ((i - 1 + r) % (m - 1)) + 1;
@@ -281,7 +243,10 @@ k_jacobi(double* __restrict__ Ag, int k, double* __restrict__ evals, double* __r
         double c = 1.0, s = 0.0;
         if (q < k) {
           const double apq = A[p + (long)q * k];
-          if (apq != 0.0) {
+          const double app0 = A[p + (long)p * k], aqq0 = A[q + (long)q * k];
+          // rotate unless the pair is already diagonal to working precision
+          if (fabs(apq) > 1e-17 * (fabs(app0) + fabs(aqq0)) && apq != 0.0) {
+            atomicAdd(&nrot, 1);
             const double app = A[p + (long)p * k], aqq = A[q + (long)q * k];
             const double theta = (aqq - app) / (2.0 * apq);
             double t;
@@ -324,6 +289,10 @@ k_jacobi(double* __restrict__ Ag, int k, double* __restrict__ evals, double* __r
       }
       __syncthreads();
     }
+    // a sweep without rotations means every pair is diagonal to working precision
+    const int rotated = nrot;
+    __syncthreads();
+    if (rotated == 0) break;
     if (threadIdx.x == 0 && sweep == 39) status[2] = 1;  // did not converge
   }
   __syncthreads();
@@ -345,13 +314,22 @@ int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, 
   if (psc_ensure_dense(ctx, k)) return 1;
   const size_t smem = 2 * (size_t)k * k * sizeof(double);
   const int use_smem = smem <= 200 * 1024;
-  // the opt-in limit covers dynamic + static shared memory (~12.5 KB static here)
-  if (use_smem)
-    PSC_CUDA(ctx, cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // V scratch in global memory when the matrices do not fit on chip
-  double* vg = use_smem ? nullptr : ctx->gram2;
-  PSC_REQUIRE(ctx, use_smem || (A != ctx->gram2 && evecs != ctx->gram2), "syev: scratch aliasing");
-  k_jacobi<<<1, 1024, use_smem ? smem : 0, st>>>(A, k, evals, evecs, use_smem, vg, ctx->dev_status);
+  double* vg = use_smem ? nullptr : ctx->jac_v;
+  const size_t dyn = use_smem ? smem : 0;
+  // CTA size matched to the k/2 x k element updates of a rotation round; the
+  // opt-in limit covers dynamic + static shared memory (~12.5 KB static)
+#define PSC_JACOBI(NTH)                                                                                   \
+  {                                                                                                       \
+    if (use_smem)                                                                                         \
+      PSC_CUDA(ctx, cudaFuncSetAttribute(k_jacobi<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    k_jacobi<NTH><<<1, NTH, dyn, st>>>(A, k, evals, evecs, use_smem, vg, ctx->dev_status);               \
+  }
+  const long work = (long)((k + 1) / 2) * k;
+  if (work <= 2048) PSC_JACOBI(256)
+  else if (work <= 8192) PSC_JACOBI(512)
+  else PSC_JACOBI(1024)
+#undef PSC_JACOBI
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }
@@ -403,4 +381,16 @@ extern "C" int psc_rayleigh_ritz(psc_ctx* ctx, int dtype, const void* W, void* V
   rc = psc_syev_impl(ctx, ctx->gram, k, ritz_dev, ctx->evec, st);
   if (rc) return rc;
   return psc_gemm_nn_impl(ctx, dtype, W, ld, k, ctx->evec, k, V, ld, st);
+}
+
+int psc_cholesky_dev(psc_ctx* ctx, double* A, int k, cudaStream_t st) {
+  k_cholesky<<<1, 1024, 0, st>>>(A, k, ctx->dev_status);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
+
+int psc_triu_inv_dev(psc_ctx* ctx, const double* R, int k, double* X, cudaStream_t st) {
+  k_triu_inv<<<psc_div_up(k, 128), 128, 0, st>>>(R, k, X);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
 }

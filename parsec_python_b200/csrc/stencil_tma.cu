@@ -177,7 +177,6 @@ k_stencil_tma(TmaArgs<T> A) {
   const bool own = loc < seff;
   const int q = slab0 + loc;
   const int xi = own ? q % nx : 0;
-  const int yi = own ? q / nx : 0;
   const int s_c = H + loc;  // window offset of the pair
 
   // z queue from direct loads of the planes below the chunk
@@ -196,6 +195,7 @@ k_stencil_tma(TmaArgs<T> A) {
   }
   bool fail = false;
   // planes z0 .. z0+R-1 enter the queue from the ring
+#pragma unroll
   for (int i = 0; i < R; ++i) {
     const int p = z0 + i;
     if (p < nz) {
@@ -209,91 +209,99 @@ k_stencil_tma(TmaArgs<T> A) {
     }
   }
 
+  // per-thread x-boundary weights: a neighbour across the row edge gets 0
+  T cl0[R], cr0[R], cl1[R], cr1[R];
+#pragma unroll
+  for (int d = 1; d <= R; ++d) {
+    const T cd = A.c[d - 1];
+    cl0[d - 1] = (xi - d >= 0) ? cd : T(0);
+    cr0[d - 1] = (xi + d < nx) ? cd : T(0);
+    cl1[d - 1] = (xi + 1 - d >= 0) ? cd : T(0);
+    cr1[d - 1] = (xi + 1 + d < nx) ? cd : T(0);
+  }
   const T c0 = A.c0;
-  for (int z = z0; z < z1; ++z) {
-    // queue front: plane z + R
-    const int pf = z + R;
-    T f0 = T(0), f1 = T(0);
-    if (pf < nz) {
-      const int s = (pf - z0) % NBUF;
-      if (!fail && !mbar_wait(&bars[s], ((pf - z0) / NBUF) & 1)) fail = true;
+  // z loop unrolled by Q = 2R+1 so the register queue rotates by renaming:
+  // at unrolled position u, plane z - R + i lives in zq[(u + i) % Q]
+  constexpr int Q = 2 * R + 1;
+#pragma unroll 1
+  for (int zb = z0; zb < z1; zb += Q) {
+#pragma unroll
+    for (int u = 0; u < Q; ++u) {
+      const int z = zb + u;
+      if (z >= z1) break;
+      // queue front: plane z + R
+      const int pf = z + R;
+      T f0 = T(0), f1 = T(0);
+      if (pf < nz) {
+        const int s = (pf - z0) % NBUF;
+        if (!fail && !mbar_wait(&bars[s], ((pf - z0) / NBUF) & 1)) fail = true;
+        if (own) {
+          const V2 v = *reinterpret_cast<const V2*>(ring + (size_t)s * WIN + s_c);
+          f0 = v.x;
+          f1 = v.y;
+        }
+      }
+      zq0[(u + 2 * R) % Q] = f0;
+      zq1[(u + 2 * R) % Q] = f1;
+      const int sp = (z - z0) % PBUF;
+      if (Pc || has_pot) {
+        if (!fail && !mbar_wait(&bars[NBUF + sp], ((z - z0) / PBUF) & 1)) fail = true;
+      }
+      const T* pl = ring + (size_t)((z - z0) % NBUF) * WIN;
       if (own) {
-        const V2 v = *reinterpret_cast<const V2*>(ring + (size_t)s * WIN + s_c);
-        f0 = v.x;
-        f1 = v.y;
-      }
-    }
-    zq0[2 * R] = f0;
-    zq1[2 * R] = f1;
-    const int sp = (z - z0) % PBUF;
-    if (Pc || has_pot) {
-      if (!fail && !mbar_wait(&bars[NBUF + sp], ((z - z0) / PBUF) & 1)) fail = true;
-    }
-    const T* pl = ring + (size_t)((z - z0) % NBUF) * WIN;
-    if (own) {
-      // x neighbours: window values s_c - R .. s_c + R + 1, fetched as aligned
-      // pairs starting at the even offset s_c - R - (R & 1)
-      constexpr int NP = R + 1 + (R & 1);
-      T xs[2 * NP];
+        // x neighbours: window values s_c - R .. s_c + R + 1, fetched as aligned
+        // pairs starting at the even offset s_c - R - (R & 1)
+        constexpr int NP = R + 1 + (R & 1);
+        T xs[2 * NP];
 #pragma unroll
-      for (int j = 0; j < NP; ++j) {
-        const V2 v = *reinterpret_cast<const V2*>(pl + s_c - R - (R & 1) + 2 * j);
-        xs[2 * j] = v.x;
-        xs[2 * j + 1] = v.y;
-      }
-      // xs[k] holds window offset s_c - R - (R&1) + k
-      constexpr int OFF = R + (R & 1);  // index of the first point of the pair in xs
-      const T xc0 = zq0[R], xc1 = zq1[R];
-      T acc0 = c0 * xc0, acc1 = c0 * xc1;
-#pragma unroll
-      for (int d = 1; d <= R; ++d) {
-        const T cd = A.c[d - 1];
-        T s0 = zq0[R - d] + zq0[R + d];
-        T s1 = zq1[R - d] + zq1[R + d];
-        if (xi - d >= 0) s0 += xs[OFF - d];
-        if (xi + d < nx) s0 += xs[OFF + d];
-        if (xi + 1 - d >= 0) s1 += xs[OFF + 1 - d];
-        if (xi + 1 + d < nx) s1 += xs[OFF + 1 + d];
-        if (yi - d >= 0) {
-          const V2 v = *reinterpret_cast<const V2*>(pl + s_c - d * nx);
-          s0 += v.x;
-          s1 += v.y;
+        for (int j = 0; j < NP; ++j) {
+          const V2 v = *reinterpret_cast<const V2*>(pl + s_c - R - (R & 1) + 2 * j);
+          xs[2 * j] = v.x;
+          xs[2 * j + 1] = v.y;
         }
-        if (yi + d < ny) {
-          const V2 v = *reinterpret_cast<const V2*>(pl + s_c + d * nx);
-          s0 += v.x;
-          s1 += v.y;
-        }
-        acc0 += cd * s0;
-        acc1 += cd * s1;
-      }
-      const T* pp = pring + (size_t)sp * 2 * TS;
-      if (has_pot) {
-        acc0 += pp[TS + loc] * xc0;
-        acc1 += pp[TS + loc + 1] * xc1;
-      }
-      T o0 = ca * acc0 + cb * xc0;
-      T o1 = ca * acc1 + cb * xc1;
-      if (Pc) {
-        o0 += cg * pp[loc];
-        o1 += cg * pp[loc + 1];
-      }
-      V2 o;
-      o.x = o0;
-      o.y = o1;
-      *reinterpret_cast<V2*>(Yc + (long)z * nxy + q) = o;
-    }
+        constexpr int OFF = R + (R & 1);  // xs index of the pair's first point
+        const T xc0 = zq0[(u + R) % Q], xc1 = zq1[(u + R) % Q];
+        T acc0 = c0 * xc0, acc1 = c0 * xc1;
 #pragma unroll
-    for (int i = 0; i < 2 * R; ++i) {
-      zq0[i] = zq0[i + 1];
-      zq1[i] = zq1[i + 1];
-    }
-    __syncthreads();  // slot of plane z and Prev slot sp are free
-    if (threadIdx.x == 0) {
-      const int pn = z + NBUF;
-      if (pn < zlast) issue_x(pn);
-      const int pp = z + PBUF;
-      if (pp < z1) issue_p(pp);
+        for (int d = 1; d <= R; ++d) {
+          // rows outside the plane are zero in the window, so y needs no test
+          const V2 ym = *reinterpret_cast<const V2*>(pl + s_c - d * nx);
+          const V2 yp = *reinterpret_cast<const V2*>(pl + s_c + d * nx);
+          const T cd = A.c[d - 1];
+          const T t0 = (ym.x + yp.x) + (zq0[(u + R - d) % Q] + zq0[(u + R + d) % Q]);
+          const T t1 = (ym.y + yp.y) + (zq1[(u + R - d) % Q] + zq1[(u + R + d) % Q]);
+          acc0 += cd * t0;
+          acc1 += cd * t1;
+          acc0 += cl0[d - 1] * xs[OFF - d];
+          acc0 += cr0[d - 1] * xs[OFF + d];
+          acc1 += cl1[d - 1] * xs[OFF + 1 - d];
+          acc1 += cr1[d - 1] * xs[OFF + 1 + d];
+        }
+        const T* pp = pring + (size_t)sp * 2 * TS;
+        if (has_pot) {
+          const V2 pv = *reinterpret_cast<const V2*>(pp + TS + loc);
+          acc0 += pv.x * xc0;
+          acc1 += pv.y * xc1;
+        }
+        T o0 = ca * acc0 + cb * xc0;
+        T o1 = ca * acc1 + cb * xc1;
+        if (Pc) {
+          const V2 pv = *reinterpret_cast<const V2*>(pp + loc);
+          o0 += cg * pv.x;
+          o1 += cg * pv.y;
+        }
+        V2 o;
+        o.x = o0;
+        o.y = o1;
+        *reinterpret_cast<V2*>(Yc + (long)z * nxy + q) = o;
+      }
+      __syncthreads();  // slot of plane z and Prev slot sp are free
+      if (threadIdx.x == 0) {
+        const int pn = z + NBUF;
+        if (pn < zlast) issue_x(pn);
+        const int pq = z + PBUF;
+        if (pq < z1) issue_p(pq);
+      }
     }
   }
   if (fail) s_fail = 1;

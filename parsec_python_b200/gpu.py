@@ -212,6 +212,12 @@ def rayleigh_ritz(ctx: GridContext, W: torch.Tensor, V: torch.Tensor, ritz: torc
     return V, W
 
 
+def subspace_rr(ctx: GridContext, W: torch.Tensor, V: torch.Tensor, ritz: torch.Tensor):
+    """Orthonormalise + Rayleigh-Ritz in one pass (psc_subspace_rr); result in V."""
+    ctx.call("psc_subspace_rr", _dtype_code(W), _p(W), _p(V), ctx.n, W.shape[0], _p(ritz), _stream())
+    return V, W
+
+
 def lanczos_bound(ctx: GridContext, mode: int) -> torch.Tensor:
     out = ctx.empty(8)
     ctx.call("psc_lanczos_bound", mode, ctx.next_seed(), _p(out), _stream())
@@ -236,8 +242,7 @@ def first_filt(nev: int, H: Hamiltonian, polm: int = 10, dtype=torch.float64, lo
     tr0 = None
     for it in range(1, max_iter + 1):
         W, T = cheb_filter(H, W, T, polm, bounds, mode=1)
-        W, T = orthonormalize(ctx, W, T)
-        W, T = rayleigh_ritz(ctx, W, T, ritz)
+        W, T = subspace_rr(ctx, W, T, ritz)
         ctx.call("psc_filter_bounds", 2, _p(ritz), nev, _p(lz[0:1]), _p(bounds), _stream())
         tr = float(np.sum(ritz.cpu().numpy()))
         if log_trace:
@@ -263,9 +268,8 @@ def chefsi1(W: torch.Tensor, ritzv: torch.Tensor, deg: int, nev: int, H: Hamilto
     ctx.call("psc_filter_bounds", 0, _p(ritzv), k, _p(lz[0:1]), _p(bounds), _stream())
     T = torch.empty_like(W)
     W, T = cheb_filter(H, W, T, deg, bounds, mode=0)
-    W, T = orthonormalize(ctx, W, T)
     ritz = ctx.empty(k)
-    W, T = rayleigh_ritz(ctx, W, T, ritz)
+    W, T = subspace_rr(ctx, W, T, ritz)
     return W, ritz
 
 

@@ -6,7 +6,8 @@ numpy's global seed 0, and writes tests/golden/ref_<name>.npz: the final
 energy components, eigenvalues, occupations, per-iteration total energies
 and the converged density (float32, electrons per bohr^3).
 
-Usage: python tests/golden/make_golden_configs.py NAME [reference src dir]
+Usage: python tests/golden/make_golden_configs.py NAME [reference src dir] [--tol T]
+With --tol the fixture is written as ref_<name>_tol<exponent>.npz/.json.
 """
 from __future__ import annotations
 
@@ -24,7 +25,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 
 
-def main(name: str, src: str) -> None:
+def main(name: str, src: str, tol: float | None = None) -> None:
     from parsec_python_b200 import workloads as w
 
     mpl = types.ModuleType("matplotlib")
@@ -49,7 +50,9 @@ def main(name: str, src: str) -> None:
     nx = 2 * ((nx + 1) // 2)
     dom = {"radius": 0.5 * h * (nx - 1), "nx": nx, "ny": nx, "nz": nx, "h": h}
     elem, n_el = rsdft_input.load_elements(Path(src))
-    settings = SolverSettings(tol=cfg["tol"], maxits=60, poldeg=cfg["poldeg"], fd_order=8)
+    tol = cfg["tol"] if tol is None else tol
+    tag = name if tol == cfg["tol"] else f"{name}_tol{int(round(-np.log10(tol)))}"
+    settings = SolverSettings(tol=tol, maxits=80, poldeg=cfg["poldeg"], fd_order=8)
     settings.normalize()
     tmp = Path(tempfile.mkdtemp())
     paths = RunPaths(output_file=str(tmp / "run.out"), wfn_file=str(tmp / "wfn.dat"),
@@ -66,16 +69,18 @@ def main(name: str, src: str) -> None:
     hist = [float(l.split("=")[2].split()[0]) for l in text.splitlines() if "Total electronic energy" in l]
     fin = rsdft_solver.compute_energy_components(res.rho, res.hpot, res.hpot0, res.xc_potential, res.exc,
                                                  res.eigenvalues, res.occupations, cfg["nev"], res.e_nuc0, h)
-    np.savez_compressed(HERE / f"ref_{name}.npz", rho=res.rho.astype(np.float32), eigenvalues=res.eigenvalues,
+    np.savez_compressed(HERE / f"ref_{tag}.npz", rho=res.rho.astype(np.float32), eigenvalues=res.eigenvalues,
                         occupations=res.occupations, total_ry=np.array(fin.total_ry),
                         eigen_sum_ry=np.array(fin.eigen_sum_ry), hartree_ry=np.array(fin.hartree_ry),
                         xc_ry=np.array(fin.xc_ry), ion_ry=np.array(fin.ion_ry), log_total_ry=np.array(hist[:-1]))
-    meta = {"name": name, "domain": dom, "nev": cfg["nev"], "poldeg": cfg["poldeg"], "tol": cfg["tol"], "seed": 0,
+    meta = {"name": name, "domain": dom, "nev": cfg["nev"], "poldeg": cfg["poldeg"], "tol": tol, "seed": 0,
             "iterations": res.iterations, "error": float(res.error), "converged": bool(res.converged),
             "wall_s": wall, "total_ry": fin.total_ry, "cpu": os.cpu_count()}
-    (HERE / f"ref_{name}.json").write_text(json.dumps(meta, indent=1))
+    (HERE / f"ref_{tag}.json").write_text(json.dumps(meta, indent=1))
     print(json.dumps(meta))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1], sys.argv[2] if len(sys.argv) > 2 else "/root/reference/src")
+    args = [a for a in sys.argv[1:] if not a.startswith("--tol")]
+    tols = [float(a.split("=", 1)[1]) for a in sys.argv[1:] if a.startswith("--tol=")]
+    main(args[0], args[1] if len(args) > 1 else "/root/reference/src", tols[0] if tols else None)

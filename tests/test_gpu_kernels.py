@@ -291,3 +291,35 @@ def test_pcg_graph_equals_direct_launches():
     xo, its = O.pcg(O.laplacian(dom, 8), rhs.cpu().numpy(), x0.cpu().numpy(), 200, 1e-5)
     assert abs(its - res[0][1]) <= 1
     assert rel(res[0][0].cpu().numpy(), xo) < 1e-8
+
+
+@pytest.mark.parametrize("k", [27, 55, 70])
+def test_subspace_rr_matches_qr_rayleigh_ritz(h2o_box, golden_dir, k):
+    """One-pass Rayleigh-Ritz of a filtered block vs the reference's route
+    (Householder QR, then G = Q^T H Q, eigh) done by the oracle on the same W."""
+    ctx, atoms, mi = h2o_box
+    gpu.projector_setup(ctx, atoms, ElementTable(), pseudo_tables())
+    pot = np.load(golden_dir / "ref_eigs.npz")["pot"]
+    H = gpu.Hamiltonian(ctx, torch.from_numpy(pot).to(DEV))
+    B = _csr_h(mi, pot)
+    rng = np.random.default_rng(11)
+    X = rng.random((ctx.n, k))
+    Xf = O.cheb_filter_slim(B, X, 10, 5.0, 60.0)          # an ill-conditioned filtered block
+    W = block(Xf)
+    V = torch.empty_like(W)
+    ritz = ctx.empty(k)
+    R, _ = gpu.subspace_rr(ctx, W, V, ritz)
+    import scipy.linalg
+    Q, _ = scipy.linalg.qr(Xf, mode="economic")
+    G = O._gram_upper(B @ Q, Q)
+    lam, Y = scipy.linalg.eigh(G)
+    got = ritz.cpu().numpy()
+    assert np.abs(got - lam).max() < 1e-10 * np.abs(lam).max()
+    Wr = host(R)
+    assert np.abs(Wr.T @ Wr - np.eye(k)).max() < 1e-9
+    # Ritz vectors of well-separated Ritz values agree up to sign
+    gap = np.minimum(np.diff(lam, prepend=-np.inf), np.diff(lam, append=np.inf))
+    good = gap > 1e-3 * np.abs(lam).max()
+    ref_vec = Q @ Y
+    dots = np.abs(np.sum(Wr[:, good] * ref_vec[:, good], axis=0))
+    assert np.all(dots > 1 - 1e-8)
