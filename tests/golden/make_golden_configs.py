@@ -67,12 +67,14 @@ def main(name: str, src: str, tol: float | None = None) -> None:
     wall = time.time() - t0
     text = (tmp / "run.out").read_text()
     hist = [float(l.split("=")[2].split()[0]) for l in text.splitlines() if "Total electronic energy" in l]
+    errs = [float(l.split("=")[1]) for l in text.splitlines() if "SCF error =" in l]
     fin = rsdft_solver.compute_energy_components(res.rho, res.hpot, res.hpot0, res.xc_potential, res.exc,
                                                  res.eigenvalues, res.occupations, cfg["nev"], res.e_nuc0, h)
     np.savez_compressed(HERE / f"ref_{tag}.npz", rho=res.rho.astype(np.float32), eigenvalues=res.eigenvalues,
                         occupations=res.occupations, total_ry=np.array(fin.total_ry),
                         eigen_sum_ry=np.array(fin.eigen_sum_ry), hartree_ry=np.array(fin.hartree_ry),
-                        xc_ry=np.array(fin.xc_ry), ion_ry=np.array(fin.ion_ry), log_total_ry=np.array(hist[:-1]))
+                        xc_ry=np.array(fin.xc_ry), ion_ry=np.array(fin.ion_ry), log_total_ry=np.array(hist[:-1]),
+                        log_err=np.array(errs))
     meta = {"name": name, "domain": dom, "nev": cfg["nev"], "poldeg": cfg["poldeg"], "tol": tol, "seed": 0,
             "iterations": res.iterations, "error": float(res.error), "converged": bool(res.converged),
             "wall_s": wall, "total_ry": fin.total_ry, "cpu": os.cpu_count()}

@@ -70,14 +70,18 @@ def test_scf_is_deterministic():
     assert torch.equal(a.rho, b.rho)
 
 
-@pytest.mark.parametrize("name", ["h2o", "c10h8"])
-def test_benchmark_config_matches_reference(golden_dir, name):
-    f = golden_dir / f"ref_{name}.npz"
+# H2O converges to the same fixed point at the configuration's tol 1e-6 (the
+# reference's own seed-to-seed spread there is ~1e-6 Ha).  For C10H8 the
+# reference's seed-to-seed spread at tol 1e-6 is 2.2e-5 Ha, above the bar, so
+# both sides are compared at tol 1e-8.
+@pytest.mark.parametrize("name,tag", [("h2o", "h2o"), ("c10h8", "c10h8_tol8")])
+def test_benchmark_config_matches_reference(golden_dir, name, tag):
+    f = golden_dir / f"ref_{tag}.npz"
     if not f.exists():
         pytest.skip(f"{f.name} not generated")
-    meta = json.loads((golden_dir / f"ref_{name}.json").read_text())
+    meta = json.loads((golden_dir / f"ref_{tag}.json").read_text())
     ref = np.load(f)
     cfg = workloads.config_system(name)
-    prob, res = run_gpu(cfg["atoms"], cfg["h"], cfg["radius"], cfg["nev"], cfg["poldeg"], cfg["tol"])
+    prob, res = run_gpu(cfg["atoms"], cfg["h"], cfg["radius"], cfg["nev"], cfg["poldeg"], meta["tol"], maxits=80)
     assert prob.domain["nx"] == meta["domain"]["nx"]
     check(prob, res, ref, cfg["nev"])
