@@ -143,6 +143,16 @@ int psc_set_use_graphs(psc_ctx* ctx, int on);
 /* LDA (Ceperley-Alder / Perdew-Zunger), V_xc/exc_nspn.py:8-103.
  * out_dev = [exc, max rho, min rho]. */
 int psc_lda_xc(psc_ctx* ctx, const double* rho, double* vxc, double h3, double* out_dev, void* stream);
+/* LDA exchange-correlation like psc_lda_xc, for callers that cannot allocate
+ * device memory (inside a CUDA stream capture, or under a host that owns all
+ * device memory through its own pool).  No counterpart in the reference: it
+ * exists for those callers.  Needs no context and allocates nothing: its
+ * per-CTA partials live in a fixed 96 KiB device array of the library.  rho,
+ * vxc: n device doubles, 1 <= n <= 33554432 (larger n is rejected with
+ * status 2); out_dev = [exc, max rho, min rho].  The first call on a device
+ * looks up that array's address and should come before any stream capture;
+ * concurrent calls share the array and race, so serialise them. */
+int psc_lda_xc_noalloc(const double* rho, double* vxc, long n, double h3, double* out_dev, void* stream);
 /* pot_new = ppot + 0.5 vxc + hpot + hpot0, f = pot_new - pot (may be NULL),
  * out_dev = [|f|^2, |pot_new|^2, sum rho(hpot+hpot0), sum rho vxc]
  * (rsdft_solver.py:351-352 and :141-146). */

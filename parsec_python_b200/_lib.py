@@ -50,6 +50,7 @@ _SIGS = {
     "psc_pcg_poisson": ([_P, _P, _P, c_int, c_double, POINTER(c_int), _P], c_int),
     "psc_set_use_graphs": ([_P, c_int], c_int),
     "psc_lda_xc": ([_P, _P, _P, c_double, _P, _P], c_int),
+    "psc_lda_xc_noalloc": ([_P, _P, c_long, c_double, _P, _P], c_int),
     "psc_scf_update": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], c_int),
     "psc_mixer_reset": ([_P, c_int], c_int),
     "psc_mixer_step": ([_P, _P, _P, c_double, c_double, _P, POINTER(c_int), _P], c_int),

@@ -1,0 +1,66 @@
+"""psc_lda_xc_noalloc: LDA XC for callers that cannot allocate device memory.
+
+Callers inside a CUDA stream capture (cudaMalloc cannot be captured) or under
+a host that gives all device memory to its own pool cannot create a libpsc
+context, because creating one allocates.  This entry point needs no context:
+its scratch is a fixed device array inside the library.  The test calls it
+through the C ABI twice in a row, on different densities, and compares each
+result with the context-based psc_lda_xc at the tolerance of the other XC
+test (1e-13 relative on v_xc, 1e-12 on E_xc).  The file name sorts last so
+that a run stopping at the first failure has already run every other test.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from parsec_python_b200 import _lib, gpu  # noqa: E402
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _densities(n, seed):
+    rng = np.random.default_rng(seed)
+    rho = 10 ** rng.uniform(-9, 1.5, n)          # both branches (rs < 1 and rs >= 1)
+    rho[:7] = 0.0                                # vacuum
+    rho[7:11] = -1e-4                            # negative density (skipped by the formula)
+    return rho
+
+
+def test_noalloc_xc_matches_context_xc_on_two_calls():
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    h3 = 0.37 ** 3
+    for seed, n in ((1, 300_001), (2, 40_000)):   # the second call is smaller: stale partials must not leak
+        rho = torch.from_numpy(_densities(n, seed)).to(dev)
+        vxc_a = torch.empty_like(rho)
+        out_a = torch.empty(3, dtype=torch.float64, device=dev)
+        rc = lib.psc_lda_xc_noalloc(_p(rho), _p(vxc_a), n, h3, _p(out_a), st)
+        assert rc == 0, lib.psc_last_error(None)
+        ctx = gpu.GridContext({"nx": n, "ny": 1, "nz": 1, "h": 0.37, "radius": 1.0}, 8)
+        vxc_b, out_b = gpu.lda_xc(ctx, rho)
+        torch.cuda.synchronize()
+        va, vb = vxc_a.cpu().numpy(), vxc_b.cpu().numpy()
+        assert np.abs(va - vb).max() <= 1e-13 * np.abs(vb).max()
+        oa, ob = out_a.cpu().numpy(), out_b.cpu().numpy()
+        assert abs(oa[0] - ob[0]) <= 1e-12 * abs(ob[0])
+        assert oa[1] == ob[1] and oa[2] == ob[2]
+
+
+def test_noalloc_xc_rejects_sizes_beyond_its_scratch():
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    x = torch.zeros(4, dtype=torch.float64, device=dev)
+    rc = lib.psc_lda_xc_noalloc(_p(x), _p(x), 33_554_433, 1.0, _p(x), None)
+    assert rc == 2
+    assert b"33554432" in lib.psc_last_error(None)
