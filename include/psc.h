@@ -137,9 +137,11 @@ int psc_density(psc_ctx* ctx, int dtype, const void* W, long ld, int nev, const 
 /* CG on A x = rhs, warm start in x (Eigensolvers/pcg.py:7-85, backend.pcg at
  * rsdft_solver.py:345). *its_out = iterations. */
 int psc_pcg_poisson(psc_ctx* ctx, const double* rhs, double* x, int maxit, double tol, int* its_out, void* stream);
-/* 1 (default): replay captured CUDA graphs for the CG iterations; 0: launch
- * each kernel from the host. */
-int psc_set_use_graphs(psc_ctx* ctx, int on);
+/* CG execution mode: 2 (default) one persistent cooperative launch keeping
+ * x, r, p, Ap in shared memory when they fit (else as 1); 1 the two CG
+ * kernels replayed from a captured CUDA graph; 0 the two kernels launched from
+ * the host.  All modes compute the same iterates. */
+int psc_set_use_graphs(psc_ctx* ctx, int mode);
 /* LDA (Ceperley-Alder / Perdew-Zunger), V_xc/exc_nspn.py:8-103.
  * out_dev = [exc, max rho, min rho]. */
 int psc_lda_xc(psc_ctx* ctx, const double* rho, double* vxc, double h3, double* out_dev, void* stream);

@@ -108,6 +108,10 @@ struct psc_ctx {
   double* cg_part = nullptr;     // [2][cg_part_cap] per-CTA partial sums
   int cg_part_cap = 0;
   double* cg_x = nullptr;        // solution buffer the captured CG graph works on
+  double* cg_p2 = nullptr;       // second direction buffer (the two alternate)
+  double* cg_ro = nullptr;       // r.r before each iteration
+  unsigned int* cg_bar = nullptr;  // grid-barrier arrival counter of the persistent CG
+  int cg_persistent = 1;         // 1: persistent cooperative CG when the vectors fit in shared memory
   cudaGraphExec_t cg_exec = nullptr;
   cudaStream_t cap_stream = nullptr;  // private stream used only for graph capture
   int use_graphs = 1;

@@ -16,7 +16,7 @@ torch = pytest.importorskip("torch")
 if not torch.cuda.is_available():  # pragma: no cover - collected on CPU runs
     pytest.skip("needs a CUDA device", allow_module_level=True)
 
-from parsec_python_b200 import gpu  # noqa: E402
+from parsec_python_b200 import _lib, gpu  # noqa: E402
 from parsec_python_b200._lib import F32, F64  # noqa: E402
 from parsec_python_b200.inputs import ElementTable, pseudo_tables  # noqa: E402
 
@@ -282,8 +282,8 @@ def test_pcg_graph_equals_direct_launches():
     x0 = torch.randn(ctx.n, dtype=torch.float64, device=DEV, generator=g) * 0.1
     A = gpu.Laplacian(ctx)
     res = []
-    for on in (1, 0):
-        ctx.call("psc_set_use_graphs", on)
+    for mode in (1, 0):
+        ctx.call("psc_set_use_graphs", mode)
         res.append(gpu.pcg(A, rhs, x0, 200, 1e-5))
     assert res[0][1] == res[1][1]
     assert torch.equal(res[0][0], res[1][0])
@@ -291,6 +291,47 @@ def test_pcg_graph_equals_direct_launches():
     xo, its = O.pcg(O.laplacian(dom, 8), rhs.cpu().numpy(), x0.cpu().numpy(), 200, 1e-5)
     assert abs(its - res[0][1]) <= 1
     assert rel(res[0][0].cpu().numpy(), xo) < 1e-8
+
+
+@pytest.mark.parametrize("shape,order,maxit", [((40, 40, 40), 8, 200), ((78, 78, 78), 8, 200),
+                                               ((21, 17, 13), 6, 200), ((16, 12, 20), 4, 7),
+                                               ((9, 11, 10), 2, 200)])
+def test_pcg_persistent_matches_graph_and_oracle(shape, order, maxit):
+    """The one-launch persistent CG against the graph-replayed kernels and the
+    oracle.  Partial sums are grouped differently, so iterates agree to
+    rounding, not bit for bit."""
+    nx, ny, nz = shape
+    dom = {"nx": nx, "ny": ny, "nz": nz, "h": 0.4, "radius": 0.2 * (nx - 1)}
+    ctx = gpu.GridContext(dom, order)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    rhs = torch.randn(ctx.n, dtype=torch.float64, device=DEV, generator=g)
+    x0 = torch.randn(ctx.n, dtype=torch.float64, device=DEV, generator=g) * 0.1
+    A = gpu.Laplacian(ctx)
+    res, launches = [], []
+    for mode in (2, 1):
+        ctx.call("psc_set_use_graphs", mode)
+        before = _lib.load().psc_launch_count()
+        res.append(gpu.pcg(A, rhs, x0, maxit, 1e-5))
+        launches.append(_lib.load().psc_launch_count() - before)
+    assert launches[0] == 1                      # the persistent kernel ran
+    assert abs(res[0][1] - res[1][1]) <= 1
+    assert rel(res[0][0].cpu().numpy(), res[1][0].cpu().numpy()) < 1e-9
+    xo, its = O.pcg(O.laplacian(dom, order), rhs.cpu().numpy(), x0.cpu().numpy(), maxit, 1e-5)
+    assert abs(its - res[0][1]) <= 1
+    assert rel(res[0][0].cpu().numpy(), xo) < 1e-8
+    assert int(ctx.status()[4]) == 0
+
+
+def test_pcg_persistent_falls_back_when_vectors_do_not_fit():
+    dom = {"nx": 132, "ny": 132, "nz": 132, "h": 0.4, "radius": 26.2}   # 4 x 2.3M doubles > shared memory
+    ctx = gpu.GridContext(dom, 8)
+    g = torch.Generator(device="cuda").manual_seed(6)
+    rhs = torch.randn(ctx.n, dtype=torch.float64, device=DEV, generator=g)
+    x0 = torch.zeros(ctx.n, dtype=torch.float64, device=DEV)
+    before = _lib.load().psc_launch_count()
+    x, its = gpu.pcg(gpu.Laplacian(ctx), rhs, x0, 12, 1e-5)
+    assert _lib.load().psc_launch_count() - before > 1
+    assert its == 12
 
 
 @pytest.mark.parametrize("k", [27, 55, 70])
