@@ -39,7 +39,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 CFG_NAME = "c10h8"
-METRIC = "SCF time-to-1e-5 Ha (C10H8, FP64 GPU SCF); H.X GB/s"
+METRIC = "SCF time-to-1e-5 Ha: mixed-prec+learned init vs plain FP64 GPU; H\u00b7X GB/s"
+HA_TOL = 1e-5          # energy bar, Hartree
 
 
 def workload_config(precision: str) -> dict:
@@ -159,11 +160,20 @@ def gpu_problem(precision: str, seed: int, name: str = CFG_NAME):
 
 
 def reference_energy(name: str = CFG_NAME):
-    f = ROOT / "tests" / "golden" / f"ref_{name}.json"
-    if f.exists():
-        m = json.loads(f.read_text())
-        return m["total_ry"], m["iterations"]
-    return None, None
+    """Converged total energy (Ry) of the reference CPU path run to tol 1e-8
+    (its tol-1e-6 energies scatter by 2e-5 Ha between random starts, more
+    than the bar), and the reference's iteration count at the config's tol."""
+    e_star, its = None, None
+    f8 = ROOT / "tests" / "golden" / f"ref_{name}_tol8.json"
+    f6 = ROOT / "tests" / "golden" / f"ref_{name}.json"
+    if f8.exists():
+        e_star = json.loads(f8.read_text())["total_ry"]
+    if f6.exists():
+        m = json.loads(f6.read_text())
+        its = m["iterations"]
+        if e_star is None:
+            e_star = m["total_ry"]
+    return e_star, its
 
 
 def solve_once(precision: str, seed: int):
@@ -347,7 +357,7 @@ def run_gpu_arm(args, rank, local, world):
         solve_once(prec, seed=100 + w)
     torch.cuda.synchronize()
     barrier(world)
-    times, energies, iters = [], [], []
+    times, energies, iters, setups = [], [], [], []
     launches0 = lib.psc_launch_count()
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
@@ -361,14 +371,20 @@ def run_gpu_arm(args, rank, local, world):
             times.append(e0.elapsed_time(e1) / 1000.0)
             energies.append(res.history[-1]["total_ry"])
             iters.append(res.iterations)
+            setups.append(res.timings.get("setup_total", 0.0))
         torch.cuda.synchronize()
         barrier(world)
     launches = (lib.psc_launch_count() - launches0) // max(1, args.steps)
     clocks = clk.summary()
+    if args.scf_only:
+        if rank == 0:
+            print(json.dumps({"scf_only": True, "step_times_s": times, "iterations": iters}), flush=True)
+        return
     t_step = allmax(float(np.mean(times)), world)
     roof = stencil_roofline()
     peak, peak_kind = measured_peak()
     err_ha = None if e_ref is None else max(abs(e - e_ref) for e in energies) / 2.0
+    within = None if err_ha is None else bool(err_ha <= HA_TOL)
     e2e_t = h2d = d2h = None
     if rank == 0:
         with tempfile.TemporaryDirectory() as td:
@@ -394,13 +410,14 @@ def run_gpu_arm(args, rank, local, world):
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": roof["gbs"], "peak": peak, "unit": "GB/s",
                          "frac": roof["gbs"] / peak, "traffic": stencil_traffic(),
-                         "kernel": "k_stencil<double,4,2> (one Chebyshev step, k=55)",
+                         "kernel": "k_stencil_tma<double,4> (one FP64 Chebyshev step, k=55, C10H8 grid)",
                          "peak_kind": peak_kind, "launch_s": roof["seconds"],
                          "algorithmic_bytes": roof["bytes"]},
             "hx_gbs": roof["gbs"], "hx_gflops": roof["gflops"],
             "cpu_baseline": cpu, "clocks": clocks,
             "iterations": int(np.median(iters)), "energy_error_ha_vs_reference": err_ha,
-            "reference_iterations": ref_its, "step_times_s": times}
+            "energy_within_1e-5_ha": within, "reference_energy_ry": e_ref,
+            "setup_s": float(np.mean(setups)), "reference_iterations": ref_its, "step_times_s": times}
     print(json.dumps(line), flush=True)
 
 
@@ -412,6 +429,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scf-only", action="store_true",
+                    help="run only the warm-up and timed SCF solves (for launch-list profiling)")
     args = ap.parse_args()
     rank, local, world = dist_init()
     try:
