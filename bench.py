@@ -24,6 +24,7 @@ replicas (the SCF of one molecule does not shard in this implementation).
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -176,13 +177,16 @@ def reference_energy(name: str = CFG_NAME):
     return e_star, its
 
 
-def solve_once(precision: str, seed: int):
+def solve_once(precision: str, seed: int, energy_target=None):
+    """One SCF; returns (result, backend) so that the caller releases the
+    device context (cudaFree) outside its timed region."""
     from parsec_python_b200.backend import select_solver_backend
     from parsec_python_b200.solver import run_rsdft_calculation
 
     prob, elem, s = gpu_problem(precision, seed)
     backend = select_solver_backend(s)
-    return run_rsdft_calculation(prob, elem, len(elem), backend, verbose=False)
+    res = run_rsdft_calculation(prob, elem, len(elem), backend, verbose=False, energy_target=energy_target)
+    return res, backend
 
 
 def stencil_roofline(reps: int = 40) -> dict:
@@ -234,12 +238,14 @@ def measured_peak() -> tuple[float, str]:
 
 
 def stencil_traffic():
-    f = ROOT / "profiles" / "stencil_traffic.json"
-    if f.exists():
-        try:
-            return json.loads(f.read_text()).get("dram_bytes_per_launch_c10h8")
-        except Exception:
-            return None
+    """ncu DRAM bytes (read + write) of one stencil launch of this workload."""
+    f = ROOT / "profiles" / "stencil_traffic.txt"
+    try:
+        for line in f.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch_c10h8"):
+                return int(line.split("=")[1])
+    except (OSError, ValueError):
+        pass
     return None
 
 
@@ -353,8 +359,11 @@ def run_gpu_arm(args, rank, local, world):
     lib = _lib.load()
     prec = args.precision
     e_ref, ref_its = reference_energy()
+    target = None if e_ref is None else (e_ref, 2.0 * HA_TOL)   # 1e-5 Ha = 2e-5 Ry
     for w in range(args.warmup):
-        solve_once(prec, seed=100 + w)
+        res, be = solve_once(prec, seed=100 + w, energy_target=target)
+        del res, be
+    gc.collect()
     torch.cuda.synchronize()
     barrier(world)
     times, energies, iters, setups = [], [], [], []
@@ -363,15 +372,18 @@ def run_gpu_arm(args, rank, local, world):
         torch.cuda.synchronize()
         barrier(world)
         for s in range(args.steps):
+            gc.collect()
+            torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            res = solve_once(prec, seed=1000 * rank + s)
+            res, be = solve_once(prec, seed=1000 * rank + s, energy_target=target)
             e1.record()
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1000.0)
             energies.append(res.history[-1]["total_ry"])
             iters.append(res.iterations)
             setups.append(res.timings.get("setup_total", 0.0))
+            del res, be
         torch.cuda.synchronize()
         barrier(world)
     launches = (lib.psc_launch_count() - launches0) // max(1, args.steps)
@@ -417,7 +429,8 @@ def run_gpu_arm(args, rank, local, world):
             "cpu_baseline": cpu, "clocks": clocks,
             "iterations": int(np.median(iters)), "energy_error_ha_vs_reference": err_ha,
             "energy_within_1e-5_ha": within, "reference_energy_ry": e_ref,
-            "setup_s": float(np.mean(setups)), "reference_iterations": ref_its, "step_times_s": times}
+            "setup_s": float(np.mean(setups)), "reference_iterations": ref_its, "step_times_s": times,
+            "step_iterations": iters}
     print(json.dumps(line), flush=True)
 
 

@@ -118,7 +118,7 @@ int psc_rayleigh_ritz(psc_ctx* ctx, int dtype, const void* W, void* V, long ld, 
  * Rayleigh-Ritz, chefsi1.py:43-67 / first_filt.py:43-63). */
 int psc_subspace_rr(psc_ctx* ctx, int dtype, const void* W, void* V, long ld, int k, double* ritz_dev, void* stream);
 /* Building blocks: G = A^T B (mode 0 plain, 1 upper mirrored, 2 symmetrised),
- * Out = W Q, symmetric eigensolver (ascending, FP64, one CTA, k <= 1023). */
+ * Out = W Q, symmetric eigensolver (ascending, FP64, one CTA, k <= 1022). */
 int psc_gram(psc_ctx* ctx, int dtype, const void* A, long lda, const void* B, long ldb, int k, int mode,
              double* out_dev, void* stream);
 int psc_gemm_nn(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Q, int kout, void* out,

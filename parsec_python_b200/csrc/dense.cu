@@ -93,7 +93,8 @@ int psc_ensure_dense(psc_ctx* ctx, int k) {
   cudaFree(ctx->jac_v);
   const int cap = std::max(k, 64);
   const size_t kk = (size_t)cap * cap;
-  PSC_CUDA(ctx, cudaMalloc(&ctx->jac_v, kk * sizeof(double)));
+  // Jacobi scratch: padded A and V of order <= cap + 1 when they do not fit on chip
+  PSC_CUDA(ctx, cudaMalloc(&ctx->jac_v, 2 * (size_t)(cap + 1) * (cap + 1) * sizeof(double)));
   PSC_CUDA(ctx, cudaMalloc(&ctx->gram, kk * sizeof(double)));
   PSC_CUDA(ctx, cudaMalloc(&ctx->gram2, kk * sizeof(double)));
   PSC_CUDA(ctx, cudaMalloc(&ctx->evec, kk * sizeof(double)));
@@ -197,95 +198,100 @@ __global__ void k_triu_inv(const double* __restrict__ R, int k, double* __restri
 }
 
 // ---------------------------------------------------------------------------
-// Cyclic Jacobi eigensolver, one CTA.  Round-robin pairing (circle method):
-// every round rotates k/2 disjoint (p,q) planes -- columns of A and V first,
-// then rows of A -- so each sweep annihilates every off-diagonal pair once.
-// The input is symmetrised first.  A pair is rotated only while
-// |a_pq| > 1e-17 (|a_pp| + |a_qq|); the solver has converged when a whole
-// sweep rotates nothing (at most 40 sweeps).  Eigenvalues ascending,
+// Cyclic Jacobi eigensolver, one CTA.  The matrix is padded to even order m
+// (a zero row/column when k is odd) and symmetrised.  Each round of a sweep
+// pairs the m indices into m/2 disjoint planes (circle method); the round is
+// two steps separated by one barrier each:
+//   1. every plane computes its rotation (Rutishauser's tangent form) or
+//      skips it while |a_pq| <= 1e-17 (|a_pp| + |a_qq|);
+//   2. the two-sided update A <- P^T A P is done as independent 2x2 blocks
+//      (rows of plane i, columns of plane j), with the rotated pair's own
+//      diagonal block set exactly (a_pq = 0, a_pp -= t a_pq, a_qq += t a_pq),
+//      together with V <- V P.
+// The solver has converged when a whole sweep rotates nothing (at most 60
+// sweeps; status word 2 is set otherwise).  Eigenvalues ascending,
 // eigenvectors permuted to match.
 // ---------------------------------------------------------------------------
 template <int NT>
 __global__ void __launch_bounds__(NT)
-k_jacobi(double* __restrict__ Ag, int k, double* __restrict__ evals, double* __restrict__ Vout, int use_smem,
-         double* __restrict__ Vg, int* status) {
+k_jacobi(const double* __restrict__ Ain, int k, double* __restrict__ evals, double* __restrict__ Vout,
+         int use_smem, double* __restrict__ scratch, int* status) {
   extern __shared__ double sm[];
   __shared__ int rp[512], rq[512];
-  __shared__ double rc[512], rs[512];
+  __shared__ double rc[512], rs[512], rt[512];
   __shared__ int nrot;
-  double* A = use_smem ? sm : Ag;
-  double* V = use_smem ? sm + (long)k * k : Vg;
-  const long kk = (long)k * k;
-  if (use_smem)
-    for (long e = threadIdx.x; e < kk; e += blockDim.x) A[e] = Ag[e];
-  for (long e = threadIdx.x; e < kk; e += blockDim.x) V[e] = ((e % k) == (e / k)) ? 1.0 : 0.0;
-  __syncthreads();
-  // symmetrise: callers may pass a matrix that is symmetric only to rounding
-  for (long e = threadIdx.x; e < kk; e += blockDim.x) {
-    const int i = (int)(e % k), j = (int)(e / k);
-    if (i < j) {
-      const double v = 0.5 * (A[i + (long)j * k] + A[j + (long)i * k]);
-      A[i + (long)j * k] = v;
-      A[j + (long)i * k] = v;
-    }
-  }
   const int m = k + (k & 1);
   const int half = m / 2;
+  const int mm = m * m;
+  double* A = use_smem ? sm : scratch;
+  double* V = A + mm;
+  for (int e = threadIdx.x; e < mm; e += NT) {
+    const int i = e % m, j = e / m;
+    double a = 0.0;
+    if (i < k && j < k) a = (i == j) ? Ain[i + j * k] : 0.5 * (Ain[i + j * k] + Ain[j + i * k]);
+    A[e] = a;
+    V[e] = (i == j) ? 1.0 : 0.0;
+  }
   __syncthreads();
-  for (int sweep = 0; sweep < 40 && k > 1; ++sweep) {
+  for (int sweep = 0; sweep < 60 && k > 1; ++sweep) {
     if (threadIdx.x == 0) nrot = 0;
     __syncthreads();
     for (int r = 0; r < m - 1; ++r) {
-      for (int i = threadIdx.x; i < half; i += blockDim.x) {
+      for (int i = threadIdx.x; i < half; i += NT) {
         const int a = (i == 0) ? 0 : ((i - 1 + r) % (m - 1)) + 1;
-        const int b = ((m - 1 - i - 1 + r) % (m - 1)) + 1;
+        const int b = ((m - 2 - i + r) % (m - 1)) + 1;
         const int p = min(a, b), q = max(a, b);
-        double c = 1.0, s = 0.0;
-        if (q < k) {
-          const double apq = A[p + (long)q * k];
-          const double app0 = A[p + (long)p * k], aqq0 = A[q + (long)q * k];
-          // rotate unless the pair is already diagonal to working precision
-          if (fabs(apq) > 1e-17 * (fabs(app0) + fabs(aqq0)) && apq != 0.0) {
-            atomicAdd(&nrot, 1);
-            const double app = A[p + (long)p * k], aqq = A[q + (long)q * k];
-            const double theta = (aqq - app) / (2.0 * apq);
-            double t;
-            if (fabs(theta) > 1e150) t = 0.5 / theta;
-            else t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-            c = 1.0 / sqrt(t * t + 1.0);
-            s = t * c;
-          }
+        double c = 1.0, s = 0.0, t = 0.0;
+        const double apq = A[p + q * m];
+        const double app = A[p + p * m], aqq = A[q + q * m];
+        if (apq != 0.0 && fabs(apq) > 1e-17 * (fabs(app) + fabs(aqq))) {
+          nrot = 1;   // benign: every writer stores the same value
+          const double theta = (aqq - app) / (2.0 * apq);
+          if (fabs(theta) > 1e150) t = 0.5 / theta;
+          else t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          c = 1.0 / sqrt(t * t + 1.0);
+          s = t * c;
         }
-        rp[i] = p; rq[i] = q; rc[i] = c; rs[i] = s;
+        rp[i] = p; rq[i] = q; rc[i] = c; rs[i] = s; rt[i] = t;
       }
       __syncthreads();
-      // columns: A <- A P, V <- V P
-      for (long e = threadIdx.x; e < (long)half * k; e += blockDim.x) {
-        const int i = (int)(e / k), row = (int)(e % k);
-        if (rq[i] >= k || rs[i] == 0.0) continue;
-        const int p = rp[i], q = rq[i];
-        const double c = rc[i], s = rs[i];
-        double* ap = A + (long)p * k;
-        double* aq = A + (long)q * k;
-        const double x = ap[row], y = aq[row];
-        ap[row] = c * x - s * y;
-        aq[row] = s * x + c * y;
-        double* vp = V + (long)p * k;
-        double* vq = V + (long)q * k;
-        const double vx = vp[row], vy = vq[row];
-        vp[row] = c * vx - s * vy;
-        vq[row] = s * vx + c * vy;
-      }
-      __syncthreads();
-      // rows: A <- P^T A
-      for (long e = threadIdx.x; e < (long)half * k; e += blockDim.x) {
-        const int i = (int)(e / k), col = (int)(e % k);
-        if (rq[i] >= k || rs[i] == 0.0) continue;
-        const int p = rp[i], q = rq[i];
-        const double c = rc[i], s = rs[i];
-        const double x = A[p + (long)col * k], y = A[q + (long)col * k];
-        A[p + (long)col * k] = c * x - s * y;
-        A[q + (long)col * k] = s * x + c * y;
+      const int nb = half * half;
+      for (int e = threadIdx.x; e < nb + half * m; e += NT) {
+        if (e < nb) {
+          const int i = e / half, j = e - i * half;
+          const double si = rs[i], sj = rs[j];
+          if (si == 0.0 && sj == 0.0) continue;
+          const int pi = rp[i], qi = rq[i], pj = rp[j], qj = rq[j];
+          if (i == j) {
+            const double apq = A[pi + qi * m], tt = rt[i];
+            A[pi + pi * m] -= tt * apq;
+            A[qi + qi * m] += tt * apq;
+            A[pi + qi * m] = 0.0;
+            A[qi + pi * m] = 0.0;
+            continue;
+          }
+          const double ci = rc[i], cj = rc[j];
+          double x00 = A[pi + pj * m], x01 = A[pi + qj * m], x10 = A[qi + pj * m], x11 = A[qi + qj * m];
+          // columns (plane j): [x.0 x.1] <- [c x.0 - s x.1, s x.0 + c x.1]
+          double y00 = cj * x00 - sj * x01, y01 = sj * x00 + cj * x01;
+          double y10 = cj * x10 - sj * x11, y11 = sj * x10 + cj * x11;
+          // rows (plane i)
+          A[pi + pj * m] = ci * y00 - si * y10;
+          A[qi + pj * m] = si * y00 + ci * y10;
+          A[pi + qj * m] = ci * y01 - si * y11;
+          A[qi + qj * m] = si * y01 + ci * y11;
+        } else {
+          const int f = e - nb;
+          const int j = f / m, row = f - j * m;
+          const double sj = rs[j];
+          if (sj == 0.0) continue;
+          const double cj = rc[j];
+          double* vp = V + rp[j] * m;
+          double* vq = V + rq[j] * m;
+          const double x = vp[row], y = vq[row];
+          vp[row] = cj * x - sj * y;
+          vq[row] = sj * x + cj * y;
+        }
       }
       __syncthreads();
     }
@@ -293,41 +299,39 @@ k_jacobi(double* __restrict__ Ag, int k, double* __restrict__ evals, double* __r
     const int rotated = nrot;
     __syncthreads();
     if (rotated == 0) break;
-    if (threadIdx.x == 0 && sweep == 39) status[2] = 1;  // did not converge
+    if (threadIdx.x == 0 && sweep == 59) status[2] = 1;  // did not converge
   }
   __syncthreads();
   // sort ascending (stable by index) and permute eigenvectors
-  for (int i = threadIdx.x; i < k; i += blockDim.x) {
-    const double li = A[i + (long)i * k];
+  for (int i = threadIdx.x; i < k; i += NT) {
+    const double li = A[i + i * m];
     int rank = 0;
     for (int j = 0; j < k; ++j) {
-      const double lj = A[j + (long)j * k];
+      const double lj = A[j + j * m];
       rank += (lj < li) || (lj == li && j < i);
     }
     evals[rank] = li;
-    for (int r = 0; r < k; ++r) Vout[r + (long)rank * k] = V[r + (long)i * k];
+    for (int r = 0; r < k; ++r) Vout[r + rank * k] = V[r + i * m];
   }
 }
 
 int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, cudaStream_t st) {
-  PSC_REQUIRE(ctx, k >= 1 && k <= 1023, "syev: k out of range");
+  PSC_REQUIRE(ctx, k >= 1 && k <= 1022, "syev: k out of range");
   if (psc_ensure_dense(ctx, k)) return 1;
-  const size_t smem = 2 * (size_t)k * k * sizeof(double);
+  const int m = k + (k & 1);
+  const size_t smem = 2 * (size_t)m * m * sizeof(double);
   const int use_smem = smem <= 200 * 1024;
-  // V scratch in global memory when the matrices do not fit on chip
-  double* vg = use_smem ? nullptr : ctx->jac_v;
   const size_t dyn = use_smem ? smem : 0;
-  // CTA size matched to the k/2 x k element updates of a rotation round; the
-  // opt-in limit covers dynamic + static shared memory (~12.5 KB static)
+  // CTA size matched to the (m/2)^2 blocks + (m/2) m rows of a rotation round
 #define PSC_JACOBI(NTH)                                                                                   \
   {                                                                                                       \
     if (use_smem)                                                                                         \
       PSC_CUDA(ctx, cudaFuncSetAttribute(k_jacobi<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    k_jacobi<NTH><<<1, NTH, dyn, st>>>(A, k, evals, evecs, use_smem, vg, ctx->dev_status);               \
+    k_jacobi<NTH><<<1, NTH, dyn, st>>>(A, k, evals, evecs, use_smem, ctx->jac_v, ctx->dev_status);       \
   }
-  const long work = (long)((k + 1) / 2) * k;
-  if (work <= 2048) PSC_JACOBI(256)
-  else if (work <= 8192) PSC_JACOBI(512)
+  const long work = (long)(m / 2) * (m / 2) + (long)(m / 2) * m;
+  if (work <= 4096) PSC_JACOBI(256)
+  else if (work <= 16384) PSC_JACOBI(512)
   else PSC_JACOBI(1024)
 #undef PSC_JACOBI
   PSC_LAUNCH_CHECK(ctx);

@@ -45,13 +45,18 @@ class _Events:
 
 
 def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: SolverBackend, *,
-                          init_density=None, verbose: bool = True, on_iteration=None) -> SCFResult:
+                          init_density=None, verbose: bool = True, on_iteration=None,
+                          energy_target: tuple[float, float] | None = None) -> SCFResult:
     """Run one SCF to convergence (or maxits).
 
     init_density: optional callable (ctx, rho0, hpot0, ppot, A) -> (rho1, hpot1)
     replacing the SAD starting density and its Hartree potential (the
     contract of V_ion/pseudoDiag_ML4Den_poisson.py); None keeps SAD.
     on_iteration: optional callable(dict) receiving each iteration's record.
+    energy_target: optional (E_ry, tol_ry); the loop then also requires
+    |E_total - E_ry| <= tol_ry before it stops (a time-to-accuracy
+    measurement: the reference's stop test err <= tol alone can stop at an
+    energy that is off by more than the bar).
     """
     say = print if verbose else (lambda *a, **k: None)
     rt = backend.runtime
@@ -134,7 +139,14 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
     exc = float(xc0[0].item())
     host = torch.empty(2 * k + 8, dtype=torch.float64, pin_memory=True)
     t_loop = time.perf_counter()
-    while err > s.tol and its < s.maxits:
+    def _done() -> bool:
+        if err > s.tol:
+            return False
+        if energy_target is None:
+            return True
+        return energies is not None and abs(energies.total_ry - energy_target[0]) <= energy_target[1]
+
+    while not _done() and its < s.maxits:
         its += 1
         say(f"  Working ... SCF iter # {its} ... ")
         ev = _Events()
