@@ -42,8 +42,10 @@ int psc_ctx_create(int nx, int ny, int nz, double h, int fd_order, psc_ctx** out
 int psc_ctx_destroy(psc_ctx* ctx);
 /* out[8] = nx, ny, nz, n, projector atoms, projector points, touched points, stencil radius */
 int psc_ctx_info(const psc_ctx* ctx, long* out);
-/* host flags[8] of device-side checks (1: filter bounds inverted, 2: Cholesky
- * pivot <= 0 at column flags[1]-1, 3: Jacobi not converged); clear != 0 resets */
+/* host flags[8] of device-side checks: [0] filter bounds inverted, [1]
+ * Cholesky pivot <= 0 at column flags[1]-1, [2] Jacobi not converged, [3] TMA
+ * stencil wait timed out, [4] persistent CG grid barrier timed out; [6] is
+ * informational: Jacobi sweeps of the last eigensolve.  clear != 0 resets */
 int psc_status(psc_ctx* ctx, int* host_flags, int clear, void* stream);
 
 /* ---- ionic setup ------------------------------------------------------ */

@@ -94,7 +94,7 @@ int psc_ensure_dense(psc_ctx* ctx, int k) {
   const int cap = std::max(k, 64);
   const size_t kk = (size_t)cap * cap;
   // Jacobi scratch: padded A and V of order <= cap + 1 when they do not fit on chip
-  PSC_CUDA(ctx, cudaMalloc(&ctx->jac_v, 2 * (size_t)(cap + 1) * (cap + 1) * sizeof(double)));
+  PSC_CUDA(ctx, cudaMalloc(&ctx->jac_v, 2 * (size_t)(cap + 2) * (cap + 2) * sizeof(double)));
   PSC_CUDA(ctx, cudaMalloc(&ctx->gram, kk * sizeof(double)));
   PSC_CUDA(ctx, cudaMalloc(&ctx->gram2, kk * sizeof(double)));
   PSC_CUDA(ctx, cudaMalloc(&ctx->evec, kk * sizeof(double)));
@@ -202,12 +202,14 @@ __global__ void k_triu_inv(const double* __restrict__ R, int k, double* __restri
 // (a zero row/column when k is odd) and symmetrised.  Each round of a sweep
 // pairs the m indices into m/2 disjoint planes (circle method); the round is
 // two steps separated by one barrier each:
-//   1. every plane computes its rotation (Rutishauser's tangent form) or
-//      skips it while |a_pq| <= 1e-17 (|a_pp| + |a_qq|);
-//   2. the two-sided update A <- P^T A P is done as independent 2x2 blocks
-//      (rows of plane i, columns of plane j), with the rotated pair's own
-//      diagonal block set exactly (a_pq = 0, a_pp -= t a_pq, a_qq += t a_pq),
-//      together with V <- V P.
+//   1. every plane computes its rotation or skips it while
+//      |a_pq| <= 1e-17 (|a_pp| + |a_qq|).  The angle comes from FP32
+//      arithmetic (short latency); c and s are normalised in FP64, so every
+//      rotation is orthogonal to FP64 rounding and the a_pq it leaves
+//      (~1e-7 of the old one) is annihilated by later sweeps;
+//   2. the two-sided update A <- P^T A P as independent 2x2 blocks (rows of
+//      plane i, columns of plane j) on a 32-wide thread grid, together with
+//      V <- V P.
 // The solver has converged when a whole sweep rotates nothing (at most 60
 // sweeps; status word 2 is set otherwise).  Eigenvalues ascending,
 // eigenvectors permuted to match.
@@ -218,22 +220,25 @@ k_jacobi(const double* __restrict__ Ain, int k, double* __restrict__ evals, doub
          int use_smem, double* __restrict__ scratch, int* status) {
   extern __shared__ double sm[];
   __shared__ int rp[512], rq[512];
-  __shared__ double rc[512], rs[512], rt[512];
+  __shared__ double rc[512], rs[512];
+  __shared__ int rank_of[1024];
   __shared__ int nrot;
   const int m = k + (k & 1);
   const int half = m / 2;
-  const int mm = m * m;
+  const int ld = m + 1;   // odd leading dimension: a warp's strided accesses spread over the banks
   double* A = use_smem ? sm : scratch;
-  double* V = A + mm;
-  for (int e = threadIdx.x; e < mm; e += NT) {
+  double* V = A + m * ld;
+  for (int e = threadIdx.x; e < m * m; e += NT) {
     const int i = e % m, j = e / m;
     double a = 0.0;
     if (i < k && j < k) a = (i == j) ? Ain[i + j * k] : 0.5 * (Ain[i + j * k] + Ain[j + i * k]);
-    A[e] = a;
-    V[e] = (i == j) ? 1.0 : 0.0;
+    A[i + j * ld] = a;
+    V[i + j * ld] = (i == j) ? 1.0 : 0.0;
   }
   __syncthreads();
+  int sweeps_done = 0;
   for (int sweep = 0; sweep < 60 && k > 1; ++sweep) {
+    sweeps_done = sweep + 1;
     if (threadIdx.x == 0) nrot = 0;
     __syncthreads();
     for (int r = 0; r < m - 1; ++r) {
@@ -241,56 +246,79 @@ k_jacobi(const double* __restrict__ Ain, int k, double* __restrict__ evals, doub
         const int a = (i == 0) ? 0 : ((i - 1 + r) % (m - 1)) + 1;
         const int b = ((m - 2 - i + r) % (m - 1)) + 1;
         const int p = min(a, b), q = max(a, b);
-        double c = 1.0, s = 0.0, t = 0.0;
-        const double apq = A[p + q * m];
-        const double app = A[p + p * m], aqq = A[q + q * m];
+        double c = 1.0, s = 0.0;
+        const double apq = A[p + q * ld];
+        const double app = A[p + p * ld], aqq = A[q + q * ld];
         if (apq != 0.0 && fabs(apq) > 1e-17 * (fabs(app) + fabs(aqq))) {
           nrot = 1;   // benign: every writer stores the same value
+          s = 1.0;
           const double theta = (aqq - app) / (2.0 * apq);
-          if (fabs(theta) > 1e150) t = 0.5 / theta;
-          else t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-          c = 1.0 / sqrt(t * t + 1.0);
-          s = t * c;
+          double t;
+          if (fabs(theta) > 1e18) {
+            t = 0.5 / theta;
+          } else {
+            // tan of the annihilating angle to FP32 accuracy (Rutishauser's
+            // form); the rotation stays exactly orthogonal below, and the
+            // remainder of a_pq is removed by later sweeps
+            const float th = (float)theta;
+            t = (double)(copysignf(1.0f, th) / (fabsf(th) + sqrtf(fmaf(th, th, 1.0f))));
+          }
+          // c = 1/sqrt(1+t^2) in FP64: FP32 estimate plus two Newton-Raphson
+          // steps y <- y (3 - x y^2) / 2
+          const double x = fma(t, t, 1.0);
+          double y = (double)rsqrtf((float)x);
+          y = y * (1.5 - 0.5 * x * y * y);
+          y = y * (1.5 - 0.5 * x * y * y);
+          c = y;
+          s = t * y;
         }
-        rp[i] = p; rq[i] = q; rc[i] = c; rs[i] = s; rt[i] = t;
+        rp[i] = p; rq[i] = q; rc[i] = c; rs[i] = s;
       }
       __syncthreads();
-      const int nb = half * half;
-      for (int e = threadIdx.x; e < nb + half * m; e += NT) {
-        if (e < nb) {
-          const int i = e / half, j = e - i * half;
-          const double si = rs[i], sj = rs[j];
-          if (si == 0.0 && sj == 0.0) continue;
-          const int pi = rp[i], qi = rq[i], pj = rp[j], qj = rq[j];
-          if (i == j) {
-            const double apq = A[pi + qi * m], tt = rt[i];
-            A[pi + pi * m] -= tt * apq;
-            A[qi + qi * m] += tt * apq;
-            A[pi + qi * m] = 0.0;
-            A[qi + pi * m] = 0.0;
-            continue;
+      // 2x2 blocks (i, j) on a 32-wide thread grid, then the V columns
+      {
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+        for (int i = ty; i < half; i += NT / 32) {
+          const double si = rs[i];
+          const int pi = rp[i], qi = rq[i];
+          const double ci = rc[i];
+          for (int j = tx; j < half; j += 32) {
+            const double sj = rs[j];
+            if (si == 0.0 && sj == 0.0) continue;
+            const int pj = rp[j], qj = rq[j];
+            const double cj = rc[j];
+            const double x00 = A[pi + pj * ld], x01 = A[pi + qj * ld], x10 = A[qi + pj * ld], x11 = A[qi + qj * ld];
+            // columns (plane j): [x.0 x.1] <- [c x.0 - s x.1, s x.0 + c x.1]
+            const double y00 = cj * x00 - sj * x01, y01 = sj * x00 + cj * x01;
+            const double y10 = cj * x10 - sj * x11, y11 = sj * x10 + cj * x11;
+            // rows (plane i); the rotated pair's own block is kept exactly symmetric
+            const double z00 = ci * y00 - si * y10, z10 = si * y00 + ci * y10;
+            const double z01 = ci * y01 - si * y11, z11 = si * y01 + ci * y11;
+            if (i == j) {
+              const double off = 0.5 * (z01 + z10);
+              A[pi + pj * ld] = z00;
+              A[qi + qj * ld] = z11;
+              A[qi + pj * ld] = off;
+              A[pi + qj * ld] = off;
+            } else {
+              A[pi + pj * ld] = z00;
+              A[qi + pj * ld] = z10;
+              A[pi + qj * ld] = z01;
+              A[qi + qj * ld] = z11;
+            }
           }
-          const double ci = rc[i], cj = rc[j];
-          double x00 = A[pi + pj * m], x01 = A[pi + qj * m], x10 = A[qi + pj * m], x11 = A[qi + qj * m];
-          // columns (plane j): [x.0 x.1] <- [c x.0 - s x.1, s x.0 + c x.1]
-          double y00 = cj * x00 - sj * x01, y01 = sj * x00 + cj * x01;
-          double y10 = cj * x10 - sj * x11, y11 = sj * x10 + cj * x11;
-          // rows (plane i)
-          A[pi + pj * m] = ci * y00 - si * y10;
-          A[qi + pj * m] = si * y00 + ci * y10;
-          A[pi + qj * m] = ci * y01 - si * y11;
-          A[qi + qj * m] = si * y01 + ci * y11;
-        } else {
-          const int f = e - nb;
-          const int j = f / m, row = f - j * m;
+        }
+        for (int j = ty; j < half; j += NT / 32) {
           const double sj = rs[j];
           if (sj == 0.0) continue;
           const double cj = rc[j];
-          double* vp = V + rp[j] * m;
-          double* vq = V + rq[j] * m;
-          const double x = vp[row], y = vq[row];
-          vp[row] = cj * x - sj * y;
-          vq[row] = sj * x + cj * y;
+          double* vp = V + rp[j] * ld;
+          double* vq = V + rq[j] * ld;
+          for (int row = tx; row < m; row += 32) {
+            const double x = vp[row], y = vq[row];
+            vp[row] = cj * x - sj * y;
+            vq[row] = sj * x + cj * y;
+          }
         }
       }
       __syncthreads();
@@ -301,17 +329,24 @@ k_jacobi(const double* __restrict__ Ain, int k, double* __restrict__ evals, doub
     if (rotated == 0) break;
     if (threadIdx.x == 0 && sweep == 59) status[2] = 1;  // did not converge
   }
+  if (threadIdx.x == 0) status[6] = sweeps_done;   // diagnostic: sweeps of the last solve
   __syncthreads();
-  // sort ascending (stable by index) and permute eigenvectors
+  // sort ascending (stable by index), then permute the eigenvectors with
+  // coalesced stores
   for (int i = threadIdx.x; i < k; i += NT) {
-    const double li = A[i + i * m];
+    const double li = A[i + i * ld];
     int rank = 0;
     for (int j = 0; j < k; ++j) {
-      const double lj = A[j + j * m];
+      const double lj = A[j + j * ld];
       rank += (lj < li) || (lj == li && j < i);
     }
     evals[rank] = li;
-    for (int r = 0; r < k; ++r) Vout[r + rank * k] = V[r + i * m];
+    rank_of[rank] = i;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < k * k; e += NT) {
+    const int col = e / k, r = e - col * k;
+    Vout[e] = V[r + rank_of[col] * ld];
   }
 }
 
@@ -319,7 +354,7 @@ int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, 
   PSC_REQUIRE(ctx, k >= 1 && k <= 1022, "syev: k out of range");
   if (psc_ensure_dense(ctx, k)) return 1;
   const int m = k + (k & 1);
-  const size_t smem = 2 * (size_t)m * m * sizeof(double);
+  const size_t smem = 2 * (size_t)m * (m + 1) * sizeof(double);
   const int use_smem = smem <= 200 * 1024;
   const size_t dyn = use_smem ? smem : 0;
   // CTA size matched to the (m/2)^2 blocks + (m/2) m rows of a rotation round
@@ -329,9 +364,10 @@ int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, 
       PSC_CUDA(ctx, cudaFuncSetAttribute(k_jacobi<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
     k_jacobi<NTH><<<1, NTH, dyn, st>>>(A, k, evals, evecs, use_smem, ctx->jac_v, ctx->dev_status);       \
   }
-  const long work = (long)(m / 2) * (m / 2) + (long)(m / 2) * m;
-  if (work <= 4096) PSC_JACOBI(256)
-  else if (work <= 16384) PSC_JACOBI(512)
+  // 32 x (NT/32) thread grid over the (m/2)^2 blocks of a rotation round
+  const int half = m / 2;
+  if (half <= 8) PSC_JACOBI(256)
+  else if (half <= 16) PSC_JACOBI(512)
   else PSC_JACOBI(1024)
 #undef PSC_JACOBI
   PSC_LAUNCH_CHECK(ctx);

@@ -193,6 +193,38 @@ def test_dense_building_blocks():
         assert rel(host(out), W @ Qm) < 1e-13
 
 
+@pytest.mark.parametrize("k,kind", [(1, "rand"), (2, "rand"), (7, "rand"), (55, "diag"), (56, "degenerate"),
+                                    (111, "rand"), (143, "neardiag")])
+def test_syev_edge_cases(k, kind):
+    """Jacobi eigensolver: odd/even orders (padding), the shared-memory /
+    global-memory switch (k = 111 no longer fits on chip), an input that is
+    already diagonal, repeated eigenvalues, a nearly diagonal RR matrix."""
+    ctx = gpu.GridContext({"nx": 8, "ny": 8, "nz": 8, "h": 0.5, "radius": 1.75}, 8)
+    rng = np.random.default_rng(k)
+    if kind == "rand":
+        S = rng.standard_normal((k, k))
+        S = S + S.T
+    elif kind == "diag":
+        S = np.diag(rng.standard_normal(k))
+    elif kind == "degenerate":
+        Q, _ = np.linalg.qr(rng.standard_normal((k, k)))
+        S = (Q * np.repeat([1.0, 2.0, -3.0, 2.0], k // 4)) @ Q.T
+    else:
+        S = np.diag(np.sort(rng.standard_normal(k))) + 1e-4 * rng.standard_normal((k, k))
+        S = 0.5 * (S + S.T)
+    A = torch.from_numpy(np.asfortranarray(S).ravel(order="F").copy()).to(DEV)
+    ev, vec = ctx.empty(k), ctx.empty(k * k)
+    ctx.call("psc_syev", gpu._p(A), k, gpu._p(ev), gpu._p(vec), gpu._stream())
+    assert ctx.status()[2] == 0
+    lam = ev.cpu().numpy()
+    Q = vec.cpu().numpy().reshape(k, k).T
+    ref = np.linalg.eigvalsh(S)
+    scale = max(1.0, np.abs(ref).max())
+    assert np.abs(lam - ref).max() < 1e-12 * scale
+    assert np.abs(S @ Q - Q * lam).max() < 1e-11 * scale
+    assert np.abs(Q.T @ Q - np.eye(k)).max() < 1e-12
+
+
 def test_occupations_match_reference(golden_dir):
     oc = np.load(golden_dir / "ref_occupations.npz")
     ctx = gpu.GridContext({"nx": 8, "ny": 8, "nz": 8, "h": 0.5, "radius": 1.75}, 8)
