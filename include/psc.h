@@ -181,6 +181,51 @@ int psc_axpby(psc_ctx* ctx, const double* x, const double* y, double a, double b
 /* Deterministic dot product, result on the device. */
 int psc_dot(psc_ctx* ctx, const double* a, const double* b, long n, double* out_dev, void* stream);
 
+/* Gram pairs of FP32 blocks (mixed precision) on tcgen05 tensor cores with
+ * split-precision TF32 (1, default) or on CUDA cores with FP64 accumulation
+ * (0).  No counterpart in the reference (its GPU path is cuBLAS FP32). */
+int psc_set_gram_impl(psc_ctx* ctx, int tensor_cores);
+/* S = W^T W and K = W^T V for n x k blocks (leading dimension ld), k x k
+ * column-major FP64 results on the device (the Gram and projected-Hamiltonian
+ * products of Rayleighritz.py:4-30). */
+int psc_gram_pair(psc_ctx* ctx, int dtype, const void* W, const void* V, long ld, int k, double* S, double* K,
+                  void* stream);
+
+/* ---- learned initial density (3-D conv encoder-decoder) ------------------
+ * No counterpart in the reference: it only consumes a predicted density
+ * (V_ion/pseudoDiag_ML4Den_poisson.py:12-586, dispatched at
+ * rsdft_solver.py:95-108).  Activations are channels-last BF16 [voxel][C]
+ * (x fastest), C a multiple of 8; weights BF16 [tap][Cin][Cout] with
+ * tap = dx + 3 (dy + 3 dz); biases and all gradients FP32; accumulation FP32.
+ * geom[15] = {nxi, nyi, nzi, nxa, nya, nza, up, Ca, Cs, nxo, nyo, nzo,
+ * stride, ksize, Cout}: the input is Ca channels of A (nearest-upsampled x2
+ * when up = 1, A's grid is then the input grid halved, rounded up) followed by
+ * Cs channels of the skip tensor S on the input grid; stride 1 or 2 (output
+ * grid ceil(n / stride)), ksize 3 (padding 1) or 1. */
+int psc_conv3d_fwd(psc_ctx* ctx, const int* geom, const void* A, const void* S, const void* W, const float* bias,
+                   int relu, void* out, float* out32, void* stream);
+/* Backward of one convolution.  gout: dL/d(out) FP32 [nvo][Cout]; out: the
+ * forward's BF16 output when the layer has a ReLU (NULL for a linear layer);
+ * gm: FP32 scratch [nvo][Cout] (may alias gout); dvin: FP32 scratch
+ * [nvi][Ca+Cs] or NULL to skip the input gradient; dA / dS: FP32 gradients of
+ * A and S, overwritten (acc = 0) or accumulated (acc = 1), NULL to skip; dW,
+ * dB: FP32 weight and bias gradients (overwritten); work: FP32 scratch of
+ * work_floats (>= chunks x 27 Cin Cout). */
+int psc_conv3d_bwd(psc_ctx* ctx, const int* geom, const void* A, const void* S, const void* W, const float* gout,
+                   const void* out, float* gm, float* dvin, float* dA, int acc_a, float* dS, int acc_s, float* dW,
+                   float* dB, float* work, long work_floats, void* stream);
+/* Mean squared error on channel 0 of y [n][C] against target [n]; grad [n][C]
+ * = d loss / d y; loss_dev = one double on the device. */
+int psc_mse_loss(psc_ctx* ctx, const float* y, int C, const float* target, long n, float* grad, double* loss_dev,
+                 void* stream);
+/* Adam step on FP32 master weights w (n), refreshing the BF16 copy wb (may be
+ * NULL); step counts from 1. */
+int psc_adam_step(psc_ctx* ctx, float* w, void* wb, const float* grad, float* m, float* v, long n, float lr,
+                  float b1, float b2, float eps, int step, void* stream);
+int psc_f32_to_bf16(psc_ctx* ctx, const float* x, void* y, long n, void* stream);
+/* Network input on the context's grid: BF16 [n][8], ch0 = a0 x0, ch1 = a1 x1, rest 0. */
+int psc_pack_input(psc_ctx* ctx, const double* x0, const double* x1, double a0, double a1, void* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

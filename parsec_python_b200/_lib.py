@@ -51,6 +51,15 @@ _SIGS = {
     "psc_set_use_graphs": ([_P, c_int], c_int),
     "psc_lda_xc": ([_P, _P, _P, c_double, _P, _P], c_int),
     "psc_lda_xc_noalloc": ([_P, _P, c_long, c_double, _P, _P], c_int),
+    "psc_set_gram_impl": ([_P, c_int], c_int),
+    "psc_gram_pair": ([_P, c_int, _P, _P, c_long, c_int, _P, _P, _P], c_int),
+    "psc_conv3d_fwd": ([_P, _P, _P, _P, _P, _P, c_int, _P, _P, _P], c_int),
+    "psc_conv3d_bwd": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, c_int, _P, c_int, _P, _P, _P, c_long, _P], c_int),
+    "psc_mse_loss": ([_P, _P, c_int, _P, c_long, _P, _P, _P], c_int),
+    "psc_adam_step": ([_P, _P, _P, _P, _P, _P, c_long, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                       ctypes.c_float, c_int, _P], c_int),
+    "psc_f32_to_bf16": ([_P, _P, _P, c_long, _P], c_int),
+    "psc_pack_input": ([_P, _P, _P, c_double, c_double, _P, _P], c_int),
     "psc_scf_update": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], c_int),
     "psc_mixer_reset": ([_P, c_int], c_int),
     "psc_mixer_step": ([_P, _P, _P, c_double, c_double, _P, POINTER(c_int), _P], c_int),

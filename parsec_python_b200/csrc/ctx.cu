@@ -111,6 +111,7 @@ extern "C" int psc_ctx_destroy(psc_ctx* ctx) {
   cudaFree(ctx->cg_ap); cudaFree(ctx->cg_part); cudaFree(ctx->mix_dx); cudaFree(ctx->mix_df);
   cudaFree(ctx->mix_nv); cudaFree(ctx->mix_tmp); cudaFree(ctx->mix_coef); cudaFree(ctx->mix_partial);
   cudaFree(ctx->cg_x); cudaFree(ctx->jac_v); cudaFree(ctx->cg_p2); cudaFree(ctx->cg_ro); cudaFree(ctx->cg_bar);
+  cudaFree(ctx->tc_part); cudaFree(ctx->tc_pairs);
   if (ctx->cg_exec) cudaGraphExecDestroy(ctx->cg_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   delete ctx;

@@ -1,0 +1,311 @@
+// Tensor-core Gram pair for the mixed-precision subspace step:
+// S = W^T W and K = W^T V (V = H W) from FP32 blocks, on tcgen05 with TF32
+// operands and FP32 accumulation in tensor memory, with the three-term
+// split-precision correction x = hi + lo (hi = tf32(x), lo = tf32(x - hi)):
+//   W^T V ~ hi(W)^T hi(V) + hi(W)^T lo(V) + lo(W)^T hi(V),
+// which keeps FP32-level accuracy (the dropped lo*lo term is ~2^-22).
+// Replaces the dense products of Rayleighritz.py:4-30 / chefsi1.py:43-67 in
+// the mixed-precision path; the FP64 path keeps the CUDA-core kernels.
+//
+// Grid: (chunk of the n rows) x (pair of 128-column tiles, upper triangle).
+// Each CTA streams its rows through a two-deep shared-memory ring, 32 rows
+// (one 128-byte swizzle row of FP32) per stage; its threads load and split
+// the tiles into hi/lo copies in the canonical K-major 128-byte-swizzled
+// layout, one elected thread issues the MMAs (M = 128, N = tile width,
+// K = 8 per instruction) and commits them to an mbarrier.  Partial FP32
+// tiles go to global memory and are summed over the chunks in FP64.
+// Every wait is bounded; on a timeout the kernel records status word 5.
+#include "psc_internal.cuh"
+#include "../../include/psc.h"
+
+#include <algorithm>
+
+namespace {
+constexpr int TC_NT = 128;
+constexpr int TROWS = 128;               // tile rows (matrix columns), = MMA M
+constexpr int KSTAGE = 32;               // reduction rows per stage (128 bytes of FP32)
+constexpr int TILE_BYTES = TROWS * 128;  // 16 KB
+constexpr int NTILES = 6;                // A hi/lo, BS hi/lo, BK hi/lo
+constexpr int BUF_BYTES = NTILES * TILE_BYTES;
+constexpr int TMEM_COLS = 256;           // S accumulator at column 0, K at column 128
+constexpr long WAIT_LIMIT = 1L << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (start >> 4, LBO 1 (unused by swizzled K-major), SBO
+// 1024 >> 4, descriptor version 1, layout type 2 = SWIZZLE_128B)
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)2u << 61;
+  return d;
+}
+
+// instruction descriptor, kind::tf32: D F32, A and B TF32, both K-major, N, M = 128
+__host__ __device__ constexpr uint32_t idesc_tf32(int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TROWS >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (long i = 0; i < WAIT_LIMIT; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// Load rows [0, nrows) x 32 reduction entries of one tile (rows = matrix
+// columns col0 + r, valid below `valid`; reduction entries n0 .. n0+31 below
+// n_end), split into hi/lo and store both swizzled.
+__device__ __forceinline__ void load_split(const float* __restrict__ M, long ld, int col0, int valid, int nrows,
+                                           long n0, long n_end, bool vec, unsigned char* hi, unsigned char* lo) {
+  for (int i = threadIdx.x; i < nrows * 8; i += TC_NT) {
+    const int row = i >> 3, c = i & 7;
+    const long nn = n0 + 4 * c;
+    float x[4] = {0.f, 0.f, 0.f, 0.f};
+    if (row < valid && nn < n_end) {
+      const float* src = M + (long)(col0 + row) * ld + nn;
+      if (vec && nn + 3 < n_end) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(src));
+        x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[j] = (nn + j < n_end) ? __ldg(src + j) : 0.f;
+      }
+    }
+    float4 h, l;
+    h.x = tf32_rna(x[0]); l.x = tf32_rna(x[0] - h.x);
+    h.y = tf32_rna(x[1]); l.y = tf32_rna(x[1] - h.y);
+    h.z = tf32_rna(x[2]); l.z = tf32_rna(x[2] - h.z);
+    h.w = tf32_rna(x[3]); l.w = tf32_rna(x[3] - h.w);
+    const int off = row * 128 + ((c ^ (row & 7)) << 4);
+    *reinterpret_cast<float4*>(hi + off) = h;
+    *reinterpret_cast<float4*>(lo + off) = l;
+  }
+}
+}  // namespace
+
+__global__ void __launch_bounds__(TC_NT, 1)
+k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int k, long n, long chunk,
+          const int2* __restrict__ pairs, float* __restrict__ part, int* status) {
+  extern __shared__ unsigned char smraw[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_fail;
+  unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5;
+  const int2 pr = pairs[blockIdx.y];
+  const int mt = pr.x, nt = pr.y;
+  const int col_a = mt * TROWS, col_b = nt * TROWS;
+  const int valid_a = min(TROWS, k - col_a), valid_b = min(TROWS, k - col_b);
+  const int N = (valid_b + 15) & ~15;   // MMA N: multiple of 16 for M = 128
+  const bool same = mt == nt;
+  const long n_begin = (long)blockIdx.x * chunk;
+  const long n_end = min(n, n_begin + chunk);
+  const int nstage = (int)((max(0L, n_end - n_begin) + KSTAGE - 1) / KSTAGE);
+  const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(W) & 15) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(V) & 15) == 0);
+  const uint32_t idesc = idesc_tf32(N);
+
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  const uint32_t tmem_s = tmem, tmem_k = tmem + 128;
+
+  for (int s = 0; s < nstage; ++s) {
+    const int b = s & 1;
+    unsigned char* buf = sm + b * BUF_BYTES;
+    unsigned char* a_hi = buf;
+    unsigned char* a_lo = buf + TILE_BYTES;
+    unsigned char* bs_hi = same ? a_hi : buf + 2 * TILE_BYTES;
+    unsigned char* bs_lo = same ? a_lo : buf + 3 * TILE_BYTES;
+    unsigned char* bk_hi = buf + 4 * TILE_BYTES;
+    unsigned char* bk_lo = buf + 5 * TILE_BYTES;
+    if (s >= 2) {
+      // the MMAs of stage s-2 read this buffer: wait for their commit
+      if (!mbar_wait(smem_u32(&mbar[b]), (uint32_t)(((s - 2) >> 1) & 1))) s_fail = 1;
+    }
+    __syncthreads();
+    if (s_fail) break;
+    const long n0 = n_begin + (long)s * KSTAGE;
+    load_split(W, ld, col_a, valid_a, TROWS, n0, n_end, vec, a_hi, a_lo);
+    if (!same) load_split(W, ld, col_b, valid_b, N, n0, n_end, vec, bs_hi, bs_lo);
+    load_split(V, ld, col_b, valid_b, N, n0, n_end, vec, bk_hi, bk_lo);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo);
+      const uint32_t sh_ = smem_u32(bs_hi), sl = smem_u32(bs_lo);
+      const uint32_t kh = smem_u32(bk_hi), kl = smem_u32(bk_lo);
+#pragma unroll
+      for (int kk = 0; kk < KSTAGE / 8; ++kk) {
+        const uint32_t o = kk * 32;   // 8 TF32 = 32 bytes along K inside the swizzled row
+        const uint32_t acc = (s > 0 || kk > 0) ? 1u : 0u;
+        mma_tf32(tmem_s, sw128_desc(ah + o), sw128_desc(sh_ + o), idesc, acc);
+        mma_tf32(tmem_s, sw128_desc(ah + o), sw128_desc(sl + o), idesc, 1u);
+        mma_tf32(tmem_s, sw128_desc(al + o), sw128_desc(sh_ + o), idesc, 1u);
+        mma_tf32(tmem_k, sw128_desc(ah + o), sw128_desc(kh + o), idesc, acc);
+        mma_tf32(tmem_k, sw128_desc(ah + o), sw128_desc(kl + o), idesc, 1u);
+        mma_tf32(tmem_k, sw128_desc(al + o), sw128_desc(kh + o), idesc, 1u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar[b]))
+                   : "memory");
+    }
+  }
+  // the last commit covers every MMA issued before it
+  if (nstage > 0 && !s_fail) {
+    const int sl = nstage - 1;
+    if (!mbar_wait(smem_u32(&mbar[sl & 1]), (uint32_t)((sl >> 1) & 1))) s_fail = 1;
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (s_fail) {
+    if (threadIdx.x == 0) atomicExch(&status[5], 1);
+  } else if (nstage > 0) {
+    // epilogue: warp w owns TMEM lanes (= rows) 32w .. 32w+31
+    const int row = warp * 32 + (threadIdx.x & 31);
+    float* ps = part + (((long)blockIdx.x * gridDim.y + blockIdx.y) * 2) * (TROWS * TROWS);
+    float* pk = ps + TROWS * TROWS;
+    for (int which = 0; which < 2; ++which) {
+      const uint32_t base = (which == 0 ? tmem_s : tmem_k) + ((uint32_t)(warp * 32) << 16);
+      float* dst = which == 0 ? ps : pk;
+      for (int c0 = 0; c0 < N; c0 += 16) {
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(base + (uint32_t)c0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < valid_a) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (c0 + j < valid_b) dst[row * TROWS + c0 + j] = __uint_as_float(r[j]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+}
+
+// S, K (k x k, column-major FP64) = sums over the chunks.  Diagonal tiles are
+// symmetrised as 0.5 (X + X^T) (as the CUDA-core path does); off-diagonal
+// tiles are computed above the diagonal only and mirrored.
+__global__ void k_gram_tc_final(const float* __restrict__ part, int nchunk, int npair, const int2* __restrict__ pairs,
+                                int k, double* __restrict__ S, double* __restrict__ K) {
+  const long total = (long)npair * TROWS * TROWS;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int p = (int)(e / (TROWS * TROWS));
+    const int rc = (int)(e % (TROWS * TROWS));
+    const int r = rc / TROWS, c = rc % TROWS;
+    const int i = pairs[p].x * TROWS + r, j = pairs[p].y * TROWS + c;
+    if (i >= k || j >= k) continue;
+    const bool diag = pairs[p].x == pairs[p].y;
+    const int cr = c * TROWS + r;
+    double s = 0.0, kv = 0.0, st = 0.0, kt = 0.0;
+    for (int ch = 0; ch < nchunk; ++ch) {
+      const float* ps = part + (((long)ch * npair + p) * 2) * (TROWS * TROWS);
+      s += (double)ps[rc];
+      kv += (double)ps[TROWS * TROWS + rc];
+      if (diag) {
+        st += (double)ps[cr];
+        kt += (double)ps[TROWS * TROWS + cr];
+      }
+    }
+    if (diag) {
+      S[i + (long)j * k] = 0.5 * (s + st);
+      K[i + (long)j * k] = 0.5 * (kv + kt);
+    } else {
+      S[i + (long)j * k] = s;
+      K[i + (long)j * k] = kv;
+      S[j + (long)i * k] = s;
+      K[j + (long)i * k] = kv;
+    }
+  }
+}
+
+// Host side: returns -1 when the tensor-core path does not apply (the caller
+// then uses the CUDA-core kernels).
+int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int k, double* S, double* K,
+                     cudaStream_t st) {
+  if (!ctx->gram_tc || k < 1 || k > 512) return -1;
+  const long n = ctx->n;
+  const int tiles = (k + TROWS - 1) / TROWS;
+  const int npair = tiles * (tiles + 1) / 2;
+  int nchunk = std::max(1, 148 / npair);
+  long chunk = ((n + nchunk - 1) / nchunk + KSTAGE - 1) / KSTAGE * KSTAGE;
+  nchunk = (int)((n + chunk - 1) / chunk);
+  const size_t part_floats = (size_t)nchunk * npair * 2 * TROWS * TROWS;
+  if (ctx->tc_part_floats < part_floats) {
+    cudaFree(ctx->tc_part);
+    ctx->tc_part = nullptr;
+    ctx->tc_part_floats = 0;
+    PSC_CUDA(ctx, cudaMalloc(&ctx->tc_part, part_floats * sizeof(float)));
+    ctx->tc_part_floats = part_floats;
+  }
+  if (!ctx->tc_pairs) PSC_CUDA(ctx, cudaMalloc(&ctx->tc_pairs, 64 * sizeof(int2)));
+  if (ctx->tc_pairs_k != k) {
+    int2 hp[64];
+    int q = 0;
+    for (int a = 0; a < tiles; ++a)
+      for (int b = a; b < tiles; ++b) hp[q++] = make_int2(a, b);
+    PSC_CUDA(ctx, cudaMemcpy(ctx->tc_pairs, hp, npair * sizeof(int2), cudaMemcpyHostToDevice));
+    ctx->tc_pairs_k = k;
+  }
+  const size_t smem = 2 * (size_t)BUF_BYTES + 1024;
+  PSC_CUDA(ctx, cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_gram_tc<<<dim3(nchunk, npair), TC_NT, smem, st>>>(W, V, ld, k, n, chunk, (const int2*)ctx->tc_pairs,
+                                                      ctx->tc_part, ctx->dev_status);
+  PSC_LAUNCH_CHECK(ctx);
+  const long total = (long)npair * TROWS * TROWS;
+  k_gram_tc_final<<<std::max(1, (int)std::min<long>(592, (total + 255) / 256)), 256, 0, st>>>(
+      ctx->tc_part, nchunk, npair, (const int2*)ctx->tc_pairs, k, S, K);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
+
+extern "C" int psc_set_gram_impl(psc_ctx* ctx, int tensor_cores) {
+  if (!ctx) return 2;
+  ctx->gram_tc = tensor_cores ? 1 : 0;
+  return 0;
+}

@@ -97,6 +97,12 @@ struct psc_ctx {
   double* gram_partial = nullptr;// [gram_blocks][cap*cap] Gram partial sums
   int gram_blocks = 0;
   int* dev_status = nullptr;     // device-side error flags [8]
+  // tensor-core Gram pair (mixed precision)
+  int gram_tc = 1;               // 1: FP32 Gram pairs on tcgen05 (3xTF32), 0: CUDA cores
+  float* tc_part = nullptr;      // per-chunk FP32 partial tiles
+  size_t tc_part_floats = 0;
+  void* tc_pairs = nullptr;      // int2 tile pairs (upper triangle)
+  int tc_pairs_k = 0;
 
   // Lanczos vectors (double)
   double* lz_v = nullptr;        // [3][n]
@@ -216,3 +222,6 @@ int psc_laplacian_fused(psc_ctx* ctx, const double* x, const double* prev, doubl
                         double g, double* dot_partial, int* nblocks, cudaStream_t st);
 int psc_random_impl(psc_ctx* ctx, int dtype, int dist, unsigned long long seed, void* out, long ld,
                     long rows, int cols, cudaStream_t st);
+// FP32 Gram pair on tensor cores; -1 when it does not apply
+int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int k, double* S, double* K,
+                     cudaStream_t st);

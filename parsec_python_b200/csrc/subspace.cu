@@ -200,6 +200,10 @@ int psc_gemm_tall(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const
 
 static int gram_pair(psc_ctx* ctx, int dtype, const void* W, const void* V, long ld, int k, double* S, double* K,
                      cudaStream_t st) {
+  if (dtype == PSC_F32) {
+    const int rc = psc_gram_pair_tc(ctx, (const float*)W, (const float*)V, ld, k, S, K, st);
+    if (rc >= 0) return rc;
+  }
   const long n = ctx->n;
   const int tiles = (k + GP_T - 1) / GP_T;
   const int ntile = tiles * tiles;
@@ -222,6 +226,15 @@ static int gram_pair(psc_ctx* ctx, int dtype, const void* W, const void* V, long
                                                                                                  nchunk, k, S, K);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
+}
+
+// S = W^T W and K = W^T V (k x k, column-major FP64 on the device).
+extern "C" int psc_gram_pair(psc_ctx* ctx, int dtype, const void* W, const void* V, long ld, int k, double* S,
+                             double* K, void* stream) {
+  if (!ctx) return 2;
+  if (psc_ensure_dense(ctx, k)) return 1;
+  PSC_REQUIRE(ctx, W && V && S && K && ld >= ctx->n, "gram_pair: bad arguments");
+  return gram_pair(ctx, dtype, W, V, ld, k, S, K, (cudaStream_t)stream);
 }
 
 // Rayleigh-Ritz of the (not necessarily orthonormal) block W: V = H W,

@@ -1,0 +1,439 @@
+"""Learned initial density: a 3-D convolutional encoder-decoder that maps the
+SAD density and the local ionic potential on the grid to a correction of the
+density, used only as the SCF's starting point.
+
+Contract (the consumer side of the reference, V_ion/pseudoDiag_ML4Den_poisson.py
+:448-538, dispatched at rsdft_solver.py:95-108): the predicted density is
+clamped at zero, renormalised to the valence charge, and the Hartree potential
+of its difference from the SAD density is solved by the same CG (tol 1e-5, 200
+iterations) and added to the SAD Hartree potential.  SAD stays the fallback:
+with no trained weights the solver runs from SAD.
+
+Network (1.29 M parameters; channels-last BF16 activations, BF16 weights,
+FP32 accumulation; all kernels in csrc/unet.cu):
+
+    e0  3^3  8 -> 8           full grid           (input: rho_SAD, V_loc, 6 zero channels)
+    d1  3^3  8 -> 32  /2      half
+    e1  3^3  32 -> 32         half
+    d2  3^3  32 -> 64 /2      quarter
+    e2  3^3  64 -> 64         quarter
+    d3  3^3  64 -> 128 /2     eighth
+    b   3^3  128 -> 128       eighth
+    u2  3^3  up(b) + e2 -> 64   quarter
+    u1  3^3  up(u2) + e1 -> 32  half
+    u0  3^3  up(u1) + e0 -> 8   full
+    out 1^3  8 -> 8 (channel 0 = correction), linear
+
+Training data come from this project's own FP64 GPU SCF on seeded water
+clusters; training runs on the GPU through psc_conv3d_fwd / psc_conv3d_bwd /
+psc_adam_step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from ctypes import byref, c_int
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import gpu, workloads
+from .models import A0_ANG, SolverSettings
+
+DATA_DIR = Path(__file__).resolve().parent / "data"
+DEFAULT_WEIGHTS = DATA_DIR / "learned_init_water.npz"
+
+
+@dataclass(frozen=True)
+class Layer:
+    name: str
+    src: str          # A input
+    up: int           # A is upsampled x2
+    skip: str | None  # S input
+    ca: int
+    cs: int
+    cout: int
+    stride: int
+    ksize: int
+    relu: bool
+
+
+LAYERS = (
+    Layer("e0", "in", 0, None, 8, 0, 8, 1, 3, True),
+    Layer("d1", "e0", 0, None, 8, 0, 32, 2, 3, True),
+    Layer("e1", "d1", 0, None, 32, 0, 32, 1, 3, True),
+    Layer("d2", "e1", 0, None, 32, 0, 64, 2, 3, True),
+    Layer("e2", "d2", 0, None, 64, 0, 64, 1, 3, True),
+    Layer("d3", "e2", 0, None, 64, 0, 128, 2, 3, True),
+    Layer("b", "d3", 0, None, 128, 0, 128, 1, 3, True),
+    Layer("u2", "b", 1, "e2", 128, 64, 64, 1, 3, True),
+    Layer("u1", "u2", 1, "e1", 64, 32, 32, 1, 3, True),
+    Layer("u0", "u1", 1, "e0", 32, 8, 8, 1, 3, True),
+    Layer("out", "u0", 0, None, 8, 0, 8, 1, 1, False),
+)
+
+
+def n_params() -> int:
+    return sum(l.ksize ** 3 * (l.ca + l.cs) * l.cout + l.cout for l in LAYERS)
+
+
+def _half(d):
+    return tuple((x + 1) // 2 for x in d)
+
+
+class UNet3D:
+    """Parameters, activations and gradients of the encoder-decoder on one
+    grid, all in device memory of the context's GPU."""
+
+    WORK_FLOATS = 16 * 1024 * 1024
+
+    def __init__(self, ctx: gpu.GridContext, seed: int = 0, params: dict | None = None):
+        self.ctx = ctx
+        self.dev = ctx.device
+        dims = {"in": (ctx.nx, ctx.ny, ctx.nz)}
+        level = {"in": dims["in"]}
+        for l in LAYERS:
+            src = level[l.src]
+            if l.up:
+                out = level[l.skip]
+                if _half(out) != src:
+                    raise ValueError(f"layer {l.name}: grid mismatch for upsampling")
+            elif l.stride == 2:
+                out = _half(src)
+            else:
+                out = src
+            level[l.name] = out
+        self.grid = level
+        # one flat FP32 master vector for all weights and biases
+        self.offsets = {}
+        off = 0
+        for l in LAYERS:
+            nw = l.ksize ** 3 * (l.ca + l.cs) * l.cout
+            self.offsets[l.name] = (off, nw, off + nw, l.cout)
+            off += nw + l.cout
+        self.n = off
+        self.w = torch.zeros(self.n, dtype=torch.float32, device=self.dev)
+        if params is None:
+            rng = np.random.default_rng(seed)
+            host = np.zeros(self.n, dtype=np.float32)
+            for l in LAYERS:
+                o, nw, ob, nb = self.offsets[l.name]
+                fan_in = l.ksize ** 3 * (l.ca + l.cs)
+                std = np.sqrt(2.0 / fan_in) * (0.1 if l.name == "out" else 1.0)
+                host[o:o + nw] = rng.standard_normal(nw).astype(np.float32) * std
+            self.w.copy_(torch.from_numpy(host))
+            self.scales = {"a0": 1.0, "a1": 1.0, "at": 1.0}
+        else:
+            self.w.copy_(torch.from_numpy(np.asarray(params["w"], dtype=np.float32)))
+            self.scales = {k: float(params[k]) for k in ("a0", "a1", "at")}
+        self.wb = torch.empty(self.n, dtype=torch.bfloat16, device=self.dev)
+        self.ctx.call("psc_f32_to_bf16", gpu._p(self.w), gpu._p(self.wb), self.n, gpu._stream())
+        self.grad = torch.zeros(self.n, dtype=torch.float32, device=self.dev)
+        self.m = torch.zeros_like(self.grad)
+        self.v = torch.zeros_like(self.grad)
+        self.step_count = 0
+        self.acts: dict[str, torch.Tensor] = {}
+        self.work = None
+        self.loss_dev = torch.zeros(1, dtype=torch.float64, device=self.dev)
+
+    # -- helpers -------------------------------------------------------------
+    def _nvox(self, name):
+        x, y, z = self.grid[name]
+        return x * y * z
+
+    def _geom(self, l: Layer):
+        gi = self.grid[l.skip] if l.up else self.grid[l.src]
+        ga = self.grid[l.src]
+        go = self.grid[l.name]
+        g = (c_int * 15)(gi[0], gi[1], gi[2], ga[0], ga[1], ga[2], l.up, l.ca, l.cs, go[0], go[1], go[2],
+                         l.stride, l.ksize, l.cout)
+        return g
+
+    def _wviews(self, l: Layer, t: torch.Tensor):
+        o, nw, ob, nb = self.offsets[l.name]
+        return t[o:o + nw], t[ob:ob + nb]
+
+    # -- forward / backward --------------------------------------------------
+    def forward(self, x: torch.Tensor) -> torch.Tensor:
+        """x: BF16 [n][8] network input; returns FP32 [n][8] (channel 0 is the output)."""
+        self.acts = {"in": x}
+        out32 = None
+        for l in LAYERS:
+            a = self.acts[l.src]
+            s = self.acts[l.skip] if l.skip else None
+            wv, bv = self._wviews(l, self.wb)
+            _, bias = self._wviews(l, self.w)
+            y = torch.empty(self._nvox(l.name), l.cout, dtype=torch.bfloat16, device=self.dev)
+            if l.name == "out":
+                out32 = torch.empty(self._nvox(l.name), l.cout, dtype=torch.float32, device=self.dev)
+            self.ctx.call("psc_conv3d_fwd", self._geom(l), gpu._p(a), gpu._p(s), gpu._p(wv), gpu._p(bias),
+                          int(l.relu), gpu._p(y), gpu._p(out32 if l.name == "out" else None), gpu._stream())
+            self.acts[l.name] = y
+        return out32
+
+    def backward(self, gout: torch.Tensor) -> None:
+        """gout: FP32 [n][8] = dL/d(out); fills self.grad (weights and biases)."""
+        if self.work is None:
+            self.work = torch.empty(self.WORK_FLOATS, dtype=torch.float32, device=self.dev)
+        grads = {"out": gout}
+        for l in reversed(LAYERS):
+            g = grads.pop(l.name)
+            a = self.acts[l.src]
+            s = self.acts[l.skip] if l.skip else None
+            nvo = self._nvox(l.name)
+            gm = torch.empty(nvo, l.cout, dtype=torch.float32, device=self.dev)
+            need_in = l.src != "in"
+            dvin = dA = dS = None
+            acc_a = acc_s = 0
+            if need_in:
+                nvi = self._nvox(l.skip if l.up else l.src)
+                dvin = torch.empty(nvi, l.ca + l.cs, dtype=torch.float32, device=self.dev)
+                if l.src in grads:
+                    acc_a = 1
+                else:
+                    grads[l.src] = torch.empty(self._nvox(l.src), l.ca, dtype=torch.float32, device=self.dev)
+                dA = grads[l.src]
+                if l.skip:
+                    if l.skip in grads:
+                        acc_s = 1
+                    else:
+                        grads[l.skip] = torch.empty(self._nvox(l.skip), l.cs, dtype=torch.float32, device=self.dev)
+                    dS = grads[l.skip]
+            dW, dB = self._wviews(l, self.grad)
+            wv, _ = self._wviews(l, self.wb)
+            self.ctx.call("psc_conv3d_bwd", self._geom(l), gpu._p(a), gpu._p(s), gpu._p(wv), gpu._p(g),
+                          gpu._p(self.acts[l.name] if l.relu else None), gpu._p(gm), gpu._p(dvin), gpu._p(dA),
+                          acc_a, gpu._p(dS), acc_s, gpu._p(dW), gpu._p(dB), gpu._p(self.work), self.WORK_FLOATS,
+                          gpu._stream())
+
+    def loss_and_grad(self, out32: torch.Tensor, target: torch.Tensor):
+        grad = torch.empty_like(out32)
+        self.ctx.call("psc_mse_loss", gpu._p(out32), out32.shape[1], gpu._p(target), target.numel(), gpu._p(grad),
+                      gpu._p(self.loss_dev), gpu._stream())
+        return self.loss_dev, grad
+
+    def adam(self, lr: float, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
+        self.step_count += 1
+        self.ctx.call("psc_adam_step", gpu._p(self.w), gpu._p(self.wb), gpu._p(self.grad), gpu._p(self.m),
+                      gpu._p(self.v), self.n, float(lr), float(b1), float(b2), float(eps), self.step_count,
+                      gpu._stream())
+
+    # -- input / output --------------------------------------------------------
+    def pack(self, rho_bohr3: torch.Tensor, vloc: torch.Tensor) -> torch.Tensor:
+        x = torch.empty(self.ctx.n, 8, dtype=torch.bfloat16, device=self.dev)
+        self.ctx.call("psc_pack_input", gpu._p(rho_bohr3.contiguous()), gpu._p(vloc.contiguous()),
+                      self.scales["a0"], self.scales["a1"], gpu._p(x), gpu._stream())
+        return x
+
+    def predict_delta(self, rho_bohr3: torch.Tensor, vloc: torch.Tensor) -> torch.Tensor:
+        """Density correction (e/bohr^3, FP64) on the context's grid."""
+        out = self.forward(self.pack(rho_bohr3, vloc))
+        return out[:, 0].double() / self.scales["at"]
+
+    def save(self, path: Path, meta: dict) -> None:
+        np.savez(path, w=self.w.cpu().numpy(), a0=self.scales["a0"], a1=self.scales["a1"], at=self.scales["at"],
+                 meta=json.dumps(meta))
+
+
+def load_weights(path: Path | str = DEFAULT_WEIGHTS) -> dict | None:
+    p = Path(path)
+    if not p.exists():
+        return None
+    z = np.load(p, allow_pickle=False)
+    return {"w": z["w"], "a0": float(z["a0"]), "a1": float(z["a1"]), "at": float(z["at"]),
+            "meta": json.loads(str(z["meta"]))}
+
+
+class LearnedInit:
+    """init_density callback for solver.run_rsdft_calculation: SAD density ->
+    network correction -> clamp, renormalise, Hartree of the difference
+    (pseudoDiag_ML4Den_poisson.py:448-538)."""
+
+    def __init__(self, params: dict):
+        if params["w"].size != n_params():
+            raise ValueError("weights do not match the network")
+        self.params = params
+        self.net = None
+        self.last = {}
+
+    def __call__(self, ctx: gpu.GridContext, rho0, hpot0, ppot, A):
+        if self.net is None or self.net.ctx is not ctx:
+            self.net = UNet3D(ctx, params=self.params)
+        h3 = ctx.h ** 3
+        rho_b = rho0 / h3
+        delta = self.net.predict_delta(rho_b, ppot)
+        rho1 = torch.clamp(rho_b + delta, min=0.0) * h3
+        zsum = gpu.numpy_sum(ctx, rho0)
+        rho1 = rho1 * (zsum / gpu.numpy_sum(ctx, rho1))
+        hrhs = (4 * np.pi / h3) * (rho1 - rho0)
+        dh, its = gpu.pcg(A, hrhs, torch.zeros_like(hrhs), 200, 1e-5)
+        self.last = {"cg_its": its}
+        return rho1, hpot0 + dh
+
+
+# ---------------------------------------------------------------------------
+# data, training, evaluation
+# ---------------------------------------------------------------------------
+WATER_H_ANG = 0.2
+WATER_RADIUS_ANG = 9.0   # clusters live in a 6 A ball; 3 A margin for the density tails
+
+
+def water_system(seed: int, settings: SolverSettings):
+    from .inputs import ElementTable
+    from .system import system_from_atoms
+
+    atoms = workloads.water_cluster(seed)
+    f = 1.0 / A0_ANG
+    atoms = [{"typ": a["typ"], "coord": np.asarray(a["coord"], dtype=float).reshape(-1, 3) * f} for a in atoms]
+    nmol = sum(np.asarray(a["coord"]).reshape(-1, 3).shape[0] for a in atoms if a["typ"] == "O")
+    nev = 4 * nmol + 4
+    elem = ElementTable()
+    prob = system_from_atoms(atoms, h=WATER_H_ANG * f, radius=WATER_RADIUS_ANG * f, nev=nev, settings=settings,
+                             elem=elem)
+    return prob, elem
+
+
+def run_scf(seed: int, init=None, tol: float = 1e-6, scf_seed: int = 0, energy_target=None):
+    from .backend import select_solver_backend
+    from .solver import run_rsdft_calculation
+
+    s = SolverSettings(tol=tol, poldeg=10, maxits=80, seed=scf_seed)
+    s.normalize()
+    prob, elem = water_system(seed, s)
+    backend = select_solver_backend(s)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = run_rsdft_calculation(prob, elem, len(elem), backend, verbose=False, init_density=init,
+                                energy_target=energy_target)
+    torch.cuda.synchronize()
+    return res, time.perf_counter() - t0, backend
+
+
+def make_sample(seed: int):
+    """(SAD density e/bohr^3, V_loc, converged - SAD density) on the water grid."""
+    res, _, backend = run_scf(seed)
+    rt = backend.runtime
+    prob, elem = water_system(seed, rt.settings)
+    ctx = rt.context(prob.domain)
+    rho0, _, ppot, _ = backend.pseudo_diag(prob.domain, prob.input_data.atoms, elem, len(elem), return_info=True)
+    h3 = ctx.h ** 3
+    rho_sad = rho0 / h3
+    return ctx, rho_sad, ppot.clone(), (res.rho - rho_sad).float(), res
+
+
+def train(n_train: int, epochs: int, out: Path, lr: float = 2e-3, seed: int = 0, log=print) -> dict:
+    t_data = time.perf_counter()
+    samples = []
+    ctx0 = None
+    skipped = []
+    sd = 0
+    while len(samples) < n_train:
+        try:
+            ctx, rs, vl, dt, res = make_sample(sd)
+        except ValueError as exc:   # e.g. the reference's "Bounds are incorrect" stop in chefsi1
+            skipped.append(sd)
+            log(f"  seed {sd} skipped: {exc}")
+            sd += 1
+            continue
+        if ctx0 is None:
+            ctx0 = ctx
+        samples.append((rs, vl, dt))
+        if len(samples) % 32 == 1:
+            log(f"  sample {len(samples) - 1} (seed {sd}): {res.iterations} SCF iterations")
+        sd += 1
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t_data
+    # fixed input / target scales from the training set
+    a0 = 1.0 / float(torch.stack([s[0].std() for s in samples]).mean())
+    a1 = 1.0 / float(torch.stack([s[1].std() for s in samples]).mean())
+    at = 1.0 / float(torch.stack([s[2].std() for s in samples]).mean())
+    net = UNet3D(ctx0, seed=seed)
+    net.scales = {"a0": a0, "a1": a1, "at": at}
+    xs = [net.pack(s[0], s[1]) for s in samples]
+    ts = [(s[2] * at).contiguous() for s in samples]
+    del samples
+    rng = np.random.default_rng(seed)
+    t_train = time.perf_counter()
+    steps = epochs * n_train
+    losses = []
+    for ep in range(epochs):
+        order = rng.permutation(n_train)
+        ep_loss = torch.zeros(1, dtype=torch.float64, device=net.dev)
+        for i in order:
+            out32 = net.forward(xs[i])
+            loss, g = net.loss_and_grad(out32, ts[i])
+            ep_loss += loss
+            net.backward(g)
+            # cosine decay over the run
+            lr_t = lr * 0.5 * (1 + np.cos(np.pi * net.step_count / steps))
+            net.adam(lr_t)
+        losses.append(float(ep_loss.item()) / n_train)
+        log(f"  epoch {ep}: mean loss {losses[-1]:.4e} (relative to the target variance)")
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t_train
+    meta = {"n_train": n_train, "epochs": epochs, "lr": lr, "seed": seed, "losses": losses,
+            "seeds_used": [0, sd], "seeds_skipped": skipped,
+            "data_seconds": t_data, "train_seconds": t_train, "grid": list(net.grid["in"]),
+            "h_ang": WATER_H_ANG, "radius_ang": WATER_RADIUS_ANG, "params": n_params()}
+    net.save(out, meta)
+    return meta
+
+
+def evaluate(seeds, weights: Path, log=print) -> dict:
+    params = load_weights(weights)
+    if params is None:
+        raise FileNotFoundError(weights)
+    rows = []
+    skipped = []
+    for sd in seeds:
+        try:
+            r_sad, t_sad, _ = run_scf(sd)
+            init = LearnedInit(params)
+            r_ml, t_ml, _ = run_scf(sd, init=init)
+        except ValueError as exc:
+            skipped.append(sd)
+            log(f"  seed {sd} skipped: {exc}")
+            continue
+        e_sad, e_ml = r_sad.history[-1]["total_ry"], r_ml.history[-1]["total_ry"]
+        rows.append({"seed": sd, "its_sad": r_sad.iterations, "its_learned": r_ml.iterations, "t_sad": t_sad,
+                     "t_learned": t_ml, "e_sad_ry": e_sad, "e_learned_ry": e_ml, "de_ha": abs(e_sad - e_ml) / 2})
+        log(f"  seed {sd}: SAD {r_sad.iterations} its {t_sad:.3f}s, learned {r_ml.iterations} its {t_ml:.3f}s, "
+            f"|dE| {rows[-1]['de_ha']:.2e} Ha")
+    its_s = np.array([r["its_sad"] for r in rows])
+    its_l = np.array([r["its_learned"] for r in rows])
+    summary = {"n": len(rows), "mean_its_sad": float(its_s.mean()), "mean_its_learned": float(its_l.mean()),
+               "mean_t_sad": float(np.mean([r["t_sad"] for r in rows])),
+               "mean_t_learned": float(np.mean([r["t_learned"] for r in rows])),
+               "max_de_ha": float(max(r["de_ha"] for r in rows)), "skipped": skipped, "rows": rows}
+    return summary
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m parsec_python_b200.learned")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--n-train", type=int, default=512)
+    t.add_argument("--epochs", type=int, default=12)
+    t.add_argument("--lr", type=float, default=2e-3)
+    t.add_argument("--out", type=Path, default=DEFAULT_WEIGHTS)
+    e = sub.add_parser("eval")
+    e.add_argument("--first", type=int, default=512)
+    e.add_argument("--count", type=int, default=64)
+    e.add_argument("--weights", type=Path, default=DEFAULT_WEIGHTS)
+    e.add_argument("--json", type=Path, default=None)
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        meta = train(a.n_train, a.epochs, a.out, lr=a.lr)
+        print(json.dumps({k: v for k, v in meta.items() if k != "losses"} | {"final_loss": meta["losses"][-1]}))
+    else:
+        summ = evaluate(range(a.first, a.first + a.count), a.weights)
+        if a.json:
+            a.json.write_text(json.dumps(summ, indent=1))
+        print(json.dumps({k: v for k, v in summ.items() if k != "rows"}))
+
+
+if __name__ == "__main__":
+    main()

@@ -225,6 +225,46 @@ def test_syev_edge_cases(k, kind):
     assert np.abs(Q.T @ Q - np.eye(k)).max() < 1e-12
 
 
+@pytest.mark.parametrize("shape,k", [((30, 28, 26), 27), ((40, 40, 40), 55), ((33, 31, 29), 128),
+                                     ((24, 24, 24), 143), ((21, 20, 19), 300)])
+def test_gram_pair_tensor_cores_match_fp64(shape, k):
+    """FP32 Gram pair on tcgen05 (3xTF32, FP32 accumulation in tensor memory
+    per chunk of rows, FP64 across chunks) and on CUDA cores (FP64
+    accumulation), against FP64 products of the same FP32 values; odd n
+    exercises the scalar-load edge.  The tensor-core bound 2e-5 (relative to
+    the largest entry) is the FP32 accumulation over a chunk of a few hundred
+    rows; the products themselves are exact."""
+    nx, ny, nz = shape
+    ctx = gpu.GridContext({"nx": nx, "ny": ny, "nz": nz, "h": 0.4, "radius": 0.2 * (nx - 1)}, 8)
+    n = ctx.n
+    rng = np.random.default_rng(k)
+    W = rng.standard_normal((k, n)).astype(np.float32)
+    V = (W * 0.3 + rng.standard_normal((k, n)).astype(np.float32)).astype(np.float32)
+    Wd, Vd = torch.from_numpy(W).to(DEV), torch.from_numpy(V).to(DEV)
+    W64, V64 = W.astype(np.float64), V.astype(np.float64)
+    S_ref, K_ref = W64 @ W64.T, W64 @ V64.T
+    out = {}
+    for impl in (1, 0):
+        ctx.call("psc_set_gram_impl", impl)
+        S, K = ctx.empty(k, k), ctx.empty(k, k)
+        ctx.call("psc_gram_pair", F32, gpu._p(Wd), gpu._p(Vd), n, k, gpu._p(S), gpu._p(K), gpu._stream())
+        out[impl] = (S.cpu().numpy().T, K.cpu().numpy().T)
+    assert ctx.status()[5] == 0
+    # both paths return symmetric matrices: K = 0.5 (K + K^T), except that the
+    # tensor-core path forms off-diagonal 128-column tiles above the diagonal only
+    K_sym = 0.5 * (K_ref + K_ref.T)
+    K_tc = K_sym.copy()
+    t = np.arange(k) // 128
+    off = t[:, None] < t[None, :]
+    K_tc[off] = K_ref[off]
+    K_tc.T[off] = K_ref[off]
+    for impl, (S, K) in out.items():
+        tol = 2e-5 if impl == 1 else 1e-12
+        assert np.abs(S - S_ref).max() <= tol * np.abs(S_ref).max(), impl
+        assert np.abs(K - (K_tc if impl == 1 else K_sym)).max() <= tol * np.abs(K_ref).max(), impl
+        assert np.array_equal(S, S.T) and np.array_equal(K, K.T)
+
+
 def test_occupations_match_reference(golden_dir):
     oc = np.load(golden_dir / "ref_occupations.npz")
     ctx = gpu.GridContext({"nx": 8, "ny": 8, "nz": 8, "h": 0.5, "radius": 1.75}, 8)

@@ -1,0 +1,161 @@
+"""Learned initial density: the BF16 convolution kernels against a float64
+PyTorch-CPU oracle (forward, and backward by autograd), training on the GPU,
+and the trained network's effect on the SCF."""
+import ctypes
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import torch.nn.functional as F  # noqa: E402
+
+from parsec_python_b200 import gpu, learned  # noqa: E402
+
+DEV = torch.device("cuda", 0)
+
+
+def _ctx():
+    return gpu.GridContext({"nx": 8, "ny": 8, "nz": 8, "h": 0.5, "radius": 1.75}, 8)
+
+
+def _to_ncdhw(t, grid, c):
+    nx, ny, nz = grid
+    return t.reshape(nz, ny, nx, c).permute(3, 0, 1, 2).unsqueeze(0)
+
+
+def _from_ncdhw(t):
+    c = t.shape[1]
+    return t[0].permute(1, 2, 3, 0).reshape(-1, c)
+
+
+def _torch_weight(w, k, cin, cout):
+    # ours [tap][ci][co], tap = dx + k (dy + k dz) -> torch [co][ci][dz][dy][dx]
+    return w.reshape(k, k, k, cin, cout).permute(4, 3, 0, 1, 2)
+
+
+CASES = [
+    # name, grid_in, up, Ca, Cs, Cout, stride, ksize, relu
+    ("s1", (11, 9, 7), 0, 8, 0, 16, 1, 3, True),
+    ("s2-odd", (11, 9, 7), 0, 8, 0, 32, 2, 3, True),
+    ("s2-even", (12, 10, 8), 0, 16, 0, 8, 2, 3, False),
+    ("up-skip", (11, 9, 7), 1, 16, 8, 8, 1, 3, True),
+    ("up-skip-wide", (10, 7, 9), 1, 32, 16, 32, 1, 3, True),
+    ("1x1", (9, 8, 7), 0, 8, 0, 8, 1, 1, False),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_conv3d_forward_backward_match_float64_oracle(case):
+    name, gi, up, ca, cs, cout, stride, k, relu = case
+    ctx = _ctx()
+    rng = np.random.default_rng(sum(map(ord, name)))
+    ga = tuple((x + 1) // 2 for x in gi) if up else gi
+    go = gi if stride == 1 else tuple((x + 1) // 2 for x in gi)
+    nva, nvi, nvo = np.prod(ga), np.prod(gi), np.prod(go)
+    cin = ca + cs
+    bf = torch.bfloat16
+    a = torch.from_numpy(rng.standard_normal((nva, ca)).astype(np.float32)).to(bf)
+    s = torch.from_numpy(rng.standard_normal((nvi, cs)).astype(np.float32)).to(bf) if cs else None
+    w = torch.from_numpy((rng.standard_normal((k ** 3, cin, cout)) / np.sqrt(cin * k ** 3)).astype(np.float32)).to(bf)
+    b = torch.from_numpy(rng.standard_normal(cout).astype(np.float32))
+    geom = (ctypes.c_int * 15)(*gi, *ga, up, ca, cs, *go, stride, k, cout)
+    ad, sd, wd, bd = a.to(DEV), (s.to(DEV) if s is not None else None), w.to(DEV), b.to(DEV)
+    y = torch.empty(nvo, cout, dtype=bf, device=DEV)
+    y32 = torch.empty(nvo, cout, dtype=torch.float32, device=DEV)
+    ctx.call("psc_conv3d_fwd", geom, gpu._p(ad), gpu._p(sd), gpu._p(wd), gpu._p(bd), int(relu), gpu._p(y),
+             gpu._p(y32), gpu._stream())
+    # float64 oracle on the same BF16 values
+    A = _to_ncdhw(a.double(), ga, ca).requires_grad_(True)
+    x = A
+    if up:
+        x = x.repeat_interleave(2, 2).repeat_interleave(2, 3).repeat_interleave(2, 4)[:, :, :gi[2], :gi[1], :gi[0]]
+    S = None
+    if cs:
+        S = _to_ncdhw(s.double(), gi, cs).requires_grad_(True)
+        x = torch.cat([x, S], 1)
+    Wt = _torch_weight(w.double(), k, cin, cout).requires_grad_(True)
+    Bt = b.double().requires_grad_(True)
+    pre = F.conv3d(x, Wt, Bt, stride=stride, padding=k // 2)
+    ref = torch.relu(pre) if relu else pre
+    ref_flat = _from_ncdhw(ref).detach()
+    got = y32.double().cpu()
+    assert (got - ref_flat).abs().max() <= 2e-5 * max(1.0, ref_flat.abs().max().item())
+    # BF16 output is the FP32 result rounded
+    assert torch.equal(y.cpu(), y32.cpu().to(bf))
+    # backward against autograd, with the ReLU mask taken from the kernel's own output
+    R = torch.from_numpy(rng.standard_normal((nvo, cout)).astype(np.float32))
+    mask = (y.cpu().float() > 0).double() if relu else torch.ones(nvo, cout, dtype=torch.float64)
+    g_pre = _to_ncdhw(R.double() * mask, go, cout)
+    pre.backward(g_pre)
+    gm = torch.empty(nvo, cout, dtype=torch.float32, device=DEV)
+    dvin = torch.empty(nvi, cin, dtype=torch.float32, device=DEV)
+    dA = torch.full((nva, ca), 7.0, dtype=torch.float32, device=DEV)        # accumulated into
+    dS = torch.empty(nvi, cs, dtype=torch.float32, device=DEV) if cs else None
+    dW = torch.empty(k ** 3 * cin * cout, dtype=torch.float32, device=DEV)
+    dB = torch.empty(cout, dtype=torch.float32, device=DEV)
+    work = torch.empty(4 * 1024 * 1024, dtype=torch.float32, device=DEV)
+    ctx.call("psc_conv3d_bwd", geom, gpu._p(ad), gpu._p(sd), gpu._p(wd), gpu._p(R.to(DEV)),
+             gpu._p(y if relu else None), gpu._p(gm), gpu._p(dvin), gpu._p(dA), 1, gpu._p(dS), 0, gpu._p(dW),
+             gpu._p(dB), gpu._p(work), work.numel(), gpu._stream())
+
+    def close(got, ref, tol=2e-5):
+        got, ref = got.double().cpu(), ref.detach().double()
+        assert (got - ref).abs().max() <= tol * max(1.0, ref.abs().max().item())
+
+    close(dW.reshape(k, k, k, cin, cout).permute(4, 3, 0, 1, 2), Wt.grad)
+    close(dB, Bt.grad)
+    close(dA - 7.0, _from_ncdhw(A.grad))
+    if cs:
+        close(dS, _from_ncdhw(S.grad))
+    assert ctx.status()[0] == 0
+
+
+def test_conv3d_rejects_bad_geometry():
+    ctx = _ctx()
+    x = torch.zeros(64, dtype=torch.bfloat16, device=DEV)
+    f = torch.zeros(64, dtype=torch.float32, device=DEV)
+    geom = (ctypes.c_int * 15)(4, 4, 4, 4, 4, 4, 0, 6, 0, 4, 4, 4, 1, 3, 8)     # Ca not a multiple of 8
+    with pytest.raises(gpu.PscError, match="multiples of 8"):
+        ctx.call("psc_conv3d_fwd", geom, gpu._p(x), None, gpu._p(x), gpu._p(f), 1, gpu._p(x), None, gpu._stream())
+    geom = (ctypes.c_int * 15)(4, 4, 4, 4, 4, 4, 0, 8, 0, 4, 4, 4, 2, 3, 8)     # stride 2 needs a halved grid
+    with pytest.raises(gpu.PscError, match="stride"):
+        ctx.call("psc_conv3d_fwd", geom, gpu._p(x), None, gpu._p(x), gpu._p(f), 1, gpu._p(x), None, gpu._stream())
+
+
+def test_unet_trains_on_a_small_grid():
+    """The full encoder-decoder learns a fixed smooth map on a 23x21x19 grid:
+    200 Adam steps through the kernels cut the loss at least fivefold."""
+    ctx = gpu.GridContext({"nx": 23, "ny": 21, "nz": 19, "h": 0.5, "radius": 5.5}, 8)
+    net = learned.UNet3D(ctx, seed=1)
+    n = ctx.n
+    z, y, x = np.meshgrid(np.arange(19), np.arange(21), np.arange(23), indexing="ij")
+    r0 = np.exp(-((x - 11) ** 2 + (y - 10) ** 2 + (z - 9) ** 2) / 20.0).ravel()
+    v = -np.exp(-((x - 8) ** 2 + (y - 12) ** 2 + (z - 9) ** 2) / 8.0).ravel()
+    t = (0.5 * r0 - 0.3 * v * r0).astype(np.float32)
+    rho = torch.from_numpy(r0).to(DEV)
+    vl = torch.from_numpy(v).to(DEV)
+    xin = net.pack(rho, vl)
+    tgt = torch.from_numpy(t / t.std()).to(DEV)
+    losses = []
+    for i in range(200):
+        out = net.forward(xin)
+        loss, g = net.loss_and_grad(out, tgt)
+        losses.append(loss.item())
+        net.backward(g)
+        net.adam(2e-3)
+    assert np.isfinite(losses).all()
+    assert losses[-1] < 0.2 * losses[0]
+    assert learned.n_params() == net.n
+
+
+def test_learned_init_saves_iterations_on_held_out_water_clusters():
+    params = learned.load_weights()
+    if params is None:
+        pytest.skip("no trained weights in parsec_python_b200/data")
+    summ = learned.evaluate([600, 601], learned.DEFAULT_WEIGHTS, log=lambda *a: None)
+    assert summ["max_de_ha"] < 1e-5
+    assert summ["mean_its_learned"] < summ["mean_its_sad"]

@@ -122,3 +122,22 @@ def test_oracle_and_product_grid_rules_agree():
     for h, r in ((0.378, 9.45), (0.34, 13.2), (0.4724, 17.0)):
         assert cube_for_radius(r, h) == O.build_system([], h=h, radius=r)
     assert s.precision == "fp64" and len(elem) == 18
+
+
+def test_learned_network_layout():
+    """Channel bookkeeping of the encoder-decoder: every layer reads the
+    channels its sources produce; about 1.3 M parameters."""
+    from parsec_python_b200 import learned
+
+    cout = {"in": 8}
+    for l in learned.LAYERS:
+        assert l.ca == cout[l.src], l.name
+        assert l.cs == (cout[l.skip] if l.skip else 0), l.name
+        assert l.ca % 8 == 0 and l.cs % 8 == 0 and l.cout % 8 == 0
+        assert not (l.up and l.stride != 1)
+        cout[l.name] = l.cout
+    assert 1.2e6 < learned.n_params() < 1.4e6
+    w = learned.load_weights()
+    if w is not None:
+        assert w["w"].size == learned.n_params()
+        assert w["a0"] > 0 and w["a1"] > 0 and w["at"] > 0
