@@ -189,27 +189,28 @@ def solve_once(precision: str, seed: int, energy_target=None):
     return res, backend
 
 
-def stencil_roofline(reps: int = 40) -> dict:
+def stencil_roofline(reps: int = 40, dtype: str = "f64") -> dict:
     """Time the fused stencil (one Chebyshev step Out = a H In + b In + g Prev,
-    FP64, k = 55, no projectors so that only the stencil kernel launches) on
-    the C10H8 grid; algorithmic bytes = read In + read Prev + write Out + read
-    pot = (3 k + 1) n 8."""
+    k = 55, no projectors so that only the stencil kernel launches) on the
+    C10H8 grid; algorithmic bytes = read In + read Prev + write Out + read pot
+    = (3 k + 1) n s, s = 8 (FP64) or 4 (FP32, the mixed-precision filter)."""
     import torch
 
     from parsec_python_b200 import gpu
-    from parsec_python_b200._lib import F64
+    from parsec_python_b200._lib import F32, F64
 
     prob, _, _ = gpu_problem("fp64", 0)
     ctx = gpu.GridContext(prob.domain, 8)
     n, k = ctx.n, prob.nev + 15
+    tdt, code, size = (torch.float64, F64, 8) if dtype == "f64" else (torch.float32, F32, 4)
     pot = torch.randn(n, dtype=torch.float64, device="cuda")
     gpu.Hamiltonian(ctx, pot)
-    X = torch.randn(k, n, dtype=torch.float64, device="cuda")
-    Y = torch.randn(k, n, dtype=torch.float64, device="cuda")
+    X = torch.randn(k, n, dtype=tdt, device="cuda")
+    Y = torch.randn(k, n, dtype=tdt, device="cuda")
     st = gpu._stream()
 
     def step(a, b):
-        ctx.call("psc_apply_h_axpby", F64, gpu._p(a), n, gpu._p(b), n, gpu._p(b), n, k, 0.1, -0.3, -0.5, st)
+        ctx.call("psc_apply_h_axpby", code, gpu._p(a), n, gpu._p(b), n, gpu._p(b), n, k, 0.1, -0.3, -0.5, st)
 
     for _ in range(5):
         step(X, Y)
@@ -222,9 +223,54 @@ def stencil_roofline(reps: int = 40) -> dict:
     e1.record()
     torch.cuda.synchronize()
     t = e0.elapsed_time(e1) / 1000.0 / reps
-    bytes_ = (3 * k + 1) * n * 8
+    bytes_ = (3 * k + 1) * n * size
     flops = n * k * (2 * (3 * 8 + 1) + 2 + 4)
     return {"seconds": t, "bytes": bytes_, "gbs": bytes_ / t / 1e9, "gflops": flops / t / 1e9, "n": n, "k": k}
+
+
+def mixed_leg(target, steps: int = 3) -> dict:
+    """The same C10H8 solve in mixed precision: FP32 filter and subspace
+    blocks, tensor-core (3xTF32) Gram pairs, FP64 small dense work, energies
+    and the last iterations (FP64 blocks once the SCF error is below 1e-4);
+    stopped on the same energy bar."""
+    import torch
+
+    res, be = solve_once("mixed", seed=7, energy_target=target)   # warm-up
+    del res, be
+    gc.collect()
+    times, its, errs, f32_its = [], [], [], []
+    for s in range(steps):
+        gc.collect()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res, be = solve_once("mixed", seed=2000 + s, energy_target=target)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1000.0)
+        its.append(res.iterations)
+        f32_its.append(sum(1 for h in res.history if h.get("block_dtype") == "f32"))
+        if target is not None:
+            errs.append(abs(res.history[-1]["total_ry"] - target[0]) / 2.0)
+        del res, be
+    return {"value": float(np.mean(times)), "unit": "s", "step_times_s": times, "iterations": its,
+            "fp32_iterations": f32_its, "energy_error_ha_vs_reference": max(errs) if errs else None}
+
+
+def learned_leg(seeds=(512, 513, 514, 515)) -> dict | None:
+    """Learned initial density on held-out water clusters (the network is
+    trained on seeds 0..; these seeds are not in its training set): SCF
+    iterations and time from SAD and from the network's density, same input,
+    tol 1e-6; None when no trained weights are present."""
+    from parsec_python_b200 import learned
+
+    if learned.load_weights() is None:
+        return None
+    learned.run_scf(seeds[0])   # warm-up of the water grid
+    summ = learned.evaluate(seeds, learned.DEFAULT_WEIGHTS, log=lambda *a: None)
+    summ.pop("rows", None)
+    summ["workload"] = "(H2O)n, n in 2..8, held-out seeds %d-%d, h 0.2 A, sphere radius 9 A" % (seeds[0], seeds[-1])
+    return summ
 
 
 def measured_peak() -> tuple[float, str]:
@@ -393,7 +439,10 @@ def run_gpu_arm(args, rank, local, world):
             print(json.dumps({"scf_only": True, "step_times_s": times, "iterations": iters}), flush=True)
         return
     t_step = allmax(float(np.mean(times)), world)
+    mixed = mixed_leg(target) if not args.scf_only else None
+    learned_res = learned_leg() if rank == 0 else None
     roof = stencil_roofline()
+    roof32 = stencil_roofline(dtype="f32")
     peak, peak_kind = measured_peak()
     err_ha = None if e_ref is None else max(abs(e - e_ref) for e in energies) / 2.0
     within = None if err_ha is None else bool(err_ha <= HA_TOL)
@@ -426,11 +475,18 @@ def run_gpu_arm(args, rank, local, world):
                          "peak_kind": peak_kind, "launch_s": roof["seconds"],
                          "algorithmic_bytes": roof["bytes"]},
             "hx_gbs": roof["gbs"], "hx_gflops": roof["gflops"],
+            "roofline_f32": {"bound": "hbm", "achieved": roof32["gbs"], "peak": peak, "unit": "GB/s",
+                             "frac": roof32["gbs"] / peak, "peak_kind": peak_kind, "launch_s": roof32["seconds"],
+                             "algorithmic_bytes": roof32["bytes"],
+                             "kernel": "k_stencil_tma<float,4> (one FP32 Chebyshev step of the mixed-precision "
+                                       "filter, k=55, C10H8 grid)"},
             "cpu_baseline": cpu, "clocks": clocks,
             "iterations": int(np.median(iters)), "energy_error_ha_vs_reference": err_ha,
             "energy_within_1e-5_ha": within, "reference_energy_ry": e_ref,
             "setup_s": float(np.mean(setups)), "reference_iterations": ref_its, "step_times_s": times,
-            "step_iterations": iters}
+            "step_iterations": iters, "mixed_precision": mixed,
+            "mixed_speedup_vs_fp64": (t_step / mixed["value"]) if mixed else None,
+            "learned_init": learned_res}
     print(json.dumps(line), flush=True)
 
 

@@ -203,17 +203,18 @@ int psc_gram_pair(psc_ctx* ctx, int dtype, const void* W, const void* V, long ld
  * Cs channels of the skip tensor S on the input grid; stride 1 or 2 (output
  * grid ceil(n / stride)), ksize 3 (padding 1) or 1. */
 int psc_conv3d_fwd(psc_ctx* ctx, const int* geom, const void* A, const void* S, const void* W, const float* bias,
-                   int relu, void* out, float* out32, void* stream);
-/* Backward of one convolution.  gout: dL/d(out) FP32 [nvo][Cout]; out: the
- * forward's BF16 output when the layer has a ReLU (NULL for a linear layer);
+                   int act, void* out, float* out32, void* stream);
+/* act: 0 identity, 1 ReLU, 2 leaky ReLU (slope 1/16 below zero).
+ * Backward of one convolution.  gout: dL/d(out) FP32 [nvo][Cout]; out: the
+ * forward's BF16 output (needed when act != 0);
  * gm: FP32 scratch [nvo][Cout] (may alias gout); dvin: FP32 scratch
  * [nvi][Ca+Cs] or NULL to skip the input gradient; dA / dS: FP32 gradients of
  * A and S, overwritten (acc = 0) or accumulated (acc = 1), NULL to skip; dW,
  * dB: FP32 weight and bias gradients (overwritten); work: FP32 scratch of
  * work_floats (>= chunks x 27 Cin Cout). */
 int psc_conv3d_bwd(psc_ctx* ctx, const int* geom, const void* A, const void* S, const void* W, const float* gout,
-                   const void* out, float* gm, float* dvin, float* dA, int acc_a, float* dS, int acc_s, float* dW,
-                   float* dB, float* work, long work_floats, void* stream);
+                   const void* out, int act, float* gm, float* dvin, float* dA, int acc_a, float* dS, int acc_s,
+                   float* dW, float* dB, float* work, long work_floats, void* stream);
 /* Mean squared error on channel 0 of y [n][C] against target [n]; grad [n][C]
  * = d loss / d y; loss_dev = one double on the device. */
 int psc_mse_loss(psc_ctx* ctx, const float* y, int C, const float* target, long n, float* grad, double* loss_dev,

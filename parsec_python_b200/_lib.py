@@ -54,7 +54,8 @@ _SIGS = {
     "psc_set_gram_impl": ([_P, c_int], c_int),
     "psc_gram_pair": ([_P, c_int, _P, _P, c_long, c_int, _P, _P, _P], c_int),
     "psc_conv3d_fwd": ([_P, _P, _P, _P, _P, _P, c_int, _P, _P, _P], c_int),
-    "psc_conv3d_bwd": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, c_int, _P, c_int, _P, _P, _P, c_long, _P], c_int),
+    "psc_conv3d_bwd": ([_P, _P, _P, _P, _P, _P, _P, c_int, _P, _P, _P, c_int, _P, c_int, _P, _P, _P, c_long, _P],
+                       c_int),
     "psc_mse_loss": ([_P, _P, c_int, _P, c_long, _P, _P, _P], c_int),
     "psc_adam_step": ([_P, _P, _P, _P, _P, _P, c_long, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                        ctypes.c_float, c_int, _P], c_int),

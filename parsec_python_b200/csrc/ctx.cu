@@ -67,32 +67,32 @@ extern "C" int psc_ctx_create(int nx, int ny, int nz, double h, int fd_order, ps
     return 1;
   };
   cudaError_t e;
-  if ((e = cudaMalloc(&ctx->pot64, n * sizeof(double))) != cudaSuccess) return fail(e, "pot64");
-  if ((e = cudaMalloc(&ctx->pot32, n * sizeof(float))) != cudaSuccess) return fail(e, "pot32");
+  if ((e = psc_dmalloc(&ctx->pot64, n * sizeof(double))) != cudaSuccess) return fail(e, "pot64");
+  if ((e = psc_dmalloc(&ctx->pot32, n * sizeof(float))) != cudaSuccess) return fail(e, "pot32");
   if ((e = cudaMemset(ctx->pot64, 0, n * sizeof(double))) != cudaSuccess) return fail(e, "pot64");
   if ((e = cudaMemset(ctx->pot32, 0, n * sizeof(float))) != cudaSuccess) return fail(e, "pot32");
-  if ((e = cudaMalloc(&ctx->cheb_coef, (PSC_MAX_DEG + 1) * 3 * sizeof(double))) != cudaSuccess)
+  if ((e = psc_dmalloc(&ctx->cheb_coef, (PSC_MAX_DEG + 1) * 3 * sizeof(double))) != cudaSuccess)
     return fail(e, "coef");
-  if ((e = cudaMalloc(&ctx->red_partial, (size_t)PSC_RED_SLOTS * PSC_RED_BLOCKS * sizeof(double))) !=
+  if ((e = psc_dmalloc(&ctx->red_partial, (size_t)PSC_RED_SLOTS * PSC_RED_BLOCKS * sizeof(double))) !=
       cudaSuccess)
     return fail(e, "partials");
-  if ((e = cudaMalloc(&ctx->scalars, 256 * sizeof(double))) != cudaSuccess) return fail(e, "scalars");
+  if ((e = psc_dmalloc(&ctx->scalars, 256 * sizeof(double))) != cudaSuccess) return fail(e, "scalars");
   if ((e = cudaMemset(ctx->scalars, 0, 256 * sizeof(double))) != cudaSuccess) return fail(e, "scalars");
   if ((e = cudaMallocHost(&ctx->host_scalars, 256 * sizeof(double))) != cudaSuccess)
     return fail(e, "host scalars");
-  if ((e = cudaMalloc(&ctx->dev_status, 8 * sizeof(int))) != cudaSuccess) return fail(e, "status");
+  if ((e = psc_dmalloc(&ctx->dev_status, 8 * sizeof(int))) != cudaSuccess) return fail(e, "status");
   if ((e = cudaMemset(ctx->dev_status, 0, 8 * sizeof(int))) != cudaSuccess) return fail(e, "status");
-  if ((e = cudaMalloc(&ctx->lz_v, 3 * n * sizeof(double))) != cudaSuccess) return fail(e, "lanczos");
-  if ((e = cudaMalloc(&ctx->cg_r, n * sizeof(double))) != cudaSuccess) return fail(e, "cg");
-  if ((e = cudaMalloc(&ctx->cg_p, n * sizeof(double))) != cudaSuccess) return fail(e, "cg");
-  if ((e = cudaMalloc(&ctx->cg_ap, n * sizeof(double))) != cudaSuccess) return fail(e, "cg");
+  if ((e = psc_dmalloc(&ctx->lz_v, 3 * n * sizeof(double))) != cudaSuccess) return fail(e, "lanczos");
+  if ((e = psc_dmalloc(&ctx->cg_r, n * sizeof(double))) != cudaSuccess) return fail(e, "cg");
+  if ((e = psc_dmalloc(&ctx->cg_p, n * sizeof(double))) != cudaSuccess) return fail(e, "cg");
+  if ((e = psc_dmalloc(&ctx->cg_ap, n * sizeof(double))) != cudaSuccess) return fail(e, "cg");
   *out = ctx;
   return 0;
 }
 
 static void free_species(psc_species& s) {
   for (int i = 0; i < 5; ++i) {
-    cudaFree(s.x[i]); cudaFree(s.z[i]); cudaFree(s.c[i]); cudaFree(s.d[i]);
+    psc_dfree(s.x[i]); psc_dfree(s.z[i]); psc_dfree(s.c[i]); psc_dfree(s.d[i]);
     s.x[i] = s.z[i] = s.c[i] = s.d[i] = nullptr;
   }
   s.valid = 0;
@@ -104,14 +104,14 @@ extern "C" int psc_ctx_destroy(psc_ctx* ctx) {
   if (!ctx) return 0;
   for (auto& s : ctx->species) free_species(s);
   psc_free_projectors(ctx);
-  cudaFree(ctx->pot64); cudaFree(ctx->pot32); cudaFree(ctx->cheb_coef); cudaFree(ctx->red_partial);
-  cudaFree(ctx->scalars); cudaFreeHost(ctx->host_scalars); cudaFree(ctx->dev_status);
-  cudaFree(ctx->gram); cudaFree(ctx->gram2); cudaFree(ctx->evec); cudaFree(ctx->tri);
-  cudaFree(ctx->gram_partial); cudaFree(ctx->lz_v); cudaFree(ctx->cg_r); cudaFree(ctx->cg_p);
-  cudaFree(ctx->cg_ap); cudaFree(ctx->cg_part); cudaFree(ctx->mix_dx); cudaFree(ctx->mix_df);
-  cudaFree(ctx->mix_nv); cudaFree(ctx->mix_tmp); cudaFree(ctx->mix_coef); cudaFree(ctx->mix_partial);
-  cudaFree(ctx->cg_x); cudaFree(ctx->jac_v); cudaFree(ctx->cg_p2); cudaFree(ctx->cg_ro); cudaFree(ctx->cg_bar);
-  cudaFree(ctx->tc_part); cudaFree(ctx->tc_pairs);
+  psc_dfree(ctx->pot64); psc_dfree(ctx->pot32); psc_dfree(ctx->cheb_coef); psc_dfree(ctx->red_partial);
+  psc_dfree(ctx->scalars); cudaFreeHost(ctx->host_scalars); psc_dfree(ctx->dev_status);
+  psc_dfree(ctx->gram); psc_dfree(ctx->gram2); psc_dfree(ctx->evec); psc_dfree(ctx->tri);
+  psc_dfree(ctx->gram_partial); psc_dfree(ctx->lz_v); psc_dfree(ctx->cg_r); psc_dfree(ctx->cg_p);
+  psc_dfree(ctx->cg_ap); psc_dfree(ctx->cg_part); psc_dfree(ctx->mix_dx); psc_dfree(ctx->mix_df);
+  psc_dfree(ctx->mix_nv); psc_dfree(ctx->mix_tmp); psc_dfree(ctx->mix_coef); psc_dfree(ctx->mix_partial);
+  psc_dfree(ctx->cg_x); psc_dfree(ctx->jac_v); psc_dfree(ctx->cg_p2); psc_dfree(ctx->cg_ro); psc_dfree(ctx->cg_bar);
+  psc_dfree(ctx->tc_part); psc_dfree(ctx->tc_pairs);
   if (ctx->cg_exec) cudaGraphExecDestroy(ctx->cg_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   delete ctx;
@@ -199,10 +199,10 @@ extern "C" int psc_set_species(psc_ctx* ctx, int species_id, int nknots, const d
     PSC_REQUIRE(ctx, natural_spline(xk, yk, z, c, d) == 0, "spline needs >= 3 distinct knots");
     const int nk = (int)xk.size();
     s.nk[f] = nk;
-    PSC_CUDA(ctx, cudaMalloc(&s.x[f], nk * sizeof(double)));
-    PSC_CUDA(ctx, cudaMalloc(&s.z[f], nk * sizeof(double)));
-    PSC_CUDA(ctx, cudaMalloc(&s.c[f], (nk - 1) * sizeof(double)));
-    PSC_CUDA(ctx, cudaMalloc(&s.d[f], (nk - 1) * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&s.x[f], nk * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&s.z[f], nk * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&s.c[f], (nk - 1) * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&s.d[f], (nk - 1) * sizeof(double)));
     PSC_CUDA(ctx, cudaMemcpy(s.x[f], xk.data(), nk * sizeof(double), cudaMemcpyHostToDevice));
     PSC_CUDA(ctx, cudaMemcpy(s.z[f], z.data(), nk * sizeof(double), cudaMemcpyHostToDevice));
     PSC_CUDA(ctx, cudaMemcpy(s.c[f], c.data(), (nk - 1) * sizeof(double), cudaMemcpyHostToDevice));
@@ -392,6 +392,36 @@ extern "C" int psc_axpby(psc_ctx* ctx, const double* x, const double* y, double 
 }
 
 #include <atomic>
+#include <mutex>
 static std::atomic<long long> g_launches{0};
+
+cudaError_t psc_dmalloc_bytes(void** p, size_t bytes) {
+  static std::mutex mu;
+  static bool pool_ready[64] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64) {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pool_ready[dev]) {
+      cudaMemPool_t pool;
+      e = cudaDeviceGetDefaultMemPool(&pool, dev);
+      if (e != cudaSuccess) return e;
+      uint64_t keep = ~0ull;
+      e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+      pool_ready[dev] = true;
+    }
+  }
+  e = cudaMallocAsync(p, bytes, cudaStreamLegacy);
+  if (e != cudaSuccess) return e;
+  // a block reused from the pool may still be the target of work queued
+  // before its free; make it safe for any stream
+  return cudaStreamSynchronize(cudaStreamLegacy);
+}
+
+void psc_dfree(void* p) {
+  if (p) cudaFreeAsync(p, cudaStreamLegacy);
+}
 void psc_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 extern "C" long long psc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }

@@ -89,18 +89,18 @@ __global__ void k_gram_final(const double* __restrict__ partial, int nchunk, int
 int psc_ensure_dense(psc_ctx* ctx, int k) {
   PSC_REQUIRE(ctx, k >= 1 && k <= PSC_MAX_K, "subspace width out of range");
   if (k <= ctx->dense_cap) return 0;
-  cudaFree(ctx->gram); cudaFree(ctx->gram2); cudaFree(ctx->evec); cudaFree(ctx->tri); cudaFree(ctx->gram_partial);
-  cudaFree(ctx->jac_v);
+  psc_dfree(ctx->gram); psc_dfree(ctx->gram2); psc_dfree(ctx->evec); psc_dfree(ctx->tri); psc_dfree(ctx->gram_partial);
+  psc_dfree(ctx->jac_v);
   const int cap = std::max(k, 64);
   const size_t kk = (size_t)cap * cap;
   // Jacobi scratch: padded A and V of order <= cap + 1 when they do not fit on chip
-  PSC_CUDA(ctx, cudaMalloc(&ctx->jac_v, 2 * (size_t)(cap + 2) * (cap + 2) * sizeof(double)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->gram, kk * sizeof(double)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->gram2, kk * sizeof(double)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->evec, kk * sizeof(double)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->tri, kk * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->jac_v, 2 * (size_t)(cap + 2) * (cap + 2) * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->gram, kk * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->gram2, kk * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->evec, kk * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->tri, kk * sizeof(double)));
   ctx->gram_blocks = 296;
-  PSC_CUDA(ctx, cudaMalloc(&ctx->gram_partial, (size_t)ctx->gram_blocks * kk * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->gram_partial, (size_t)ctx->gram_blocks * kk * sizeof(double)));
   ctx->dense_cap = cap;
   return 0;
 }

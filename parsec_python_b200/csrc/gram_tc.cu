@@ -277,13 +277,13 @@ int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int 
   nchunk = (int)((n + chunk - 1) / chunk);
   const size_t part_floats = (size_t)nchunk * npair * 2 * TROWS * TROWS;
   if (ctx->tc_part_floats < part_floats) {
-    cudaFree(ctx->tc_part);
+    psc_dfree(ctx->tc_part);
     ctx->tc_part = nullptr;
     ctx->tc_part_floats = 0;
-    PSC_CUDA(ctx, cudaMalloc(&ctx->tc_part, part_floats * sizeof(float)));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->tc_part, part_floats * sizeof(float)));
     ctx->tc_part_floats = part_floats;
   }
-  if (!ctx->tc_pairs) PSC_CUDA(ctx, cudaMalloc(&ctx->tc_pairs, 64 * sizeof(int2)));
+  if (!ctx->tc_pairs) PSC_CUDA(ctx, psc_dmalloc(&ctx->tc_pairs, 64 * sizeof(int2)));
   if (ctx->tc_pairs_k != k) {
     int2 hp[64];
     int q = 0;

@@ -138,16 +138,16 @@ extern "C" int psc_mixer_reset(psc_ctx* ctx, int capacity) {
   if (!ctx) return 2;
   PSC_REQUIRE(ctx, capacity >= 1 && capacity <= 255, "mixer: capacity must be 1..255");
   if (capacity > ctx->mix_cap) {
-    cudaFree(ctx->mix_dx); cudaFree(ctx->mix_df); cudaFree(ctx->mix_nv); cudaFree(ctx->mix_tmp);
-    cudaFree(ctx->mix_coef); cudaFree(ctx->mix_partial);
+    psc_dfree(ctx->mix_dx); psc_dfree(ctx->mix_df); psc_dfree(ctx->mix_nv); psc_dfree(ctx->mix_tmp);
+    psc_dfree(ctx->mix_coef); psc_dfree(ctx->mix_partial);
     ctx->mix_dx = ctx->mix_df = ctx->mix_nv = ctx->mix_tmp = ctx->mix_coef = ctx->mix_partial = nullptr;
     const size_t n = ctx->n;
-    PSC_CUDA(ctx, cudaMalloc(&ctx->mix_dx, (size_t)(capacity + 1) * n * sizeof(double)));
-    PSC_CUDA(ctx, cudaMalloc(&ctx->mix_df, (size_t)(capacity + 1) * n * sizeof(double)));
-    PSC_CUDA(ctx, cudaMalloc(&ctx->mix_nv, n * sizeof(double)));
-    PSC_CUDA(ctx, cudaMalloc(&ctx->mix_tmp, n * sizeof(double)));
-    PSC_CUDA(ctx, cudaMalloc(&ctx->mix_coef, (3 * (size_t)capacity + 8) * sizeof(double)));
-    PSC_CUDA(ctx, cudaMalloc(&ctx->mix_partial, (3 * (size_t)capacity + 2) * PSC_RED_BLOCKS * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->mix_dx, (size_t)(capacity + 1) * n * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->mix_df, (size_t)(capacity + 1) * n * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->mix_nv, n * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->mix_tmp, n * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->mix_coef, (3 * (size_t)capacity + 8) * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->mix_partial, (3 * (size_t)capacity + 2) * PSC_RED_BLOCKS * sizeof(double)));
     ctx->mix_cap = capacity;
   }
   ctx->mix_m = 0;

@@ -80,9 +80,9 @@ __global__ void k_nl_scatter(T* Y, long ldy, int k, long ntouched, const int* __
 int psc_ensure_proj(psc_ctx* ctx, int k) {
   size_t need = (size_t)std::max(ctx->nl_atoms, 1) * 3 * k * sizeof(double);
   if (need > ctx->nl_proj_bytes) {
-    cudaFree(ctx->nl_proj);
+    psc_dfree(ctx->nl_proj);
     ctx->nl_proj = nullptr;
-    PSC_CUDA(ctx, cudaMalloc(&ctx->nl_proj, need));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_proj, need));
     ctx->nl_proj_bytes = need;
   }
   return 0;
@@ -118,9 +118,9 @@ int psc_nl_scatter(psc_ctx* ctx, int dtype, void* Y, long ldy, int k, const doub
 }
 
 void psc_free_projectors(psc_ctx* ctx) {
-  cudaFree(ctx->nl_atom_off); cudaFree(ctx->nl_idx); cudaFree(ctx->nl_u64); cudaFree(ctx->nl_u32);
-  cudaFree(ctx->nl_w); cudaFree(ctx->nl_t_idx); cudaFree(ctx->nl_t_off); cudaFree(ctx->nl_t_ent);
-  cudaFree(ctx->nl_point_atom); cudaFree(ctx->nl_proj);
+  psc_dfree(ctx->nl_atom_off); psc_dfree(ctx->nl_idx); psc_dfree(ctx->nl_u64); psc_dfree(ctx->nl_u32);
+  psc_dfree(ctx->nl_w); psc_dfree(ctx->nl_t_idx); psc_dfree(ctx->nl_t_off); psc_dfree(ctx->nl_t_ent);
+  psc_dfree(ctx->nl_point_atom); psc_dfree(ctx->nl_proj);
   ctx->nl_atom_off = ctx->nl_idx = ctx->nl_t_idx = ctx->nl_t_off = ctx->nl_t_ent = ctx->nl_point_atom = nullptr;
   ctx->nl_u64 = nullptr; ctx->nl_u32 = nullptr; ctx->nl_w = nullptr; ctx->nl_proj = nullptr;
   ctx->nl_proj_bytes = 0;
@@ -176,12 +176,12 @@ extern "C" int psc_projector_setup(psc_ctx* ctx, int natoms, const int* species,
   long* start_d = nullptr;
   double* xyz_d = nullptr;
   unsigned char* mask_d = nullptr;
-  auto cleanup = [&]() { cudaFree(box_d); cudaFree(start_d); cudaFree(xyz_d); cudaFree(mask_d); cudaFree(asp_d); };
-  PSC_CUDA(ctx, cudaMalloc(&box_d, box.size() * sizeof(int)));
-  PSC_CUDA(ctx, cudaMalloc(&start_d, start.size() * sizeof(long)));
-  PSC_CUDA(ctx, cudaMalloc(&xyz_d, xyzv.size() * sizeof(double)));
-  PSC_CUDA(ctx, cudaMalloc(&asp_d, atom_species.size() * sizeof(int)));
-  PSC_CUDA(ctx, cudaMalloc(&mask_d, total));
+  auto cleanup = [&]() { psc_dfree(box_d); psc_dfree(start_d); psc_dfree(xyz_d); psc_dfree(mask_d); psc_dfree(asp_d); };
+  PSC_CUDA(ctx, psc_dmalloc(&box_d, box.size() * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&start_d, start.size() * sizeof(long)));
+  PSC_CUDA(ctx, psc_dmalloc(&xyz_d, xyzv.size() * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&asp_d, atom_species.size() * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&mask_d, total));
   PSC_CUDA(ctx, cudaMemcpyAsync(box_d, box.data(), box.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(start_d, start.data(), start.size() * sizeof(long), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(xyz_d, xyzv.data(), xyzv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -211,7 +211,7 @@ extern "C" int psc_projector_setup(psc_ctx* ctx, int natoms, const int* species,
   }
   const int nla = (int)nl_atom_of_box.size();
   const long npts = (long)idx.size();
-  cudaFree(mask_d); mask_d = nullptr;
+  psc_dfree(mask_d); mask_d = nullptr;
   if (nla == 0) { cleanup(); return 0; }
   // touched points: entries sorted by grid index, ties in atom order
   std::vector<int> order(npts);
@@ -240,17 +240,17 @@ extern "C" int psc_projector_setup(psc_ctx* ctx, int natoms, const int* species,
   ctx->nl_atoms = nla;
   ctx->nl_points = npts;
   ctx->nl_touched = (long)t_idx.size();
-  PSC_CUDA(ctx, cudaMalloc(&ctx->nl_atom_off, atom_off.size() * sizeof(int)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->nl_idx, npts * sizeof(int)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->nl_point_atom, npts * sizeof(int)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->nl_u64, 3 * npts * sizeof(double)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->nl_u32, 3 * npts * sizeof(float)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->nl_w, nla * sizeof(double)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->nl_t_idx, t_idx.size() * sizeof(int)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->nl_t_off, t_off.size() * sizeof(int)));
-  PSC_CUDA(ctx, cudaMalloc(&ctx->nl_t_ent, t_ent.size() * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_atom_off, atom_off.size() * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_idx, npts * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_point_atom, npts * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_u64, 3 * npts * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_u32, 3 * npts * sizeof(float)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_w, nla * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_t_idx, t_idx.size() * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_t_off, t_off.size() * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_t_ent, t_ent.size() * sizeof(int)));
   int* pt_orig_d = nullptr;
-  PSC_CUDA(ctx, cudaMalloc(&pt_orig_d, npts * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&pt_orig_d, npts * sizeof(int)));
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->nl_atom_off, atom_off.data(), atom_off.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->nl_idx, idx.data(), npts * sizeof(int), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->nl_point_atom, pt_atom.data(), npts * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -262,7 +262,7 @@ extern "C" int psc_projector_setup(psc_ctx* ctx, int natoms, const int* species,
   int rc = psc_nl_eval_u(ctx, npts, ctx->nl_idx, pt_orig_d, asp_d, xyz_d, radius, ctx->nl_u64, st);
   if (!rc) rc = psc_cast(ctx, PSC_F32, ctx->nl_u64, ctx->nl_u32, 3 * npts, st);
   PSC_CUDA(ctx, cudaStreamSynchronize(st));
-  cudaFree(pt_orig_d);
+  psc_dfree(pt_orig_d);
   cleanup();
   return rc;
 }

@@ -277,14 +277,14 @@ extern "C" int psc_pcg_poisson(psc_ctx* ctx, const double* rhs, double* x, int m
   const CgPlan pl = cg_plan(ctx);
   const int need = std::max((int)(pl.grid.x * pl.grid.y), PSC_RED_BLOCKS);
   if (ctx->cg_part_cap < need) {
-    cudaFree(ctx->cg_part);
+    psc_dfree(ctx->cg_part);
     ctx->cg_part = nullptr;
-    PSC_CUDA(ctx, cudaMalloc(&ctx->cg_part, 2 * (size_t)need * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->cg_part, 2 * (size_t)need * sizeof(double)));
     ctx->cg_part_cap = need;
   }
-  if (!ctx->cg_x) PSC_CUDA(ctx, cudaMalloc(&ctx->cg_x, n * sizeof(double)));
-  if (!ctx->cg_p2) PSC_CUDA(ctx, cudaMalloc(&ctx->cg_p2, n * sizeof(double)));
-  if (!ctx->cg_ro) PSC_CUDA(ctx, cudaMalloc(&ctx->cg_ro, CG_RO_SLOTS * sizeof(double)));
+  if (!ctx->cg_x) PSC_CUDA(ctx, psc_dmalloc(&ctx->cg_x, n * sizeof(double)));
+  if (!ctx->cg_p2) PSC_CUDA(ctx, psc_dmalloc(&ctx->cg_p2, n * sizeof(double)));
+  if (!ctx->cg_ro) PSC_CUDA(ctx, psc_dmalloc(&ctx->cg_ro, CG_RO_SLOTS * sizeof(double)));
   double* sc = ctx->scalars;
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->cg_x, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
   // r = rhs - A x

@@ -236,12 +236,12 @@ int psc_pcg_persistent(psc_ctx* ctx, const double* rhs, double* x, int maxit, do
   int per_sm = 0;
   PSC_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PNT, smem));
   if (per_sm < 1) return -1;
-  if (!ctx->cg_r) PSC_CUDA(ctx, cudaMalloc(&ctx->cg_r, n * sizeof(double)));
-  if (!ctx->cg_bar) PSC_CUDA(ctx, cudaMalloc(&ctx->cg_bar, 64 * sizeof(unsigned int)));
+  if (!ctx->cg_r) PSC_CUDA(ctx, psc_dmalloc(&ctx->cg_r, n * sizeof(double)));
+  if (!ctx->cg_bar) PSC_CUDA(ctx, psc_dmalloc(&ctx->cg_bar, 64 * sizeof(unsigned int)));
   if (ctx->cg_part_cap < G) {
-    cudaFree(ctx->cg_part);
+    psc_dfree(ctx->cg_part);
     ctx->cg_part = nullptr;
-    PSC_CUDA(ctx, cudaMalloc(&ctx->cg_part, 2 * (size_t)std::max(G, PSC_RED_BLOCKS) * sizeof(double)));
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->cg_part, 2 * (size_t)std::max(G, PSC_RED_BLOCKS) * sizeof(double)));
     ctx->cg_part_cap = std::max(G, PSC_RED_BLOCKS);
   }
   PSC_CUDA(ctx, cudaMemsetAsync(ctx->cg_bar, 0, 64 * sizeof(unsigned int), st));

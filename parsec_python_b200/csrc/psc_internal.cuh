@@ -137,6 +137,20 @@ struct psc_ctx {
 };
 
 // ---------------------------------------------------------------------------
+// device memory
+// ---------------------------------------------------------------------------
+// Context memory comes from CUDA's stream-ordered pool (legacy default
+// stream), whose release threshold is raised once per device so that freed
+// blocks stay in the pool: a process that runs many SCFs pays the cost of
+// mapping fresh device memory once, not at every context creation.
+cudaError_t psc_dmalloc_bytes(void** p, size_t bytes);
+void psc_dfree(void* p);
+template <typename T>
+inline cudaError_t psc_dmalloc(T** p, size_t bytes) {
+  return psc_dmalloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
+
+// ---------------------------------------------------------------------------
 // error plumbing
 // ---------------------------------------------------------------------------
 void psc_set_error(psc_ctx* ctx, const std::string& msg);

@@ -127,9 +127,9 @@ extern "C" int psc_numpy_sum(psc_ctx* ctx, const double* x, long n, double* out_
   const long nl = (long)lo.size();
   long *lo_d = nullptr, *len_d = nullptr;
   double* leaf_d = nullptr;
-  PSC_CUDA(ctx, cudaMalloc(&lo_d, nl * sizeof(long)));
-  PSC_CUDA(ctx, cudaMalloc(&len_d, nl * sizeof(long)));
-  PSC_CUDA(ctx, cudaMalloc(&leaf_d, nl * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&lo_d, nl * sizeof(long)));
+  PSC_CUDA(ctx, psc_dmalloc(&len_d, nl * sizeof(long)));
+  PSC_CUDA(ctx, psc_dmalloc(&leaf_d, nl * sizeof(double)));
   PSC_CUDA(ctx, cudaMemcpyAsync(lo_d, lo.data(), nl * sizeof(long), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(len_d, len.data(), nl * sizeof(long), cudaMemcpyHostToDevice, st));
   k_pw_leaf<<<std::max(1, (int)std::min<long>(1184, (nl + 127) / 128)), 128, 0, st>>>(x, lo_d, len_d, nl, leaf_d);
@@ -137,7 +137,7 @@ extern "C" int psc_numpy_sum(psc_ctx* ctx, const double* x, long n, double* out_
   k_pw_root<<<1, 32, 0, st>>>(n, leaf_d, out_dev);
   PSC_LAUNCH_CHECK(ctx);
   PSC_CUDA(ctx, cudaStreamSynchronize(st));
-  cudaFree(lo_d); cudaFree(len_d); cudaFree(leaf_d);
+  psc_dfree(lo_d); psc_dfree(len_d); psc_dfree(leaf_d);
   return 0;
 }
 
@@ -148,7 +148,7 @@ static int upload_spline_table(psc_ctx* ctx, psc_spline_dev** out) {
       const psc_species& sp = ctx->species[s];
       t[5 * s + f] = {sp.x[f], sp.z[f], sp.c[f], sp.d[f], sp.nk[f]};
     }
-  PSC_CUDA(ctx, cudaMalloc(out, t.size() * sizeof(psc_spline_dev)));
+  PSC_CUDA(ctx, psc_dmalloc(out, t.size() * sizeof(psc_spline_dev)));
   PSC_CUDA(ctx, cudaMemcpy(*out, t.data(), t.size() * sizeof(psc_spline_dev), cudaMemcpyHostToDevice));
   return 0;
 }
@@ -169,8 +169,8 @@ extern "C" int psc_sad_setup(psc_ctx* ctx, int natoms, const int* species, const
   if (upload_spline_table(ctx, &tab)) return 1;
   int* sp_d = nullptr;
   double* xyz_d = nullptr;
-  PSC_CUDA(ctx, cudaMalloc(&sp_d, natoms * sizeof(int)));
-  PSC_CUDA(ctx, cudaMalloc(&xyz_d, 3 * natoms * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&sp_d, natoms * sizeof(int)));
+  PSC_CUDA(ctx, psc_dmalloc(&xyz_d, 3 * natoms * sizeof(double)));
   PSC_CUDA(ctx, cudaMemcpyAsync(sp_d, species, natoms * sizeof(int), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(xyz_d, xyz, 3 * natoms * sizeof(double), cudaMemcpyHostToDevice, st));
   k_sad<<<148 * 8, 256, 0, st>>>(ctx->nx, ctx->ny, ctx->nz, ctx->h, radius, natoms, sp_d, xyz_d, tab, h3, fourpi,
@@ -187,7 +187,7 @@ extern "C" int psc_sad_setup(psc_ctx* ctx, int natoms, const int* species, const
   PSC_CUDA(ctx, cudaMemcpyAsync(&ctx->host_scalars[201], sum_d + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
   PSC_CUDA(ctx, cudaStreamSynchronize(st));
   if (info) { info[0] = ctx->host_scalars[200]; info[1] = ctx->host_scalars[201]; }
-  cudaFree(tab); cudaFree(sp_d); cudaFree(xyz_d);
+  psc_dfree(tab); psc_dfree(sp_d); psc_dfree(xyz_d);
   return 0;
 }
 
@@ -227,13 +227,13 @@ int psc_nl_box_distances(psc_ctx* ctx, int nbox, const int* box_dev, const doubl
   std::vector<double> rc(nbox);
   for (int i = 0; i < nbox; ++i) rc[i] = ctx->species[box[8 * i + 7]].rcut;
   double* rc_d = nullptr;
-  PSC_CUDA(ctx, cudaMalloc(&rc_d, nbox * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&rc_d, nbox * sizeof(double)));
   PSC_CUDA(ctx, cudaMemcpyAsync(rc_d, rc.data(), nbox * sizeof(double), cudaMemcpyHostToDevice, st));
   const int nb = (int)std::max<long>(1, std::min<long>(148L * 8, (total + 255) / 256));
   k_nl_box<<<nb, 256, 0, st>>>(nbox, box_dev, box_start_dev, total, xyz_dev, rc_d, ctx->h, radius, mask_dev);
   PSC_LAUNCH_CHECK(ctx);
   PSC_CUDA(ctx, cudaStreamSynchronize(st));
-  cudaFree(rc_d);
+  psc_dfree(rc_d);
   return 0;
 }
 
@@ -267,6 +267,6 @@ int psc_nl_eval_u(psc_ctx* ctx, long npts, const int* idx_dev, const int* pt_ato
                              radius, u_dev);
   PSC_LAUNCH_CHECK(ctx);
   PSC_CUDA(ctx, cudaStreamSynchronize(st));
-  cudaFree(tab);
+  psc_dfree(tab);
   return 0;
 }

@@ -9,9 +9,10 @@
 // a ring of NBUF = R + 1 + D shared-memory windows, completing on the slot's
 // mbarrier.  The z neighbours of each point live in a register queue fed from
 // the ring; x and y neighbours are read from the current plane's window with
-// 16-byte loads (each thread owns two adjacent x points).  Prev and pot for
-// the current plane arrive the same way in a second ring.  D planes are in
-// flight per CTA at all times, which is what keeps HBM busy.
+// 16-byte loads (each thread owns two adjacent x points; the pair itself comes
+// from the queue).  Prev and pot are read straight from global memory one
+// plane ahead, so they cost no shared-memory traffic.  D planes are in flight
+// per CTA at all times, which is what keeps HBM busy.
 //
 // Every mbarrier wait is bounded: on timeout the CTA records the failure in
 // status[3] and carries on without waiting (results are then garbage but the
@@ -101,15 +102,13 @@ __global__ void __launch_bounds__(TNT)
 k_stencil_tma(TmaArgs<T> A) {
   using V2 = typename Vec2<T>::type;
   constexpr int NBUF = R + 1 + TD;   // X plane windows resident
-  constexpr int PBUF = TD + 1;       // Prev/pot planes resident
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nx = A.nx, ny = A.ny, nz = A.nz;
   const int nxy = nx * ny;
   const int H = R * nx;
   const int WIN = TS + 2 * H;
   T* ring = reinterpret_cast<T*>(smem_raw);                 // [NBUF][WIN]
-  T* pring = ring + (size_t)NBUF * WIN;                     // [PBUF][2][TS]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(pring + (size_t)PBUF * 2 * TS);  // [NBUF + PBUF]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + (size_t)NBUF * WIN);  // [NBUF]
   __shared__ int s_fail;
 
   const int slab0 = blockIdx.x * TS;
@@ -131,7 +130,6 @@ k_stencil_tma(TmaArgs<T> A) {
   const int v0 = max(0, w0), v1 = min(nxy, slab0 + TS + H);
   const uint32_t xbytes = (uint32_t)((v1 - v0) * sizeof(T));
   const int seff = min(TS, nxy - slab0);
-  const uint32_t sbytes = (uint32_t)(seff * sizeof(T));
 
   // zero the parts of every window that lie outside the plane (never written by the copies)
   for (int s = 0; s < NBUF; ++s) {
@@ -141,10 +139,9 @@ k_stencil_tma(TmaArgs<T> A) {
       if (f < v0 || f >= v1) w[i] = T(0);
     }
   }
-  for (int i = threadIdx.x; i < PBUF * 2 * TS; i += TNT) pring[i] = T(0);
   if (threadIdx.x == 0) {
     s_fail = 0;
-    for (int i = 0; i < NBUF + PBUF; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i < NBUF; ++i) mbar_init(&bars[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -156,20 +153,8 @@ k_stencil_tma(TmaArgs<T> A) {
     mbar_expect_tx(bar, xbytes);
     bulk_g2s(ring + (size_t)s * WIN + (v0 - w0), Xc + (long)p * nxy + v0, xbytes, bar);
   };
-  auto issue_p = [&](int p) {  // Prev / pot of plane p (z0 <= p < z1)
-    const int s = (p - z0) % PBUF;
-    uint64_t* bar = &bars[NBUF + s];
-    const uint32_t bytes = (Pc ? sbytes : 0u) + (has_pot ? sbytes : 0u);
-    if (bytes == 0) return;
-    mbar_expect_tx(bar, bytes);
-    T* dst = pring + (size_t)s * 2 * TS;
-    if (Pc) bulk_g2s(dst, Pc + (long)p * nxy + slab0, sbytes, bar);
-    if (has_pot) bulk_g2s(dst + TS, A.pot + (long)p * nxy + slab0, sbytes, bar);
-  };
-
   if (threadIdx.x == 0) {
     for (int p = z0; p < min(zlast, z0 + NBUF); ++p) issue_x(p);
-    for (int p = z0; p < min(z1, z0 + PBUF); ++p) issue_p(p);
   }
 
   // own pair of points
@@ -178,6 +163,16 @@ k_stencil_tma(TmaArgs<T> A) {
   const int q = slab0 + loc;
   const int xi = own ? q % nx : 0;
   const int s_c = H + loc;  // window offset of the pair
+
+  // Prev and pot of the pair, one plane ahead in registers (P may alias Y:
+  // a point of P is read before this thread overwrites it)
+  V2 pv_next{T(0), T(0)}, po_next{T(0), T(0)};
+  auto load_pp = [&](int z) {
+    if (!own || z >= z1) return;
+    if (Pc) pv_next = *reinterpret_cast<const V2*>(Pc + (long)z * nxy + q);
+    if (has_pot) po_next = *reinterpret_cast<const V2*>(A.pot + (long)z * nxy + q);
+  };
+  load_pp(z0);
 
   // z queue from direct loads of the planes below the chunk
   T zq0[2 * R + 1], zq1[2 * R + 1];
@@ -243,25 +238,32 @@ k_stencil_tma(TmaArgs<T> A) {
       }
       zq0[(u + 2 * R) % Q] = f0;
       zq1[(u + 2 * R) % Q] = f1;
-      const int sp = (z - z0) % PBUF;
-      if (Pc || has_pot) {
-        if (!fail && !mbar_wait(&bars[NBUF + sp], ((z - z0) / PBUF) & 1)) fail = true;
-      }
+      const V2 pvv = pv_next, pov = po_next;
+      load_pp(z + 1);
       const T* pl = ring + (size_t)((z - z0) % NBUF) * WIN;
       if (own) {
         // x neighbours: window values s_c - R .. s_c + R + 1, fetched as aligned
-        // pairs starting at the even offset s_c - R - (R & 1)
+        // pairs starting at the even offset s_c - R - (R & 1); the pair itself
+        // (pair index CJ) is the queue's centre
         constexpr int NP = R + 1 + (R & 1);
+        constexpr int OFF = R + (R & 1);  // xs index of the pair's first point
+        constexpr int CJ = OFF / 2;
+        const T xc0 = zq0[(u + R) % Q], xc1 = zq1[(u + R) % Q];
         T xs[2 * NP];
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
-          const V2 v = *reinterpret_cast<const V2*>(pl + s_c - R - (R & 1) + 2 * j);
-          xs[2 * j] = v.x;
-          xs[2 * j + 1] = v.y;
+          if (j == CJ) {
+            xs[2 * j] = xc0;
+            xs[2 * j + 1] = xc1;
+          } else {
+            const V2 v = *reinterpret_cast<const V2*>(pl + s_c - R - (R & 1) + 2 * j);
+            xs[2 * j] = v.x;
+            xs[2 * j + 1] = v.y;
+          }
         }
-        constexpr int OFF = R + (R & 1);  // xs index of the pair's first point
-        const T xc0 = zq0[(u + R) % Q], xc1 = zq1[(u + R) % Q];
+        // two partial sums per point: y + z terms, x terms
         T acc0 = c0 * xc0, acc1 = c0 * xc1;
+        T ax0 = T(0), ax1 = T(0);
 #pragma unroll
         for (int d = 1; d <= R; ++d) {
           // rows outside the plane are zero in the window, so y needs no test
@@ -272,35 +274,32 @@ k_stencil_tma(TmaArgs<T> A) {
           const T t1 = (ym.y + yp.y) + (zq1[(u + R - d) % Q] + zq1[(u + R + d) % Q]);
           acc0 += cd * t0;
           acc1 += cd * t1;
-          acc0 += cl0[d - 1] * xs[OFF - d];
-          acc0 += cr0[d - 1] * xs[OFF + d];
-          acc1 += cl1[d - 1] * xs[OFF + 1 - d];
-          acc1 += cr1[d - 1] * xs[OFF + 1 + d];
+          ax0 += cl0[d - 1] * xs[OFF - d];
+          ax0 += cr0[d - 1] * xs[OFF + d];
+          ax1 += cl1[d - 1] * xs[OFF + 1 - d];
+          ax1 += cr1[d - 1] * xs[OFF + 1 + d];
         }
-        const T* pp = pring + (size_t)sp * 2 * TS;
+        acc0 += ax0;
+        acc1 += ax1;
         if (has_pot) {
-          const V2 pv = *reinterpret_cast<const V2*>(pp + TS + loc);
-          acc0 += pv.x * xc0;
-          acc1 += pv.y * xc1;
+          acc0 += pov.x * xc0;
+          acc1 += pov.y * xc1;
         }
         T o0 = ca * acc0 + cb * xc0;
         T o1 = ca * acc1 + cb * xc1;
         if (Pc) {
-          const V2 pv = *reinterpret_cast<const V2*>(pp + loc);
-          o0 += cg * pv.x;
-          o1 += cg * pv.y;
+          o0 += cg * pvv.x;
+          o1 += cg * pvv.y;
         }
         V2 o;
         o.x = o0;
         o.y = o1;
         *reinterpret_cast<V2*>(Yc + (long)z * nxy + q) = o;
       }
-      __syncthreads();  // slot of plane z and Prev slot sp are free
+      __syncthreads();  // slot of plane z is free
       if (threadIdx.x == 0) {
         const int pn = z + NBUF;
         if (pn < zlast) issue_x(pn);
-        const int pq = z + PBUF;
-        if (pq < z1) issue_p(pq);
       }
     }
   }
@@ -335,9 +334,9 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   const int zmin = std::min(ctx->nz, 8);
   if (zchunk < zmin) zchunk = zmin;
   nzc = (ctx->nz + zchunk - 1) / zchunk;
-  constexpr int NBUF = R + 1 + TD, PBUF = TD + 1;
+  constexpr int NBUF = R + 1 + TD;
   const size_t win = TS + 2 * (size_t)R * ctx->nx;
-  const size_t smem = (NBUF * win + PBUF * 2 * TS) * sizeof(T) + (NBUF + PBUF) * sizeof(uint64_t);
+  const size_t smem = NBUF * win * sizeof(T) + NBUF * sizeof(uint64_t);
   if (smem > 220 * 1024) return -1;  // window too wide: the register-queue kernel takes it
   auto kern = k_stencil_tma<T, R>;
   PSC_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -54,18 +54,20 @@ __device__ __forceinline__ uint4 vin8(const __nv_bfloat16* A, const __nv_bfloat1
 }
 
 constexpr int FWD_NT = 128;
+constexpr float LEAK = 0.0625f;   // leaky-ReLU slope below zero
 constexpr int WTILE = 256;   // weights staged per tap: input-chunk x output-chunk = 256 floats (27 KB for 27 taps)
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // forward: out[o][co] = act(b[co] + sum_tap sum_ci vin(o s + tap - pad)[ci] W[tap][ci][co])
+// act: 0 identity, 1 ReLU, 2 leaky ReLU (slope 1/16 below zero).
 // One thread per output voxel, COT output channels per CTA (blockIdx.y).
 // ---------------------------------------------------------------------------
 template <int COT>
 __global__ void __launch_bounds__(FWD_NT)
 k_conv_fwd(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ S,
-           const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias, ConvGeom g, int relu,
+           const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias, ConvGeom g, int act,
            __nv_bfloat16* __restrict__ out, float* __restrict__ out32) {
   constexpr int CIN_CHUNK = WTILE / COT;
   __shared__ __align__(16) float ws[27 * WTILE];
@@ -122,7 +124,8 @@ k_conv_fwd(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict_
   if (!valid) return;
 #pragma unroll
   for (int j = 0; j < COT; ++j) {
-    const float v = relu ? fmaxf(acc[j], 0.0f) : acc[j];
+    const float a = acc[j];
+    const float v = act == 1 ? fmaxf(a, 0.0f) : (act == 2 ? (a > 0.0f ? a : LEAK * a) : a);
     out[vo * g.Cout + co0 + j] = __float2bfloat16_rn(v);
     if (out32) out32[vo * g.Cout + co0 + j] = v;
   }
@@ -296,11 +299,12 @@ k_bias_partial(const float* __restrict__ gm, long nvo, int Cout, int vchunk, flo
   }
 }
 
-// gm = g * (out > 0) (ReLU backward; out is the BF16 activation)
+// gm = g * act'(pre) from the BF16 activation (out > 0 exactly when pre > 0):
+// 1 above zero, 0 (ReLU) or the leak slope (leaky ReLU) below
 __global__ void k_relu_grad(const float* __restrict__ gin, const __nv_bfloat16* __restrict__ out, long n,
-                            float* __restrict__ gm) {
+                            float below, float* __restrict__ gm) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    gm[i] = __bfloat162float(out[i]) > 0.0f ? gin[i] : 0.0f;
+    gm[i] = __bfloat162float(out[i]) > 0.0f ? gin[i] : below * gin[i];
 }
 
 // Split the virtual-input gradient: dA (+)= pool(dvin[:, :Ca]) (sum over the
@@ -431,10 +435,11 @@ int geom_from(psc_ctx* ctx, const int* gi, ConvGeom& g) {
 }  // namespace
 
 extern "C" int psc_conv3d_fwd(psc_ctx* ctx, const int* geom, const void* A, const void* S, const void* W,
-                              const float* bias, int relu, void* out, float* out32, void* stream) {
+                              const float* bias, int act, void* out, float* out32, void* stream) {
   if (!ctx) return 2;
   ConvGeom g;
   if (int rc = geom_from(ctx, geom, g)) return rc;
+  PSC_REQUIRE(ctx, act >= 0 && act <= 2, "conv3d_fwd: act must be 0 (identity), 1 (ReLU) or 2 (leaky ReLU)");
   PSC_REQUIRE(ctx, A && W && bias && out && (g.Cs == 0 || S), "conv3d_fwd: NULL pointer");
   cudaStream_t st = (cudaStream_t)stream;
   const long nvo = (long)g.nxo * g.nyo * g.nzo;
@@ -444,22 +449,23 @@ extern "C" int psc_conv3d_fwd(psc_ctx* ctx, const int* geom, const void* A, cons
   auto* o = static_cast<__nv_bfloat16*>(out);
   if (g.Cout % 16 == 0) {
     dim3 grid(psc_div_up(nvo, FWD_NT), g.Cout / 16);
-    k_conv_fwd<16><<<grid, FWD_NT, 0, st>>>(a, s, w, bias, g, relu, o, out32);
+    k_conv_fwd<16><<<grid, FWD_NT, 0, st>>>(a, s, w, bias, g, act, o, out32);
   } else {
     dim3 grid(psc_div_up(nvo, FWD_NT), g.Cout / 8);
-    k_conv_fwd<8><<<grid, FWD_NT, 0, st>>>(a, s, w, bias, g, relu, o, out32);
+    k_conv_fwd<8><<<grid, FWD_NT, 0, st>>>(a, s, w, bias, g, act, o, out32);
   }
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }
 
 extern "C" int psc_conv3d_bwd(psc_ctx* ctx, const int* geom, const void* A, const void* S, const void* W,
-                              const float* gout, const void* out, float* gm, float* dvin, float* dA, int acc_a,
-                              float* dS, int acc_s, float* dW, float* dB, float* work, long work_floats,
+                              const float* gout, const void* out, int act, float* gm, float* dvin, float* dA,
+                              int acc_a, float* dS, int acc_s, float* dW, float* dB, float* work, long work_floats,
                               void* stream) {
   if (!ctx) return 2;
   ConvGeom g;
   if (int rc = geom_from(ctx, geom, g)) return rc;
+  PSC_REQUIRE(ctx, act >= 0 && act <= 2 && (act == 0 || out), "conv3d_bwd: bad activation arguments");
   PSC_REQUIRE(ctx, A && W && gout && gm && dW && dB && work && (g.Cs == 0 || S), "conv3d_bwd: NULL pointer");
   cudaStream_t st = (cudaStream_t)stream;
   const long nvo = (long)g.nxo * g.nyo * g.nzo;
@@ -468,9 +474,10 @@ extern "C" int psc_conv3d_bwd(psc_ctx* ctx, const int* geom, const void* A, cons
   const auto* a = static_cast<const __nv_bfloat16*>(A);
   const auto* s = static_cast<const __nv_bfloat16*>(S);
   const auto* w = static_cast<const __nv_bfloat16*>(W);
-  // 1. masked output gradient (ReLU backward when `out` is given)
-  if (out) {
-    k_relu_grad<<<148 * 8, 256, 0, st>>>(gout, static_cast<const __nv_bfloat16*>(out), nvo * g.Cout, gm);
+  // 1. output gradient through the activation
+  if (act != 0) {
+    k_relu_grad<<<148 * 8, 256, 0, st>>>(gout, static_cast<const __nv_bfloat16*>(out), nvo * g.Cout,
+                                         act == 2 ? LEAK : 0.0f, gm);
     PSC_LAUNCH_CHECK(ctx);
   } else if (gm != gout) {
     PSC_CUDA(ctx, cudaMemcpyAsync(gm, gout, nvo * g.Cout * sizeof(float), cudaMemcpyDeviceToDevice, st));

@@ -12,6 +12,7 @@ with no trained weights the solver runs from SAD.
 Network (1.29 M parameters; channels-last BF16 activations, BF16 weights,
 FP32 accumulation; all kernels in csrc/unet.cu):
 
+    (leaky ReLU after every layer but the last)
     e0  3^3  8 -> 8           full grid           (input: rho_SAD, V_loc, 6 zero channels)
     d1  3^3  8 -> 32  /2      half
     e1  3^3  32 -> 32         half
@@ -58,21 +59,21 @@ class Layer:
     cout: int
     stride: int
     ksize: int
-    relu: bool
+    act: int          # 0 identity, 2 leaky ReLU
 
 
 LAYERS = (
-    Layer("e0", "in", 0, None, 8, 0, 8, 1, 3, True),
-    Layer("d1", "e0", 0, None, 8, 0, 32, 2, 3, True),
-    Layer("e1", "d1", 0, None, 32, 0, 32, 1, 3, True),
-    Layer("d2", "e1", 0, None, 32, 0, 64, 2, 3, True),
-    Layer("e2", "d2", 0, None, 64, 0, 64, 1, 3, True),
-    Layer("d3", "e2", 0, None, 64, 0, 128, 2, 3, True),
-    Layer("b", "d3", 0, None, 128, 0, 128, 1, 3, True),
-    Layer("u2", "b", 1, "e2", 128, 64, 64, 1, 3, True),
-    Layer("u1", "u2", 1, "e1", 64, 32, 32, 1, 3, True),
-    Layer("u0", "u1", 1, "e0", 32, 8, 8, 1, 3, True),
-    Layer("out", "u0", 0, None, 8, 0, 8, 1, 1, False),
+    Layer("e0", "in", 0, None, 8, 0, 8, 1, 3, 2),
+    Layer("d1", "e0", 0, None, 8, 0, 32, 2, 3, 2),
+    Layer("e1", "d1", 0, None, 32, 0, 32, 1, 3, 2),
+    Layer("d2", "e1", 0, None, 32, 0, 64, 2, 3, 2),
+    Layer("e2", "d2", 0, None, 64, 0, 64, 1, 3, 2),
+    Layer("d3", "e2", 0, None, 64, 0, 128, 2, 3, 2),
+    Layer("b", "d3", 0, None, 128, 0, 128, 1, 3, 2),
+    Layer("u2", "b", 1, "e2", 128, 64, 64, 1, 3, 2),
+    Layer("u1", "u2", 1, "e1", 64, 32, 32, 1, 3, 2),
+    Layer("u0", "u1", 1, "e0", 32, 8, 8, 1, 3, 2),
+    Layer("out", "u0", 0, None, 8, 0, 8, 1, 1, 0),
 )
 
 
@@ -170,7 +171,7 @@ class UNet3D:
             if l.name == "out":
                 out32 = torch.empty(self._nvox(l.name), l.cout, dtype=torch.float32, device=self.dev)
             self.ctx.call("psc_conv3d_fwd", self._geom(l), gpu._p(a), gpu._p(s), gpu._p(wv), gpu._p(bias),
-                          int(l.relu), gpu._p(y), gpu._p(out32 if l.name == "out" else None), gpu._stream())
+                          l.act, gpu._p(y), gpu._p(out32 if l.name == "out" else None), gpu._stream())
             self.acts[l.name] = y
         return out32
 
@@ -205,7 +206,7 @@ class UNet3D:
             dW, dB = self._wviews(l, self.grad)
             wv, _ = self._wviews(l, self.wb)
             self.ctx.call("psc_conv3d_bwd", self._geom(l), gpu._p(a), gpu._p(s), gpu._p(wv), gpu._p(g),
-                          gpu._p(self.acts[l.name] if l.relu else None), gpu._p(gm), gpu._p(dvin), gpu._p(dA),
+                          gpu._p(self.acts[l.name] if l.act else None), l.act, gpu._p(gm), gpu._p(dvin), gpu._p(dA),
                           acc_a, gpu._p(dS), acc_s, gpu._p(dW), gpu._p(dB), gpu._p(self.work), self.WORK_FLOATS,
                           gpu._stream())
 
@@ -265,6 +266,9 @@ class LearnedInit:
         h3 = ctx.h ** 3
         rho_b = rho0 / h3
         delta = self.net.predict_delta(rho_b, ppot)
+        if not bool(torch.isfinite(delta).all()):
+            self.last = {"fallback": "non-finite prediction"}
+            return rho0, hpot0
         rho1 = torch.clamp(rho_b + delta, min=0.0) * h3
         zsum = gpu.numpy_sum(ctx, rho0)
         rho1 = rho1 * (zsum / gpu.numpy_sum(ctx, rho1))
@@ -324,13 +328,16 @@ def make_sample(seed: int):
     return ctx, rho_sad, ppot.clone(), (res.rho - rho_sad).float(), res
 
 
-def train(n_train: int, epochs: int, out: Path, lr: float = 2e-3, seed: int = 0, log=print) -> dict:
+TRAIN_SEEDS = 512        # geometries 0..511 train the network; 512.. are held out
+
+
+def train(n_train: int, epochs: int, out: Path, lr: float = 2e-4, seed: int = 0, log=print) -> dict:
     t_data = time.perf_counter()
     samples = []
     ctx0 = None
     skipped = []
     sd = 0
-    while len(samples) < n_train:
+    while len(samples) < n_train and sd < TRAIN_SEEDS:
         try:
             ctx, rs, vl, dt, res = make_sample(sd)
         except ValueError as exc:   # e.g. the reference's "Bounds are incorrect" stop in chefsi1
@@ -346,6 +353,7 @@ def train(n_train: int, epochs: int, out: Path, lr: float = 2e-3, seed: int = 0,
         sd += 1
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t_data
+    n_train = len(samples)
     # fixed input / target scales from the training set
     a0 = 1.0 / float(torch.stack([s[0].std() for s in samples]).mean())
     a1 = 1.0 / float(torch.stack([s[1].std() for s in samples]).mean())
@@ -367,8 +375,10 @@ def train(n_train: int, epochs: int, out: Path, lr: float = 2e-3, seed: int = 0,
             loss, g = net.loss_and_grad(out32, ts[i])
             ep_loss += loss
             net.backward(g)
-            # cosine decay over the run
-            lr_t = lr * 0.5 * (1 + np.cos(np.pi * net.step_count / steps))
+            # linear warm-up over the first 10 % of the steps, then cosine decay
+            st = net.step_count
+            warm = max(1, steps // 10)
+            lr_t = lr * (st + 1) / warm if st < warm else lr * 0.5 * (1 + np.cos(np.pi * (st - warm) / (steps - warm)))
             net.adam(lr_t)
         losses.append(float(ep_loss.item()) / n_train)
         log(f"  epoch {ep}: mean loss {losses[-1]:.4e} (relative to the target variance)")
@@ -399,15 +409,21 @@ def evaluate(seeds, weights: Path, log=print) -> dict:
             continue
         e_sad, e_ml = r_sad.history[-1]["total_ry"], r_ml.history[-1]["total_ry"]
         rows.append({"seed": sd, "its_sad": r_sad.iterations, "its_learned": r_ml.iterations, "t_sad": t_sad,
-                     "t_learned": t_ml, "e_sad_ry": e_sad, "e_learned_ry": e_ml, "de_ha": abs(e_sad - e_ml) / 2})
+                     "t_learned": t_ml, "e_sad_ry": e_sad, "e_learned_ry": e_ml, "de_ha": abs(e_sad - e_ml) / 2,
+                     "converged": bool(r_sad.converged and r_ml.converged)})
         log(f"  seed {sd}: SAD {r_sad.iterations} its {t_sad:.3f}s, learned {r_ml.iterations} its {t_ml:.3f}s, "
             f"|dE| {rows[-1]['de_ha']:.2e} Ha")
+    # energies are compared where both runs converged; the iteration and time
+    # means are over all seeds
+    conv = [r for r in rows if r["converged"]]
     its_s = np.array([r["its_sad"] for r in rows])
     its_l = np.array([r["its_learned"] for r in rows])
     summary = {"n": len(rows), "mean_its_sad": float(its_s.mean()), "mean_its_learned": float(its_l.mean()),
                "mean_t_sad": float(np.mean([r["t_sad"] for r in rows])),
                "mean_t_learned": float(np.mean([r["t_learned"] for r in rows])),
-               "max_de_ha": float(max(r["de_ha"] for r in rows)), "skipped": skipped, "rows": rows}
+               "n_converged_both": len(conv),
+               "max_de_ha": float(max(r["de_ha"] for r in conv)) if conv else None,
+               "not_converged": [r["seed"] for r in rows if not r["converged"]], "skipped": skipped, "rows": rows}
     return summary
 
 
@@ -417,7 +433,7 @@ def main(argv=None):
     t = sub.add_parser("train")
     t.add_argument("--n-train", type=int, default=512)
     t.add_argument("--epochs", type=int, default=12)
-    t.add_argument("--lr", type=float, default=2e-3)
+    t.add_argument("--lr", type=float, default=2e-4)
     t.add_argument("--out", type=Path, default=DEFAULT_WEIGHTS)
     e = sub.add_parser("eval")
     e.add_argument("--first", type=int, default=512)

@@ -54,6 +54,7 @@ class SolverSettings:
     precision: str = "fp64"      # fp64 | mixed
     init: str = "sad"            # sad | learned
     seed: int = 0
+    mixed_switch: float = 1e-4   # mixed precision: FP64 subspace blocks once the SCF error is below this
 
     _KEYS = {
         "fd_order": ("fd_order", int), "maxits": ("maxits", int), "tol": ("tol", _parse_tol),
@@ -63,7 +64,7 @@ class SolverSettings:
         "adaptive_scheme": ("adaptive_scheme", int), "use_gpu": ("use_gpu", _parse_bool),
         "gpu": ("use_gpu", _parse_bool), "recenter_atoms": ("recenter_atoms", _parse_bool),
         "recenter": ("recenter_atoms", _parse_bool), "precision": ("precision", str),
-        "init": ("init", str), "seed": ("seed", int),
+        "init": ("init", str), "seed": ("seed", int), "mixed_switch": ("mixed_switch", float),
     }
 
     def normalize(self) -> None:
@@ -86,6 +87,7 @@ class SolverSettings:
         self.init = str(self.init).lower()
         if self.init not in ("sad", "learned"):
             self.init = "sad"
+        self.mixed_switch = float(self.mixed_switch)
 
     def apply_overrides(self, overrides: dict[str, Any] | None) -> dict[str, Any]:
         """Apply known keys (case-insensitive), drop unknown ones, return what changed."""

@@ -86,6 +86,14 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
     e_nuc0 = gpu.nuclear(atoms, elem)
     stage("Ion-ion repulsion setup", t0)
 
+    if init_density is None and s.init == "learned":
+        from . import learned
+
+        params = learned.load_weights()
+        if params is not None:
+            init_density = learned.LearnedInit(params)
+        else:
+            say("No trained density network found: using the SAD initial density.")
     t0 = time.perf_counter()
     rho0, hpot0, ppot, diag_info = backend.pseudo_diag(dom, atoms, elem, n_elements, return_info=True)
     if init_density is not None:
@@ -151,6 +159,9 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         say(f"  Working ... SCF iter # {its} ... ")
         ev = _Events()
         H.set_potential(pot)
+        if W is not None and W.dtype == torch.float32 and err <= s.mixed_switch:
+            # mixed precision: the last iterations run with FP64 subspace blocks
+            W = W.double()
         ev.mark("d0")
         deg = _scaled_poldeg(s.poldeg, deg_mod)
         if its == 1 and s.diagmeth == 3:
@@ -197,7 +208,8 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         diag_t, hart_t = ev.seconds("d0", "d1"), ev.seconds("h0", "h1")
         rec = {"iter": its, "err": err, "total_ry": energies.total_ry, "eigen_sum_ry": energies.eigen_sum_ry,
                "hartree_ry": energies.hartree_ry, "xc_ry": energies.xc_ry, "lam": lam_h, "occ": occ_h,
-               "cg_its": cg_its, "diag_s": diag_t, "hartree_s": hart_t, "iter_s": ev.seconds("d0", "end")}
+               "cg_its": cg_its, "diag_s": diag_t, "hartree_s": hart_t, "iter_s": ev.seconds("d0", "end"),
+               "block_dtype": "f32" if W.dtype == torch.float32 else "f64"}
         history.append(rec)
         if on_iteration:
             on_iteration(rec)

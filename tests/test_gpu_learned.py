@@ -38,19 +38,20 @@ def _torch_weight(w, k, cin, cout):
 
 
 CASES = [
-    # name, grid_in, up, Ca, Cs, Cout, stride, ksize, relu
-    ("s1", (11, 9, 7), 0, 8, 0, 16, 1, 3, True),
-    ("s2-odd", (11, 9, 7), 0, 8, 0, 32, 2, 3, True),
-    ("s2-even", (12, 10, 8), 0, 16, 0, 8, 2, 3, False),
-    ("up-skip", (11, 9, 7), 1, 16, 8, 8, 1, 3, True),
-    ("up-skip-wide", (10, 7, 9), 1, 32, 16, 32, 1, 3, True),
-    ("1x1", (9, 8, 7), 0, 8, 0, 8, 1, 1, False),
+    # name, grid_in, up, Ca, Cs, Cout, stride, ksize, act (0 identity, 1 ReLU, 2 leaky ReLU)
+    ("s1", (11, 9, 7), 0, 8, 0, 16, 1, 3, 1),
+    ("s2-odd", (11, 9, 7), 0, 8, 0, 32, 2, 3, 2),
+    ("s2-even", (12, 10, 8), 0, 16, 0, 8, 2, 3, 0),
+    ("up-skip", (11, 9, 7), 1, 16, 8, 8, 1, 3, 1),
+    ("up-skip-wide", (10, 7, 9), 1, 32, 16, 32, 1, 3, 2),
+    ("1x1", (9, 8, 7), 0, 8, 0, 8, 1, 1, 0),
 ]
+LEAK = 0.0625
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
 def test_conv3d_forward_backward_match_float64_oracle(case):
-    name, gi, up, ca, cs, cout, stride, k, relu = case
+    name, gi, up, ca, cs, cout, stride, k, act = case
     ctx = _ctx()
     rng = np.random.default_rng(sum(map(ord, name)))
     ga = tuple((x + 1) // 2 for x in gi) if up else gi
@@ -66,7 +67,7 @@ def test_conv3d_forward_backward_match_float64_oracle(case):
     ad, sd, wd, bd = a.to(DEV), (s.to(DEV) if s is not None else None), w.to(DEV), b.to(DEV)
     y = torch.empty(nvo, cout, dtype=bf, device=DEV)
     y32 = torch.empty(nvo, cout, dtype=torch.float32, device=DEV)
-    ctx.call("psc_conv3d_fwd", geom, gpu._p(ad), gpu._p(sd), gpu._p(wd), gpu._p(bd), int(relu), gpu._p(y),
+    ctx.call("psc_conv3d_fwd", geom, gpu._p(ad), gpu._p(sd), gpu._p(wd), gpu._p(bd), act, gpu._p(y),
              gpu._p(y32), gpu._stream())
     # float64 oracle on the same BF16 values
     A = _to_ncdhw(a.double(), ga, ca).requires_grad_(True)
@@ -80,15 +81,16 @@ def test_conv3d_forward_backward_match_float64_oracle(case):
     Wt = _torch_weight(w.double(), k, cin, cout).requires_grad_(True)
     Bt = b.double().requires_grad_(True)
     pre = F.conv3d(x, Wt, Bt, stride=stride, padding=k // 2)
-    ref = torch.relu(pre) if relu else pre
+    ref = {0: pre, 1: torch.relu(pre), 2: torch.where(pre > 0, pre, LEAK * pre)}[act]
     ref_flat = _from_ncdhw(ref).detach()
     got = y32.double().cpu()
     assert (got - ref_flat).abs().max() <= 2e-5 * max(1.0, ref_flat.abs().max().item())
     # BF16 output is the FP32 result rounded
     assert torch.equal(y.cpu(), y32.cpu().to(bf))
-    # backward against autograd, with the ReLU mask taken from the kernel's own output
+    # backward against autograd, with the activation's slope taken from the kernel's own output
     R = torch.from_numpy(rng.standard_normal((nvo, cout)).astype(np.float32))
-    mask = (y.cpu().float() > 0).double() if relu else torch.ones(nvo, cout, dtype=torch.float64)
+    below = {0: 1.0, 1: 0.0, 2: LEAK}[act]
+    mask = torch.where(y.cpu().float() > 0, 1.0, below).double() if act else torch.ones(nvo, cout, dtype=torch.float64)
     g_pre = _to_ncdhw(R.double() * mask, go, cout)
     pre.backward(g_pre)
     gm = torch.empty(nvo, cout, dtype=torch.float32, device=DEV)
@@ -99,7 +101,7 @@ def test_conv3d_forward_backward_match_float64_oracle(case):
     dB = torch.empty(cout, dtype=torch.float32, device=DEV)
     work = torch.empty(4 * 1024 * 1024, dtype=torch.float32, device=DEV)
     ctx.call("psc_conv3d_bwd", geom, gpu._p(ad), gpu._p(sd), gpu._p(wd), gpu._p(R.to(DEV)),
-             gpu._p(y if relu else None), gpu._p(gm), gpu._p(dvin), gpu._p(dA), 1, gpu._p(dS), 0, gpu._p(dW),
+             gpu._p(y if act else None), act, gpu._p(gm), gpu._p(dvin), gpu._p(dA), 1, gpu._p(dS), 0, gpu._p(dW),
              gpu._p(dB), gpu._p(work), work.numel(), gpu._stream())
 
     def close(got, ref, tol=2e-5):
@@ -157,5 +159,6 @@ def test_learned_init_saves_iterations_on_held_out_water_clusters():
     if params is None:
         pytest.skip("no trained weights in parsec_python_b200/data")
     summ = learned.evaluate([600, 601], learned.DEFAULT_WEIGHTS, log=lambda *a: None)
+    assert summ["n_converged_both"] == 2
     assert summ["max_de_ha"] < 1e-5
     assert summ["mean_its_learned"] < summ["mean_its_sad"]
