@@ -259,9 +259,9 @@ def mixed_leg(target, steps: int = 3) -> dict:
 
 def learned_leg(seeds=(512, 513, 514, 515)) -> dict | None:
     """Learned initial density on held-out water clusters (the network is
-    trained on seeds 0..; these seeds are not in its training set): SCF
-    iterations and time from SAD and from the network's density, same input,
-    tol 1e-6; None when no trained weights are present."""
+    trained on geometries 0..511): SCF iterations and time to 1e-5 Ha of the
+    geometry's tol-1e-8 energy, from SAD and from the network's density;
+    None when no trained weights are present."""
     from parsec_python_b200 import learned
 
     if learned.load_weights() is None:

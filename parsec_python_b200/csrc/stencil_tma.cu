@@ -6,7 +6,7 @@
 // z planes.  For every plane the points it needs -- its own S points plus R
 // rows of y halo on each side -- are one contiguous range of the plane, so a
 // single cp.async.bulk (no tensor map, no multicast) moves it into a slot of
-// a ring of NBUF = R + 1 + D shared-memory windows, completing on the slot's
+// a ring of NBUF = R + 1 + D shared-memory windows (D = 3 FP64, 4 FP32), completing on the slot's
 // mbarrier.  The z neighbours of each point live in a register queue fed from
 // the ring; x and y neighbours are read from the current plane's window with
 // 16-byte loads (each thread owns two adjacent x points; the pair itself comes
@@ -22,12 +22,17 @@
 #include "../../include/psc.h"
 
 #include <cstdint>
+#include <type_traits>
 
 namespace {
 
 constexpr int TNT = 256;          // threads per CTA
-constexpr int TS = 2 * TNT;       // points per slab (two per thread)
-constexpr int TD = 2;             // planes prefetched beyond the one consumed next
+// planes prefetched beyond the one consumed next: deeper for FP32, whose
+// planes are consumed twice as fast
+template <typename T>
+__host__ __device__ constexpr int prefetch_depth() {
+  return sizeof(T) == 8 ? 3 : 4;
+}
 constexpr long WAIT_LIMIT = 1L << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -68,16 +73,63 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
+// 16-byte vectors: two FP64 or four FP32 points per thread
 template <typename T>
-struct Vec2;
+struct VecOf;
 template <>
-struct Vec2<double> {
+struct VecOf<double> {
   using type = double2;
+  static constexpr int W = 2;
 };
 template <>
-struct Vec2<float> {
-  using type = float2;
+struct VecOf<float> {
+  using type = float4;
+  static constexpr int W = 4;
 };
+
+template <typename T>
+__device__ __forceinline__ void vload(const T* p, T* out) {
+  using V = typename VecOf<T>::type;
+  const V v = *reinterpret_cast<const V*>(p);
+  const T* e = reinterpret_cast<const T*>(&v);
+#pragma unroll
+  for (int j = 0; j < VecOf<T>::W; ++j) out[j] = e[j];
+}
+
+template <typename T>
+__device__ __forceinline__ void vstore(T* p, const T* in) {
+  using V = typename VecOf<T>::type;
+  V v;
+  T* e = reinterpret_cast<T*>(&v);
+#pragma unroll
+  for (int j = 0; j < VecOf<T>::W; ++j) e[j] = in[j];
+  *reinterpret_cast<V*>(p) = v;
+}
+
+// load VW consecutive values from an address aligned to A elements (A | VW)
+template <typename T, int A>
+__device__ __forceinline__ void vload_a(const T* p, T* out) {
+  constexpr int VW = VecOf<T>::W;
+  if constexpr (A == VW) {
+    vload(p, out);
+  } else if constexpr (A == 2) {
+    using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+#pragma unroll
+    for (int h = 0; h < VW / 2; ++h) {
+      const V2 v = *reinterpret_cast<const V2*>(p + 2 * h);
+      out[2 * h] = v.x;
+      out[2 * h + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < VW; ++j) out[j] = p[j];
+  }
+}
+
+template <typename T>
+__host__ __device__ constexpr int slab_points() {
+  return VecOf<T>::W * TNT;
+}
 
 template <typename T>
 struct TmaArgs {
@@ -97,17 +149,24 @@ struct TmaArgs {
 
 }  // namespace
 
-template <typename T, int R>
+// YA: alignment (in elements) of the y-neighbour rows, the largest of VW, 2, 1
+// that divides nx; their loads are split to match.
+template <typename T, int R, int YA>
 __global__ void __launch_bounds__(TNT)
 k_stencil_tma(TmaArgs<T> A) {
-  using V2 = typename Vec2<T>::type;
-  constexpr int NBUF = R + 1 + TD;   // X plane windows resident
+  constexpr int VW = VecOf<T>::W;          // points per thread
+  constexpr int TS = slab_points<T>();     // points per slab
+  constexpr int NBUF = R + 1 + prefetch_depth<T>();   // X plane windows resident
+  constexpr int Q = 2 * R + 1;             // z queue length
+  constexpr int HV = (R + VW - 1) / VW;    // x-halo vectors on each side
+  constexpr int NPV = 2 * HV + 1;          // x vectors per row (the centre one comes from the queue)
+  constexpr int OFF = HV * VW;             // xs index of the thread's first point
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nx = A.nx, ny = A.ny, nz = A.nz;
   const int nxy = nx * ny;
   const int H = R * nx;
   const int WIN = TS + 2 * H;
-  T* ring = reinterpret_cast<T*>(smem_raw);                 // [NBUF][WIN]
+  T* ring = reinterpret_cast<T*>(smem_raw);                                  // [NBUF][WIN]
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + (size_t)NBUF * WIN);  // [NBUF]
   __shared__ int s_fail;
 
@@ -157,39 +216,39 @@ k_stencil_tma(TmaArgs<T> A) {
     for (int p = z0; p < min(zlast, z0 + NBUF); ++p) issue_x(p);
   }
 
-  // own pair of points
-  const int loc = 2 * threadIdx.x;
+  // own run of VW points (it may cross a row boundary: every point has its own x)
+  const int loc = VW * threadIdx.x;
   const bool own = loc < seff;
   const int q = slab0 + loc;
-  const int xi = own ? q % nx : 0;
-  const int s_c = H + loc;  // window offset of the pair
+  const int s_c = H + loc;  // window offset of the run
 
-  // Prev and pot of the pair, one plane ahead in registers (P may alias Y:
+  // Prev and pot of the run, one plane ahead in registers (P may alias Y:
   // a point of P is read before this thread overwrites it)
-  V2 pv_next{T(0), T(0)}, po_next{T(0), T(0)};
+  T pv_next[VW], po_next[VW];
+#pragma unroll
+  for (int j = 0; j < VW; ++j) pv_next[j] = po_next[j] = T(0);
   auto load_pp = [&](int z) {
     if (!own || z >= z1) return;
-    if (Pc) pv_next = *reinterpret_cast<const V2*>(Pc + (long)z * nxy + q);
-    if (has_pot) po_next = *reinterpret_cast<const V2*>(A.pot + (long)z * nxy + q);
+    if (Pc) vload(Pc + (long)z * nxy + q, pv_next);
+    if (has_pot) vload(A.pot + (long)z * nxy + q, po_next);
   };
   load_pp(z0);
 
-  // z queue from direct loads of the planes below the chunk
-  T zq0[2 * R + 1], zq1[2 * R + 1];
+  // z queue: planes below the chunk from global memory, z0 .. z0+R-1 from the ring
+  T zq[VW][Q];
 #pragma unroll
   for (int i = 0; i < 2 * R; ++i) {
     const int zz = z0 - R + i;
-    zq0[i] = zq1[i] = T(0);
-    if (zz < z0) {
-      if (own && zz >= 0) {
-        const V2 v = *reinterpret_cast<const V2*>(Xc + (long)zz * nxy + q);
-        zq0[i] = v.x;
-        zq1[i] = v.y;
-      }
+#pragma unroll
+    for (int j = 0; j < VW; ++j) zq[j][i] = T(0);
+    if (zz < z0 && own && zz >= 0) {
+      T v[VW];
+      vload(Xc + (long)zz * nxy + q, v);
+#pragma unroll
+      for (int j = 0; j < VW; ++j) zq[j][i] = v[j];
     }
   }
   bool fail = false;
-  // planes z0 .. z0+R-1 enter the queue from the ring
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     const int p = z0 + i;
@@ -197,27 +256,29 @@ k_stencil_tma(TmaArgs<T> A) {
       const int s = (p - z0) % NBUF;
       if (!fail && !mbar_wait(&bars[s], ((p - z0) / NBUF) & 1)) fail = true;
       if (own) {
-        const V2 v = *reinterpret_cast<const V2*>(ring + (size_t)s * WIN + s_c);
-        zq0[R + i] = v.x;
-        zq1[R + i] = v.y;
+        T v[VW];
+        vload(ring + (size_t)s * WIN + s_c, v);
+#pragma unroll
+        for (int j = 0; j < VW; ++j) zq[j][R + i] = v[j];
       }
     }
   }
 
-  // per-thread x-boundary weights: a neighbour across the row edge gets 0
-  T cl0[R], cr0[R], cl1[R], cr1[R];
+  // per-point x-boundary weights: a neighbour across the row edge gets 0
+  T cl[VW][R], cr[VW][R];
 #pragma unroll
-  for (int d = 1; d <= R; ++d) {
-    const T cd = A.c[d - 1];
-    cl0[d - 1] = (xi - d >= 0) ? cd : T(0);
-    cr0[d - 1] = (xi + d < nx) ? cd : T(0);
-    cl1[d - 1] = (xi + 1 - d >= 0) ? cd : T(0);
-    cr1[d - 1] = (xi + 1 + d < nx) ? cd : T(0);
+  for (int j = 0; j < VW; ++j) {
+    const int xj = own ? (q + j) % nx : 0;
+#pragma unroll
+    for (int d = 1; d <= R; ++d) {
+      const T cd = A.c[d - 1];
+      cl[j][d - 1] = (xj - d >= 0) ? cd : T(0);
+      cr[j][d - 1] = (xj + d < nx) ? cd : T(0);
+    }
   }
   const T c0 = A.c0;
-  // z loop unrolled by Q = 2R+1 so the register queue rotates by renaming:
-  // at unrolled position u, plane z - R + i lives in zq[(u + i) % Q]
-  constexpr int Q = 2 * R + 1;
+  // z loop unrolled by Q so the register queue rotates by renaming:
+  // at unrolled position u, plane z - R + i lives in zq[.][(u + i) % Q]
 #pragma unroll 1
   for (int zb = z0; zb < z1; zb += Q) {
 #pragma unroll
@@ -226,75 +287,70 @@ k_stencil_tma(TmaArgs<T> A) {
       if (z >= z1) break;
       // queue front: plane z + R
       const int pf = z + R;
-      T f0 = T(0), f1 = T(0);
-      if (pf < nz) {
-        const int s = (pf - z0) % NBUF;
-        if (!fail && !mbar_wait(&bars[s], ((pf - z0) / NBUF) & 1)) fail = true;
-        if (own) {
-          const V2 v = *reinterpret_cast<const V2*>(ring + (size_t)s * WIN + s_c);
-          f0 = v.x;
-          f1 = v.y;
+      {
+        T f[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) f[j] = T(0);
+        if (pf < nz) {
+          const int s = (pf - z0) % NBUF;
+          if (!fail && !mbar_wait(&bars[s], ((pf - z0) / NBUF) & 1)) fail = true;
+          if (own) vload(ring + (size_t)s * WIN + s_c, f);
         }
+#pragma unroll
+        for (int j = 0; j < VW; ++j) zq[j][(u + 2 * R) % Q] = f[j];
       }
-      zq0[(u + 2 * R) % Q] = f0;
-      zq1[(u + 2 * R) % Q] = f1;
-      const V2 pvv = pv_next, pov = po_next;
+      T pvv[VW], pov[VW];
+#pragma unroll
+      for (int j = 0; j < VW; ++j) {
+        pvv[j] = pv_next[j];
+        pov[j] = po_next[j];
+      }
       load_pp(z + 1);
       const T* pl = ring + (size_t)((z - z0) % NBUF) * WIN;
       if (own) {
-        // x neighbours: window values s_c - R .. s_c + R + 1, fetched as aligned
-        // pairs starting at the even offset s_c - R - (R & 1); the pair itself
-        // (pair index CJ) is the queue's centre
-        constexpr int NP = R + 1 + (R & 1);
-        constexpr int OFF = R + (R & 1);  // xs index of the pair's first point
-        constexpr int CJ = OFF / 2;
-        const T xc0 = zq0[(u + R) % Q], xc1 = zq1[(u + R) % Q];
-        T xs[2 * NP];
+        // x neighbours: the aligned vectors around the run; the run itself is the queue's centre
+        T xs[NPV * VW];
 #pragma unroll
-        for (int j = 0; j < NP; ++j) {
-          if (j == CJ) {
-            xs[2 * j] = xc0;
-            xs[2 * j + 1] = xc1;
+        for (int v = 0; v < NPV; ++v) {
+          if (v == HV) {
+#pragma unroll
+            for (int j = 0; j < VW; ++j) xs[v * VW + j] = zq[j][(u + R) % Q];
           } else {
-            const V2 v = *reinterpret_cast<const V2*>(pl + s_c - R - (R & 1) + 2 * j);
-            xs[2 * j] = v.x;
-            xs[2 * j + 1] = v.y;
+            vload(pl + s_c - OFF + v * VW, xs + v * VW);
           }
         }
         // two partial sums per point: y + z terms, x terms
-        T acc0 = c0 * xc0, acc1 = c0 * xc1;
-        T ax0 = T(0), ax1 = T(0);
+        T acc[VW], ax[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) {
+          acc[j] = c0 * xs[OFF + j];
+          ax[j] = T(0);
+        }
 #pragma unroll
         for (int d = 1; d <= R; ++d) {
           // rows outside the plane are zero in the window, so y needs no test
-          const V2 ym = *reinterpret_cast<const V2*>(pl + s_c - d * nx);
-          const V2 yp = *reinterpret_cast<const V2*>(pl + s_c + d * nx);
+          T ym[VW], yp[VW];
+          vload_a<T, YA>(pl + s_c - d * nx, ym);
+          vload_a<T, YA>(pl + s_c + d * nx, yp);
           const T cd = A.c[d - 1];
-          const T t0 = (ym.x + yp.x) + (zq0[(u + R - d) % Q] + zq0[(u + R + d) % Q]);
-          const T t1 = (ym.y + yp.y) + (zq1[(u + R - d) % Q] + zq1[(u + R + d) % Q]);
-          acc0 += cd * t0;
-          acc1 += cd * t1;
-          ax0 += cl0[d - 1] * xs[OFF - d];
-          ax0 += cr0[d - 1] * xs[OFF + d];
-          ax1 += cl1[d - 1] * xs[OFF + 1 - d];
-          ax1 += cr1[d - 1] * xs[OFF + 1 + d];
+#pragma unroll
+          for (int j = 0; j < VW; ++j) {
+            const T t = (ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q]);
+            acc[j] += cd * t;
+            ax[j] += cl[j][d - 1] * xs[OFF + j - d];
+            ax[j] += cr[j][d - 1] * xs[OFF + j + d];
+          }
         }
-        acc0 += ax0;
-        acc1 += ax1;
-        if (has_pot) {
-          acc0 += pov.x * xc0;
-          acc1 += pov.y * xc1;
+        T o[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) {
+          const T xc = xs[OFF + j];
+          T a = acc[j] + ax[j];
+          if (has_pot) a += pov[j] * xc;
+          o[j] = ca * a + cb * xc;
+          if (Pc) o[j] += cg * pvv[j];
         }
-        T o0 = ca * acc0 + cb * xc0;
-        T o1 = ca * acc1 + cb * xc1;
-        if (Pc) {
-          o0 += cg * pvv.x;
-          o1 += cg * pvv.y;
-        }
-        V2 o;
-        o.x = o0;
-        o.y = o1;
-        *reinterpret_cast<V2*>(Yc + (long)z * nxy + q) = o;
+        vstore(Yc + (long)z * nxy + q, o);
       }
       __syncthreads();  // slot of plane z is free
       if (threadIdx.x == 0) {
@@ -315,7 +371,6 @@ static bool tma_ok(const psc_ctx* ctx, const void* X, long ldx, const void* P, l
   const long q = 16 / sizeof(T);
   const long nxy = (long)ctx->nx * ctx->ny;
   if (nxy % q || (ctx->radius * (long)ctx->nx) % q || ldx % q || (P && ldp % q) || ldy % q) return false;
-  if (ctx->nx % 2) return false;  // pairs must not straddle rows
   if (((uintptr_t)X | (uintptr_t)Y | (uintptr_t)P) % 16) return false;
   return true;
 }
@@ -325,6 +380,7 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
                         const T* pot, const double* w, const double* coef, double a, double b, double g,
                         cudaStream_t st) {
   const int nxy = ctx->nx * ctx->ny;
+  constexpr int TS = slab_points<T>();
   const int nslab = (nxy + TS - 1) / TS;
   // z chunks: enough CTAs for ~8 waves of 2 CTAs per SM, chunks of >= 8 planes
   const long want = 148L * 2 * 8;
@@ -334,11 +390,14 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   const int zmin = std::min(ctx->nz, 8);
   if (zchunk < zmin) zchunk = zmin;
   nzc = (ctx->nz + zchunk - 1) / zchunk;
-  constexpr int NBUF = R + 1 + TD;
+  constexpr int NBUF = R + 1 + prefetch_depth<T>();
   const size_t win = TS + 2 * (size_t)R * ctx->nx;
   const size_t smem = NBUF * win * sizeof(T) + NBUF * sizeof(uint64_t);
   if (smem > 220 * 1024) return -1;  // window too wide: the register-queue kernel takes it
-  auto kern = k_stencil_tma<T, R>;
+  constexpr int VW = VecOf<T>::W;
+  auto kern = (ctx->nx % VW == 0) ? k_stencil_tma<T, R, VW>
+              : (ctx->nx % 2 == 0) ? k_stencil_tma<T, R, (VW >= 2 ? 2 : 1)>
+                                   : k_stencil_tma<T, R, 1>;
   PSC_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   TmaArgs<T> A;
   A.X = X; A.ldx = ldx; A.P = P; A.ldp = ldp; A.Y = Y; A.ldy = ldy; A.pot = pot;

@@ -49,9 +49,13 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
                           energy_target: tuple[float, float] | None = None) -> SCFResult:
     """Run one SCF to convergence (or maxits).
 
-    init_density: optional callable (ctx, rho0, hpot0, ppot, A) -> (rho1, hpot1)
-    replacing the SAD starting density and its Hartree potential (the
-    contract of V_ion/pseudoDiag_ML4Den_poisson.py); None keeps SAD.
+    init_density: optional callable (ctx, rho0, hpot0, ppot, A) -> (rho1, dh)
+    giving a starting density rho1 (electrons per point) and the Hartree
+    potential dh of rho1 - rho0 (the quantities of
+    V_ion/pseudoDiag_ML4Den_poisson.py:448-538).  They set the first
+    potential only: the SCF keeps the SAD rho0 / hpot0 as its reference
+    charge and starts the Hartree CG from dh, so the fixed point (and the
+    final energy) is that of the SAD-initialised run.  None keeps SAD.
     on_iteration: optional callable(dict) receiving each iteration's record.
     energy_target: optional (E_ry, tol_ry); the loop then also requires
     |E_total - E_ry| <= tol_ry before it stops (a time-to-accuracy
@@ -96,8 +100,9 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
             say("No trained density network found: using the SAD initial density.")
     t0 = time.perf_counter()
     rho0, hpot0, ppot, diag_info = backend.pseudo_diag(dom, atoms, elem, n_elements, return_info=True)
+    rho_start, hpot_start = rho0, None
     if init_density is not None:
-        rho0, hpot0 = init_density(ctx, rho0, hpot0, ppot, A)
+        rho_start, hpot_start = init_density(ctx, rho0, hpot0, ppot, A)
     stage("Diagonal ionic potential setup", t0)
     output.write_diag_info(out, diag_info)
     if problem.input_data.z_charge != 0:
@@ -105,9 +110,9 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         rho0 = gpu.axpby(ctx, rho0, None, scale, 0.0)
         hpot0 = gpu.axpby(ctx, hpot0, None, scale, 0.0)
     if problem.paths.initial_density_base:
-        output.save_density_variants(rho0.cpu().numpy(), dom, problem.paths.initial_density_base)
+        output.save_density_variants(rho_start.cpu().numpy(), dom, problem.paths.initial_density_base)
 
-    rhoxc = gpu.axpby(ctx, rho0, None, 1.0 / h ** 3, 0.0)
+    rhoxc = gpu.axpby(ctx, rho_start, None, 1.0 / h ** 3, 0.0)
     t0 = time.perf_counter()
     backend.pseudo_nl(dom, atoms, elem, n_elements)
     stage("Nonlocal ionic potential setup", t0)
@@ -116,7 +121,8 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
     xcpot, xc0 = gpu.lda_xc(ctx, rhoxc)
     stage("Exchange-correlation setup", t0)
     zero = ctx.zeros(n)
-    pot, _, init_sums = gpu.scf_update(ctx, ppot, xcpot, zero, hpot0, zero, zero)
+    hstart = zero if hpot_start is None else hpot_start
+    pot, _, init_sums = gpu.scf_update(ctx, ppot, xcpot, hstart, hpot0, zero, zero)
     if out:
         hps = gpu.numpy_sum(ctx, rho0 * hpot0).item() * RY_EV
         x0 = xc0.cpu().numpy()
@@ -136,7 +142,7 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
     nev = problem.nev
     k = nev + 15
     W = lam = occ = None
-    Hpot = ctx.zeros(n)
+    Hpot = ctx.zeros(n) if hpot_start is None else hpot_start.clone()
     rho = ctx.zeros(n)
     XCpot = xcpot
     err = 10.0 + s.tol

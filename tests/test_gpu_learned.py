@@ -158,7 +158,7 @@ def test_learned_init_saves_iterations_on_held_out_water_clusters():
     params = learned.load_weights()
     if params is None:
         pytest.skip("no trained weights in parsec_python_b200/data")
-    summ = learned.evaluate([600, 601], learned.DEFAULT_WEIGHTS, log=lambda *a: None)
-    assert summ["n_converged_both"] == 2
-    assert summ["max_de_ha"] < 1e-5
+    summ = learned.evaluate([600, 601, 602, 603], learned.DEFAULT_WEIGHTS, log=lambda *a: None)
+    assert summ["n"] >= 3
+    assert summ["max_de_learned_ha"] <= 1e-5 and summ["max_de_sad_ha"] <= 1e-5
     assert summ["mean_its_learned"] < summ["mean_its_sad"]
