@@ -226,8 +226,9 @@ k_jacobi(const double* __restrict__ Ain, int k, double* __restrict__ evals, doub
   const int m = k + (k & 1);
   const int half = m / 2;
   const int ld = m + 1;   // odd leading dimension: a warp's strided accesses spread over the banks
+  // use_smem: 2 = A and V on chip, 1 = A on chip and V in global scratch, 0 = both in scratch
   double* A = use_smem ? sm : scratch;
-  double* V = A + m * ld;
+  double* V = use_smem == 2 ? A + m * ld : scratch + (use_smem ? 0 : m * ld);
   for (int e = threadIdx.x; e < m * m; e += NT) {
     const int i = e % m, j = e / m;
     double a = 0.0;
@@ -354,14 +355,14 @@ int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, 
   PSC_REQUIRE(ctx, k >= 1 && k <= 1022, "syev: k out of range");
   if (psc_ensure_dense(ctx, k)) return 1;
   const int m = k + (k & 1);
-  const size_t smem = 2 * (size_t)m * (m + 1) * sizeof(double);
-  const int use_smem = smem <= 200 * 1024;
-  const size_t dyn = use_smem ? smem : 0;
+  const size_t tile = (size_t)m * (m + 1) * sizeof(double);
+  const int use_smem = 2 * tile <= 200 * 1024 ? 2 : (tile <= 200 * 1024 ? 1 : 0);
+  const size_t dyn = use_smem * tile;
   // CTA size matched to the (m/2)^2 blocks + (m/2) m rows of a rotation round
 #define PSC_JACOBI(NTH)                                                                                   \
   {                                                                                                       \
     if (use_smem)                                                                                         \
-      PSC_CUDA(ctx, cudaFuncSetAttribute(k_jacobi<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+      PSC_CUDA(ctx, cudaFuncSetAttribute(k_jacobi<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)); \
     k_jacobi<NTH><<<1, NTH, dyn, st>>>(A, k, evals, evecs, use_smem, ctx->jac_v, ctx->dev_status);       \
   }
   // 32 x (NT/32) thread grid over the (m/2)^2 blocks of a rotation round

@@ -194,11 +194,12 @@ def test_dense_building_blocks():
 
 
 @pytest.mark.parametrize("k,kind", [(1, "rand"), (2, "rand"), (7, "rand"), (55, "diag"), (56, "degenerate"),
-                                    (111, "rand"), (143, "neardiag")])
+                                    (111, "rand"), (143, "neardiag"), (200, "neardiag")])
 def test_syev_edge_cases(k, kind):
-    """Jacobi eigensolver: odd/even orders (padding), the shared-memory /
-    global-memory switch (k = 111 no longer fits on chip), an input that is
-    already diagonal, repeated eigenvalues, a nearly diagonal RR matrix."""
+    """Jacobi eigensolver: odd/even orders (padding), the three placements
+    (A and V on chip up to k = 110, A on chip up to k = 157, both in global
+    memory beyond), an input that is already diagonal, repeated eigenvalues,
+    nearly diagonal RR matrices."""
     ctx = gpu.GridContext({"nx": 8, "ny": 8, "nz": 8, "h": 0.5, "radius": 1.75}, 8)
     rng = np.random.default_rng(k)
     if kind == "rand":
