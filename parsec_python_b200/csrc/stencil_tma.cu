@@ -264,17 +264,14 @@ k_stencil_tma(TmaArgs<T> A) {
     }
   }
 
-  // per-point x-boundary weights: a neighbour across the row edge gets 0
-  T cl[VW][R], cr[VW][R];
+  // per-point distances to the row edges, capped at R: a neighbour d > el
+  // (left) or d > er (right) lies across the edge and gets weight 0
+  int el[VW], er[VW];
 #pragma unroll
   for (int j = 0; j < VW; ++j) {
     const int xj = own ? (q + j) % nx : 0;
-#pragma unroll
-    for (int d = 1; d <= R; ++d) {
-      const T cd = A.c[d - 1];
-      cl[j][d - 1] = (xj - d >= 0) ? cd : T(0);
-      cr[j][d - 1] = (xj + d < nx) ? cd : T(0);
-    }
+    el[j] = min(R, xj);
+    er[j] = min(R, nx - 1 - xj);
   }
   const T c0 = A.c0;
   // z loop unrolled by Q so the register queue rotates by renaming:
@@ -337,8 +334,8 @@ k_stencil_tma(TmaArgs<T> A) {
           for (int j = 0; j < VW; ++j) {
             const T t = (ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q]);
             acc[j] += cd * t;
-            ax[j] += cl[j][d - 1] * xs[OFF + j - d];
-            ax[j] += cr[j][d - 1] * xs[OFF + j + d];
+            const T xsum = (d <= el[j] ? xs[OFF + j - d] : T(0)) + (d <= er[j] ? xs[OFF + j + d] : T(0));
+            ax[j] += cd * xsum;
           }
         }
         T o[VW];

@@ -299,7 +299,7 @@ class LearnedInit:
         rho1 = rho1 * (zsum / gpu.numpy_sum(ctx, rho1))
         hrhs = (4 * np.pi / h3) * (rho1 - rho0)
         dh, its = gpu.pcg(A, hrhs, torch.zeros_like(hrhs), 200, 1e-5)
-        self.last = {"cg_its": its}
+        self.last = {"cg_its": its, "rho_start": rho1}
         return rho1, dh
 
 
@@ -438,18 +438,30 @@ def evaluate(seeds, weights: Path, log=print) -> dict:
             target = (e_star, 2e-5)   # 1e-5 Ha
             r_sad, t_sad, _ = run_scf(sd, energy_target=target)
             init = LearnedInit(params)
-            r_ml, t_ml, _ = run_scf(sd, init=init, energy_target=target)
+            r_ml, t_ml, backend = run_scf(sd, init=init, energy_target=target)
         except ValueError as exc:
             skipped.append(sd)
             log(f"  seed {sd} skipped: {exc}")
             continue
         e_sad, e_ml = r_sad.history[-1]["total_ry"], r_ml.history[-1]["total_ry"]
+        # distance of each starting density from the converged one, in electrons: h^3 sum |rho_start - rho|
+        rt = backend.runtime
+        prob, elem = water_system(sd, rt.settings)
+        ctx = rt.context(prob.domain)
+        rho0, _, _, _ = backend.pseudo_diag(prob.domain, prob.input_data.atoms, elem, len(elem), return_info=True)
+        h3 = ctx.h ** 3
+        conv_pt = r_ref.rho * h3
+        d_sad = float((rho0 - conv_pt).abs().sum())
+        d_ml = float((init.last.get("rho_start", rho0) - conv_pt).abs().sum())
         rows.append({"seed": sd, "its_sad": r_sad.iterations, "its_learned": r_ml.iterations, "t_sad": t_sad,
                      "t_learned": t_ml, "e_star_ry": e_star, "de_sad_ha": abs(e_sad - e_star) / 2,
-                     "de_learned_ha": abs(e_ml - e_star) / 2,
+                     "de_learned_ha": abs(e_ml - e_star) / 2, "start_drho_sad_e": d_sad,
+                     "start_drho_learned_e": d_ml, "start_e_err_sad_ha": abs(r_sad.history[0]["total_ry"] - e_star) / 2,
+                     "start_e_err_learned_ha": abs(r_ml.history[0]["total_ry"] - e_star) / 2,
                      "converged": bool(r_sad.converged and r_ml.converged)})
         log(f"  seed {sd}: SAD {r_sad.iterations} its {t_sad:.3f}s, learned {r_ml.iterations} its {t_ml:.3f}s, "
-            f"|dE| SAD {rows[-1]['de_sad_ha']:.1e} learned {rows[-1]['de_learned_ha']:.1e} Ha")
+            f"|dE| SAD {rows[-1]['de_sad_ha']:.1e} learned {rows[-1]['de_learned_ha']:.1e} Ha, "
+            f"start |drho| SAD {d_sad:.3f} learned {d_ml:.3f} e")
     conv = [r for r in rows if r["converged"]]
     its_s = np.array([r["its_sad"] for r in conv])
     its_l = np.array([r["its_learned"] for r in conv])
@@ -457,6 +469,10 @@ def evaluate(seeds, weights: Path, log=print) -> dict:
                "mean_t_sad": float(np.mean([r["t_sad"] for r in conv])),
                "mean_t_learned": float(np.mean([r["t_learned"] for r in conv])),
                "max_de_sad_ha": float(max(r["de_sad_ha"] for r in conv)),
+               "mean_start_drho_sad_e": float(np.mean([r["start_drho_sad_e"] for r in conv])),
+               "mean_start_drho_learned_e": float(np.mean([r["start_drho_learned_e"] for r in conv])),
+               "mean_first_iter_e_err_sad_ha": float(np.mean([r["start_e_err_sad_ha"] for r in conv])),
+               "mean_first_iter_e_err_learned_ha": float(np.mean([r["start_e_err_learned_ha"] for r in conv])),
                "max_de_learned_ha": float(max(r["de_learned_ha"] for r in conv)),
                "not_converged": [r["seed"] for r in rows if not r["converged"]], "skipped": skipped, "rows": rows}
     return summary
