@@ -272,7 +272,9 @@ int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int 
   const long n = ctx->n;
   const int tiles = (k + TROWS - 1) / TROWS;
   const int npair = tiles * (tiles + 1) / 2;
-  int nchunk = std::max(1, 148 / npair);
+  // four waves of one CTA per SM: shorter chunks keep the FP32 accumulation
+  // in tensor memory short (its rounding error grows with the chunk length)
+  int nchunk = std::max(1, 4 * 148 / npair);
   long chunk = ((n + nchunk - 1) / nchunk + KSTAGE - 1) / KSTAGE * KSTAGE;
   nchunk = (int)((n + chunk - 1) / chunk);
   const size_t part_floats = (size_t)nchunk * npair * 2 * TROWS * TROWS;

@@ -2,15 +2,15 @@
 //   Out = a * (W In) + b * In + g * Prev,  W = c0 + sum_d c_d (shifts) [+ diag(pot)]
 // with plane windows streamed into shared memory by 1-D bulk copies.
 //
-// A CTA owns S = 512 consecutive flat xy points of one column and a chunk of
-// z planes.  For every plane the points it needs -- its own S points plus R
+// A CTA owns S = 512 (FP64) or 1024 (FP32) consecutive flat xy points of one
+// column and a chunk of z planes.  For every plane the points it needs -- its own S points plus R
 // rows of y halo on each side -- are one contiguous range of the plane, so a
 // single cp.async.bulk (no tensor map, no multicast) moves it into a slot of
-// a ring of NBUF = R + 1 + D shared-memory windows (D = 3 FP64, 4 FP32), completing on the slot's
-// mbarrier.  The z neighbours of each point live in a register queue fed from
+// a ring of NBUF = R + 1 + D shared-memory windows (D = 3 FP64, 4 FP32),
+// completing on the slot's mbarrier.  The z neighbours of each point live in a register queue fed from
 // the ring; x and y neighbours are read from the current plane's window with
-// 16-byte loads (each thread owns two adjacent x points; the pair itself comes
-// from the queue).  Prev and pot are read straight from global memory one
+// 16-byte loads (each thread owns a run of 2 FP64 or 4 FP32 points, which may
+// cross a row edge; the run itself comes from the queue).  Prev and pot are read straight from global memory one
 // plane ahead, so they cost no shared-memory traffic.  D planes are in flight
 // per CTA at all times, which is what keeps HBM busy.
 //
@@ -379,13 +379,25 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   const int nxy = ctx->nx * ctx->ny;
   constexpr int TS = slab_points<T>();
   const int nslab = (nxy + TS - 1) / TS;
-  // z chunks: enough CTAs for ~8 waves of 2 CTAs per SM, chunks of >= 8 planes
-  const long want = 148L * 2 * 8;
-  long per_col = (want + k - 1) / k;
-  int nzc = (int)std::max<long>(1, std::min<long>(ctx->nz, (per_col + nslab - 1) / nslab));
-  int zchunk = (ctx->nz + nzc - 1) / nzc;
-  const int zmin = std::min(ctx->nz, 8);
-  if (zchunk < zmin) zchunk = zmin;
+  // z chunks: each CTA pays a pipeline fill of about R + D planes, and the
+  // last wave of CTAs may be partly empty; pick the chunk count that
+  // minimises waves x (planes per chunk + fill), chunks of >= 8 planes
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const long slots = 2L * sms;   // two CTAs per SM (registers and shared memory)
+  const int fill = R + prefetch_depth<T>() + 2;
+  int nzc = 1;
+  double best = 1e300;
+  for (int c = 1; c <= std::max(1, ctx->nz / 8); ++c) {
+    const int zc = (ctx->nz + c - 1) / c;
+    const long ctas = (long)nslab * c * k;
+    const double cost = (double)((ctas + slots - 1) / slots) * (zc + fill);
+    if (cost < best - 1e-9) {
+      best = cost;
+      nzc = c;
+    }
+  }
+  const int zchunk = (ctx->nz + nzc - 1) / nzc;
   nzc = (ctx->nz + zchunk - 1) / zchunk;
   constexpr int NBUF = R + 1 + prefetch_depth<T>();
   const size_t win = TS + 2 * (size_t)R * ctx->nx;
