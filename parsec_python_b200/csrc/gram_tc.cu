@@ -21,7 +21,7 @@
 #include <algorithm>
 
 namespace {
-constexpr int TC_NT = 128;
+constexpr int TC_NT = 256;              // 8 warps: loads in flight; warps 0-3 also drain TMEM
 constexpr int TROWS = 128;               // tile rows (matrix columns), = MMA M
 constexpr int KSTAGE = 32;               // reduction rows per stage (128 bytes of FP32)
 constexpr int TILE_BYTES = TROWS * 128;  // 16 KB
@@ -78,30 +78,51 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
-// Load rows [0, nrows) x 32 reduction entries of one tile (rows = matrix
+// One tile of a stage: rows [0, nrows) x 32 reduction entries (rows = matrix
 // columns col0 + r, valid below `valid`; reduction entries n0 .. n0+31 below
-// n_end), split into hi/lo and store both swizzled.
-__device__ __forceinline__ void load_split(const float* __restrict__ M, long ld, int col0, int valid, int nrows,
-                                           long n0, long n_end, bool vec, unsigned char* hi, unsigned char* lo) {
-  for (int i = threadIdx.x; i < nrows * 8; i += TC_NT) {
+// n_end).  Each thread owns up to PER 16-byte pieces; all loads of a stage
+// are issued before any is used, then split into hi/lo and stored swizzled.
+constexpr int PER = TROWS * 8 / TC_NT;   // pieces per thread and tile
+
+struct TileLoad {
+  float4 v[PER];
+};
+
+__device__ __forceinline__ void tile_load(const float* __restrict__ M, long ld, int col0, int valid, int nrows,
+                                          long n0, long n_end, bool vec, TileLoad& t) {
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int i = threadIdx.x + u * TC_NT;
     const int row = i >> 3, c = i & 7;
     const long nn = n0 + 4 * c;
-    float x[4] = {0.f, 0.f, 0.f, 0.f};
-    if (row < valid && nn < n_end) {
+    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (row < nrows && row < valid && nn < n_end) {
       const float* src = M + (long)(col0 + row) * ld + nn;
       if (vec && nn + 3 < n_end) {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(src));
-        x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+        x = __ldg(reinterpret_cast<const float4*>(src));
       } else {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) x[j] = (nn + j < n_end) ? __ldg(src + j) : 0.f;
+        x.x = __ldg(src);
+        if (nn + 1 < n_end) x.y = __ldg(src + 1);
+        if (nn + 2 < n_end) x.z = __ldg(src + 2);
+        if (nn + 3 < n_end) x.w = __ldg(src + 3);
       }
     }
+    t.v[u] = x;
+  }
+}
+
+__device__ __forceinline__ void tile_store_split(const TileLoad& t, int nrows, unsigned char* hi, unsigned char* lo) {
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int i = threadIdx.x + u * TC_NT;
+    const int row = i >> 3, c = i & 7;
+    if (row >= nrows) continue;
+    const float4 x = t.v[u];
     float4 h, l;
-    h.x = tf32_rna(x[0]); l.x = tf32_rna(x[0] - h.x);
-    h.y = tf32_rna(x[1]); l.y = tf32_rna(x[1] - h.y);
-    h.z = tf32_rna(x[2]); l.z = tf32_rna(x[2] - h.z);
-    h.w = tf32_rna(x[3]); l.w = tf32_rna(x[3] - h.w);
+    h.x = tf32_rna(x.x); l.x = tf32_rna(x.x - h.x);
+    h.y = tf32_rna(x.y); l.y = tf32_rna(x.y - h.y);
+    h.z = tf32_rna(x.z); l.z = tf32_rna(x.z - h.z);
+    h.w = tf32_rna(x.w); l.w = tf32_rna(x.w - h.w);
     const int off = row * 128 + ((c ^ (row & 7)) << 4);
     *reinterpret_cast<float4*>(hi + off) = h;
     *reinterpret_cast<float4*>(lo + off) = l;
@@ -164,9 +185,15 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
     __syncthreads();
     if (s_fail) break;
     const long n0 = n_begin + (long)s * KSTAGE;
-    load_split(W, ld, col_a, valid_a, TROWS, n0, n_end, vec, a_hi, a_lo);
-    if (!same) load_split(W, ld, col_b, valid_b, N, n0, n_end, vec, bs_hi, bs_lo);
-    load_split(V, ld, col_b, valid_b, N, n0, n_end, vec, bk_hi, bk_lo);
+    {
+      TileLoad ta, tb, tk;
+      tile_load(W, ld, col_a, valid_a, TROWS, n0, n_end, vec, ta);
+      if (!same) tile_load(W, ld, col_b, valid_b, N, n0, n_end, vec, tb);
+      tile_load(V, ld, col_b, valid_b, N, n0, n_end, vec, tk);
+      tile_store_split(ta, TROWS, a_hi, a_lo);
+      if (!same) tile_store_split(tb, N, bs_hi, bs_lo);
+      tile_store_split(tk, N, bk_hi, bk_lo);
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -199,8 +226,8 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (s_fail) {
     if (threadIdx.x == 0) atomicExch(&status[5], 1);
-  } else if (nstage > 0) {
-    // epilogue: warp w owns TMEM lanes (= rows) 32w .. 32w+31
+  } else if (nstage > 0 && warp < 4) {
+    // epilogue: warp w (< 4) owns TMEM lanes (= rows) 32w .. 32w+31
     const int row = warp * 32 + (threadIdx.x & 31);
     float* ps = part + (((long)blockIdx.x * gridDim.y + blockIdx.y) * 2) * (TROWS * TROWS);
     float* pk = ps + TROWS * TROWS;
@@ -228,22 +255,25 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
-// S, K (k x k, column-major FP64) = sums over the chunks.  Diagonal tiles are
-// symmetrised as 0.5 (X + X^T) (as the CUDA-core path does); off-diagonal
+// S, K (k x k, column-major FP64) = sums over the chunks, one warp per entry
+// (lanes take every 32nd chunk, then a fixed shuffle tree).  Diagonal tiles
+// are symmetrised as 0.5 (X + X^T) (as the CUDA-core path does); off-diagonal
 // tiles are computed above the diagonal only and mirrored.
 __global__ void k_gram_tc_final(const float* __restrict__ part, int nchunk, int npair, const int2* __restrict__ pairs,
                                 int k, double* __restrict__ S, double* __restrict__ K) {
+  const int lane = threadIdx.x & 31;
+  const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
   const long total = (long)npair * TROWS * TROWS;
-  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+  for (long e = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < total; e += nwarps) {
     const int p = (int)(e / (TROWS * TROWS));
     const int rc = (int)(e % (TROWS * TROWS));
     const int r = rc / TROWS, c = rc % TROWS;
     const int i = pairs[p].x * TROWS + r, j = pairs[p].y * TROWS + c;
-    if (i >= k || j >= k) continue;
+    if (i >= k || j >= k) continue;   // uniform across the warp
     const bool diag = pairs[p].x == pairs[p].y;
     const int cr = c * TROWS + r;
     double s = 0.0, kv = 0.0, st = 0.0, kt = 0.0;
-    for (int ch = 0; ch < nchunk; ++ch) {
+    for (int ch = lane; ch < nchunk; ch += 32) {
       const float* ps = part + (((long)ch * npair + p) * 2) * (TROWS * TROWS);
       s += (double)ps[rc];
       kv += (double)ps[TROWS * TROWS + rc];
@@ -252,14 +282,20 @@ __global__ void k_gram_tc_final(const float* __restrict__ part, int nchunk, int 
         kt += (double)ps[TROWS * TROWS + cr];
       }
     }
-    if (diag) {
-      S[i + (long)j * k] = 0.5 * (s + st);
-      K[i + (long)j * k] = 0.5 * (kv + kt);
-    } else {
-      S[i + (long)j * k] = s;
-      K[i + (long)j * k] = kv;
-      S[j + (long)i * k] = s;
-      K[j + (long)i * k] = kv;
+    s = psc_warp_sum(s);
+    kv = psc_warp_sum(kv);
+    st = psc_warp_sum(st);
+    kt = psc_warp_sum(kt);
+    if (lane == 0) {
+      if (diag) {
+        S[i + (long)j * k] = 0.5 * (s + st);
+        K[i + (long)j * k] = 0.5 * (kv + kt);
+      } else {
+        S[i + (long)j * k] = s;
+        K[i + (long)j * k] = kv;
+        S[j + (long)i * k] = s;
+        K[j + (long)i * k] = kv;
+      }
     }
   }
 }
@@ -300,7 +336,7 @@ int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int 
                                                       ctx->tc_part, ctx->dev_status);
   PSC_LAUNCH_CHECK(ctx);
   const long total = (long)npair * TROWS * TROWS;
-  k_gram_tc_final<<<std::max(1, (int)std::min<long>(592, (total + 255) / 256)), 256, 0, st>>>(
+  k_gram_tc_final<<<std::max(1, (int)std::min<long>(148 * 8, (total + 7) / 8)), 256, 0, st>>>(
       ctx->tc_part, nchunk, npair, (const int2*)ctx->tc_pairs, k, S, K);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
