@@ -34,50 +34,41 @@ namespace {
 constexpr int PNT = 1024;
 constexpr long BAR_LIMIT = 1L << 26;
 
-// Grid-wide sum of one value per thread, which is also the grid barrier:
-// warps reduce by shuffles, thread 0 adds the warp sums in a fixed order,
-// publishes the CTA's partial, arrives at the monotone counter and spins
-// (bounded: 2^26 polls, then status word 4 and `failed`); warp 0 then sums
-// the G partials, again in a fixed order, so every CTA gets the same value.
-// Two CTA barriers per call; global writes made before the call are visible
-// to every CTA after it.
-__device__ __forceinline__ double grid_allreduce(double v, double* part, int G, unsigned int* ctr,
-                                                 unsigned int target, int* status, bool& failed, double* sh,
-                                                 double* bc) {
-  v = psc_warp_sum(v);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) sh[w] = v;
+__device__ __forceinline__ void grid_barrier(unsigned int* ctr, unsigned int target, int* status, bool& failed) {
   __syncthreads();
-  if (w == 0) {
-    if (l == 0) {
-      double s = 0.0;
-      for (int i = 0; i < PNT / 32; ++i) s += sh[i];
-      part[blockIdx.x] = s;
-      __threadfence();
-      atomicAdd(ctr, 1u);
-      if (!failed) {
-        long spins = 0;
-        while (true) {
-          unsigned int c;
-          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(ctr) : "memory");
-          if (c >= target) break;
-          if (++spins > BAR_LIMIT) {
-            failed = true;
-            atomicExch(&status[4], 1);
-            break;
-          }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(ctr, 1u);
+    if (!failed) {
+      long spins = 0;
+      while (true) {
+        unsigned int v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
+        if (v >= target) break;
+        if (++spins > BAR_LIMIT) {
+          failed = true;
+          atomicExch(&status[4], 1);
+          break;
         }
       }
-      __threadfence();
     }
-    __syncwarp();
-    double s = 0.0;
-    for (int t = l; t < G; t += 32) s += __ldcg(part + t);
-    s = psc_warp_sum(s);
-    if (l == 0) *bc = s;
+    __threadfence();
   }
   __syncthreads();
-  return *bc;
+}
+
+// Sum of the G per-CTA partials part[0..G) by warp 0 in a fixed order, the
+// same in every CTA; the result is broadcast through shared memory.
+__device__ __forceinline__ double grid_sum(const double* part, int G, double* bc) {
+  if (threadIdx.x < 32) {
+    double s = 0.0;
+    for (int t = threadIdx.x; t < G; t += 32) s += __ldcg(part + t);
+    s = psc_warp_sum(s);
+    if (threadIdx.x == 0) *bc = s;
+  }
+  __syncthreads();
+  const double r = *bc;
+  return r;
 }
 }  // namespace
 
@@ -157,7 +148,10 @@ k_cg_persistent(const double* __restrict__ rhs, double* __restrict__ xg, double*
     rg[a + t] = ri;
     rr += ri * ri;
   }
-  double ro = grid_allreduce(rr, part + G, G, bar, (++nbar) * G, status, failed, sh, &bc[0]);
+  rr = psc_block_sum<double, PNT>(rr, sh);
+  if (threadIdx.x == 0) part[G + blockIdx.x] = rr;
+  grid_barrier(bar, (++nbar) * G, status, failed);
+  double ro = grid_sum(part + G, G, &bc[0]);
   const double tol1 = tol * tol * ro;
   int it = 0;
   bool active = maxit > 0 && ro > tol1;
@@ -179,7 +173,10 @@ k_cg_persistent(const double* __restrict__ rhs, double* __restrict__ xg, double*
       aps[t] = av;
       pap += av * pv;
     }
-    pap = grid_allreduce(pap, part, G, bar, (++nbar) * G, status, failed, sh, &bc[0]);
+    pap = psc_block_sum<double, PNT>(pap, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = pap;
+    grid_barrier(bar, (++nbar) * G, status, failed);
+    pap = grid_sum(part, G, &bc[0]);
     // B: alpha, updates, partial of r.r
     const double alp = ro / pap;
     rr = 0.0;
@@ -190,8 +187,11 @@ k_cg_persistent(const double* __restrict__ rhs, double* __restrict__ xg, double*
       rg[a + t] = ri;
       rr += ri * ri;
     }
+    rr = psc_block_sum<double, PNT>(rr, sh);
+    if (threadIdx.x == 0) part[G + blockIdx.x] = rr;
+    grid_barrier(bar, (++nbar) * G, status, failed);
     // C: stop test and beta, identical in every CTA
-    const double ro1 = grid_allreduce(rr, part + G, G, bar, (++nbar) * G, status, failed, sh, &bc[1]);
+    const double ro1 = grid_sum(part + G, G, &bc[1]);
     beta = ro1 / ro;
     ro = ro1;
     active = it < maxit && ro1 > tol1;
