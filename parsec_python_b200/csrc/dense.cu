@@ -99,7 +99,9 @@ int psc_ensure_dense(psc_ctx* ctx, int k) {
   PSC_CUDA(ctx, psc_dmalloc(&ctx->gram2, kk * sizeof(double)));
   PSC_CUDA(ctx, psc_dmalloc(&ctx->evec, kk * sizeof(double)));
   PSC_CUDA(ctx, psc_dmalloc(&ctx->tri, kk * sizeof(double)));
-  ctx->gram_blocks = 296;
+  // per-chunk partial k x k tiles: enough chunks for two waves of two CTAs per
+  // SM at small k, at most 128 MB of partials at large k
+  ctx->gram_blocks = std::min(1184, std::max(296, (int)(16777216 / (long)kk)));
   PSC_CUDA(ctx, psc_dmalloc(&ctx->gram_partial, (size_t)ctx->gram_blocks * kk * sizeof(double)));
   ctx->dense_cap = cap;
   return 0;

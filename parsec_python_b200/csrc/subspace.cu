@@ -90,22 +90,27 @@ k_gram_pair(const T* __restrict__ A, const T* __restrict__ B, long ld, int k, lo
     }
 }
 
-// sum partials in fixed order; S symmetrised as 0.5 (S + S^T), K likewise
+// sum partials in fixed order, one warp per entry (lanes take every 32nd
+// chunk, then a fixed shuffle tree); S symmetrised as 0.5 (S + S^T), K likewise
 __global__ void k_gram_pair_final(const double* __restrict__ partS, const double* __restrict__ partK, int nchunk,
                                   int k, double* __restrict__ S, double* __restrict__ K) {
   const long kk = (long)k * k;
-  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < 2 * kk; e += (long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
+  for (long e = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < 2 * kk; e += nwarps) {
     const bool isK = e >= kk;
     const long f = isK ? e - kk : e;
     const int i = (int)(f % k), j = (int)(f / k);
     const long t = j + (long)i * k;
     const double* P = isK ? partK : partS;
     double s = 0.0, u = 0.0;
-    for (int c = 0; c < nchunk; ++c) {
+    for (int c = lane; c < nchunk; c += 32) {
       s += P[(long)c * kk + f];
       u += P[(long)c * kk + t];
     }
-    (isK ? K : S)[f] = 0.5 * (s + u);
+    s = psc_warp_sum(s);
+    u = psc_warp_sum(u);
+    if (lane == 0) (isK ? K : S)[f] = 0.5 * (s + u);
   }
 }
 
@@ -207,6 +212,7 @@ static int gram_pair(psc_ctx* ctx, int dtype, const void* W, const void* V, long
   const long n = ctx->n;
   const int tiles = (k + GP_T - 1) / GP_T;
   const int ntile = tiles * tiles;
+  // two waves of two CTAs per SM (the kernel holds 204 registers per thread)
   int nchunk = std::max(1, std::min(ctx->gram_blocks / 2, (148 * 4 + ntile - 1) / ntile));
   nchunk = (int)std::min<long>(nchunk, std::max<long>(1, n / GP_R));
   const long chunk = ((n + nchunk - 1) / nchunk + GP_R - 1) / GP_R * GP_R;
@@ -222,8 +228,8 @@ static int gram_pair(psc_ctx* ctx, int dtype, const void* W, const void* V, long
                                               partK);
   PSC_LAUNCH_CHECK(ctx);
   const long kk = (long)k * k;
-  k_gram_pair_final<<<std::max(1, (int)std::min<long>(592, (2 * kk + 255) / 256)), 256, 0, st>>>(partS, partK,
-                                                                                                 nchunk, k, S, K);
+  k_gram_pair_final<<<std::max(1, (int)std::min<long>(148 * 8, (2 * kk + 7) / 8)), 256, 0, st>>>(partS, partK,
+                                                                                               nchunk, k, S, K);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }
