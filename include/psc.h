@@ -101,6 +101,33 @@ int psc_cheb_filter(psc_ctx* ctx, int dtype, int mode, int deg, const double* bo
  * out = [uppbnd, ritz_0..ritz_5]; mode 1: Eigensolvers/lanczosForChefsi1.py:5-99,
  * out = [bound].  The start vector is drawn from `seed`. */
 int psc_lanczos_bound(psc_ctx* ctx, int mode, unsigned long long seed, double* out_dev, void* stream);
+/* Lanczos with a kept basis (Eigensolvers/lanczosForChsubsp.py:33-119 and
+ * lanczos.py:38-139, no reorthogonalisation): runs steps k0 .. k1-1 of
+ * w = H v_j - beta_{j-1} v_{j-1}, alpha_j = v_j.w, w -= alpha_j v_j,
+ * beta_j = |w|, v_{j+1} = w / beta_j.  VV (n x >= k1+1, column-major, ld
+ * ldv) holds v_j in column j; ab[2j] = alpha_j, ab[2j+1] = beta_j (device).
+ * With k0 = 0 the start vector is v_start / |v_start|, or a standard normal
+ * vector drawn from `seed` when v_start is NULL (np.random.randn at
+ * chsubsp.py:34 and rsdft_solver.py:63-68).  Calls with k0 > 0 continue a
+ * run, so a caller can test convergence between them. */
+int psc_lanczos_run(psc_ctx* ctx, const double* v_start, unsigned long long seed, int k0, int k1, double* VV,
+                    long ldv, double* ab, void* stream);
+/* Eigenpairs of the k x k symmetric tridiagonal with diagonal ab[2i] and
+ * off-diagonal ab[2i+1] (k <= 4096): all eigenvalues ascending into evals,
+ * eigenvectors of the nvec lowest into Z (k x nvec, ld ldz >= k) when
+ * nvec > 0 (replaces scipy.linalg.eigh(Tmat[:k, :k]) at
+ * lanczosForChsubsp.py:101-128 and lanczos.py:129-146). */
+int psc_tridiag_eig(psc_ctx* ctx, const double* ab, int k, int nvec, double* evals, double* Z, long ldz,
+                    void* stream);
+/* Orthonormal basis of the numerically independent columns of W (n x k):
+ * a column whose part orthogonal to the kept columns before it has squared
+ * norm <= tol |w_j|^2 is dropped, the rest are orthonormalised by
+ * CholeskyQR2.  *rank = kept columns, stored as the first *rank columns of W
+ * (*which = 0) or T (*which = 1).  Replaces the Householder QR of
+ * W = VV X at lanczosForChsubsp.py:167 and lanczos.py:195, whose input has
+ * near-copies of the same Ritz vector. */
+int psc_orthonormalize_rank(psc_ctx* ctx, int dtype, void* W, void* T, long ld, int k, double tol, int* rank,
+                            int* which, void* stream);
 /* Filter interval from device values: mode 0 chefsi1.py:29-38
  * ([min ritz, max ritz, upper]); mode 1 first_filt.py:28-29; mode 2 first_filt.py:62. */
 int psc_filter_bounds(psc_ctx* ctx, int mode, const double* ritz_dev, int k, const double* upper_dev,

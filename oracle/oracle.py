@@ -505,6 +505,131 @@ def chefsi1(Vin, ritzv, deg, nev, H):
     return W @ Q[:, order], ritzv_raw[order]
 
 
+def lanczos_krylov(B, v, m: int, nev: int, test: int, tol: float = 1e-5):
+    """m-step Lanczos without reorthogonalisation that keeps its basis:
+    Eigensolvers/lanczosForChsubsp.py:33-132 and lanczos.py:38-146.
+
+    test 0: no convergence test (the reference's choice for n > 35000);
+    test 1: lanczosForChsubsp.py:99-119, stop when |tr1 - tr0| < tol * tr0
+            (no absolute value on the right, so a negative trace never stops);
+    test 2: lanczos_gpu.py:128-137, |tr1 - tr0| < tol * |tr0| (the CPU
+            lanczos.py:125-134 indexes an empty list there and cannot run).
+    Traces are the sums of the nev lowest eigenvalues of T_k, taken at
+    k >= min(8 nev, m) with k % 10 == 0 and at k = m.
+
+    Returns (VV[:, :k], alpha[:k], beta[:k], k, rr, X): rr ascending
+    eigenvalues of T_k and X its eigenvectors (scipy.linalg.eigh as the
+    reference), beta[k-1] the residual norm of the last step."""
+    n = B.shape[0]
+    v1 = np.asarray(v, dtype=float).reshape(-1)
+    v1 = v1 / np.linalg.norm(v1)
+    v0 = np.zeros(n)
+    bet = 0.0
+    VV = np.zeros((n, m))
+    alpha, beta = np.zeros(m), np.zeros(m)
+    traces = []
+    n_test = min(8 * nev, m)
+    k = 0
+    while k < m:
+        VV[:, k] = v1
+        w = B @ v1 - bet * v0
+        alp = np.vdot(v1, w)
+        w = w - alp * v1
+        bet = np.linalg.norm(w)
+        v0 = v1
+        v1 = w * (1.0 / bet)
+        alpha[k], beta[k] = alp, bet
+        k += 1
+        if test and ((k >= n_test and k % 10 == 0) or k == m):
+            T = np.diag(alpha[:k]) + np.diag(beta[:k - 1], 1) + np.diag(beta[:k - 1], -1)
+            traces.append(np.sum(np.sort(np.linalg.eigvalsh(T))[:nev]))
+            if len(traces) > 1:
+                lim = tol * traces[-2] if test == 1 else tol * abs(traces[-2])
+                if abs(traces[-1] - traces[-2]) < lim:
+                    break
+    T = np.diag(alpha[:k]) + np.diag(beta[:k - 1], 1) + np.diag(beta[:k - 1], -1)
+    rr, X = scipy.linalg.eigh(T)
+    order = np.argsort(rr)
+    return VV[:, :k], alpha[:k], beta[:k], k, rr[order], X[:, order]
+
+
+def distinct_count(rr, gap: float = 1e-5) -> int:
+    """Number of values left after the reference's near-duplicate pruning of
+    the ascending Ritz values (lanczosForChsubsp.py:148-154, lanczos.py:165-174):
+    walking upwards, a value within `gap` of the last kept one is dropped."""
+    rr = np.asarray(rr)
+    if rr.size == 0:
+        return 0
+    kept, anchor = 1, rr[0]
+    for x in rr[1:]:
+        if abs(anchor - x) >= gap:
+            kept += 1
+            anchor = x
+    return kept
+
+
+def ghost_width(nev: int, rr, k: int) -> int:
+    """mev = int(min(nev * min(1.8 ** (len(rr)/distinct), 3.2), k)):
+    lanczosForChsubsp.py:156-157, lanczos.py:177-179."""
+    mult = min(1.8 ** (len(rr) / distinct_count(rr)), 3.2)
+    return int(min(nev * mult, k))
+
+
+def _krylov_ritz(B, VV, X, mev, nev):
+    """W = VV X[:, :mev], Householder QR, Rayleigh-Ritz (upper triangle
+    mirrored), the nev lowest pairs: lanczosForChsubsp.py:159-190 and
+    lanczos.py:182-221."""
+    W = VV @ X[:, :mev]
+    W, _ = scipy.linalg.qr(W, mode="economic", pivoting=False)
+    G = _gram_upper(B @ W, W)
+    rr, Q = scipy.linalg.eigh(G)
+    order = np.argsort(rr)
+    return W @ Q[:, order[:nev]], rr[order][:nev]
+
+
+def lanczos_for_chsubsp(B, nev: int, v, m: int):
+    """Eigensolvers/lanczosForChsubsp.py:7-193 (reorth = 0): returns
+    (W n x nev, lam[nev], bound) with bound = max|theta| + beta_k."""
+    n = B.shape[0]
+    VV, _, beta, k, rr, X = lanczos_krylov(B, v, m, nev, 0 if n > 35000 else 1)
+    bound = float(np.max(np.abs(rr)) + beta[k - 1])
+    W, lam = _krylov_ritz(B, VV, X, ghost_width(nev, rr, k), nev)
+    return W, lam, bound
+
+
+def chsubsp(deg: int, nev: int, H):
+    """Chebyshev subspace iteration from a Lanczos start,
+    Eigensolvers/chsubsp.py:10-91: Lanczos with max(3 nev, 450) steps, then
+    at most 30 rounds of scaled filter + QR + Rayleigh-Ritz until the Ritz
+    trace moves by less than 5 %."""
+    n = H.shape[0]
+    W, ritzv, upperb = lanczos_for_chsubsp(H, nev, np.random.randn(n), max(3 * nev, 450))
+    tr0 = np.sum(ritzv)
+    for _ in range(30):
+        lam1, lowerb = np.min(ritzv), np.max(ritzv)
+        if lowerb > upperb:
+            raise ValueError("bounds are wrong")
+        W = ch_filter(H, W, deg, lam1, lowerb, upperb)
+        W, _ = scipy.linalg.qr(W, mode="economic", pivoting=False)
+        G = _gram_upper(H @ W, W)
+        ritzv, Q = scipy.linalg.eigh(G)
+        W = W @ Q
+        tr1 = np.sum(ritzv[:nev])
+        if abs(tr1 - tr0) < 0.05 * abs(tr1):
+            break
+        tr0 = tr1
+    return W, ritzv
+
+
+def lanczos(B, nev: int, v, m: int, tol: float = 1e-5):
+    """Eigensolvers/lanczos.py:10-223 (reorth = 0, no polynomial filtering),
+    with the convergence test of its GPU twin (lanczos_gpu.py:128-137) for
+    n <= 35000.  Returns (W n x nev, lam[nev])."""
+    n = B.shape[0]
+    VV, _, _, k, rr, X = lanczos_krylov(B, v, m, nev, 0 if n > 35000 else 2, tol)
+    return _krylov_ritz(B, VV, X, ghost_width(nev, rr, k), nev)
+
+
 def fermi_dirac(lam, ef, temp, nelec):
     """Eigensolvers/FermiDirac.py:3-31 (kT = T * 6.33327186e-06, spin 1)."""
     kT = temp * 6.33327186e-06
@@ -681,14 +806,17 @@ def build_system(atoms: list, *, h: float, radius: float, elements: dict | None 
 
 class OracleSCF:
     """The SCF of rsdft_solver.run_rsdft_calculation (rsdft_solver.py:156-462)
-    for density_method = sad, diagmeth = 3, adaptive_scheme = 0, cg_prec = 0,
+    for density_method = sad, adaptive_scheme = 0, cg_prec = 0, any diagmeth
+    (rsdft_solver.py:287-317: 3 first_filt, 2 chsubsp, 0 lanczos, then chefsi1;
+    1 lanczos at every iteration),
     split into setup() and step() so that a bounded number of iterations can
     be timed.  Wall times (s) are kept in t_setup and in each history entry."""
 
     def __init__(self, domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
                  maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, z_charge: float = 0.0,
-                 elements=None, tables=None):
+                 elements=None, tables=None, diagmeth: int = 3):
         self.domain, self.atoms, self.nev, self.poldeg, self.tol = domain, atoms, nev, poldeg, tol
+        self.diagmeth = diagmeth
         self.maxits, self.fd_order, self.fermi_temp, self.z_charge = maxits, fd_order, fermi_temp, z_charge
         self.elements = elements or load_elements()
         self.tables = tables or load_tables()
@@ -729,7 +857,13 @@ class OracleSCF:
         n, h, nev = self.n, self.domain["h"], self.nev
         self.its += 1
         B = (self.half_a_plus_vnl + sp.diags(self.pot, 0, shape=(n, n))).tocsr()
-        if self.its == 1:
+        dm = self.diagmeth
+        if dm == 1 or (self.its == 1 and dm == 0):
+            # rsdft_solver.py:63-68 (CPU vector) and :47-49 (nev + 500 steps)
+            self.W, self.lam = lanczos(B, nev + 15, np.random.randn(n, 1), nev + 500, 1e-5)
+        elif self.its == 1 and dm == 2:
+            self.W, self.lam = chsubsp(self.poldeg, nev + 15, B)
+        elif self.its == 1:
             self.W, self.lam = first_filt(nev + 15, B, self.poldeg)
         else:
             self.W, self.lam = chefsi1(self.W, self.lam, self.poldeg, nev, B)
@@ -761,13 +895,13 @@ class OracleSCF:
 
 def run_scf(domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
             maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, seed: int | None = None,
-            z_charge: float = 0.0, elements=None, tables=None, log=None) -> dict:
+            z_charge: float = 0.0, elements=None, tables=None, log=None, diagmeth: int = 3) -> dict:
     """Run OracleSCF to convergence; with a seed, numpy's global generator is
     seeded first so the random draws match a reference run with that seed."""
     if seed is not None:
         np.random.seed(seed)
     scf = OracleSCF(domain, atoms, nev=nev, poldeg=poldeg, tol=tol, maxits=maxits, fd_order=fd_order,
-                    fermi_temp=fermi_temp, z_charge=z_charge, elements=elements, tables=tables)
+                    fermi_temp=fermi_temp, z_charge=z_charge, elements=elements, tables=tables, diagmeth=diagmeth)
     scf.setup()
     while not scf.done():
         rec = scf.step()

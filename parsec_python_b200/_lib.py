@@ -38,6 +38,10 @@ _SIGS = {
     "psc_laplacian_apply": ([_P, _P, _P, c_int, c_long, _P], c_int),
     "psc_cheb_filter": ([_P, c_int, c_int, c_int, _P, _P, _P, c_long, c_int, POINTER(c_int), _P], c_int),
     "psc_lanczos_bound": ([_P, c_int, c_ulonglong, _P, _P], c_int),
+    "psc_lanczos_run": ([_P, _P, c_ulonglong, c_int, c_int, _P, c_long, _P, _P], c_int),
+    "psc_tridiag_eig": ([_P, _P, c_int, c_int, _P, _P, c_long, _P], c_int),
+    "psc_orthonormalize_rank": ([_P, c_int, _P, _P, c_long, c_int, c_double, POINTER(c_int), POINTER(c_int), _P],
+                                c_int),
     "psc_filter_bounds": ([_P, c_int, _P, c_int, _P, _P, _P], c_int),
     "psc_orthonormalize": ([_P, c_int, _P, _P, c_long, c_int, c_int, POINTER(c_int), _P], c_int),
     "psc_rayleigh_ritz": ([_P, c_int, _P, _P, c_long, c_int, _P, _P], c_int),

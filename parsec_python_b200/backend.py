@@ -44,12 +44,12 @@ class GpuRuntime:
     def chefsi1(self, W, ritzv, deg, nev, H):
         return gpu.chefsi1(W, ritzv, deg, nev, H)
 
-    def lanczos(self, *args, **kwargs):
-        raise NotImplementedError("diagmeth 0/1 (full Lanczos, Eigensolvers/lanczos.py) is not implemented; "
-                                  "use diagmeth = 3")
+    def lanczos(self, B, nev, v, m, tol, *args):
+        """Eigensolvers/lanczos.py:10 signature; v None draws the start on the device."""
+        return gpu.lanczos(B, nev, v, m, tol, dtype=self.block_dtype)
 
-    def chsubsp(self, *args, **kwargs):
-        raise NotImplementedError("diagmeth 2 (Eigensolvers/chsubsp.py) is not implemented; use diagmeth = 3")
+    def chsubsp(self, deg, nev, H):
+        return gpu.chsubsp(deg, nev, H, dtype=self.block_dtype)
 
     def occupations(self, lam, temp, nelec, tol):
         return gpu.occupations(self.ctx, lam, temp, nelec, tol)

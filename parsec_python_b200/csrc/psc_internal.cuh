@@ -106,6 +106,9 @@ struct psc_ctx {
 
   // Lanczos vectors (double)
   double* lz_v = nullptr;        // [3][n]
+  // tridiagonal eigensolver: LU factors of T - lambda I per cluster start
+  double* tri_work = nullptr;
+  size_t tri_work_doubles = 0;
 
   // PCG vectors (double)
   double* cg_r = nullptr;

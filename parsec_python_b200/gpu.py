@@ -277,6 +277,154 @@ def chefsi1(W: torch.Tensor, ritzv: torch.Tensor, deg: int, nev: int, H: Hamilto
     return W, ritz
 
 
+def _start_vector(ctx: GridContext, v) -> torch.Tensor | None:
+    if v is None:
+        return None
+    if isinstance(v, torch.Tensor):
+        t = v.reshape(-1).to(device=ctx.device, dtype=torch.float64)
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(-1))).to(ctx.device)
+    if t.numel() != ctx.n:
+        raise ValueError(f"start vector has {t.numel()} entries, expected {ctx.n}")
+    return t.contiguous()
+
+
+def distinct_count(rr: np.ndarray, gap: float = 1e-5) -> int:
+    """Values left after the reference's near-duplicate pruning of the
+    ascending Lanczos Ritz values (Eigensolvers/lanczosForChsubsp.py:148-154,
+    lanczos.py:165-174): walking upwards, a value within `gap` of the last
+    kept one is dropped."""
+    if rr.size == 0:
+        return 0
+    kept, anchor = 1, rr[0]
+    for x in rr[1:]:
+        if abs(anchor - x) >= gap:
+            kept += 1
+            anchor = x
+    return kept
+
+
+def lanczos_krylov(H: Hamiltonian, nev: int, m: int, test: int, v=None, tol: float = 1e-5):
+    """m Lanczos steps with the basis kept in VV ((m+1) x n rows = columns of
+    an n x (m+1) block); Eigensolvers/lanczosForChsubsp.py:33-132 and
+    lanczos.py:38-146.  test 0: none; 1: lanczosForChsubsp's stop rule
+    |tr1 - tr0| < tol * tr0; 2: lanczos_gpu.py:128-137's |tr1 - tr0| < tol |tr0|,
+    with traces of the nev lowest eigenvalues of T_k at k >= min(8 nev, m),
+    k % 10 == 0, and at k = m.  Returns (VV, ab, k, rr) with rr on the host."""
+    ctx = H.ctx
+    n = ctx.n
+    VV = ctx.empty(m + 1, n)
+    ab = ctx.zeros(2 * m)
+    evals = ctx.empty(m)
+    v0 = _start_vector(ctx, v)
+    seed = ctx.next_seed()
+    if not test:
+        ctx.call("psc_lanczos_run", _p(v0), seed, 0, m, _p(VV), n, _p(ab), _stream())
+        k = m
+    else:
+        n_test = min(8 * nev, m)
+        stops = sorted({c for c in range(10, m + 1, 10) if c >= n_test} | {m})
+        traces, k = [], 0
+        for c in stops:
+            ctx.call("psc_lanczos_run", _p(v0), seed, k, c, _p(VV), n, _p(ab), _stream())
+            k = c
+            ctx.call("psc_tridiag_eig", _p(ab), k, 0, _p(evals), None, 0, _stream())
+            traces.append(float(evals[:min(nev, k)].sum().item()))
+            if len(traces) > 1:
+                lim = tol * traces[-2] if test == 1 else tol * abs(traces[-2])
+                if abs(traces[-1] - traces[-2]) < lim:
+                    break
+    ctx.call("psc_tridiag_eig", _p(ab), k, 0, _p(evals), None, 0, _stream())
+    return VV, ab, k, evals[:k].cpu().numpy()
+
+
+def _krylov_ritz(H: Hamiltonian, VV: torch.Tensor, ab: torch.Tensor, k: int, rr: np.ndarray, nev: int,
+                 dtype=torch.float64):
+    """W = VV X[:, :mev] with mev = int(min(nev * min(1.8 ** (k / distinct), 3.2), k)),
+    orthonormalised (dependent columns dropped), Rayleigh-Ritz, the nev lowest
+    pairs (lanczosForChsubsp.py:148-190, lanczos.py:164-221)."""
+    ctx = H.ctx
+    n = ctx.n
+    mev = int(min(nev * min(1.8 ** (len(rr) / distinct_count(rr)), 3.2), k))
+    evals = ctx.empty(k)
+    X = ctx.empty(mev, k)                       # k x mev, column-major, ld k
+    ctx.call("psc_tridiag_eig", _p(ab), k, mev, _p(evals), _p(X), k, _stream())
+    W = ctx.empty(max(mev, nev), n)
+    ctx.call("psc_gemm_nn", F64, _p(VV), n, k, _p(X), mev, _p(W), n, _stream())
+    T = torch.empty_like(W)
+    rank, which = c_int(), c_int()
+    ctx.call("psc_orthonormalize_rank", F64, _p(W), _p(T), n, mev, 1e-10, byref(rank), byref(which), _stream())
+    B, S = (T, W) if which.value else (W, T)
+    r = rank.value
+    if r < nev:
+        # as many directions as the reference's QR returns: fresh random
+        # columns after the kept ones, then the whole block orthonormalised
+        ctx.call("psc_random", F64, 1, ctx.next_seed(), _p(B[r:]), n, n, nev - r, _stream())
+        B, S = orthonormalize(ctx, B[:nev], S[:nev])
+        r = nev
+    V = S[:r]
+    ritz = ctx.empty(r)
+    ctx.call("psc_rayleigh_ritz", F64, _p(B[:r]), _p(V), n, r, _p(ritz), _stream())
+    W = V[:nev].contiguous() if dtype == torch.float64 else V[:nev].to(dtype)
+    return W, ritz[:nev].clone(), mev, r
+
+
+def lanczos_for_chsubsp(H: Hamiltonian, nev: int, m: int, v=None, dtype=torch.float64):
+    """Eigensolvers/lanczosForChsubsp.py:7-193: (W, lam, bound) with bound =
+    max|theta| + beta_k of the Lanczos tridiagonal."""
+    ctx = H.ctx
+    VV, ab, k, rr = lanczos_krylov(H, nev, m, 0 if ctx.n > 35000 else 1, v)
+    beta = float(ab[2 * k - 1].item())
+    bound = float(np.max(np.abs(rr)) + beta)
+    W, lam, _, _ = _krylov_ritz(H, VV, ab, k, rr, nev, dtype)
+    del VV
+    return W, lam, bound
+
+
+def chsubsp(deg: int, nev: int, H: Hamiltonian, v=None, dtype=torch.float64, log_trace=None):
+    """Chebyshev subspace iteration from a Lanczos start
+    (Eigensolvers/chsubsp.py:10-91): Lanczos with max(3 nev, 450) steps, then
+    at most 30 rounds of scaled filter + orthonormalisation + Rayleigh-Ritz
+    until the Ritz trace moves by less than 5 %."""
+    ctx = H.ctx
+    W, ritzv, upperb = lanczos_for_chsubsp(H, nev, max(3 * nev, 450), v, dtype)
+    up = torch.tensor([upperb], dtype=torch.float64).to(ctx.device)
+    bounds = ctx.empty(3)
+    T = torch.empty_like(W)
+    k = W.shape[0]
+    ritz_h = ritzv.cpu().numpy()
+    tr0 = float(np.sum(ritz_h))
+    for it in range(30):
+        if np.max(ritz_h) > upperb:
+            raise ValueError("bounds are wrong")
+        ctx.call("psc_filter_bounds", 0, _p(ritzv), k, _p(up), _p(bounds), _stream())
+        W, T = cheb_filter(H, W, T, deg, bounds, mode=0)
+        ritzv = ctx.empty(k)
+        W, T = subspace_rr(ctx, W, T, ritzv)
+        ritz_h = ritzv.cpu().numpy()
+        tr1 = float(np.sum(ritz_h[:nev]))
+        if log_trace:
+            log_trace(it + 1, tr1)
+        if abs(tr1 - tr0) < 0.05 * abs(tr1):
+            break
+        tr0 = tr1
+    ctx.check_status()
+    return W, ritzv
+
+
+def lanczos(H: Hamiltonian, nev: int, v=None, m: int | None = None, tol: float = 1e-5, dtype=torch.float64):
+    """Eigensolvers/lanczos.py:10-223 (reorth = 0), convergence test as its
+    GPU twin lanczos_gpu.py:128-137 for n <= 35000: (W, lam)."""
+    ctx = H.ctx
+    if m is None:
+        raise ValueError("lanczos needs the number of steps m")
+    VV, ab, k, rr = lanczos_krylov(H, nev, int(m), 0 if ctx.n > 35000 else 2, v, tol)
+    W, lam, _, _ = _krylov_ritz(H, VV, ab, k, rr, nev, dtype)
+    del VV
+    ctx.check_status()
+    return W, lam
+
+
 def occupations(ctx: GridContext, lam: torch.Tensor, temp: float, nelec: float, tol: float):
     """Fermi level and occupations (Eigensolvers/occupations.py:5-56)."""
     lam = lam.contiguous()

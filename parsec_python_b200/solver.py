@@ -22,6 +22,11 @@ def _scaled_poldeg(poldeg: int, modifier: float) -> int:
     return max(1, int(round(poldeg * modifier)))
 
 
+def _scaled_lanczos_steps(nev: int, modifier: float) -> int:
+    """rsdft_solver.py:47-49: Lanczos steps of diagmeth 0/1."""
+    return nev + max(1, int(round(500 * modifier)))
+
+
 def energy_components(lam, occ, nev, sums, exc, e_nuc, h) -> EnergyComponents:
     """rsdft_solver.py:128-153: E = 4 sum(lam f) - E_H + E_xc - int(rho V_xc) + E_nuc (Ry)."""
     eig = 4.0 * float(np.sum(lam[:nev] * occ[:nev]))
@@ -136,9 +141,9 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
     mixer = gpu.Mixer(ctx, capacity=s.maxits + 2)
     H = gpu.Hamiltonian(ctx, pot)
     if s.adaptive_scheme != 0 and sum(problem.input_data.n_atom) <= 2:
-        deg_mod = 0.75
+        deg_mod, m_mod = 0.75, 0.95
     else:
-        deg_mod = 1.0
+        deg_mod, m_mod = 1.0, 1.0
     nev = problem.nev
     k = nev + 15
     W = lam = occ = None
@@ -178,7 +183,7 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
             W, lam = backend.chsubsp(deg, k, H)
         elif s.diagmeth == 1 or (its == 1 and s.diagmeth == 0):
             label = f"lanczos_{backend.label} (diagmeth={s.diagmeth})"
-            W, lam = backend.lanczos(H, k)
+            W, lam = backend.lanczos(H, k, None, _scaled_lanczos_steps(nev, m_mod), 1e-5)
         else:
             label = f"chebsf_{backend.label} (diagmeth={s.diagmeth})"
             W, lam = backend.chefsi1(W, lam, deg, nev, H)
@@ -204,11 +209,13 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         exc = float(hv[2 * k + 4])
         err_new = float(np.sqrt(sm[0]) / np.sqrt(sm[1]))
         if s.adaptive_scheme == 0 or err_new > 1 or err_new > 2 * err:
-            deg_mod = 1.0
+            deg_mod, m_mod = 1.0, 1.0
         elif err_new > err:
             deg_mod = min(1.1, deg_mod + 0.2)
+            m_mod = min(1.1, deg_mod + 0.05)
         elif 3 * err_new < err:
             deg_mod = max(0.5, deg_mod - 0.1)
+            m_mod = max(0.9, deg_mod - 0.025)
         err = err_new
         energies = energy_components(lam_h, occ_h, nev, sm, exc, e_nuc0, h)
         diag_t, hart_t = ev.seconds("d0", "d1"), ev.seconds("h0", "h1")

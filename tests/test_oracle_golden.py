@@ -160,3 +160,83 @@ def test_scf_h2o_small_matches_reference(golden_dir, meta, tables):
     assert np.abs(r["eigenvalues"] - sc["eigenvalues"]).max() < 1e-10
     h = ms["domain"]["h"]
     assert np.abs(r["rho"] - sc["rho"]).sum() * h ** 3 < 1e-9
+
+
+# ---- Lanczos-based eigensolvers (diagmeth 0/1/2), tests/golden/make_golden_lanczos.py ----
+H2O = [("O", [[0.0, 0.0, 0.0]]), ("H", [[0.757, 0.586, 0.0], [-0.757, 0.586, 0.0]])]
+
+
+def _h2o_atoms():
+    return [{"typ": t, "coord": np.array(c) / O.A0_ANG} for t, c in H2O]
+
+
+@pytest.fixture(scope="module")
+def lz(golden_dir):
+    return np.load(golden_dir / "ref_lanczos.npz"), json.loads((golden_dir / "ref_lanczos.json").read_text())
+
+
+def _hamiltonian(dom, tables, pot_ref):
+    elements, tab = tables
+    n = dom["nx"] ** 3
+    rho0, hpot0, ppot, _ = O.pseudo_diag(dom, _h2o_atoms(), elements, tab)
+    pot = ppot + hpot0
+    np.testing.assert_array_equal(pot, pot_ref)
+    vnl = O.nonlocal_csr(O.projectors(dom, _h2o_atoms(), elements, tab), n)
+    return (0.5 * O.laplacian(dom, 8) + vnl + sp.diags(pot, 0, shape=(n, n))).tocsr()
+
+
+@pytest.mark.parametrize("tag", ["small", "big"])
+def test_lanczos_for_chsubsp_matches_reference(lz, tables, tag):
+    """Both branches of lanczosForChsubsp: with the convergence test
+    (n = 13824) and without it (n = 39304 > 35000)."""
+    g, meta = lz
+    dom = meta[tag]["domain"]
+    B = _hamiltonian(dom, tables, g[f"{tag}_pot"])
+    W, lam, bound = O.lanczos_for_chsubsp(B, 27, g[f"{tag}_v"].copy(), 450)
+    assert np.abs(lam - g[f"{tag}_lfc_lam"]).max() < 1e-12
+    assert abs(bound - float(g[f"{tag}_lfc_bound"])) < 1e-12 * abs(bound)
+    assert np.abs((W[:, :4] ** 2).sum(1) - g[f"{tag}_lfc_rho4"]).max() < 1e-12
+
+
+def test_chsubsp_and_lanczos_match_reference(lz, tables):
+    g, meta = lz
+    B = _hamiltonian(meta["small"]["domain"], tables, g["small_pot"])
+    np.random.seed(meta["small"]["chsubsp_seed"])
+    W, ritz = O.chsubsp(10, 27, B)
+    assert np.abs(ritz - g["small_ch_ritz"]).max() < 1e-12
+    assert np.abs((W[:, :4] ** 2).sum(1) - g["small_ch_rho4"]).max() < 1e-12
+    # the CPU lanczos.py cannot run its own convergence test (n <= 35000)
+    assert meta["small"]["lanczos_cpu"] != "ran"
+    B = _hamiltonian(meta["big"]["domain"], tables, g["big_pot"])
+    W, lam = O.lanczos(B, 27, g["big_lz_v"].copy(), 512, 1e-5)
+    assert np.abs(lam - g["big_lz_lam"]).max() < 1e-12
+    assert np.abs((W[:, :4] ** 2).sum(1) - g["big_lz_rho4"]).max() < 1e-12
+
+
+def test_distinct_count_is_the_reference_pruning():
+    """The greedy walk equals the reference's repeated np.delete pruning
+    (lanczosForChsubsp.py:148-154) on sorted inputs with ties and chains."""
+    rng = np.random.default_rng(5)
+    for trial in range(200):
+        base = np.sort(rng.uniform(-2, 2, rng.integers(1, 40)))
+        rr = np.sort(np.concatenate([base, base[: rng.integers(0, len(base) + 1)] + rng.uniform(-2e-5, 2e-5)]))
+        ref = rr.copy()
+        c = 0
+        while c < len(ref) - 1:
+            ref = np.delete(ref, np.where(np.abs(ref[c] - ref[c + 1:]) < 1e-5)[0] + c + 1)
+            c += 1
+        assert O.distinct_count(rr) == len(ref)
+
+
+def test_scf_diagmeth2_matches_reference(lz, tables):
+    elements, tab = tables
+    g, meta = lz
+    ms = meta["scf_diagmeth2"]
+    r = O.run_scf(ms["domain"], _h2o_atoms(), nev=12, poldeg=10, tol=1e-6, seed=0, elements=elements, tables=tab,
+                  diagmeth=2)
+    assert r["iterations"] == ms["iterations"]
+    # 450 Lanczos steps without reorthogonalisation amplify the last-bit
+    # differences of the sparse products (the oracle's CSR column order is not
+    # the reference's), so the trajectory agrees to 1e-9 Ry here, not 1e-12
+    assert abs(r["energies"]["total_ry"] - ms["total_ry"]) < 1e-8
+    assert np.abs(r["eigenvalues"][:12] - g["scf2_eigenvalues"][:12]).max() < 1e-8
