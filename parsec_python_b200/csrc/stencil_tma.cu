@@ -3,16 +3,21 @@
 // with plane windows streamed into shared memory by 1-D bulk copies.
 //
 // A CTA owns S = 512 (FP64) or 1024 (FP32) consecutive flat xy points of one
-// column and a chunk of z planes.  For every plane the points it needs -- its own S points plus R
-// rows of y halo on each side -- are one contiguous range of the plane, so a
-// single cp.async.bulk (no tensor map, no multicast) moves it into a slot of
-// a ring of NBUF = R + 1 + D shared-memory windows (D = 3 FP64, 4 FP32),
-// completing on the slot's mbarrier.  The z neighbours of each point live in a register queue fed from
-// the ring; x and y neighbours are read from the current plane's window with
-// 16-byte loads (each thread owns a run of 2 FP64 or 4 FP32 points, which may
-// cross a row edge; the run itself comes from the queue).  Prev and pot are read straight from global memory one
-// plane ahead, so they cost no shared-memory traffic.  D planes are in flight
-// per CTA at all times, which is what keeps HBM busy.
+// column and a chunk of z planes.  For every plane the points it needs -- its
+// own S points plus R rows of y halo on each side -- are one contiguous range
+// of the plane, so a single cp.async.bulk (no tensor map, no multicast) moves
+// it into a slot of a ring of NBUF = R + 1 + D shared-memory windows (D = 3),
+// completing on the slot's mbarrier.  Each slot ends with one zero vector.
+// The z neighbours of each point live in a register queue fed from the ring;
+// x and y neighbours are read from the current plane's window with 16-byte
+// loads (each thread owns a run of 2 FP64 or 4 FP32 points).  When the run
+// cannot cross a row edge (2 | nx for FP64, 4 | nx for FP32) the x vectors
+// outside the row are read from the zero vector, so the x terms need no
+// per-point masks; otherwise each point masks its x neighbours by its
+// distances to the row edges.  Prev and pot are prefetched three planes ahead
+// by per-thread 16-byte cp.async copies into a small shared-memory ring that
+// each thread reads back itself (no block-wide handshake).  D planes of X are
+// in flight per CTA at all times, which is what keeps HBM busy.
 //
 // Every mbarrier wait is bounded: on timeout the CTA records the failure in
 // status[3] and carries on without waiting (results are then garbage but the
@@ -29,10 +34,20 @@ namespace {
 constexpr int TNT = 256;          // threads per CTA
 // planes prefetched beyond the one consumed next: deeper for FP32, whose
 // planes are consumed twice as fast
+#ifndef PSC_STENCIL_PREFETCH_F64
+#define PSC_STENCIL_PREFETCH_F64 3
+#endif
+#ifndef PSC_STENCIL_PREFETCH_F32
+#define PSC_STENCIL_PREFETCH_F32 3
+#endif
+#ifndef PSC_STENCIL_PP_SLOTS
+#define PSC_STENCIL_PP_SLOTS 4
+#endif
 template <typename T>
 __host__ __device__ constexpr int prefetch_depth() {
-  return sizeof(T) == 8 ? 3 : 4;
+  return sizeof(T) == 8 ? PSC_STENCIL_PREFETCH_F64 : PSC_STENCIL_PREFETCH_F32;
 }
+constexpr int PP_SLOTS = PSC_STENCIL_PP_SLOTS;  // Prev/pot slots: the plane in use + the prefetched
 constexpr long WAIT_LIMIT = 1L << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -64,6 +79,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
@@ -157,6 +179,7 @@ k_stencil_tma(TmaArgs<T> A) {
   constexpr int VW = VecOf<T>::W;          // points per thread
   constexpr int TS = slab_points<T>();     // points per slab
   constexpr int NBUF = R + 1 + prefetch_depth<T>();   // X plane windows resident
+  constexpr int NS = PP_SLOTS;
   constexpr int Q = 2 * R + 1;             // z queue length
   constexpr int HV = (R + VW - 1) / VW;    // x-halo vectors on each side
   constexpr int NPV = 2 * HV + 1;          // x vectors per row (the centre one comes from the queue)
@@ -166,8 +189,10 @@ k_stencil_tma(TmaArgs<T> A) {
   const int nxy = nx * ny;
   const int H = R * nx;
   const int WIN = TS + 2 * H;
-  T* ring = reinterpret_cast<T*>(smem_raw);                                  // [NBUF][WIN]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + (size_t)NBUF * WIN);  // [NBUF]
+  const int WS = WIN + VW;  // slot stride: the window and one zero vector
+  T* ring = reinterpret_cast<T*>(smem_raw);                                   // [NBUF][WS]
+  T* pring = ring + (size_t)NBUF * WS;                                        // [NS][2][TS]: Prev, pot
+  uint64_t* bars = reinterpret_cast<uint64_t*>(pring + (size_t)NS * 2 * TS);  // [NBUF]
   __shared__ int s_fail;
 
   const int slab0 = blockIdx.x * TS;
@@ -190,12 +215,13 @@ k_stencil_tma(TmaArgs<T> A) {
   const uint32_t xbytes = (uint32_t)((v1 - v0) * sizeof(T));
   const int seff = min(TS, nxy - slab0);
 
-  // zero the parts of every window that lie outside the plane (never written by the copies)
+  // zero the parts of every window that lie outside the plane and the pad
+  // vector after it (neither is ever written by the copies)
   for (int s = 0; s < NBUF; ++s) {
-    T* w = ring + (size_t)s * WIN;
-    for (int i = threadIdx.x; i < WIN; i += TNT) {
+    T* w = ring + (size_t)s * WS;
+    for (int i = threadIdx.x; i < WS; i += TNT) {
       const int f = w0 + i;
-      if (f < v0 || f >= v1) w[i] = T(0);
+      if (i >= WIN || f < v0 || f >= v1) w[i] = T(0);
     }
   }
   if (threadIdx.x == 0) {
@@ -210,7 +236,7 @@ k_stencil_tma(TmaArgs<T> A) {
     const int s = (p - z0) % NBUF;
     uint64_t* bar = &bars[s];
     mbar_expect_tx(bar, xbytes);
-    bulk_g2s(ring + (size_t)s * WIN + (v0 - w0), Xc + (long)p * nxy + v0, xbytes, bar);
+    bulk_g2s(ring + (size_t)s * WS + (v0 - w0), Xc + (long)p * nxy + v0, xbytes, bar);
   };
   if (threadIdx.x == 0) {
     for (int p = z0; p < min(zlast, z0 + NBUF); ++p) issue_x(p);
@@ -222,17 +248,23 @@ k_stencil_tma(TmaArgs<T> A) {
   const int q = slab0 + loc;
   const int s_c = H + loc;  // window offset of the run
 
-  // Prev and pot of the run, one plane ahead in registers (P may alias Y:
-  // a point of P is read before this thread overwrites it)
-  T pv_next[VW], po_next[VW];
-#pragma unroll
-  for (int j = 0; j < VW; ++j) pv_next[j] = po_next[j] = T(0);
-  auto load_pp = [&](int z) {
-    if (!own || z >= z1) return;
-    if (Pc) vload(Pc + (long)z * nxy + q, pv_next);
-    if (has_pot) vload(A.pot + (long)z * nxy + q, po_next);
+  // Prev and pot of the run, NS-1 planes ahead: each thread copies its own
+  // 16-byte run with cp.async into slot (z - z0) mod NS and reads it back
+  // itself, so no block-wide handshake is needed.  One commit group per
+  // plane (empty ones too), so "wait until at most NS-2 groups are pending"
+  // means plane z has landed.  (P may alias Y: plane z of P is read before
+  // this thread stores plane z of Y.)
+  const bool use_pp = Pc || has_pot;
+  auto copy_pp = [&](int z) {
+    if (own && z < z1) {
+      T* d = pring + (size_t)((z - z0) % NS) * 2 * TS + loc;
+      if (Pc) cp_async16(d, Pc + (long)z * nxy + q);
+      if (has_pot) cp_async16(d + TS, A.pot + (long)z * nxy + q);
+    }
+    cp_async_commit();
   };
-  load_pp(z0);
+  if (use_pp)
+    for (int z = z0; z < z0 + NS - 1; ++z) copy_pp(z);
 
   // z queue: planes below the chunk from global memory, z0 .. z0+R-1 from the ring
   T zq[VW][Q];
@@ -257,15 +289,26 @@ k_stencil_tma(TmaArgs<T> A) {
       if (!fail && !mbar_wait(&bars[s], ((p - z0) / NBUF) & 1)) fail = true;
       if (own) {
         T v[VW];
-        vload(ring + (size_t)s * WIN + s_c, v);
+        vload(ring + (size_t)s * WS + s_c, v);
 #pragma unroll
         for (int j = 0; j < VW; ++j) zq[j][R + i] = v[j];
       }
     }
   }
 
-  // per-point distances to the row edges, capped at R: a neighbour d > el
-  // (left) or d > er (right) lies across the edge and gets weight 0
+  // When VW divides nx, a thread's run lies in one row and every aligned
+  // x vector around it is either wholly in that row or wholly outside it:
+  // the outside ones are read from the slot's zero pad, so the x terms need
+  // no per-point masks.  Otherwise (FP32 runs crossing a row edge) each point
+  // keeps its distances to the row edges, capped at R: a neighbour d > el
+  // (left) or d > er (right) lies across the edge and gets weight 0.
+  constexpr bool EXACT = (YA == VW);
+  int xo[NPV];
+#pragma unroll
+  for (int v = 0; v < NPV; ++v) {
+    const int xv = (own ? q % nx : 0) - OFF + v * VW;  // first x of vector v
+    xo[v] = (xv >= 0 && xv + VW <= nx) ? s_c - OFF + v * VW : WIN;
+  }
   int el[VW], er[VW];
 #pragma unroll
   for (int j = 0; j < VW; ++j) {
@@ -291,20 +334,63 @@ k_stencil_tma(TmaArgs<T> A) {
         if (pf < nz) {
           const int s = (pf - z0) % NBUF;
           if (!fail && !mbar_wait(&bars[s], ((pf - z0) / NBUF) & 1)) fail = true;
-          if (own) vload(ring + (size_t)s * WIN + s_c, f);
+          if (own) vload(ring + (size_t)s * WS + s_c, f);
         }
 #pragma unroll
         for (int j = 0; j < VW; ++j) zq[j][(u + 2 * R) % Q] = f[j];
       }
       T pvv[VW], pov[VW];
 #pragma unroll
-      for (int j = 0; j < VW; ++j) {
-        pvv[j] = pv_next[j];
-        pov[j] = po_next[j];
+      for (int j = 0; j < VW; ++j) pvv[j] = pov[j] = T(0);
+      if (use_pp) {
+        copy_pp(z + NS - 1);
+        cp_async_wait<NS - 1>();
+        if (own) {
+          const T* pp = pring + (size_t)((z - z0) % NS) * 2 * TS + loc;
+          if (Pc) vload(pp, pvv);
+          if (has_pot) vload(pp + TS, pov);
+        }
       }
-      load_pp(z + 1);
-      const T* pl = ring + (size_t)((z - z0) % NBUF) * WIN;
-      if (own) {
+      const T* pl = ring + (size_t)((z - z0) % NBUF) * WS;
+      if (EXACT && own) {
+        T xs[NPV * VW];
+#pragma unroll
+        for (int v = 0; v < NPV; ++v) {
+          if (v == HV) {
+#pragma unroll
+            for (int j = 0; j < VW; ++j) xs[v * VW + j] = zq[j][(u + R) % Q];
+          } else {
+            vload(pl + xo[v], xs + v * VW);
+          }
+        }
+        const T* pc = pl + s_c;
+        T acc[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) acc[j] = c0 * xs[OFF + j];
+#pragma unroll
+        for (int d = 1; d <= R; ++d) {
+          T ym[VW], yp[VW];
+          vload(pc - d * nx, ym);
+          vload(pc + d * nx, yp);
+          const T cd = A.c[d - 1];
+#pragma unroll
+          for (int j = 0; j < VW; ++j) {
+            const T t = ((ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q])) +
+                        (xs[OFF + j - d] + xs[OFF + j + d]);
+            acc[j] += cd * t;
+          }
+        }
+        T o[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) {
+          const T xc = xs[OFF + j];
+          T a = acc[j];
+          if (has_pot) a += pov[j] * xc;
+          o[j] = ca * a + cb * xc;
+          if (Pc) o[j] += cg * pvv[j];
+        }
+        vstore(Yc + (long)z * nxy + q, o);
+      } else if (own) {
         // x neighbours: the aligned vectors around the run; the run itself is the queue's centre
         T xs[NPV * VW];
 #pragma unroll
@@ -400,8 +486,8 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   const int zchunk = (ctx->nz + nzc - 1) / nzc;
   nzc = (ctx->nz + zchunk - 1) / zchunk;
   constexpr int NBUF = R + 1 + prefetch_depth<T>();
-  const size_t win = TS + 2 * (size_t)R * ctx->nx;
-  const size_t smem = NBUF * win * sizeof(T) + NBUF * sizeof(uint64_t);
+  const size_t win = TS + 2 * (size_t)R * ctx->nx + VecOf<T>::W;   // window + zero pad vector
+  const size_t smem = (NBUF * win + (size_t)PP_SLOTS * 2 * TS) * sizeof(T) + NBUF * sizeof(uint64_t);
   if (smem > 220 * 1024) return -1;  // window too wide: the register-queue kernel takes it
   constexpr int VW = VecOf<T>::W;
   auto kern = (ctx->nx % VW == 0) ? k_stencil_tma<T, R, VW>
