@@ -112,6 +112,7 @@ extern "C" int psc_ctx_destroy(psc_ctx* ctx) {
   psc_dfree(ctx->mix_nv); psc_dfree(ctx->mix_tmp); psc_dfree(ctx->mix_coef); psc_dfree(ctx->mix_partial);
   psc_dfree(ctx->cg_x); psc_dfree(ctx->jac_v); psc_dfree(ctx->cg_p2); psc_dfree(ctx->cg_ro); psc_dfree(ctx->cg_bar);
   psc_dfree(ctx->tc_part); psc_dfree(ctx->tc_pairs); psc_dfree(ctx->tri_work);
+  for (auto& e : ctx->st_sched) psc_dfree(e.dev);
   if (ctx->cg_exec) cudaGraphExecDestroy(ctx->cg_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   delete ctx;

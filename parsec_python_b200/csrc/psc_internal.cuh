@@ -104,6 +104,15 @@ struct psc_ctx {
   void* tc_pairs = nullptr;      // int2 tile pairs (upper triangle)
   int tc_pairs_k = 0;
 
+  // TMA stencil work tables (column, slab, z range per CTA), one per launch shape
+  struct StencilSched {
+    long long key = 0;
+    int n = 0;
+    int* dev = nullptr;
+    std::vector<int> host;   // the uploaded copy (kept alive for the asynchronous upload)
+  };
+  std::vector<StencilSched> st_sched;
+
   // Lanczos vectors (double)
   double* lz_v = nullptr;        // [3][n]
   // tridiagonal eigensolver: LU factors of T - lambda I per cluster start

@@ -27,7 +27,11 @@
 #include "../../include/psc.h"
 
 #include <cstdint>
+#include <cstring>
+#include <functional>
+#include <queue>
 #include <type_traits>
+#include <vector>
 
 namespace {
 
@@ -47,7 +51,11 @@ template <typename T>
 __host__ __device__ constexpr int prefetch_depth() {
   return sizeof(T) == 8 ? PSC_STENCIL_PREFETCH_F64 : PSC_STENCIL_PREFETCH_F32;
 }
-constexpr int PP_SLOTS = PSC_STENCIL_PP_SLOTS;  // Prev/pot slots: the plane in use + the prefetched
+constexpr int PP_SLOTS = PSC_STENCIL_PP_SLOTS;
+#ifndef PSC_STENCIL_SYNC_EVERY
+#define PSC_STENCIL_SYNC_EVERY 2
+#endif
+constexpr int SYNC_EVERY = PSC_STENCIL_SYNC_EVERY;  // planes between block barriers  // Prev/pot slots: the plane in use + the prefetched
 constexpr long WAIT_LIMIT = 1L << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -162,7 +170,8 @@ struct TmaArgs {
   T* Y;
   long ldy;
   const T* pot;
-  int nx, ny, nz, zchunk;
+  int nx, ny, nz;
+  const int4* sched;  // per CTA: column, slab, first plane, end plane
   T c0, c[4];
   const double* coef;
   double a, b, g;
@@ -181,6 +190,7 @@ k_stencil_tma(TmaArgs<T> A) {
   constexpr int NBUF = R + 1 + prefetch_depth<T>();   // X plane windows resident
   constexpr int NS = PP_SLOTS;
   constexpr int Q = 2 * R + 1;             // z queue length
+  static_assert(SYNC_EVERY >= 1 && SYNC_EVERY <= NBUF - R, "barrier interval exceeds the ring");
   constexpr int HV = (R + VW - 1) / VW;    // x-halo vectors on each side
   constexpr int NPV = 2 * HV + 1;          // x vectors per row (the centre one comes from the queue)
   constexpr int OFF = HV * VW;             // xs index of the thread's first point
@@ -195,11 +205,12 @@ k_stencil_tma(TmaArgs<T> A) {
   uint64_t* bars = reinterpret_cast<uint64_t*>(pring + (size_t)NS * 2 * TS);  // [NBUF]
   __shared__ int s_fail;
 
-  const int slab0 = blockIdx.x * TS;
-  const int z0 = blockIdx.y * A.zchunk;
-  const int z1 = min(nz, z0 + A.zchunk);
+  const int4 work = A.sched[blockIdx.x];
+  const int slab0 = work.y * TS;
+  const int z0 = work.z;
+  const int z1 = work.w;
   const int zlast = min(nz, z1 + R);  // X planes needed: [z0 - R, z1 + R) within [0, nz)
-  const long col = blockIdx.z;
+  const long col = work.x;
   const T* Xc = A.X + col * A.ldx;
   const T* Pc = A.P ? A.P + col * A.ldp : nullptr;
   T* Yc = A.Y + col * A.ldy;
@@ -238,8 +249,9 @@ k_stencil_tma(TmaArgs<T> A) {
     mbar_expect_tx(bar, xbytes);
     bulk_g2s(ring + (size_t)s * WS + (v0 - w0), Xc + (long)p * nxy + v0, xbytes, bar);
   };
+  int issued = min(zlast, z0 + NBUF);  // next plane to copy (thread 0's count)
   if (threadIdx.x == 0) {
-    for (int p = z0; p < min(zlast, z0 + NBUF); ++p) issue_x(p);
+    for (int p = z0; p < issued; ++p) issue_x(p);
   }
 
   // own run of VW points (it may cross a row boundary: every point has its own x)
@@ -435,10 +447,13 @@ k_stencil_tma(TmaArgs<T> A) {
         }
         vstore(Yc + (long)z * nxy + q, o);
       }
-      __syncthreads();  // slot of plane z is free
-      if (threadIdx.x == 0) {
-        const int pn = z + NBUF;
-        if (pn < zlast) issue_x(pn);
+      // every SYNC_EVERY planes (and after the last): the slots of all
+      // planes <= z are free, so the ring is topped up to plane z + NBUF.
+      // The queue front z + R stays covered while SYNC_EVERY <= NBUF - R.
+      if ((z - z0) % SYNC_EVERY == SYNC_EVERY - 1 || z == z1 - 1) {
+        __syncthreads();
+        if (threadIdx.x == 0)
+          for (; issued < zlast && issued <= z + NBUF; ++issued) issue_x(issued);
       }
     }
   }
@@ -458,6 +473,97 @@ static bool tma_ok(const psc_ctx* ctx, const void* X, long ldx, const void* P, l
   return true;
 }
 
+// Work table of one launch.  A CTA owns (column, slab, z range); the cost of a
+// CTA is modelled as its planes plus a pipeline fill.  CTAs are dispatched
+// about in order as resident slots free up, so the table puts whole-column
+// (or half-column) items first and splits the last m (column, slab) pairs
+// into smaller z chunks that fill the final wave.  The split is the one with
+// the shortest simulated list-scheduling makespan over `slots` resident CTAs.
+static void z_chunks(int nz, int c, std::vector<int2>& out) {
+  const int zc = (nz + c - 1) / c;
+  out.clear();
+  for (int z = 0; z < nz; z += zc) out.push_back(make_int2(z, std::min(nz, z + zc)));
+}
+
+static double makespan(const std::vector<int>& cost, int slots) {
+  std::priority_queue<double, std::vector<double>, std::greater<double>> q;
+  for (int i = 0; i < slots; ++i) q.push(0.0);
+  double end = 0.0;
+  for (int c : cost) {
+    const double t = q.top() + c;
+    q.pop();
+    q.push(t);
+    end = std::max(end, t);
+  }
+  return end;
+}
+
+static std::vector<int4> stencil_schedule(int nslab, int nz, int k, int fill, int slots) {
+  const long pairs = (long)nslab * k;
+  const int cmax = std::max(1, nz / 8);  // chunks of at least 8 planes
+  double best = 1e300;
+  int bb = 1, bs = 1;
+  long bm = 0;
+  std::vector<int2> cb, cs;
+  std::vector<int> cost;
+  for (int b = 1; b <= std::min(2, cmax); ++b) {
+    for (int sm = 1; sm <= 4; ++sm) {
+      const int sc = std::min(cmax, b * sm);
+      if (sm > 1 && sc == b) continue;
+      z_chunks(nz, b, cb);
+      z_chunks(nz, sc, cs);
+      const long step = std::max(1L, pairs / 32);
+      for (long m = 0; m <= pairs; m += step) {
+        if (sc == b && m > 0) break;
+        cost.clear();
+        for (long p = 0; p < pairs - m; ++p)
+          for (const int2& c : cb) cost.push_back(c.y - c.x + fill);
+        for (long p = 0; p < m; ++p)
+          for (const int2& c : cs) cost.push_back(c.y - c.x + fill);
+        const double t = makespan(cost, slots);
+        if (t < best - 1e-9) {
+          best = t;
+          bb = b;
+          bs = sc;
+          bm = m;
+        }
+      }
+    }
+  }
+  z_chunks(nz, bb, cb);
+  z_chunks(nz, bs, cs);
+  std::vector<int4> out;
+  for (long p = 0; p < pairs; ++p) {
+    const int col = (int)(p / nslab), slab = (int)(p % nslab);
+    for (const int2& c : (p < pairs - bm ? cb : cs)) out.push_back(make_int4(col, slab, c.x, c.y));
+  }
+  return out;
+}
+
+// Cached per context: the table of a (k, slab count, fill) combination is
+// built and uploaded once.
+static const int4* stencil_sched(psc_ctx* ctx, int nslab, int k, int fill, int slots, int* n, cudaStream_t st) {
+  const long long key = ((long long)k << 32) | ((long long)nslab << 16) | ((long long)fill << 8) | (slots & 0xff);
+  for (auto& e : ctx->st_sched)
+    if (e.key == key) {
+      *n = e.n;
+      return reinterpret_cast<const int4*>(e.dev);
+    }
+  psc_ctx::StencilSched e;
+  e.key = key;
+  std::vector<int4> tab = stencil_schedule(nslab, ctx->nz, k, fill, slots);
+  e.n = (int)tab.size();
+  e.host.resize(4 * tab.size());
+  std::memcpy(e.host.data(), tab.data(), tab.size() * sizeof(int4));
+  if (psc_dmalloc(&e.dev, tab.size() * sizeof(int4)) != cudaSuccess) return nullptr;
+  ctx->st_sched.push_back(std::move(e));
+  auto& b = ctx->st_sched.back();
+  if (cudaMemcpyAsync(b.dev, b.host.data(), b.host.size() * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return nullptr;
+  *n = b.n;
+  return reinterpret_cast<const int4*>(b.dev);
+}
+
 template <typename T, int R>
 static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy,
                         const T* pot, const double* w, const double* coef, double a, double b, double g,
@@ -465,26 +571,15 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   const int nxy = ctx->nx * ctx->ny;
   constexpr int TS = slab_points<T>();
   const int nslab = (nxy + TS - 1) / TS;
-  // z chunks: each CTA pays a pipeline fill of about R + D planes, and the
-  // last wave of CTAs may be partly empty; pick the chunk count that
-  // minimises waves x (planes per chunk + fill), chunks of >= 8 planes
+  // each CTA pays a pipeline fill of about R + D planes; two CTAs per SM
+  // are resident (registers and shared memory)
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  const long slots = 2L * sms;   // two CTAs per SM (registers and shared memory)
+  const int slots = 2 * sms;
   const int fill = R + prefetch_depth<T>() + 2;
-  int nzc = 1;
-  double best = 1e300;
-  for (int c = 1; c <= std::max(1, ctx->nz / 8); ++c) {
-    const int zc = (ctx->nz + c - 1) / c;
-    const long ctas = (long)nslab * c * k;
-    const double cost = (double)((ctas + slots - 1) / slots) * (zc + fill);
-    if (cost < best - 1e-9) {
-      best = cost;
-      nzc = c;
-    }
-  }
-  const int zchunk = (ctx->nz + nzc - 1) / nzc;
-  nzc = (ctx->nz + zchunk - 1) / zchunk;
+  int nwork = 0;
+  const int4* sched = stencil_sched(ctx, nslab, k, fill, slots, &nwork, st);
+  PSC_REQUIRE(ctx, sched != nullptr, "stencil: work table allocation failed");
   constexpr int NBUF = R + 1 + prefetch_depth<T>();
   const size_t win = TS + 2 * (size_t)R * ctx->nx + VecOf<T>::W;   // window + zero pad vector
   const size_t smem = (NBUF * win + (size_t)PP_SLOTS * 2 * TS) * sizeof(T) + NBUF * sizeof(uint64_t);
@@ -496,11 +591,11 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   PSC_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   TmaArgs<T> A;
   A.X = X; A.ldx = ldx; A.P = P; A.ldp = ldp; A.Y = Y; A.ldy = ldy; A.pot = pot;
-  A.nx = ctx->nx; A.ny = ctx->ny; A.nz = ctx->nz; A.zchunk = zchunk;
+  A.nx = ctx->nx; A.ny = ctx->ny; A.nz = ctx->nz; A.sched = sched;
   A.c0 = (T)w[0];
   for (int i = 0; i < 4; ++i) A.c[i] = (T)w[1 + i];
   A.coef = coef; A.a = a; A.b = b; A.g = g; A.status = ctx->dev_status;
-  kern<<<dim3(nslab, nzc, k), TNT, smem, st>>>(A);
+  kern<<<nwork, TNT, smem, st>>>(A);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }
