@@ -36,8 +36,7 @@
 namespace {
 
 constexpr int TNT = 256;          // threads per CTA
-// planes prefetched beyond the one consumed next: deeper for FP32, whose
-// planes are consumed twice as fast
+// planes of X prefetched beyond the one consumed next
 #ifndef PSC_STENCIL_PREFETCH_F64
 #define PSC_STENCIL_PREFETCH_F64 3
 #endif
@@ -51,11 +50,11 @@ template <typename T>
 __host__ __device__ constexpr int prefetch_depth() {
   return sizeof(T) == 8 ? PSC_STENCIL_PREFETCH_F64 : PSC_STENCIL_PREFETCH_F32;
 }
-constexpr int PP_SLOTS = PSC_STENCIL_PP_SLOTS;
+constexpr int PP_SLOTS = PSC_STENCIL_PP_SLOTS;  // Prev/pot slots: the plane in use + the prefetched
 #ifndef PSC_STENCIL_SYNC_EVERY
 #define PSC_STENCIL_SYNC_EVERY 2
 #endif
-constexpr int SYNC_EVERY = PSC_STENCIL_SYNC_EVERY;  // planes between block barriers  // Prev/pot slots: the plane in use + the prefetched
+constexpr int SYNC_EVERY = PSC_STENCIL_SYNC_EVERY;  // planes between block barriers
 constexpr long WAIT_LIMIT = 1L << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
