@@ -500,7 +500,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scf-only", action="store_true",
                     help="run only the warm-up and timed SCF solves (for launch-list profiling)")
+    ap.add_argument("--stencil", choices=["f64", "f32"], default=None,
+                    help="only time the fused stencil step (k = 55, C10H8 grid) for kernel profiling")
     args = ap.parse_args()
+    if args.stencil:
+        print(json.dumps(stencil_roofline(reps=max(1, args.steps), dtype=args.stencil)))
+        return
     rank, local, world = dist_init()
     try:
         if args.impl == "reference":
