@@ -166,6 +166,18 @@ int psc_density(psc_ctx* ctx, int dtype, const void* W, long ld, int nev, const 
 /* CG on A x = rhs, warm start in x (Eigensolvers/pcg.py:7-85, backend.pcg at
  * rsdft_solver.py:345). *its_out = iterations. */
 int psc_pcg_poisson(psc_ctx* ctx, const double* rhs, double* x, int maxit, double tol, int* its_out, void* stream);
+/* Preconditioned Hartree solve (cg_prec = 1): the preconditioned branch of
+ * Eigensolvers/pcg.py:7-85 (stop when z.r <= tol^2 z0.r0), warm start in x,
+ * with M = the inverse of the FD stencil continued by odd reflection across
+ * the box faces, applied exactly by 3-D sine transforms.  It replaces the
+ * ILU preconditioner of rsdft_solver.py:52-60,339, which the reference's CPU
+ * path cannot apply (pcg.py:43 is handed the string "precLU") and its GPU
+ * path ignores (pcg_gpu.py:38-41).  Grid dimensions up to 128.  The host
+ * reads z.r once per iteration (these solves take a few iterations). */
+int psc_pcg_poisson_prec(psc_ctx* ctx, const double* rhs, double* x, int maxit, double tol, int* its_out,
+                         void* stream);
+/* z = M r with the preconditioner above (r and z distinct device vectors). */
+int psc_poisson_precond(psc_ctx* ctx, const double* r, double* z, void* stream);
 /* CG execution mode: 2 (default) one persistent cooperative launch keeping
  * x, r, p, Ap in shared memory when they fit (else as 1); 1 the two CG
  * kernels replayed from a captured CUDA graph; 0 the two kernels launched from

@@ -690,6 +690,59 @@ def pcg(A, rhs, x0, m, tol):
     return x, its
 
 
+def pcg_prec(A, rhs, x0, m, tol, prec):
+    """The preconditioned branch of Eigensolvers/pcg.py:7-85: z = M r,
+    p = z (a fresh array, so no aliasing), ro1 = z.r, stop when
+    ro1 <= tol^2 z0.r0; each step x += alp p, r -= alp Ap, z = M r,
+    ro1 = z.r, p = z + (ro1/ro) p."""
+    x = np.array(x0, dtype=np.float64)
+    r = rhs - A.dot(x)
+    z = prec(r)
+    p = z
+    ro1 = np.dot(z, r)
+    tol1 = tol * tol * ro1
+    its = 0
+    while its < m and ro1 > tol1:
+        its += 1
+        ro = ro1
+        ap = A.dot(p)
+        alp = ro / np.dot(ap, p)
+        x += alp * p
+        r = r - alp * ap
+        z = prec(r)
+        ro1 = np.dot(z, r)
+        p = z + (ro1 / ro) * p
+    return x, its
+
+
+def spectral_preconditioner(domain: dict, order: int):
+    """M = S Lambda^-1 S with S the orthonormal 3-D DST-I of the box and
+    Lambda the FD stencil's symbol at the DST frequencies: the exact inverse
+    of the stencil continued by odd reflection across the faces (the GPU's
+    cg_prec = 1 preconditioner; the reference's own cg_prec path cannot run,
+    see pcg_spectral.cu).  Returns r -> M r on flat x-fastest vectors."""
+    import scipy.fft
+
+    nx, ny, nz, h = domain["nx"], domain["ny"], domain["nz"], domain["h"]
+    c0, cs = fd_stencil(order)
+
+    def lam(m):
+        th = np.pi * np.arange(1, m + 1) / (m + 1)
+        v = np.full(m, c0 / 3.0)
+        for d, c in enumerate(cs, start=1):
+            v += 2.0 * c * np.cos(d * th)
+        return v / (h * h)
+
+    L = lam(nz)[:, None, None] + lam(ny)[None, :, None] + lam(nx)[None, None, :]
+
+    def apply(r):
+        u = np.asarray(r, dtype=np.float64).reshape(nz, ny, nx)
+        s = scipy.fft.dstn(u, type=1, norm="ortho")
+        return scipy.fft.idstn(s / L, type=1, norm="ortho").ravel()
+
+    return apply
+
+
 # ----------------------------------------------------------------------------
 # mixer (Mixer/msecant1.py with Mixer/includemix.py parameters)
 # ----------------------------------------------------------------------------

@@ -53,6 +53,8 @@ _SIGS = {
     "psc_density": ([_P, c_int, _P, c_long, c_int, _P, _P, c_double, c_double, _P, _P, _P], c_int),
     "psc_pcg_poisson": ([_P, _P, _P, c_int, c_double, POINTER(c_int), _P], c_int),
     "psc_set_use_graphs": ([_P, c_int], c_int),
+    "psc_pcg_poisson_prec": ([_P, _P, _P, c_int, c_double, POINTER(c_int), _P], c_int),
+    "psc_poisson_precond": ([_P, _P, _P, _P], c_int),
     "psc_lda_xc": ([_P, _P, _P, c_double, _P, _P], c_int),
     "psc_lda_xc_noalloc": ([_P, _P, c_long, c_double, _P, _P], c_int),
     "psc_set_gram_impl": ([_P, c_int], c_int),

@@ -113,6 +113,13 @@ struct psc_ctx {
   };
   std::vector<StencilSched> st_sched;
 
+  // spectral Poisson preconditioner: DST-I matrices (m x mp, mp = m rounded
+  // up to 16), per-axis eigenvalues of the stencil, two work vectors
+  double* spec_S[3] = {nullptr, nullptr, nullptr};
+  double* spec_lam[3] = {nullptr, nullptr, nullptr};
+  int spec_mp[3] = {0, 0, 0};
+  double* spec_tmp = nullptr;
+
   // Lanczos vectors (double)
   double* lz_v = nullptr;        // [3][n]
   // tridiagonal eigensolver: LU factors of T - lambda I per cluster start

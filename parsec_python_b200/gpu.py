@@ -446,13 +446,23 @@ def density(ctx: GridContext, W: torch.Tensor, nev: int, occ: torch.Tensor, rho0
 
 
 def pcg(A: Laplacian, rhs: torch.Tensor, x0: torch.Tensor, maxit: int, tol: float, *prec):
-    """CG on A x = rhs from x0 (Eigensolvers/pcg.py:7-85); x0 is not modified."""
-    if prec:
-        raise NotImplementedError("the ILU-preconditioned Hartree solve (cg_prec = 1) is not implemented")
+    """CG on A x = rhs from x0 (Eigensolvers/pcg.py:7-85); x0 is not modified.
+    With the reference's (PRE, precfun) pair (cg_prec = 1) the solve is the
+    preconditioned branch of pcg.py with the spectral preconditioner of
+    psc_pcg_poisson_prec, whatever PRE holds."""
     x = x0.clone()
     its = c_int()
-    A.ctx.call("psc_pcg_poisson", _p(rhs), _p(x), int(maxit), float(tol), byref(its), _stream())
+    entry = "psc_pcg_poisson_prec" if len(prec) >= 2 else "psc_pcg_poisson"
+    A.ctx.call(entry, _p(rhs), _p(x), int(maxit), float(tol), byref(its), _stream())
     return x, its.value
+
+
+def poisson_precond(ctx: GridContext, r: torch.Tensor) -> torch.Tensor:
+    """z = M r, the cg_prec = 1 preconditioner (exact inverse of the FD stencil
+    continued by odd reflection, by 3-D sine transforms)."""
+    z = torch.empty_like(r)
+    ctx.call("psc_poisson_precond", _p(r), _p(z), _stream())
+    return z
 
 
 def lda_xc(ctx: GridContext, rho: torch.Tensor):

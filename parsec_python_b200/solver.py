@@ -191,7 +191,12 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         _, occ = backend.occupations(lam[:nev], s.fermi_temp, nelec, 1e-6)
         rho, hrhs = gpu.density(ctx, W, nev, occ, rho0)
         ev.mark("h0")
-        Hpot, cg_its = backend.pcg(A, hrhs, Hpot, 200, 1e-5)
+        if s.cg_prec:
+            # rsdft_solver.py:336-342: (PRE, precfun) handed to pcg; on the
+            # GPU the preconditioner is the spectral one of psc_pcg_poisson_prec
+            Hpot, cg_its = backend.pcg(A, hrhs, Hpot, 200, 1e-5, "spectral", "precLU")
+        else:
+            Hpot, cg_its = backend.pcg(A, hrhs, Hpot, 200, 1e-5)
         ev.mark("h1")
         XCpot, xcv = gpu.lda_xc(ctx, rho)
         pot_new, f, sums = gpu.scf_update(ctx, ppot, XCpot, Hpot, hpot0, rho, pot)
@@ -228,7 +233,7 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
             on_iteration(rec)
         if out:
             output.write_density_range(out, float(hv[2 * k + 5]), float(hv[2 * k + 6]))
-            output.write_scf_iteration(out, its, label, diag_t, nev, lam_h, occ_h, 1e-5, "no prec", hart_t, err,
+            output.write_scf_iteration(out, its, label, diag_t, nev, lam_h, occ_h, 1e-5, "spectral prec" if s.cg_prec else "no prec", hart_t, err,
                                        energies, n_atoms)
         say(f"   ... SCF error = {err:10.2e}\n")
         pot, _ = mixer(pot, f)

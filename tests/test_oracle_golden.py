@@ -240,3 +240,25 @@ def test_scf_diagmeth2_matches_reference(lz, tables):
     # the reference's), so the trajectory agrees to 1e-9 Ry here, not 1e-12
     assert abs(r["energies"]["total_ry"] - ms["total_ry"]) < 1e-8
     assert np.abs(r["eigenvalues"][:12] - g["scf2_eigenvalues"][:12]).max() < 1e-8
+
+
+# ---- preconditioned CG (cg_prec = 1), tests/golden/make_golden_pcg_prec.py ----
+def test_preconditioned_pcg_matches_reference(golden_dir):
+    g = np.load(golden_dir / "ref_pcg_prec.npz")
+    for tag in ("a", "b"):
+        nx, ny, nz, order = (int(v) for v in g[f"{tag}_dims"])
+        h = float(g[f"{tag}_h"])
+        dom = {"nx": nx, "ny": ny, "nz": nz, "h": h}
+        A = (1.0 / (h * h)) * O.fd3d(nx, ny, nz, order)
+        x, its = O.pcg_prec(A, g[f"{tag}_rhs"], g[f"{tag}_x0"], 200, 1e-5, O.spectral_preconditioner(dom, order))
+        assert its == int(g[f"{tag}_its"])
+        np.testing.assert_allclose(x, g[f"{tag}_x"], rtol=0, atol=1e-12 * np.abs(g[f"{tag}_x"]).max())
+
+
+def test_spectral_preconditioner_inverts_the_second_order_stencil():
+    """For fd_order 2 the odd-reflected stencil is A itself: M = A^-1."""
+    dom = {"nx": 9, "ny": 7, "nz": 8, "h": 0.5}
+    A = O.laplacian(dom, 2)
+    r = np.random.default_rng(3).standard_normal(9 * 7 * 8)
+    z = O.spectral_preconditioner(dom, 2)(r)
+    assert np.abs(A @ z - r).max() < 1e-12 * np.abs(r).max()
