@@ -146,14 +146,15 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def gpu_problem(precision: str, seed: int, name: str = CFG_NAME):
+def gpu_problem(precision: str, seed: int, name: str = CFG_NAME, cg_prec: int = 0):
     from parsec_python_b200 import workloads
     from parsec_python_b200.inputs import ElementTable
     from parsec_python_b200.models import SolverSettings
     from parsec_python_b200.system import system_from_atoms
 
     cfg = workloads.config_system(name)
-    s = SolverSettings(tol=cfg["tol"], poldeg=cfg["poldeg"], maxits=60, precision=precision, seed=seed)
+    s = SolverSettings(tol=cfg["tol"], poldeg=cfg["poldeg"], maxits=60, precision=precision, seed=seed,
+                       cg_prec=cg_prec)
     s.normalize()
     elem = ElementTable()
     prob = system_from_atoms(cfg["atoms"], h=cfg["h"], radius=cfg["radius"], nev=cfg["nev"], settings=s, elem=elem)
@@ -177,13 +178,13 @@ def reference_energy(name: str = CFG_NAME):
     return e_star, its
 
 
-def solve_once(precision: str, seed: int, energy_target=None):
+def solve_once(precision: str, seed: int, energy_target=None, cg_prec: int = 0):
     """One SCF; returns (result, backend) so that the caller releases the
     device context (cudaFree) outside its timed region."""
     from parsec_python_b200.backend import select_solver_backend
     from parsec_python_b200.solver import run_rsdft_calculation
 
-    prob, elem, s = gpu_problem(precision, seed)
+    prob, elem, s = gpu_problem(precision, seed, cg_prec=cg_prec)
     backend = select_solver_backend(s)
     res = run_rsdft_calculation(prob, elem, len(elem), backend, verbose=False, energy_target=energy_target)
     return res, backend
@@ -228,14 +229,60 @@ def stencil_roofline(reps: int = 40, dtype: str = "f64") -> dict:
     return {"seconds": t, "bytes": bytes_, "gbs": bytes_ / t / 1e9, "gflops": flops / t / 1e9, "n": n, "k": k}
 
 
-def mixed_leg(target, steps: int = 3) -> dict:
+def hartree_timing(reps: int = 20) -> dict:
+    """The Hartree solve on the C10H8 grid (78^3, fd_order 8): one
+    application of the spectral preconditioner (five passes of 32-line tile
+    products, 12 n m flops, 10 n 8 bytes), and whole solves A x = b from
+    x0 = 0 to tol 1e-5 with and without it (b a smooth charge-like field)."""
+    import torch
+
+    from parsec_python_b200 import gpu
+
+    prob, _, _ = gpu_problem("fp64", 0)
+    ctx = gpu.GridContext(prob.domain, 8)
+    n = ctx.n
+    nx, ny, nz = ctx.nx, ctx.ny, ctx.nz
+    z, y, x = torch.meshgrid(torch.arange(nz), torch.arange(ny), torch.arange(nx), indexing="ij")
+    c = torch.tensor([nx / 2, ny / 2, nz / 2])
+    d2 = ((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2).double()
+    b = (torch.exp(-d2 / 40.0) - 0.3 * torch.exp(-((x - c[0] - 6) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2).double()
+                                                  / 10.0)).reshape(-1).cuda()
+    zero = torch.zeros(n, dtype=torch.float64, device="cuda")
+    L = gpu.Laplacian(ctx)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    for _ in range(3):
+        gpu.poisson_precond(ctx, b)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record()
+    for _ in range(reps):
+        gpu.poisson_precond(ctx, b)
+    e1.record()
+    torch.cuda.synchronize()
+    t_prec = e0.elapsed_time(e1) / 1e3 / reps
+    out = {"precond_s": t_prec, "precond_gflops": 12 * n * 78 / t_prec / 1e9, "precond_gbs": 10 * n * 8 / t_prec / 1e9}
+    for name, args in (("pcg_prec", ("spectral", "precLU")), ("pcg", ())):
+        gpu.pcg(L, b, zero, 200, 1e-5, *args)
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        _, its = gpu.pcg(L, b, zero, 200, 1e-5, *args)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name + "_s"] = e0.elapsed_time(e1) / 1e3
+        out[name + "_its"] = its
+    return out
+
+
+def mixed_leg(target, steps: int = 3, cg_prec: int = 0) -> dict:
     """The same C10H8 solve in mixed precision: FP32 filter and subspace
     blocks, tensor-core (3xTF32) Gram pairs, FP64 small dense work, energies
     and the last iterations (FP64 blocks once the SCF error is below 1e-4);
-    stopped on the same energy bar."""
+    stopped on the same energy bar.  cg_prec = 1 adds the spectrally
+    preconditioned Hartree solve (the chosen form)."""
     import torch
 
-    res, be = solve_once("mixed", seed=7, energy_target=target)   # warm-up
+    res, be = solve_once("mixed", seed=7, energy_target=target, cg_prec=cg_prec)   # warm-up
     del res, be
     gc.collect()
     times, its, errs, f32_its = [], [], [], []
@@ -244,7 +291,7 @@ def mixed_leg(target, steps: int = 3) -> dict:
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        res, be = solve_once("mixed", seed=2000 + s, energy_target=target)
+        res, be = solve_once("mixed", seed=2000 + s, energy_target=target, cg_prec=cg_prec)
         e1.record()
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1) / 1000.0)
@@ -440,6 +487,7 @@ def run_gpu_arm(args, rank, local, world):
         return
     t_step = allmax(float(np.mean(times)), world)
     mixed = mixed_leg(target) if not args.scf_only else None
+    chosen = mixed_leg(target, cg_prec=1) if not args.scf_only else None
     learned_res = learned_leg() if rank == 0 else None
     roof = stencil_roofline()
     roof32 = stencil_roofline(dtype="f32")
@@ -486,6 +534,8 @@ def run_gpu_arm(args, rank, local, world):
             "setup_s": float(np.mean(setups)), "reference_iterations": ref_its, "step_times_s": times,
             "step_iterations": iters, "mixed_precision": mixed,
             "mixed_speedup_vs_fp64": (t_step / mixed["value"]) if mixed else None,
+            "chosen_form": chosen,
+            "chosen_form_speedup_vs_fp64": (t_step / chosen["value"]) if chosen else None,
             "learned_init": learned_res}
     print(json.dumps(line), flush=True)
 
@@ -500,9 +550,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scf-only", action="store_true",
                     help="run only the warm-up and timed SCF solves (for launch-list profiling)")
+    ap.add_argument("--hartree", action="store_true",
+                    help="only time the Hartree solve and its spectral preconditioner on the C10H8 grid")
     ap.add_argument("--stencil", choices=["f64", "f32"], default=None,
                     help="only time the fused stencil step (k = 55, C10H8 grid) for kernel profiling")
     args = ap.parse_args()
+    if args.hartree:
+        print(json.dumps(hartree_timing(reps=max(1, args.steps))))
+        return
     if args.stencil:
         print(json.dumps(stencil_roofline(reps=max(1, args.steps), dtype=args.stencil)))
         return

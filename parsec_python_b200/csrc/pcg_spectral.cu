@@ -18,10 +18,10 @@
 // confined to the boundary layer.  S is symmetric and its own inverse.
 //
 // Each application is five passes over the grid, each a batch of small
-// dense products of 32 grid lines by S held in shared memory: x forward, y
+// dense products of 16 grid lines by S held in shared memory: x forward, y
 // forward, z forward + 1/Lambda + z back in one kernel, y back, x back.  The
 // grid lines of a tile are loaded and stored in coalesced order (rows of x
-// for the x axis, 32 consecutive points of every y row or z plane for the
+// for the x axis, 16 consecutive points of every y row or z plane for the
 // others).  FP64 throughout.
 //
 // The reference's own cg_prec = 1 path has nothing to reproduce: its CPU
@@ -35,28 +35,29 @@
 #include <cmath>
 #include <vector>
 
-constexpr int SP_W = 32;    // grid lines per tile
-constexpr int SP_NT = 128;  // 8 groups of 4 lines x 16 groups of output modes
+constexpr int SP_W = 16;    // grid lines per tile
+constexpr int SP_NT = 128;  // 8 groups of 2 lines x 16 groups of output modes
+constexpr int SP_RPT = SP_W / 8;  // lines per thread
 constexpr int SP_MAXM = 128;
 
 // C[i][j] = sum_k T[i][k] S[k][j], i < w, j < m; thread (ig, jg) owns
-// i = 4 ig .. 4 ig + 3 and j = jg + 16 q
+// i = SP_RPT ig .. SP_RPT ig + SP_RPT - 1 and j = jg + 16 q
 template <int QJ>
 __device__ __forceinline__ void sp_tile_mm(const double* __restrict__ T, int tl, const double* __restrict__ S, int mp,
-                                           int m, double acc[4][QJ]) {
+                                           int m, double acc[SP_RPT][QJ]) {
   const int ig = threadIdx.x >> 4, jg = threadIdx.x & 15;
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < SP_RPT; ++a)
 #pragma unroll
     for (int q = 0; q < QJ; ++q) acc[a][q] = 0.0;
   for (int k = 0; k < m; ++k) {
-    double t[4], s[QJ];
+    double t[SP_RPT], s[QJ];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) t[a] = T[(4 * ig + a) * tl + k];
+    for (int a = 0; a < SP_RPT; ++a) t[a] = T[(SP_RPT * ig + a) * tl + k];
 #pragma unroll
     for (int q = 0; q < QJ; ++q) s[q] = S[k * mp + jg + 16 * q];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < SP_RPT; ++a)
 #pragma unroll
       for (int q = 0; q < QJ; ++q) acc[a][q] += t[a] * s[q];
   }
@@ -105,14 +106,14 @@ k_spec_pass(const double* __restrict__ in, double* __restrict__ out, int nx, int
       T[i * tl + k] = i < w ? in[base + i * is + k * as] : 0.0;
     }
     __syncthreads();
-    double acc[4][QJ];
+    double acc[SP_RPT][QJ];
     sp_tile_mm<QJ>(T, tl, S, mp, m, acc);
     if (mode == 1) {
       // spectral coordinates: i -> (kx, ky) of the flat xy index, j -> kz
       __syncthreads();  // all reads of T done before it is overwritten
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int i = 4 * ig + a;
+      for (int a = 0; a < SP_RPT; ++a) {
+        const int i = SP_RPT * ig + a;
         const long qf = base + i;
         const double lxy = i < w ? lx[qf % nx] + ly[qf / nx] : 1.0;
 #pragma unroll
@@ -128,11 +129,11 @@ k_spec_pass(const double* __restrict__ in, double* __restrict__ out, int nx, int
     // the global stores are coalesced in the same order as the loads
     __syncthreads();
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < SP_RPT; ++a)
 #pragma unroll
       for (int q = 0; q < QJ; ++q) {
         const int j = jg + 16 * q;
-        if (j < m) T[(4 * ig + a) * tl + j] = acc[a][q];
+        if (j < m) T[(SP_RPT * ig + a) * tl + j] = acc[a][q];
       }
     __syncthreads();
     for (int e = threadIdx.x; e < SP_W * m; e += SP_NT) {
