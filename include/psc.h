@@ -65,6 +65,18 @@ int psc_spline_coeffs(int nknots, const double* x, const double* y, int* nkeep, 
 int psc_sad_setup(psc_ctx* ctx, int natoms, const int* species, const double* xyz, double radius, double h3,
                   double fourpi, double z_sum, double* rho0, double* hpot0, double* ppot, double* info,
                   void* stream);
+/* The density-file start (density_method = ml):
+ * V_ion/pseudoDiag_ML4Den_poisson.py:392-530.  raw: the file's density
+ * (1/A^3) flattened x-fastest on the device; rho1 = max(0, (raw a03) h3)
+ * renormalised to z_sum (NumPy pairwise sums), hrhs = fourpi_h3 (rho1 - rho0).
+ * info (host, 3, may be NULL): electron count after the unit conversion,
+ * number of negative values set to 0, electron count after normalisation.
+ * The ML-grid variants of the setup (pseudoDiag_MLgrid.py,
+ * pseudoNL_original_MLgrid.py, pseudoNL_original_ML4Den.py) are
+ * psc_sad_setup / psc_projector_setup with radius = 0: grid point i lies at
+ * i h instead of i h - radius. */
+int psc_ml_density(psc_ctx* ctx, const double* raw, double a03, double h3, double z_sum, const double* rho0,
+                   double fourpi_h3, double* rho1, double* hrhs, double* info, void* stream);
 /* Kleinman-Bylander projector tables (factored V_nl):
  * V_ion/pseudoNL_original.py:9-208 (backend.pseudo_nl, rsdft_solver.py:116). */
 int psc_projector_setup(psc_ctx* ctx, int natoms, const int* species, const double* xyz, double radius,

@@ -263,6 +263,40 @@ def projectors(domain: dict, atoms: list, elements: dict, tables: dict) -> list:
     return out
 
 
+def ml_grid(domain: dict) -> dict:
+    """The ML-grid setups (V_ion/pseudoDiag_MLgrid.py, pseudoNL_original_MLgrid.py,
+    pseudoNL_original_ML4Den.py) are the SAD ones with grid point i at i h
+    instead of i h - radius: the same arithmetic with the radius 0."""
+    return dict(domain, radius=0.0)
+
+
+def ml_density_start(domain: dict, atoms: list, elements: dict, tables: dict, density, order: int = 8,
+                     cg_prec: int = 0):
+    """The density-file start, V_ion/pseudoDiag_ML4Den_poisson.py:12-586:
+    SAD on the ML grid; rho1 = ravel_F(density a0^3) h^3 (density in 1/A^3),
+    negatives set to 0, renormalised to Z_sum; the Hartree potential of
+    rho1 - rho0 by CG from zero (tol 1e-5, 200 iterations) added to the SAD
+    one.  Returns (rho1, hpot1, ppot, info)."""
+    rho0, hpot0, ppot, _ = pseudo_diag(ml_grid(domain), atoms, elements, tables)
+    h = domain["h"]
+    z_sum = 0.0
+    for a in atoms:
+        z_sum += elements[a["typ"]]["Z"] * np.asarray(a["coord"]).reshape(-1, 3).shape[0]
+    rho1 = np.ravel(np.asarray(density, dtype=np.float64) * (A0_ANG ** 3), order="F") * (h ** 3)
+    count0 = float(np.sum(rho1))
+    rho1[rho1 < 0] = 0.0
+    rho1 = z_sum * rho1 / np.sum(rho1)
+    hrhs = (4 * np.pi / h ** 3) * (rho1 - rho0)
+    A = laplacian(domain, order)
+    if cg_prec:
+        dh, _ = pcg_prec(A, hrhs, np.zeros(rho1.size), 200, 1e-5, spectral_preconditioner(domain, order))
+    else:
+        dh, _ = pcg(A, hrhs, np.zeros(rho1.size), 200, 1e-5)
+    info = {"electron_count_initial": count0, "electron_count_normalized": float(np.sum(rho1)),
+            "electron_target": float(z_sum)}
+    return rho1, dh + hpot0, ppot, info
+
+
 def nonlocal_csr(projs: list, n: int) -> sp.csr_matrix:
     """Assemble V_nl as the reference does (dense per-atom blocks
     outer(ux,ux)/xint + outer(uy,uy)/xint + outer(uz,uz)/xint summed over
@@ -867,9 +901,10 @@ class OracleSCF:
 
     def __init__(self, domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
                  maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, z_charge: float = 0.0,
-                 elements=None, tables=None, diagmeth: int = 3):
+                 elements=None, tables=None, diagmeth: int = 3, density_method: str = "sad", density=None):
         self.domain, self.atoms, self.nev, self.poldeg, self.tol = domain, atoms, nev, poldeg, tol
         self.diagmeth = diagmeth
+        self.density_method, self.density = density_method, density
         self.maxits, self.fd_order, self.fermi_temp, self.z_charge = maxits, fd_order, fermi_temp, z_charge
         self.elements = elements or load_elements()
         self.tables = tables or load_tables()
@@ -887,8 +922,16 @@ class OracleSCF:
         self.Hpot = np.zeros(n)
         self.err = 10.0 + self.tol
         self.e_nuc = nuclear(self.atoms, self.elements)
-        self.rho0, self.hpot0, self.ppot, self.info = pseudo_diag(d, self.atoms, self.elements, self.tables)
-        projs = projectors(d, self.atoms, self.elements, self.tables)
+        dm = self.density_method
+        if dm == "ml":   # rsdft_solver.py:96-108: the file density becomes the reference charge
+            self.rho0, self.hpot0, self.ppot, self.info = ml_density_start(d, self.atoms, self.elements,
+                                                                           self.tables, self.density,
+                                                                           self.fd_order)
+        else:
+            self.rho0, self.hpot0, self.ppot, self.info = pseudo_diag(ml_grid(d) if dm == "sad_ml_grid" else d,
+                                                                      self.atoms, self.elements, self.tables)
+        projs = projectors(ml_grid(d) if dm in ("ml", "sad_ml_grid") else d, self.atoms, self.elements,
+                           self.tables)
         vnl = nonlocal_csr(projs, n)
         xcpot, self.exc = exc_nspn(h, self.rho0 / h ** 3)
         self.XCpot = xcpot
@@ -948,13 +991,15 @@ class OracleSCF:
 
 def run_scf(domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
             maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, seed: int | None = None,
-            z_charge: float = 0.0, elements=None, tables=None, log=None, diagmeth: int = 3) -> dict:
+            z_charge: float = 0.0, elements=None, tables=None, log=None, diagmeth: int = 3,
+            density_method: str = "sad", density=None) -> dict:
     """Run OracleSCF to convergence; with a seed, numpy's global generator is
     seeded first so the random draws match a reference run with that seed."""
     if seed is not None:
         np.random.seed(seed)
     scf = OracleSCF(domain, atoms, nev=nev, poldeg=poldeg, tol=tol, maxits=maxits, fd_order=fd_order,
-                    fermi_temp=fermi_temp, z_charge=z_charge, elements=elements, tables=tables, diagmeth=diagmeth)
+                    fermi_temp=fermi_temp, z_charge=z_charge, elements=elements, tables=tables, diagmeth=diagmeth,
+                    density_method=density_method, density=density)
     scf.setup()
     while not scf.done():
         rec = scf.step()

@@ -9,7 +9,7 @@ from __future__ import annotations
 import argparse
 
 from .backend import select_solver_backend
-from .inputs import load_elements, prepare_input_data
+from .inputs import has_diagmeth_override, load_elements, prepare_input_data
 from .models import SolverSettings
 from .output import initialize_output_file, write_parameters
 from .solver import run_rsdft_calculation
@@ -25,6 +25,10 @@ def main(argv=None):
     settings.normalize()
     elem, n_el = load_elements()
     data = prepare_input_data(settings, args.input_file)
+    if data.density_method in ("ml", "sad_ml_grid") and not has_diagmeth_override(data.settings_overrides):
+        # main_new.py:76-78: ML density inputs default to chsubsp
+        settings.diagmeth = 2
+        print("No diagonalization override supplied for ML density input; using diagmeth=2 by default.")
     settings.apply_overrides(data.settings_overrides)
     if args.precision:
         settings.precision = args.precision

@@ -28,6 +28,7 @@ _SIGS = {
     "psc_spline_coeffs": ([c_int, _P, _P, POINTER(c_int), _P, _P, _P, _P], c_int),
     "psc_sad_setup": ([_P, c_int, _P, _P, c_double, c_double, c_double, c_double, _P, _P, _P, _P, _P], c_int),
     "psc_projector_setup": ([_P, c_int, _P, _P, c_double, _P], c_int),
+    "psc_ml_density": ([_P, _P, c_double, c_double, c_double, _P, c_double, _P, _P, _P, _P], c_int),
     "psc_projector_export": ([_P, _P, _P, _P, _P], c_int),
     "psc_numpy_sum": ([_P, _P, c_long, _P, _P], c_int),
     "psc_set_potential": ([_P, _P, _P], c_int),

@@ -38,6 +38,22 @@ class GpuRuntime:
     def pseudo_nl(self, domain, atoms, elem, n_elements=None):
         return gpu.projector_setup(self.context(domain), atoms, elem, pseudo_tables())
 
+    # the ML-grid setups, imported directly by the reference's driver
+    # (rsdft_solver.py:89-108,118-127)
+    def pseudo_diag_mlgrid(self, domain, atoms, elem, n_elements=None, return_info=False):
+        ctx = self.context(domain)
+        rho0, hpot0, ppot, info = gpu.sad_setup(ctx, atoms, elem, pseudo_tables(), ml_grid=True)
+        return (rho0, hpot0, ppot, info) if return_info else (rho0, hpot0, ppot)
+
+    def pseudo_nl_mlgrid(self, domain, atoms, elem, n_elements=None):
+        return gpu.projector_setup(self.context(domain), atoms, elem, pseudo_tables(), ml_grid=True)
+
+    def pseudo_diag_ml4den(self, domain, atoms, elem, n_elements, density_file, A=None, cg_prec=0, PRE=None,
+                           return_info=False):
+        ctx = self.context(domain)
+        rho1, hpot1, ppot, info = gpu.ml_density_setup(ctx, atoms, elem, pseudo_tables(), density_file, cg_prec)
+        return (rho1, hpot1, ppot, info) if return_info else (rho1, hpot1, ppot)
+
     def first_filt(self, nev, H, polm=10):
         return gpu.first_filt(nev, H, polm, dtype=self.block_dtype)
 

@@ -270,3 +270,67 @@ int psc_nl_eval_u(psc_ctx* ctx, long npts, const int* idx_dev, const int* pt_ato
   psc_dfree(tab);
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// ML density file -> starting charge (V_ion/pseudoDiag_ML4Den_poisson.py:392-530):
+//   rho1 = (d * a0^3) * h^3 (d in 1/A^3, flat x-fastest), negatives set to 0,
+//   rho1 = Z_sum * rho1 / sum(rho1), hrhs = (4 pi / h^3) (rho1 - rho0);
+// sums in NumPy's pairwise order.  info (host, 3): electron count after the
+// conversion, number of negative values, electron count after normalisation.
+// ---------------------------------------------------------------------------
+__global__ void k_ml_scale(const double* __restrict__ raw, double* __restrict__ rho, long n, double a03, double h3) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    rho[i] = (raw[i] * a03) * h3;
+}
+
+__global__ void k_ml_clamp(double* __restrict__ rho, long n, unsigned long long* neg) {
+  unsigned long long c = 0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    if (rho[i] < 0.0) { rho[i] = 0.0; ++c; }
+  if (c) atomicAdd(neg, c);
+}
+
+__global__ void k_ml_norm(double* __restrict__ rho, const double* __restrict__ rho0, double* __restrict__ hrhs, long n,
+                          double z_sum, const double* __restrict__ total, double fourpi_h3) {
+  const double s = *total;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double v = (z_sum * rho[i]) / s;
+    rho[i] = v;
+    hrhs[i] = fourpi_h3 * (v - rho0[i]);
+  }
+}
+
+extern "C" int psc_ml_density(psc_ctx* ctx, const double* raw, double a03, double h3, double z_sum, const double* rho0,
+                              double fourpi_h3, double* rho1, double* hrhs, double* info, void* stream) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, raw && rho0 && rho1 && hrhs && raw != rho1, "ml_density: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long n = ctx->n;
+  const int nb = 148 * 4;
+  double* sc = ctx->scalars + 104;  // [0] count after conversion, [1] sum before normalising, [2] count after
+  unsigned long long* neg = reinterpret_cast<unsigned long long*>(ctx->scalars + 108);
+  PSC_CUDA(ctx, cudaMemsetAsync(neg, 0, sizeof(unsigned long long), st));
+  k_ml_scale<<<nb, 256, 0, st>>>(raw, rho1, n, a03, h3);
+  PSC_LAUNCH_CHECK(ctx);
+  int rc = psc_numpy_sum(ctx, rho1, n, sc + 0, st);
+  if (rc) return rc;
+  k_ml_clamp<<<nb, 256, 0, st>>>(rho1, n, neg);
+  PSC_LAUNCH_CHECK(ctx);
+  rc = psc_numpy_sum(ctx, rho1, n, sc + 1, st);
+  if (rc) return rc;
+  k_ml_norm<<<nb, 256, 0, st>>>(rho1, rho0, hrhs, n, z_sum, sc + 1, fourpi_h3);
+  PSC_LAUNCH_CHECK(ctx);
+  rc = psc_numpy_sum(ctx, rho1, n, sc + 2, st);
+  if (rc) return rc;
+  if (info) {
+    double h[3];
+    unsigned long long negc = 0;
+    PSC_CUDA(ctx, cudaMemcpyAsync(h, sc, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PSC_CUDA(ctx, cudaMemcpyAsync(&negc, neg, sizeof(negc), cudaMemcpyDeviceToHost, st));
+    PSC_CUDA(ctx, cudaStreamSynchronize(st));
+    info[0] = h[0];
+    info[1] = (double)negc;
+    info[2] = h[2];
+  }
+  return 0;
+}

@@ -487,8 +487,10 @@ class Mixer:
         return out, m.value
 
 
-def sad_setup(ctx: GridContext, atoms, elem, tables):
-    """SAD density, local and SAD Hartree potentials (V_ion/pseudoDiag.py)."""
+def sad_setup(ctx: GridContext, atoms, elem, tables, ml_grid: bool = False):
+    """SAD density, local and SAD Hartree potentials (V_ion/pseudoDiag.py).
+    ml_grid: grid point i at i h instead of i h - radius, as
+    V_ion/pseudoDiag_MLgrid.py (the same arithmetic with the radius 0)."""
     sp, xyz = ctx.atom_arrays(atoms, elem, tables)
     z_sum = 0.0
     for a in atoms:
@@ -496,19 +498,50 @@ def sad_setup(ctx: GridContext, atoms, elem, tables):
     rho0, hpot0, ppot = ctx.empty(ctx.n), ctx.empty(ctx.n), ctx.empty(ctx.n)
     info = (ctypes.c_double * 2)()
     h = ctx.h
-    ctx.call("psc_sad_setup", len(sp), sp.ctypes.data_as(c_void_p), xyz.ctypes.data_as(c_void_p), ctx.radius,
+    ctx.call("psc_sad_setup", len(sp), sp.ctypes.data_as(c_void_p), xyz.ctypes.data_as(c_void_p),
+             0.0 if ml_grid else ctx.radius,
              h ** 3, 4 * np.pi, float(z_sum), _p(rho0), _p(hpot0), _p(ppot), info, _stream())
     diag_info = {"electron_count_initial": info[0], "electron_count_normalized": info[1],
                  "electron_target": float(z_sum)}
     return rho0, hpot0, ppot, diag_info
 
 
-def projector_setup(ctx: GridContext, atoms, elem, tables) -> NonlocalProjectors:
+def projector_setup(ctx: GridContext, atoms, elem, tables, ml_grid: bool = False) -> NonlocalProjectors:
+    """KB projectors (V_ion/pseudoNL_original.py); ml_grid as
+    pseudoNL_original_MLgrid.py / pseudoNL_original_ML4Den.py (radius 0)."""
     sp, xyz = ctx.atom_arrays(atoms, elem, tables)
     ctx.call("psc_projector_setup", len(sp), sp.ctypes.data_as(c_void_p), xyz.ctypes.data_as(c_void_p),
-             ctx.radius, _stream())
+             0.0 if ml_grid else ctx.radius, _stream())
     ctx.projectors = NonlocalProjectors(ctx)
     return ctx.projectors
+
+
+def ml_density_setup(ctx: GridContext, atoms, elem, tables, density_file: str, cg_prec: int = 0):
+    """The density-file start, V_ion/pseudoDiag_ML4Den_poisson.py:12-586:
+    SAD on the ML grid, the file's density (1/A^3, shape (nx, ny, nz), read
+    in Fortran order) converted to electrons per point, clamped at zero and
+    renormalised, and its Hartree potential by CG from zero (preconditioned
+    when cg_prec): returns (rho1, hpot0 + dV_H, ppot, diag_info)."""
+    rho0, hpot0, ppot, _ = sad_setup(ctx, atoms, elem, tables, ml_grid=True)
+    arr = np.load(density_file)
+    if arr.ndim != 3 or arr.shape != (ctx.nx, ctx.ny, ctx.nz):
+        raise ValueError(f"density file shape {arr.shape} does not match the grid {(ctx.nx, ctx.ny, ctx.nz)}")
+    raw = torch.from_numpy(np.ascontiguousarray(np.ravel(np.asarray(arr, dtype=np.float64), order="F"))).to(ctx.device)
+    z_sum = 0.0
+    for a in atoms:
+        z_sum += elem[a["typ"]]["Z"] * np.asarray(a["coord"]).reshape(-1, 3).shape[0]
+    h = ctx.h
+    a0 = 0.529177210903
+    rho1, hrhs = ctx.empty(ctx.n), ctx.empty(ctx.n)
+    info = (ctypes.c_double * 3)()
+    ctx.call("psc_ml_density", _p(raw), a0 ** 3, h ** 3, float(z_sum), _p(rho0), 4 * np.pi / h ** 3, _p(rho1),
+             _p(hrhs), info, _stream())
+    prec = ("spectral", "precLU") if cg_prec else ()
+    dh, _ = pcg(Laplacian(ctx), hrhs, ctx.zeros(ctx.n), 200, 1e-5, *prec)
+    hpot1 = axpby(ctx, dh, hpot0, 1.0, 1.0)
+    diag_info = {"electron_count_initial": info[0], "electron_count_normalized": info[2],
+                 "electron_target": float(z_sum), "negative_values_zeroed": int(info[1])}
+    return rho1, hpot1, ppot, diag_info
 
 
 def scf_update(ctx, ppot, vxc, hpot, hpot0, rho, pot):

@@ -164,7 +164,12 @@ def load_atomic_data_from_file(file_name: str) -> InputData:
         if not isinstance(overrides, dict):
             overrides = {}
         unit = overrides.get("unit", unit)
-        for key in ("nev", "grid_spacing", "h", "sphere_radius", "radius", "recenter_atoms"):
+        ml = data.get("ml_file_path") or data.get("density_file")
+        if ml:
+            cand = Path(str(ml)).expanduser()
+            ml_file = str(cand if cand.is_absolute() else path.parent / cand)
+        for key in ("nev", "grid_spacing", "h", "sphere_radius", "radius", "grid_npy_path", "grid_poscar_path",
+                    "recenter_atoms"):
             if key in data and key not in overrides:
                 overrides[key] = data[key]
         overrides = _non_empty(overrides)
@@ -212,15 +217,84 @@ def convert_units_to_bohr(atoms, overrides, input_file_path):
     return out, ov, unit
 
 
+def resolve_optional_path(raw_path, label: str, input_file_path: str | None = None) -> str | None:
+    """First existing candidate of a possibly relative path: as given
+    (absolute), under the working directory, next to the package, next to the
+    input file (rsdft_input.py:505-529)."""
+    if not raw_path:
+        return None
+    raw = Path(str(raw_path)).expanduser()
+    cands = [raw] if raw.is_absolute() else [Path.cwd() / raw, Path(__file__).resolve().parent / raw]
+    if not raw.is_absolute() and input_file_path:
+        cands.append(Path(input_file_path).resolve().parent / raw)
+    for c in cands:
+        if c.exists():
+            return str(c.resolve())
+    print(f"Warning: {label} {raw_path} not found. Tried: {[str(c) for c in cands]}")
+    return None
+
+
+def read_poscar_cube_length(poscar_path: str) -> float:
+    """Mean length (angstrom) of the three scaled lattice vectors of a POSCAR
+    file (rsdft_input.py:532-557)."""
+    lines = [ln.strip() for ln in Path(poscar_path).read_text().splitlines() if ln.strip()]
+    if len(lines) < 5:
+        raise ValueError("Incomplete POSCAR file for grid size.")
+    scale = float(lines[1].split()[0])
+    lengths = []
+    for i in range(2, 5):
+        parts = lines[i].split()
+        if len(parts) < 3:
+            raise ValueError(f'Invalid lattice vector line: "{lines[i]}"')
+        v = [float(parts[0]) * scale, float(parts[1]) * scale, float(parts[2]) * scale]
+        lengths.append(np.sqrt(v[0] ** 2 + v[1] ** 2 + v[2] ** 2))
+    return sum(lengths) / 3.0
+
+
+def load_grid_data_from_files(grid_npy: str, grid_poscar: str) -> dict[str, Any]:
+    """Grid of an ML density file: shape from the .npy (read without loading
+    it), spacing L / nx and radius L / 2 from the POSCAR cell, in bohr
+    (rsdft_input.py:560-579)."""
+    density = np.load(grid_npy, mmap_mode="r")
+    if density.ndim != 3:
+        raise ValueError("Grid .npy file must be a 3D array.")
+    nx, ny, nz = density.shape
+    if nx <= 0 or ny <= 0 or nz <= 0:
+        raise ValueError("Invalid grid shape in .npy file.")
+    length = read_poscar_cube_length(grid_poscar)
+    return {"nx": int(nx), "ny": int(ny), "nz": int(nz), "h": length / float(nx) / A0_ANG,
+            "radius": length / 2.0 / A0_ANG}
+
+
 def prepare_input_data(settings: SolverSettings, input_path: str) -> InputData:
-    """Parse an input file and convert it to bohr (the default-grid modes)."""
+    """Parse an input file, resolve its auxiliary files, convert to bohr and,
+    for the ML density modes, read the grid from the density and POSCAR files
+    (rsdft_input.py:636-701)."""
     data = load_atomic_data_from_file(input_path)
     if not data.atoms:
         raise SystemExit("No atoms loaded, exiting RSDFT.")
-    if data.density_method != "sad":
-        raise NotImplementedError(
-            f"density_method={data.density_method!r} (file-defined ML grids) is not implemented; "
-            "the learned initial density is selected with init = learned on the default grid")
+    ov = dict(data.settings_overrides or {})
+    data.grid_npy_path = ov.pop("grid_npy_path", None) or ov.pop("grid_npy", None)
+    data.grid_poscar_path = ov.pop("grid_poscar_path", None) or ov.pop("grid_poscar", None)
+    data.settings_overrides = ov
+    data.ml_file_path = resolve_optional_path(data.ml_file_path, "ML density file", data.input_file_path)
+    data.grid_npy_path = resolve_optional_path(data.grid_npy_path, "Grid npy file", data.input_file_path)
+    data.grid_poscar_path = resolve_optional_path(data.grid_poscar_path, "Grid POSCAR file", data.input_file_path)
+    if data.density_method in ("ml", "sad_ml_grid") and data.ml_file_path is None:
+        raise SystemExit("Density method requires ML .npy file but no ml_file_path was provided or found. "
+                         "Add ml_file_path to the input file.")
     data.atoms, data.settings_overrides, data.unit_used = convert_units_to_bohr(
         data.atoms, data.settings_overrides, data.input_file_path)
+    data.grid_mode = "ml" if data.density_method in ("ml", "sad_ml_grid") else "default"
+    if data.grid_mode == "ml":
+        if data.grid_npy_path is None:
+            data.grid_npy_path = data.ml_file_path
+        if data.grid_poscar_path is None:
+            raise SystemExit("Grid POSCAR file is required to set grid structure.")
+        data.grid_data = load_grid_data_from_files(data.grid_npy_path, data.grid_poscar_path)
     return data
+
+
+def has_diagmeth_override(overrides) -> bool:
+    """rsdft_input.py:39-41."""
+    return any(str(k).lower() == "diagmeth" for k in (overrides or {}))

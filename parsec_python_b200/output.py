@@ -159,3 +159,46 @@ def save_wavefunction(path, domain, potential, rho, W, nev, n_types, atoms) -> N
             fh.write(u32(len(xyz)))
             for row in xyz:
                 fh.write(f64(row))
+
+
+def load_wavefunction(path) -> dict:
+    """Read the legacy binary wfn.dat that save_wavefunction writes
+    (rsdft_output.py:298-334): magic 26, radius, h, the potential, the
+    density, n x nev wavefunctions (one column after another), then per
+    species its atom coordinates.  Returns a dict with those fields
+    (wavefunctions as an n x nev array, atoms as a list of (count, 3) arrays).
+    Species symbols are not in the file."""
+    raw = open(path, "rb").read()
+    pos = 0
+
+    def u32():
+        nonlocal pos
+        v = int(np.frombuffer(raw, dtype=np.uint32, count=1, offset=pos)[0])
+        pos += 4
+        return v
+
+    def f64(count):
+        nonlocal pos
+        v = np.frombuffer(raw, dtype=np.float64, count=count, offset=pos).copy()
+        pos += 8 * count
+        return v
+
+    magic = u32()
+    if magic != 26:
+        raise ValueError(f"{path}: not a wfn.dat file (magic {magic}, expected 26)")
+    radius, h = f64(1)[0], f64(1)[0]
+    pot = f64(u32())
+    rho = f64(u32())
+    n = u32()
+    nev = u32()
+    W = np.empty((n, nev))
+    for i in range(nev):
+        W[:, i] = f64(n)
+    atoms = []
+    for _ in range(u32()):
+        count = u32()
+        atoms.append(f64(3 * count).reshape(count, 3))
+    if pos != len(raw):
+        raise ValueError(f"{path}: {len(raw) - pos} trailing bytes")
+    return {"radius": float(radius), "h": float(h), "potential": pot, "rho": rho, "wavefunctions": W,
+            "nev": nev, "atoms": atoms}

@@ -104,7 +104,19 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         else:
             say("No trained density network found: using the SAD initial density.")
     t0 = time.perf_counter()
-    rho0, hpot0, ppot, diag_info = backend.pseudo_diag(dom, atoms, elem, n_elements, return_info=True)
+    # rsdft_solver.py:76-108: the density mode picks the setup; a density
+    # file (ml) becomes the reference charge itself, as in the reference
+    dm = problem.input_data.density_method
+    if dm == "sad_ml_grid":
+        say(f"Using SAD density on ML grid from: {problem.input_data.grid_npy_path}")
+        rho0, hpot0, ppot, diag_info = rt.pseudo_diag_mlgrid(dom, atoms, elem, n_elements, return_info=True)
+    elif dm == "ml":
+        say(f"Using ML grid/density file: {problem.input_data.ml_file_path}")
+        rho0, hpot0, ppot, diag_info = rt.pseudo_diag_ml4den(dom, atoms, elem, n_elements,
+                                                             problem.input_data.ml_file_path, A, s.cg_prec,
+                                                             return_info=True)
+    else:
+        rho0, hpot0, ppot, diag_info = backend.pseudo_diag(dom, atoms, elem, n_elements, return_info=True)
     rho_start, hpot_start = rho0, None
     if init_density is not None:
         rho_start, hpot_start = init_density(ctx, rho0, hpot0, ppot, A)
@@ -119,7 +131,10 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
 
     rhoxc = gpu.axpby(ctx, rho_start, None, 1.0 / h ** 3, 0.0)
     t0 = time.perf_counter()
-    backend.pseudo_nl(dom, atoms, elem, n_elements)
+    if dm in ("ml", "sad_ml_grid"):
+        rt.pseudo_nl_mlgrid(dom, atoms, elem, n_elements)
+    else:
+        backend.pseudo_nl(dom, atoms, elem, n_elements)
     stage("Nonlocal ionic potential setup", t0)
 
     t0 = time.perf_counter()

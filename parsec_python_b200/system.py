@@ -19,18 +19,24 @@ import numpy as np
 from .models import A0_ANG, InputData, PreparedSystem, RunPaths, SolverSettings
 
 
-def calculate_grid_spacing(atoms, elem, n_atom, z_charge, h_override=None, nev_override=None):
+def calculate_grid_spacing(atoms, elem, n_atom, z_charge, h_override=None, nev_override=None, grid_data=None):
+    """With grid_data (an ML grid) h is the file grid's spacing and an h
+    override is ignored (rsdft_setup.py:40-63)."""
     zelec = 0.0
-    hmin = 100.0
+    hmin = 100.0 if grid_data is None else grid_data["h"]
     for species, count in zip(atoms, n_atom):
         row = elem[species["typ"]]
-        hmin = min(hmin, row["h"])
+        if grid_data is None:
+            hmin = min(hmin, row["h"])
         zelec += row["Z"] * count
     ztest = zelec - z_charge
     if ztest < 0:
         raise SystemExit("Problem with charge state. Negative number of electrons.")
     h = hmin
-    if h_override is not None:
+    if grid_data is not None:
+        if h_override is not None:
+            print("Warning: grid spacing override ignored when using ML grid.")
+    elif h_override is not None:
         try:
             h = float(h_override)
         except (TypeError, ValueError):
@@ -104,16 +110,26 @@ def build_output_paths(inp: InputData, settings: SolverSettings, elem, domain) -
 
 def prepare_system(inp: InputData, settings: SolverSettings, elem, n_elements: int | None = None) -> PreparedSystem:
     ov = inp.settings_overrides
+    ml_grid = inp.grid_mode == "ml"
     h, nev, zelec, ztest = calculate_grid_spacing(inp.atoms, elem, inp.n_atom, inp.z_charge,
-                                                  ov.get("grid_spacing", ov.get("h")), ov.get("nev"))
+                                                  ov.get("grid_spacing", ov.get("h")), ov.get("nev"),
+                                                  inp.grid_data if ml_grid else None)
     atoms = inp.atoms
-    if inp.density_method == "sad" and settings.recenter_atoms:
+    if inp.density_method == "sad" and not ml_grid and settings.recenter_atoms:
         atoms = recenter_atoms(inp.atoms)
-    domain, n_types = estimate_radius_and_grid(atoms, elem, h, ov.get("sphere_radius", ov.get("radius")))
+    if ml_grid:
+        # rsdft_setup.py:106-117: the file grid as it is (atoms in its cell frame)
+        if ov.get("sphere_radius", ov.get("radius")) is not None:
+            print("Warning: radius override ignored when using ML grid.")
+        g = inp.grid_data
+        domain, n_types = {"radius": g["radius"], "nx": g["nx"], "ny": g["ny"], "nz": g["nz"], "h": h}, len(atoms)
+    else:
+        domain, n_types = estimate_radius_and_grid(atoms, elem, h, ov.get("sphere_radius", ov.get("radius")))
     prepared = InputData(atoms=atoms, n_atom=list(inp.n_atom), z_charge=inp.z_charge,
                          density_method=inp.density_method, ml_file_path=inp.ml_file_path,
                          settings_overrides=dict(ov), input_file_path=inp.input_file_path,
-                         unit_used=inp.unit_used)
+                         grid_npy_path=inp.grid_npy_path, grid_poscar_path=inp.grid_poscar_path,
+                         unit_used=inp.unit_used, grid_mode=inp.grid_mode, grid_data=deepcopy(inp.grid_data))
     paths = build_output_paths(prepared, settings, elem, domain)
     return PreparedSystem(input_data=prepared, settings=settings, domain=domain, h=h, nev=nev, zelec=zelec,
                           ztest=ztest, n_types=n_types, paths=paths)

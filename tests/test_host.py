@@ -141,3 +141,52 @@ def test_learned_network_layout():
     if w is not None:
         assert w["w"].size == learned.n_params()
         assert w["a0"] > 0 and w["a1"] > 0 and w["at"] > 0
+
+
+def test_ml_density_inputs_read_grid_from_files(golden_dir):
+    """The ML density modes take the grid from the density file's shape and the
+    POSCAR cell (rsdft_input.py:560-579, rsdft_setup.py:40-63,106-117), keep
+    the atoms in the cell frame and default to diagmeth 2 (main_new.py:76-78)."""
+    import json
+
+    from parsec_python_b200.inputs import ElementTable, has_diagmeth_override, prepare_input_data
+    from parsec_python_b200.models import SolverSettings
+    from parsec_python_b200.system import prepare_system
+
+    meta = json.loads((golden_dir / "ref_ml.json").read_text())
+    for dm in ("ml", "sad_ml_grid"):
+        s = SolverSettings()
+        s.normalize()
+        data = prepare_input_data(s, str(golden_dir / "ml" / f"h2o_{dm}.in"))
+        assert data.density_method == dm and data.grid_mode == "ml"
+        assert data.ml_file_path.endswith("density.npy") and data.grid_poscar_path.endswith("cell.POSCAR")
+        assert not has_diagmeth_override(data.settings_overrides)
+        s.apply_overrides(data.settings_overrides)
+        prob = prepare_system(data, s, ElementTable())
+        ref = meta[f"scf_{dm}"]["domain"]
+        assert prob.domain == pytest.approx(ref)
+        assert prob.nev == meta[f"scf_{dm}"]["nev"]
+        # no recentring on an ML grid: the oxygen stays at its cell position
+        assert np.allclose(prob.input_data.atoms[0]["coord"], np.array([[3.0, 3.0, 3.1]]) / 0.529177210903)
+
+
+def test_wfn_dat_round_trip(tmp_path):
+    """load_wavefunction reads back what save_wavefunction writes (the
+    reference's layout, rsdft_output.py:298-334), field by field."""
+    rng = np.random.default_rng(2)
+    n, nev = 300, 5
+    dom = {"radius": 4.25, "h": 0.35, "nx": 7, "ny": 7, "nz": 7}
+    pot, rho, W = rng.standard_normal(n), rng.random(n), rng.standard_normal((n, nev + 3))
+    atoms = [{"typ": "O", "coord": rng.standard_normal((1, 3))}, {"typ": "H", "coord": rng.standard_normal((2, 3))}]
+    f = tmp_path / "x_wfn.dat"
+    output.save_wavefunction(str(f), dom, pot, rho, W, nev, 2, atoms)
+    d = output.load_wavefunction(str(f))
+    assert (d["radius"], d["h"], d["nev"]) == (4.25, 0.35, nev)
+    np.testing.assert_array_equal(d["potential"], pot)
+    np.testing.assert_array_equal(d["rho"], rho)
+    np.testing.assert_array_equal(d["wavefunctions"], W[:, :nev])
+    for a, b in zip(d["atoms"], atoms):
+        np.testing.assert_array_equal(a, b["coord"])
+    f.write_bytes(f.read_bytes() + b"x")
+    with pytest.raises(ValueError, match="trailing"):
+        output.load_wavefunction(str(f))

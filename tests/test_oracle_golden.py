@@ -262,3 +262,44 @@ def test_spectral_preconditioner_inverts_the_second_order_stencil():
     r = np.random.default_rng(3).standard_normal(9 * 7 * 8)
     z = O.spectral_preconditioner(dom, 2)(r)
     assert np.abs(A @ z - r).max() < 1e-12 * np.abs(r).max()
+
+
+# ---- ML-grid density modes (sad_ml_grid, ml), tests/golden/make_golden_ml.py ----
+ML_ATOMS = [("O", [[3.0, 3.0, 3.1]]), ("H", [[3.757, 3.586, 3.1], [2.243, 3.586, 3.1]])]
+
+
+@pytest.fixture(scope="module")
+def mlg(golden_dir):
+    return np.load(golden_dir / "ref_ml.npz"), json.loads((golden_dir / "ref_ml.json").read_text())
+
+
+def _ml_atoms():
+    return [{"typ": t, "coord": np.array(c) / O.A0_ANG} for t, c in ML_ATOMS]
+
+
+def test_ml_grid_setup_and_density_file_match_reference(mlg, tables):
+    """pseudoDiag_MLgrid and pseudoDiag_ML4Den bit for bit, the ML-grid
+    projectors to rounding."""
+    elements, tab = tables
+    g, meta = mlg
+    dom = meta["domain"]
+    r0, h0, p0, _ = O.pseudo_diag(O.ml_grid(dom), _ml_atoms(), elements, tab)
+    assert (sha(r0), sha(h0), sha(p0)) == (meta["mlgrid"]["rho0"], meta["mlgrid"]["hpot0"], meta["mlgrid"]["ppot"])
+    vnl = O.nonlocal_csr(O.projectors(O.ml_grid(dom), _ml_atoms(), elements, tab), dom["nx"] ** 3)
+    assert np.abs(vnl @ g["vnl_x"] - g["vnl_y"]).max() <= 1e-12 * np.abs(g["vnl_y"]).max()
+    r1, hp1, pp, info = O.ml_density_start(dom, _ml_atoms(), elements, tab, g["density"])
+    assert sha(r1) == meta["ml4den"]["rho1"] and sha(pp) == meta["ml4den"]["pot"]
+    assert np.abs(hp1 - g["ml_hpot1"]).max() <= 1e-12 * np.abs(g["ml_hpot1"]).max()
+    assert info == meta["ml4den"]["info"]
+
+
+@pytest.mark.parametrize("dm", ["sad_ml_grid", "ml"])
+def test_ml_mode_scf_matches_reference(mlg, tables, dm):
+    elements, tab = tables
+    g, meta = mlg
+    ms = meta[f"scf_{dm}"]
+    r = O.run_scf(ms["domain"], _ml_atoms(), nev=12, poldeg=10, tol=1e-6, seed=0, elements=elements, tables=tab,
+                  diagmeth=ms["diagmeth"], density_method=dm, density=g["density"], maxits=60)
+    assert r["iterations"] == ms["iterations"]
+    assert abs(r["energies"]["total_ry"] - ms["total_ry"]) < 1e-7
+    assert np.abs(r["eigenvalues"][:12] - g[f"scf_{dm}_eigenvalues"][:12]).max() < 1e-8
