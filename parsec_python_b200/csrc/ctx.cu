@@ -114,7 +114,7 @@ extern "C" int psc_ctx_destroy(psc_ctx* ctx) {
   psc_dfree(ctx->tc_part); psc_dfree(ctx->tc_pairs); psc_dfree(ctx->tri_work);
   for (auto& e : ctx->st_sched) psc_dfree(e.dev);
   for (int a = 0; a < 3; ++a) { psc_dfree(ctx->spec_S[a]); psc_dfree(ctx->spec_lam[a]); }
-  psc_dfree(ctx->spec_tmp);
+  psc_dfree(ctx->spec_tmp); psc_dfree(ctx->lz_basis);
   if (ctx->cg_exec) cudaGraphExecDestroy(ctx->cg_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   delete ctx;

@@ -477,3 +477,31 @@ extern "C" int psc_orthonormalize_rank(psc_ctx* ctx, int dtype, void* W, void* T
   *which = w2 == 0 ? 1 : 0;
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// The chefsi1 spectrum bound (Eigensolvers/lanczosForChefsi1.py:5-99 with
+// m = 6): six steps of the recurrence above from a standard normal start,
+// then bound = max |theta| + beta_6 over the eigenvalues theta of T_6.
+// ---------------------------------------------------------------------------
+__global__ void k_lz_bound6(const double* __restrict__ ev, const double* __restrict__ ab, int m, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double mx = 0.0;
+    for (int i = 0; i < m; ++i) mx = fmax(mx, fabs(ev[i]));
+    out[0] = mx + ab[2 * (m - 1) + 1];
+  }
+}
+
+int psc_lanczos_bound_basis(psc_ctx* ctx, unsigned long long seed, double* out_dev, cudaStream_t st) {
+  constexpr int m = 6;
+  const long n = ctx->n;
+  if (!ctx->lz_basis) PSC_CUDA(ctx, psc_dmalloc(&ctx->lz_basis, (size_t)(m + 1) * n * sizeof(double)));
+  double* ab = ctx->scalars + 160;  // [2m] alpha, beta
+  double* ev = ctx->scalars + 176;  // [m]
+  int rc = psc_lanczos_run(ctx, nullptr, seed, 0, m, ctx->lz_basis, n, ab, st);
+  if (rc) return rc;
+  rc = psc_tridiag_eig(ctx, ab, m, 0, ev, nullptr, 0, st);
+  if (rc) return rc;
+  k_lz_bound6<<<1, 32, 0, st>>>(ev, ab, m, out_dev);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}

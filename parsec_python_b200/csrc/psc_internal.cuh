@@ -122,6 +122,7 @@ struct psc_ctx {
 
   // Lanczos vectors (double)
   double* lz_v = nullptr;        // [3][n]
+  double* lz_basis = nullptr;    // [7][n] basis of the six-step bound of chefsi1
   // tridiagonal eigensolver: LU factors of T - lambda I per cluster start
   double* tri_work = nullptr;
   size_t tri_work_doubles = 0;

@@ -73,9 +73,14 @@ __global__ void k_lz_bound(const double* sc, int m, const double* ritz, const do
 //           out = [uppbnd, ritz_0..ritz_5] (ritz ascending)
 //   mode 1: lanczosForChefsi1 (Eigensolvers/lanczosForChefsi1.py:5-99):
 //           normal start, out = [max|ritz| + beta_6]
+int psc_lanczos_bound_basis(psc_ctx* ctx, unsigned long long seed, double* out_dev, cudaStream_t st);
+
 extern "C" int psc_lanczos_bound(psc_ctx* ctx, int mode, unsigned long long seed, double* out_dev, void* stream) {
   if (!ctx) return 2;
   cudaStream_t st = (cudaStream_t)stream;
+  // mode 1 runs the three-term recurrence of psc_lanczos_run (the same steps,
+  // fused, keeping a basis of 7 vectors) and bisection on T_6
+  if (mode != 0) return psc_lanczos_bound_basis(ctx, seed, out_dev, st);
   const long n = ctx->n;
   const int m = 6;
   if (psc_ensure_dense(ctx, m)) return 1;
@@ -139,39 +144,7 @@ extern "C" int psc_lanczos_bound(psc_ctx* ctx, int mode, unsigned long long seed
     if (rc) return rc;
     k_lz_bound<<<1, 32, 0, st>>>(sc, m, sc + 40, ctx->evec, 0, out_dev);
     PSC_LAUNCH_CHECK(ctx);
-    return 0;
   }
-  // mode 1: v1 = v; v0 = 0; bet = 0; loop: w = H v1 - bet v0; alp = v1.w; w -= alp v1;
-  // bet = ||w||; v0 = v1; v1 = w / bet
-  PSC_CUDA(ctx, cudaMemsetAsync(v0, 0, n * sizeof(double), st));
-  PSC_CUDA(ctx, cudaMemsetAsync(sc + 1, 0, sizeof(double), st));
-  for (int j = 0; j < m; ++j) {
-    rc = psc_apply_h_impl(ctx, PSC_F64, v, n, f, n, nullptr, 0, 1, nullptr, 1.0, 0.0, 0.0, st);
-    if (rc) return rc;
-    k_axpy_neg<<<nb, 256, 0, st>>>(v0, f, n, sc + 1);
-    PSC_LAUNCH_CHECK(ctx);
-    const double* va[1] = {v};
-    const double* fb[1] = {f};
-    rc = psc_dots(ctx, 1, va, fb, n, sc + 0, st);
-    if (rc) return rc;
-    k_axpy_neg<<<nb, 256, 0, st>>>(v, f, n, sc + 0);
-    PSC_LAUNCH_CHECK(ctx);
-    k_lz_store_alpha<<<1, 32, 0, st>>>(sc, j);
-    PSC_LAUNCH_CHECK(ctx);
-    rc = psc_dots(ctx, 1, a1, a1, n, sc + 2, st);
-    if (rc) return rc;
-    k_lz_sqrt_beta<<<1, 32, 0, st>>>(sc, 0, j);
-    PSC_LAUNCH_CHECK(ctx);
-    std::swap(v0, v);                                   // v0 = v1
-    k_scale_by<<<nb, 256, 0, st>>>(f, v, n, sc + 1);    // v1 = w / bet
-    PSC_LAUNCH_CHECK(ctx);
-  }
-  k_lz_tridiag<<<1, 64, 0, st>>>(sc, m, ctx->gram);
-  PSC_LAUNCH_CHECK(ctx);
-  rc = psc_syev_impl(ctx, ctx->gram, m, sc + 40, ctx->evec, st);
-  if (rc) return rc;
-  k_lz_bound<<<1, 32, 0, st>>>(sc, m, sc + 40, ctx->evec, 1, out_dev);
-  PSC_LAUNCH_CHECK(ctx);
   return 0;
 }
 
