@@ -35,7 +35,13 @@
 
 namespace {
 
-constexpr int TNT = 256;          // threads per CTA
+#ifndef PSC_STENCIL_THREADS
+#define PSC_STENCIL_THREADS 256
+#endif
+constexpr int TNT = PSC_STENCIL_THREADS;  // threads per CTA
+#ifndef PSC_STENCIL_CTAS_PER_SM
+#define PSC_STENCIL_CTAS_PER_SM 2   // resident CTAs per SM (registers and shared memory)
+#endif
 // planes of X prefetched beyond the one consumed next
 #ifndef PSC_STENCIL_PREFETCH_F64
 #define PSC_STENCIL_PREFETCH_F64 3
@@ -574,7 +580,7 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   // are resident (registers and shared memory)
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  const int slots = 2 * sms;
+  const int slots = PSC_STENCIL_CTAS_PER_SM * sms;
   const int fill = R + prefetch_depth<T>() + 2;
   int nwork = 0;
   const int4* sched = stencil_sched(ctx, nslab, k, fill, slots, &nwork, st);
