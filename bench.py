@@ -550,11 +550,30 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scf-only", action="store_true",
                     help="run only the warm-up and timed SCF solves (for launch-list profiling)")
+    ap.add_argument("--fp64-gemm", action="store_true",
+                    help="only measure the cuBLAS FP64 GEMM rate (the FP64 denominator of the dense kernels)")
     ap.add_argument("--hartree", action="store_true",
                     help="only time the Hartree solve and its spectral preconditioner on the C10H8 grid")
     ap.add_argument("--stencil", choices=["f64", "f32"], default=None,
                     help="only time the fused stencil step (k = 55, C10H8 grid) for kernel profiling")
     args = ap.parse_args()
+    if args.fp64_gemm:
+        import torch
+
+        a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / 5
+        print(json.dumps({"fp64_gemm_tflops": 2 * 8192 ** 3 / t / 1e12, "n": 8192}))
+        return
     if args.hartree:
         print(json.dumps(hartree_timing(reps=max(1, args.steps))))
         return
