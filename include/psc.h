@@ -43,9 +43,9 @@ int psc_ctx_destroy(psc_ctx* ctx);
 /* out[8] = nx, ny, nz, n, projector atoms, projector points, touched points, stencil radius */
 int psc_ctx_info(const psc_ctx* ctx, long* out);
 /* host flags[8] of device-side checks: [0] filter bounds inverted, [1]
- * Cholesky pivot <= 0 at column flags[1]-1, [2] Jacobi not converged, [3] TMA
- * stencil wait timed out, [4] persistent CG grid barrier timed out; [6] is
- * informational: Jacobi sweeps of the last eigensolve.  clear != 0 resets */
+ * Cholesky pivot <= 0 at column flags[1]-1, [3] TMA stencil wait timed out,
+ * [4] persistent CG grid barrier timed out, [5] tensor-core Gram pipeline
+ * wait timed out; [2] and [6] reserved.  clear != 0 resets */
 int psc_status(psc_ctx* ctx, int* host_flags, int clear, void* stream);
 
 /* ---- ionic setup ------------------------------------------------------ */
@@ -159,7 +159,9 @@ int psc_rayleigh_ritz(psc_ctx* ctx, int dtype, const void* W, void* V, long ld, 
  * Rayleigh-Ritz, chefsi1.py:43-67 / first_filt.py:43-63). */
 int psc_subspace_rr(psc_ctx* ctx, int dtype, const void* W, void* V, long ld, int k, double* ritz_dev, void* stream);
 /* Building blocks: G = A^T B (mode 0 plain, 1 upper mirrored, 2 symmetrised),
- * Out = W Q, symmetric eigensolver (ascending, FP64, one CTA, k <= 1022). */
+ * Out = W Q, symmetric eigensolver of (A + A^T)/2 (ascending, FP64,
+ * Householder tridiagonalisation + bisection + inverse iteration, k <= 1024;
+ * replaces scipy.linalg.eigh at first_filt.py:59 and chefsi1.py:64). */
 int psc_gram(psc_ctx* ctx, int dtype, const void* A, long lda, const void* B, long ldb, int k, int mode,
              double* out_dev, void* stream);
 int psc_gemm_nn(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Q, int kout, void* out,

@@ -1,6 +1,7 @@
 // Subspace linear algebra: Gram products W^T V (n x k -> k x k), block
-// products W*Q, Cholesky, triangular inverse and a one-CTA cyclic Jacobi
-// symmetric eigensolver, plus the two subspace drivers built from them:
+// products W*Q, Cholesky, triangular inverse and a symmetric eigensolver
+// (Householder tridiagonalisation, bisection, inverse iteration), plus the
+// two subspace drivers built from them:
 // CholeskyQR2 orthonormalisation (replaces the Householder QR at
 // Eigensolvers/chefsi1.py:43 and first_filt.py:43) and Rayleigh-Ritz
 // (chefsi1.py:46-67, first_filt.py:44-63).  Small k x k work is FP64.
@@ -93,7 +94,7 @@ int psc_ensure_dense(psc_ctx* ctx, int k) {
   psc_dfree(ctx->jac_v);
   const int cap = std::max(k, 64);
   const size_t kk = (size_t)cap * cap;
-  // Jacobi scratch: padded A and V of order <= cap + 1 when they do not fit on chip
+  // eigensolver scratch: reflectors, tridiagonal eigenvectors, T and tau (>= 2 k^2 + 3 k)
   PSC_CUDA(ctx, psc_dmalloc(&ctx->jac_v, 2 * (size_t)(cap + 2) * (cap + 2) * sizeof(double)));
   PSC_CUDA(ctx, psc_dmalloc(&ctx->gram, kk * sizeof(double)));
   PSC_CUDA(ctx, psc_dmalloc(&ctx->gram2, kk * sizeof(double)));
@@ -200,179 +201,177 @@ __global__ void k_triu_inv(const double* __restrict__ R, int k, double* __restri
 }
 
 // ---------------------------------------------------------------------------
-// Cyclic Jacobi eigensolver, one CTA.  The matrix is padded to even order m
-// (a zero row/column when k is odd) and symmetrised.  Each round of a sweep
-// pairs the m indices into m/2 disjoint planes (circle method); the round is
-// two steps separated by one barrier each:
-//   1. every plane computes its rotation or skips it while
-//      |a_pq| <= 1e-17 (|a_pp| + |a_qq|).  The angle comes from FP32
-//      arithmetic (short latency); c and s are normalised in FP64, so every
-//      rotation is orthogonal to FP64 rounding and the a_pq it leaves
-//      (~1e-7 of the old one) is annihilated by later sweeps;
-//   2. the two-sided update A <- P^T A P as independent 2x2 blocks (rows of
-//      plane i, columns of plane j) on a 32-wide thread grid, together with
-//      V <- V P.
-// The solver has converged when a whole sweep rotates nothing (at most 60
-// sweeps; status word 2 is set otherwise).  Eigenvalues ascending,
-// eigenvectors permuted to match.
+// Symmetric eigensolver (ascending eigenvalues, orthonormal eigenvectors) of
+// the symmetrised matrix (A + A^T) / 2:
+//   1. k_sytrd: Householder reduction to tridiagonal form T = Q^T A Q in one
+//      CTA, the matrix in shared memory up to k = 153 and in L2-resident
+//      scratch beyond.  Step j reflects rows/columns j+1..k-1 with
+//      H_j = I - tau_j v_j v_j^T, v_j[j+1] = 1, chosen so that H_j zeroes
+//      A[j+2:, j] (dlarfg's Householder vector); the trailing block takes
+//      the rank-2 update A <- A - v w^T - w v^T with p = tau A v and
+//      w = p - (tau/2)(p.v) v.  Four barriers per step: the reflector
+//      (warp 0), partial products A v over column groups, p and p.v, the
+//      rank-2 update.
+//   2. all eigenvalues of T by Sturm-count multisection and its eigenvectors
+//      Z by inverse iteration (lanczos.cu), eigenvalues closer than 1e-3 |T|
+//      orthogonalised against each other inside one warp;
+//   3. k_ormtr: eigenvectors Q Z = H_0 H_1 ... H_{k-3} Z, one warp per column
+//      applying the reflectors from the last to the first.
+// Against the one-CTA cyclic Jacobi solver this replaces (two barriers per
+// rotation round, (k-1) rounds per sweep, 5-10 sweeps) the reduction takes
+// 4 (k-2) barriers in all.
 // ---------------------------------------------------------------------------
+constexpr int SY_GMAX = 8;   // column groups of the partial products A v
+
+static size_t sytrd_smem_doubles(int k, bool on_chip) {
+  return (on_chip ? (size_t)k * k : 0) + (size_t)(2 + SY_GMAX) * k;
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT)
-k_jacobi(const double* __restrict__ Ain, int k, double* __restrict__ evals, double* __restrict__ Vout,
-         int use_smem, double* __restrict__ scratch, int* status) {
+k_sytrd(const double* __restrict__ Ain, int k, int on_chip, double* __restrict__ hv, double* __restrict__ ab,
+        double* __restrict__ tau) {
   extern __shared__ double sm[];
-  __shared__ int rp[512], rq[512];
-  __shared__ double rc[512], rs[512];
-  __shared__ int rank_of[1024];
-  __shared__ int nrot;
-  const int m = k + (k & 1);
-  const int half = m / 2;
-  const int ld = m + 1;   // odd leading dimension: a warp's strided accesses spread over the banks
-  // use_smem: 2 = A and V on chip, 1 = A on chip and V in global scratch, 0 = both in scratch
-  double* A = use_smem ? sm : scratch;
-  double* V = use_smem == 2 ? A + m * ld : scratch + (use_smem ? 0 : m * ld);
-  for (int e = threadIdx.x; e < m * m; e += NT) {
-    const int i = e % m, j = e / m;
-    double a = 0.0;
-    if (i < k && j < k) a = (i == j) ? Ain[i + j * k] : 0.5 * (Ain[i + j * k] + Ain[j + i * k]);
-    A[i + j * ld] = a;
-    V[i + j * ld] = (i == j) ? 1.0 : 0.0;
-  }
-  __syncthreads();
-  int sweeps_done = 0;
-  for (int sweep = 0; sweep < 60 && k > 1; ++sweep) {
-    sweeps_done = sweep + 1;
-    if (threadIdx.x == 0) nrot = 0;
-    __syncthreads();
-    for (int r = 0; r < m - 1; ++r) {
-      for (int i = threadIdx.x; i < half; i += NT) {
-        const int a = (i == 0) ? 0 : ((i - 1 + r) % (m - 1)) + 1;
-        const int b = ((m - 2 - i + r) % (m - 1)) + 1;
-        const int p = min(a, b), q = max(a, b);
-        double c = 1.0, s = 0.0;
-        const double apq = A[p + q * ld];
-        const double app = A[p + p * ld], aqq = A[q + q * ld];
-        if (apq != 0.0 && fabs(apq) > 1e-17 * (fabs(app) + fabs(aqq))) {
-          nrot = 1;   // benign: every writer stores the same value
-          s = 1.0;
-          const double theta = (aqq - app) / (2.0 * apq);
-          double t;
-          if (fabs(theta) > 1e18) {
-            t = 0.5 / theta;
-          } else {
-            // tan of the annihilating angle to FP32 accuracy (Rutishauser's
-            // form); the rotation stays exactly orthogonal below, and the
-            // remainder of a_pq is removed by later sweeps
-            const float th = (float)theta;
-            t = (double)(copysignf(1.0f, th) / (fabsf(th) + sqrtf(fmaf(th, th, 1.0f))));
-          }
-          // c = 1/sqrt(1+t^2) in FP64: FP32 estimate plus two Newton-Raphson
-          // steps y <- y (3 - x y^2) / 2
-          const double x = fma(t, t, 1.0);
-          double y = (double)rsqrtf((float)x);
-          y = y * (1.5 - 0.5 * x * y * y);
-          y = y * (1.5 - 0.5 * x * y * y);
-          c = y;
-          s = t * y;
-        }
-        rp[i] = p; rq[i] = q; rc[i] = c; rs[i] = s;
-      }
-      __syncthreads();
-      // 2x2 blocks (i, j) on a 32-wide thread grid, then the V columns
-      {
-        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-        for (int i = ty; i < half; i += NT / 32) {
-          const double si = rs[i];
-          const int pi = rp[i], qi = rq[i];
-          const double ci = rc[i];
-          for (int j = tx; j < half; j += 32) {
-            const double sj = rs[j];
-            if (si == 0.0 && sj == 0.0) continue;
-            const int pj = rp[j], qj = rq[j];
-            const double cj = rc[j];
-            const double x00 = A[pi + pj * ld], x01 = A[pi + qj * ld], x10 = A[qi + pj * ld], x11 = A[qi + qj * ld];
-            // columns (plane j): [x.0 x.1] <- [c x.0 - s x.1, s x.0 + c x.1]
-            const double y00 = cj * x00 - sj * x01, y01 = sj * x00 + cj * x01;
-            const double y10 = cj * x10 - sj * x11, y11 = sj * x10 + cj * x11;
-            // rows (plane i); the rotated pair's own block is kept exactly symmetric
-            const double z00 = ci * y00 - si * y10, z10 = si * y00 + ci * y10;
-            const double z01 = ci * y01 - si * y11, z11 = si * y01 + ci * y11;
-            if (i == j) {
-              const double off = 0.5 * (z01 + z10);
-              A[pi + pj * ld] = z00;
-              A[qi + qj * ld] = z11;
-              A[qi + pj * ld] = off;
-              A[pi + qj * ld] = off;
-            } else {
-              A[pi + pj * ld] = z00;
-              A[qi + pj * ld] = z10;
-              A[pi + qj * ld] = z01;
-              A[qi + qj * ld] = z11;
-            }
-          }
-        }
-        for (int j = ty; j < half; j += NT / 32) {
-          const double sj = rs[j];
-          if (sj == 0.0) continue;
-          const double cj = rc[j];
-          double* vp = V + rp[j] * ld;
-          double* vq = V + rq[j] * ld;
-          for (int row = tx; row < m; row += 32) {
-            const double x = vp[row], y = vq[row];
-            vp[row] = cj * x - sj * y;
-            vq[row] = sj * x + cj * y;
-          }
-        }
-      }
-      __syncthreads();
+  __shared__ double red[NT / 32];
+  __shared__ double s_tau[2];   // by the parity of j: a warp may still read step j's while warp 0 writes j+1's
+  double* A = on_chip ? sm : hv;   // off chip the reflectors overwrite the columns they annihilated
+  double* v = sm + (on_chip ? (size_t)k * k : 0);
+  double* p = v + k;
+  double* part = p + k;            // [SY_GMAX][k]
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int c = w; c < k; c += NT / 32)
+    for (int r = lane; r < k; r += 32) {
+      const long e = r + (long)c * k;
+      A[e] = (r == c) ? Ain[e] : 0.5 * (Ain[e] + Ain[c + (long)r * k]);
     }
-    // a sweep without rotations means every pair is diagonal to working precision
-    const int rotated = nrot;
-    __syncthreads();
-    if (rotated == 0) break;
-    if (threadIdx.x == 0 && sweep == 59) status[2] = 1;  // did not converge
-  }
-  if (threadIdx.x == 0) status[6] = sweeps_done;   // diagnostic: sweeps of the last solve
   __syncthreads();
-  // sort ascending (stable by index), then permute the eigenvectors with
-  // coalesced stores
-  for (int i = threadIdx.x; i < k; i += NT) {
-    const double li = A[i + i * ld];
-    int rank = 0;
-    for (int j = 0; j < k; ++j) {
-      const double lj = A[j + j * ld];
-      rank += (lj < li) || (lj == li && j < i);
+  for (int j = 0; j + 2 < k; ++j) {
+    const int L = k - j - 1;   // order of the trailing block
+    double* A22 = A + (j + 1) + (long)(j + 1) * k;
+    if (w == 0) {
+      const double* x = A + (j + 1) + (long)j * k;
+      const double alpha = x[0];   // read by every lane before lane 0 overwrites it (off chip)
+      double sig = 0.0;
+      for (int i = 1 + lane; i < L; i += 32) sig += x[i] * x[i];
+      sig = psc_warp_sum(sig);
+      double t = 0.0, beta = alpha, scal = 0.0;
+      if (sig > 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + sig), alpha);
+        t = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      double* hj = hv + (j + 1) + (long)j * k;
+      for (int i = lane; i < L; i += 32) {
+        const double vi = i == 0 ? 1.0 : x[i] * scal;
+        v[i] = vi;
+        hj[i] = vi;
+      }
+      if (lane == 0) {
+        ab[2 * j] = A[j + (long)j * k];
+        ab[2 * j + 1] = beta;
+        tau[j] = t;
+        s_tau[j & 1] = t;
+      }
     }
-    evals[rank] = li;
-    rank_of[rank] = i;
+    __syncthreads();
+    const double t = s_tau[j & 1];
+    if (t == 0.0) continue;   // H_j = I (the same branch in every thread)
+    // partial products sum_{c = g mod G} A22[i, c] v[c]
+    const int R = min(NT, (L + 31) & ~31);
+    const int G = min(SY_GMAX, NT / R);
+    {
+      const int r0 = tid % R, g = tid / R;
+      if (g < G)
+        for (int i = r0; i < L; i += R) {
+          double s = 0.0;
+          for (int c = g; c < L; c += G) s += A22[i + (long)c * k] * v[c];
+          part[g * k + i] = s;
+        }
+    }
+    __syncthreads();
+    double q = 0.0;
+    for (int i = tid; i < L; i += NT) {
+      double s = 0.0;
+      for (int g = 0; g < G; ++g) s += part[g * k + i];
+      s *= t;
+      p[i] = s;
+      q += s * v[i];
+    }
+    q = psc_warp_sum(q);
+    if (lane == 0) red[w] = q;
+    __syncthreads();
+    double pv = 0.0;
+    for (int i = 0; i < NT / 32; ++i) pv += red[i];
+    const double K = 0.5 * t * pv;
+    for (int c = w; c < L; c += NT / 32) {
+      const double vc = v[c], wc = p[c] - K * vc;
+      double* col = A22 + (long)c * k;
+      for (int r = lane; r < L; r += 32) {
+        const double vr = v[r];
+        col[r] -= vr * wc + (p[r] - K * vr) * vc;
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  for (int e = threadIdx.x; e < k * k; e += NT) {
-    const int col = e / k, r = e - col * k;
-    Vout[e] = V[r + rank_of[col] * ld];
+  if (tid == 0) {
+    if (k >= 2) {
+      ab[2 * (k - 2)] = A[(k - 2) + (long)(k - 2) * k];
+      ab[2 * (k - 2) + 1] = A[(k - 1) + (long)(k - 2) * k];
+    }
+    ab[2 * (k - 1)] = A[(k - 1) + (long)(k - 1) * k];
+    ab[2 * (k - 1) + 1] = 0.0;
   }
 }
 
-int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, cudaStream_t st) {
-  PSC_REQUIRE(ctx, k >= 1 && k <= 1022, "syev: k out of range");
-  if (psc_ensure_dense(ctx, k)) return 1;
-  const int m = k + (k & 1);
-  const size_t tile = (size_t)m * (m + 1) * sizeof(double);
-  const int use_smem = 2 * tile <= 200 * 1024 ? 2 : (tile <= 200 * 1024 ? 1 : 0);
-  const size_t dyn = use_smem * tile;
-  // CTA size matched to the (m/2)^2 blocks + (m/2) m rows of a rotation round
-#define PSC_JACOBI(NTH)                                                                                   \
-  {                                                                                                       \
-    if (use_smem)                                                                                         \
-      PSC_CUDA(ctx, cudaFuncSetAttribute(k_jacobi<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)); \
-    k_jacobi<NTH><<<1, NTH, dyn, st>>>(A, k, evals, evecs, use_smem, ctx->jac_v, ctx->dev_status);       \
+// out = H_0 H_1 ... H_{k-3} Z, one warp per column of Z (k x k, ld k)
+template <int NW>
+__global__ void __launch_bounds__(NW * 32)
+k_ormtr(const double* __restrict__ hv, const double* __restrict__ tau, int k, const double* __restrict__ Z,
+        double* __restrict__ out) {
+  extern __shared__ double zs[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int col = blockIdx.x * NW + w;
+  if (col >= k) return;
+  double* z = zs + (size_t)w * k;
+  for (int i = lane; i < k; i += 32) z[i] = Z[i + (long)col * k];
+  __syncwarp();
+  for (int j = k - 3; j >= 0; --j) {
+    const double t = tau[j];
+    if (t == 0.0) continue;
+    const double* vj = hv + (long)j * k;   // rows j+1..k-1
+    double s = 0.0;
+    for (int i = j + 1 + lane; i < k; i += 32) s += vj[i] * z[i];
+    s = psc_warp_sum(s) * t;
+    for (int i = j + 1 + lane; i < k; i += 32) z[i] -= s * vj[i];
+    __syncwarp();
   }
-  // 32 x (NT/32) thread grid over the (m/2)^2 blocks of a rotation round
-  const int half = m / 2;
-  if (half <= 8) PSC_JACOBI(256)
-  else if (half <= 16) PSC_JACOBI(512)
-  else PSC_JACOBI(1024)
-#undef PSC_JACOBI
+  for (int i = lane; i < k; i += 32) out[i + (long)col * k] = z[i];
+}
+
+int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, cudaStream_t st) {
+  PSC_REQUIRE(ctx, k >= 1 && k <= PSC_MAX_K, "syev: k out of range");
+  if (psc_ensure_dense(ctx, k)) return 1;
+  const size_t kk = (size_t)k * k;
+  double* hv = ctx->jac_v;   // reflectors (and the matrix itself when it is not on chip)
+  double* Z = hv + kk;       // eigenvectors of T
+  double* ab = Z + kk;       // T: diagonal ab[2i], off-diagonal ab[2i+1]
+  double* tau = ab + 2 * k;
+  const bool on_chip = sytrd_smem_doubles(k, true) * sizeof(double) <= 200 * 1024;
+  const size_t dyn = sytrd_smem_doubles(k, on_chip) * sizeof(double);
+#define PSC_SYTRD(NTH)                                                                                      \
+  {                                                                                                         \
+    if (dyn > 48 * 1024)                                                                                    \
+      PSC_CUDA(ctx, cudaFuncSetAttribute(k_sytrd<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)); \
+    k_sytrd<NTH><<<1, NTH, dyn, st>>>(A, k, on_chip ? 1 : 0, hv, ab, tau);                                  \
+  }
+  if (!on_chip) PSC_SYTRD(1024)
+  else if (k <= 96) PSC_SYTRD(256)
+  else PSC_SYTRD(512)
+#undef PSC_SYTRD
+  PSC_LAUNCH_CHECK(ctx);
+  int rc = psc_tridiag_eig_impl(ctx, ab, k, k, evals, Z, k, 1e-3, st);
+  if (rc) return rc;
+  k_ormtr<4><<<psc_div_up(k, 4), 128, 4 * (size_t)k * sizeof(double), st>>>(hv, tau, k, Z, evecs);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }

@@ -158,7 +158,9 @@ extern "C" int psc_lanczos_run(psc_ctx* ctx, const double* v_start, unsigned lon
 // a pseudo-random start, with Gaussian elimination with partial pivoting of
 // the tridiagonal (a second superdiagonal appears where rows are
 // interchanged) and pivots below eps |T| replaced by +-eps |T|.  Eigenvalues
-// closer than 1e-7 |T| form a cluster handled by one warp in ascending order:
+// closer than crel |T| form a cluster handled by one warp in ascending order
+// (crel = 1e-7 for the Lanczos tridiagonals; 1e-3, the reorthogonalisation
+// gap of LAPACK's dstein, when the vectors must be orthonormal to ~1e-13):
 // each later member's shift is moved at least 10 eps |T| above the previous
 // one and its iterate is orthogonalised against the members before it after
 // every solve (modified Gram-Schmidt).  The entry of largest magnitude of
@@ -258,7 +260,7 @@ __device__ __forceinline__ double warp_dot_col(const double* x, const double* y,
 template <int NT>
 __global__ void __launch_bounds__(NT)
 k_tri_invit(const double* __restrict__ ab, int k, const double* __restrict__ evals, int nvec, double* __restrict__ Z,
-            long ldz, double* __restrict__ work) {
+            long ldz, double crel, double* __restrict__ work) {
   extern __shared__ double tri_sm[];
   __shared__ double red[64];
   __shared__ double s_lo, s_hi;
@@ -268,8 +270,9 @@ k_tri_invit(const double* __restrict__ ab, int k, const double* __restrict__ eva
   const int lane = threadIdx.x & 31;
   const int s0 = blockIdx.x * (NT / 32) + (threadIdx.x >> 5);
   if (s0 >= nvec) return;
-  const double tnorm = fmax(fmax(fabs(s_lo), fabs(s_hi)), DBL_MIN);
-  const double ctol = 1e-7 * tnorm;
+  // the floor keeps 1 / tiny and the squared iterates finite when T = 0
+  const double tnorm = fmax(fmax(fabs(s_lo), fabs(s_hi)), 1e-100);
+  const double ctol = crel * tnorm;
   if (s0 > 0 && evals[s0] - evals[s0 - 1] <= ctol) return;  // not the first of its cluster
   int s1 = s0 + 1;
   while (s1 < nvec && evals[s1] - evals[s1 - 1] <= ctol) ++s1;
@@ -370,12 +373,10 @@ static int tri_smem(psc_ctx* ctx, const void* func, size_t bytes) {
   return 0;
 }
 
-extern "C" int psc_tridiag_eig(psc_ctx* ctx, const double* ab, int k, int nvec, double* evals, double* Z, long ldz,
-                               void* stream) {
-  if (!ctx) return 2;
+int psc_tridiag_eig_impl(psc_ctx* ctx, const double* ab, int k, int nvec, double* evals, double* Z, long ldz,
+                         double crel, cudaStream_t st) {
   PSC_REQUIRE(ctx, ab && evals && k >= 1 && k <= TRI_MAX_K, "tridiag_eig: k out of range");
   PSC_REQUIRE(ctx, nvec >= 0 && nvec <= k && (nvec == 0 || (Z && ldz >= k)), "tridiag_eig: bad eigenvector block");
-  cudaStream_t st = (cudaStream_t)stream;
   const size_t smem = 2 * (size_t)k * sizeof(double);
   if (tri_smem(ctx, (const void*)k_tri_bisect<256>, smem)) return 1;
   k_tri_bisect<256><<<psc_div_up(k, 8), 256, smem, st>>>(ab, k, evals);
@@ -390,9 +391,15 @@ extern "C" int psc_tridiag_eig(psc_ctx* ctx, const double* ab, int k, int nvec, 
     ctx->tri_work_doubles = need;
   }
   if (tri_smem(ctx, (const void*)k_tri_invit<128>, smem)) return 1;
-  k_tri_invit<128><<<psc_div_up(nvec, 4), 128, smem, st>>>(ab, k, evals, nvec, Z, ldz, ctx->tri_work);
+  k_tri_invit<128><<<psc_div_up(nvec, 4), 128, smem, st>>>(ab, k, evals, nvec, Z, ldz, crel, ctx->tri_work);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
+}
+
+extern "C" int psc_tridiag_eig(psc_ctx* ctx, const double* ab, int k, int nvec, double* evals, double* Z, long ldz,
+                               void* stream) {
+  if (!ctx) return 2;
+  return psc_tridiag_eig_impl(ctx, ab, k, nvec, evals, Z, ldz, 1e-7, (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------

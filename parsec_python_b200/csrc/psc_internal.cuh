@@ -93,7 +93,7 @@ struct psc_ctx {
   double* gram2 = nullptr;       // [cap*cap]
   double* evec = nullptr;        // [cap*cap]
   double* tri = nullptr;         // [cap*cap]
-  double* jac_v = nullptr;       // [2 (cap+2)^2] padded Jacobi A and V when they do not fit on chip
+  double* jac_v = nullptr;       // [2 (cap+2)^2] eigensolver scratch: reflectors, eigenvectors of T, T, tau
   double* gram_partial = nullptr;// [gram_blocks][cap*cap] Gram partial sums
   int gram_blocks = 0;
   int* dev_status = nullptr;     // device-side error flags [8]
@@ -251,6 +251,8 @@ int psc_gram_impl(psc_ctx* ctx, int dtype, const void* A, long lda, const void* 
 int psc_gemm_nn_impl(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Q,
                      int kout, void* out, long ldo, cudaStream_t st);
 int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, cudaStream_t st);
+int psc_tridiag_eig_impl(psc_ctx* ctx, const double* ab, int k, int nvec, double* evals, double* Z, long ldz,
+                         double crel, cudaStream_t st);
 int psc_stencil_blocks(psc_ctx* ctx, int k);
 int psc_laplacian_fused(psc_ctx* ctx, const double* x, const double* prev, double* y, double a, double b,
                         double g, double* dot_partial, int* nblocks, cudaStream_t st);

@@ -115,12 +115,12 @@ class GridContext:
             raise ValueError("Bounds are incorrect")
         if f[1]:
             raise PscError(f"Cholesky of the overlap matrix failed at column {f[1] - 1} (subspace rank deficient)")
-        if f[2]:
-            raise PscError("Jacobi eigensolver did not converge")
         if f[3]:
             raise PscError("TMA stencil pipeline wait timed out")
         if f[4]:
             raise PscError("persistent CG grid barrier timed out")
+        if f[5]:
+            raise PscError("tensor-core Gram pipeline wait timed out")
 
     def info(self) -> dict:
         out = (c_long * 8)()

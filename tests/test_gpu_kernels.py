@@ -166,7 +166,7 @@ def test_dense_building_blocks():
         ctx.call("psc_gram", F64, gpu._p(Vd), ctx.n, gpu._p(Wd), ctx.n, k, 0, gpu._p(g), gpu._stream())
         G = g.cpu().numpy().T
         assert rel(G, V.T @ W) < 1e-13
-        # symmetric eigensolver (k x k FP64, one CTA)
+        # symmetric eigensolver (k x k FP64)
         S = rng.standard_normal((k, k))
         S = S + S.T
         A = torch.from_numpy(np.asfortranarray(S).ravel(order="F").copy()).to(DEV)
@@ -193,13 +193,17 @@ def test_dense_building_blocks():
         assert rel(host(out), W @ Qm) < 1e-13
 
 
-@pytest.mark.parametrize("k,kind", [(1, "rand"), (2, "rand"), (7, "rand"), (55, "diag"), (56, "degenerate"),
-                                    (111, "rand"), (143, "neardiag"), (200, "neardiag")])
+@pytest.mark.parametrize("k,kind", [(1, "rand"), (2, "rand"), (3, "rand"), (7, "rand"), (55, "diag"),
+                                    (56, "degenerate"), (64, "zero"), (111, "rand"), (143, "neardiag"),
+                                    (200, "neardiag"), (307, "rand"), (1024, "neardiag")])
 def test_syev_edge_cases(k, kind):
-    """Jacobi eigensolver: odd/even orders (padding), the three placements
-    (A and V on chip up to k = 110, A on chip up to k = 157, both in global
-    memory beyond), an input that is already diagonal, repeated eigenvalues,
-    nearly diagonal RR matrices."""
+    """Householder + bisection + inverse iteration eigensolver: orders with
+    no reflector (1, 2) and one (3), the three CTA sizes (256 threads up to
+    k = 96, 512 up to 153 with the matrix on chip, 1024 with it in global
+    scratch beyond), the widest block (1024), an input that is already
+    diagonal (every reflector the identity), eigenvalues of multiplicity 14
+    and 28 (one inverse-iteration cluster each), the zero matrix, nearly
+    diagonal RR matrices."""
     ctx = gpu.GridContext({"nx": 8, "ny": 8, "nz": 8, "h": 0.5, "radius": 1.75}, 8)
     rng = np.random.default_rng(k)
     if kind == "rand":
@@ -210,13 +214,15 @@ def test_syev_edge_cases(k, kind):
     elif kind == "degenerate":
         Q, _ = np.linalg.qr(rng.standard_normal((k, k)))
         S = (Q * np.repeat([1.0, 2.0, -3.0, 2.0], k // 4)) @ Q.T
+    elif kind == "zero":
+        S = np.zeros((k, k))
     else:
         S = np.diag(np.sort(rng.standard_normal(k))) + 1e-4 * rng.standard_normal((k, k))
         S = 0.5 * (S + S.T)
     A = torch.from_numpy(np.asfortranarray(S).ravel(order="F").copy()).to(DEV)
     ev, vec = ctx.empty(k), ctx.empty(k * k)
     ctx.call("psc_syev", gpu._p(A), k, gpu._p(ev), gpu._p(vec), gpu._stream())
-    assert ctx.status()[2] == 0
+    assert not any(ctx.status())
     lam = ev.cpu().numpy()
     Q = vec.cpu().numpy().reshape(k, k).T
     ref = np.linalg.eigvalsh(S)
