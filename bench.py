@@ -229,6 +229,51 @@ def stencil_roofline(reps: int = 40, dtype: str = "f64") -> dict:
     return {"seconds": t, "bytes": bytes_, "gbs": bytes_ / t / 1e9, "gflops": flops / t / 1e9, "n": n, "k": k}
 
 
+def syev_timing(cases: str = "55_rand,55_near,143_near,307_near", reps: int = 20) -> dict:
+    """The FP64 symmetric eigensolver of the Rayleigh-Ritz step (psc_syev:
+    Householder tridiagonalisation, bisection, inverse iteration,
+    back-transformation) on k x k matrices: "rand" = S + S^T of standard
+    normal entries, "near" = sorted normal diagonal + 1e-3 symmetric noise
+    (the nearly diagonal matrices of a converging SCF).  Median CUDA-event
+    time per call and the errors against numpy.linalg.eigvalsh."""
+    import torch
+
+    from parsec_python_b200 import gpu
+
+    ctx = gpu.GridContext({"nx": 8, "ny": 8, "nz": 8, "h": 0.5, "radius": 1.75}, 8)
+    rng = np.random.default_rng(1)
+    out = {}
+    for case in cases.split(","):
+        k, kind = int(case.split("_")[0]), case.split("_")[1]
+        if kind == "rand":
+            S = rng.standard_normal((k, k))
+            S = S + S.T
+        else:
+            S = np.diag(np.sort(rng.standard_normal(k))) + 1e-3 * rng.standard_normal((k, k))
+            S = 0.5 * (S + S.T)
+        A = torch.from_numpy(S.ravel(order="F").copy()).cuda()
+        ev, vec = ctx.empty(k), ctx.empty(k * k)
+        for _ in range(2):
+            ctx.call("psc_syev", gpu._p(A), k, gpu._p(ev), gpu._p(vec), gpu._stream())
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps if k < 300 else max(1, reps // 4)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ctx.call("psc_syev", gpu._p(A), k, gpu._p(ev), gpu._p(vec), gpu._stream())
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e3)
+        lam = ev.cpu().numpy()
+        Q = vec.cpu().numpy().reshape(k, k).T
+        ref = np.linalg.eigvalsh(S)
+        out[case] = {"us": float(np.median(ts)), "eigenvalue_err": float(np.abs(lam - ref).max()),
+                     "residual": float(np.abs(S @ Q - Q * lam).max()),
+                     "orthogonality": float(np.abs(Q.T @ Q - np.eye(k)).max())}
+    ctx.check_status()
+    return out
+
+
 def hartree_timing(reps: int = 20) -> dict:
     """The Hartree solve on the C10H8 grid (78^3, fd_order 8): one
     application of the spectral preconditioner (five passes of 32-line tile
@@ -556,6 +601,8 @@ def main():
                     help="only time the Hartree solve and its spectral preconditioner on the C10H8 grid")
     ap.add_argument("--stencil", choices=["f64", "f32"], default=None,
                     help="only time the fused stencil step (k = 55, C10H8 grid) for kernel profiling")
+    ap.add_argument("--syev", nargs="?", const="55_rand,55_near,143_near,307_near", default=None,
+                    help="only time the k x k symmetric eigensolver (comma-separated <k>_<rand|near> cases)")
     args = ap.parse_args()
     if args.fp64_gemm:
         import torch
@@ -579,6 +626,9 @@ def main():
         return
     if args.stencil:
         print(json.dumps(stencil_roofline(reps=max(1, args.steps), dtype=args.stencil)))
+        return
+    if args.syev:
+        print(json.dumps(syev_timing(args.syev)))
         return
     rank, local, world = dist_init()
     try:

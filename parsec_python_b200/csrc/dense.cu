@@ -200,6 +200,86 @@ __global__ void k_triu_inv(const double* __restrict__ R, int k, double* __restri
   }
 }
 
+// Cholesky and inverse in one CTA with the matrix in shared memory (k up to
+// 150): S = R^T R (R upper, written back in place with zeros below) and
+// X = R^{-1}.
+//   column j: every thread reads d = S[j,j] and takes r_jj = sqrt(d) (1, and
+//   status word 1 = j + 1, if d <= 0); row j right of the diagonal divided by
+//   r_jj goes to u; barrier; the trailing upper triangle loses u_r u_c;
+//   barrier.  The same operations as k_cholesky, two barriers per column.
+//   R^{-1}: one warp per column j, right-looking substitution on b = e_j:
+//   x_i = b_i / r_ii, then b_r -= R[r, i] x_i for r < i.
+constexpr int CI_NT = 512;
+
+static size_t chol_inv_smem_doubles(int k) { return (size_t)k * k + (size_t)(2 + CI_NT / 32) * k; }
+
+__global__ void __launch_bounds__(CI_NT) k_chol_inv(double* __restrict__ S, int k, double* __restrict__ X,
+                                                    int* status) {
+  extern __shared__ double sm[];
+  constexpr int NW = CI_NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  double* A = sm;
+  double* u = A + (size_t)k * k;
+  double* dg = u + k;
+  double* b = dg + k + (size_t)w * k;   // this warp's right-hand side
+  for (int c = w; c < k; c += NW)
+    for (int r = lane; r < k; r += 32) A[r + (long)c * k] = S[r + (long)c * k];
+  __syncthreads();
+  for (int j = 0; j < k; ++j) {
+    const double d = A[j + (long)j * k];
+    const double rjj = d > 0.0 ? sqrt(d) : 1.0;
+    if (tid == 0) {
+      dg[j] = rjj;
+      if (!(d > 0.0)) status[1] = j + 1;   // not positive definite
+    }
+    for (int c = j + 1 + tid; c < k; c += CI_NT) {
+      const double v = A[j + (long)c * k] / rjj;
+      u[c] = v;
+      A[j + (long)c * k] = v;
+    }
+    __syncthreads();
+    for (int c = j + 1 + w; c < k; c += NW) {
+      const double uc = u[c];
+      for (int r = j + 1 + lane; r <= c; r += 32) A[r + (long)c * k] -= u[r] * uc;
+    }
+    __syncthreads();
+  }
+  for (int c = w; c < k; c += NW)
+    for (int r = lane; r < k; r += 32) S[r + (long)c * k] = r < c ? A[r + (long)c * k] : (r == c ? dg[c] : 0.0);
+  for (int j = w; j < k; j += NW) {
+    double* xj = X + (long)j * k;
+    for (int r = lane; r < k; r += 32) {
+      if (r <= j) b[r] = r == j ? 1.0 : 0.0;
+      else xj[r] = 0.0;
+    }
+    __syncwarp();
+    for (int i = j; i >= 0; --i) {
+      const double xi = b[i] / dg[i];
+      const double* ri = A + (long)i * k;   // column i of R above the diagonal
+      for (int r = lane; r < i; r += 32) b[r] -= ri[r] * xi;
+      if (lane == 0) xj[i] = xi;
+      __syncwarp();
+    }
+  }
+}
+
+// R and R^{-1} of S = R^T R (S overwritten by R)
+int psc_chol_inv_dev(psc_ctx* ctx, double* S, int k, double* X, cudaStream_t st) {
+  const size_t dyn = chol_inv_smem_doubles(k) * sizeof(double);
+  if (dyn <= 200 * 1024) {
+    if (dyn > 48 * 1024)
+      PSC_CUDA(ctx, cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    k_chol_inv<<<1, CI_NT, dyn, st>>>(S, k, X, ctx->dev_status);
+    PSC_LAUNCH_CHECK(ctx);
+    return 0;
+  }
+  k_cholesky<<<1, 1024, 0, st>>>(S, k, ctx->dev_status);
+  PSC_LAUNCH_CHECK(ctx);
+  k_triu_inv<<<psc_div_up(k, 128), 128, 0, st>>>(S, k, X);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 // Symmetric eigensolver (ascending eigenvalues, orthonormal eigenvectors) of
 // the symmetrised matrix (A + A^T) / 2:
@@ -209,22 +289,56 @@ __global__ void k_triu_inv(const double* __restrict__ R, int k, double* __restri
 //      H_j = I - tau_j v_j v_j^T, v_j[j+1] = 1, chosen so that H_j zeroes
 //      A[j+2:, j] (dlarfg's Householder vector); the trailing block takes
 //      the rank-2 update A <- A - v w^T - w v^T with p = tau A v and
-//      w = p - (tau/2)(p.v) v.  Four barriers per step: the reflector
-//      (warp 0), partial products A v over column groups, p and p.v, the
-//      rank-2 update.
+//      w = p - (tau/2)(p.v) v.  Three barriers per step: partial products
+//      A v over column groups, p and p.v, the rank-2 update; warp 0 builds
+//      reflector j+1 inside the update, right after column j+1.
 //   2. all eigenvalues of T by Sturm-count multisection and its eigenvectors
 //      Z by inverse iteration (lanczos.cu), eigenvalues closer than 1e-3 |T|
 //      orthogonalised against each other inside one warp;
 //   3. k_ormtr: eigenvectors Q Z = H_0 H_1 ... H_{k-3} Z, one warp per column
-//      applying the reflectors from the last to the first.
+//      applying the reflectors from the last to the first, staged in shared
+//      memory in chunks.
 // Against the one-CTA cyclic Jacobi solver this replaces (two barriers per
 // rotation round, (k-1) rounds per sweep, 5-10 sweeps) the reduction takes
-// 4 (k-2) barriers in all.
+// 3 (k-2) barriers in all.
 // ---------------------------------------------------------------------------
 constexpr int SY_GMAX = 8;   // column groups of the partial products A v
 
 static size_t sytrd_smem_doubles(int k, bool on_chip) {
-  return (on_chip ? (size_t)k * k : 0) + (size_t)(2 + SY_GMAX) * k;
+  return (on_chip ? (size_t)k * k : 0) + (size_t)(3 + SY_GMAX) * k;
+}
+
+// Reflector j from column j below the diagonal (one warp): v -> v (shared)
+// and hv column j (rows j+1..k-1), d_j, e_j = beta -> ab, tau_j -> tau and
+// *s_t.  Off chip hv is A, so every lane reads x[i] before it writes hv[i].
+__device__ __forceinline__ void sy_reflector(const double* A, int k, int j, double* __restrict__ hv, double* v,
+                                             double* __restrict__ ab, double* __restrict__ tau, double* s_t,
+                                             int lane) {
+  const int L = k - j - 1;
+  const double* x = A + (j + 1) + (long)j * k;
+  const double alpha = x[0];   // read by every lane before lane 0 overwrites it (off chip)
+  const double dj = A[j + (long)j * k];
+  double sig = 0.0;
+  for (int i = 1 + lane; i < L; i += 32) sig += x[i] * x[i];
+  sig = psc_warp_sum(sig);
+  double t = 0.0, beta = alpha, scal = 0.0;
+  if (sig > 0.0) {
+    beta = -copysign(sqrt(alpha * alpha + sig), alpha);
+    t = (beta - alpha) / beta;
+    scal = 1.0 / (alpha - beta);
+  }
+  double* hj = hv + (j + 1) + (long)j * k;
+  for (int i = lane; i < L; i += 32) {
+    const double vi = i == 0 ? 1.0 : x[i] * scal;
+    v[i] = vi;
+    hj[i] = vi;
+  }
+  if (lane == 0) {
+    ab[2 * j] = dj;
+    ab[2 * j + 1] = beta;
+    tau[j] = t;
+    *s_t = t;
+  }
 }
 
 template <int NT>
@@ -232,84 +346,75 @@ __global__ void __launch_bounds__(NT)
 k_sytrd(const double* __restrict__ Ain, int k, int on_chip, double* __restrict__ hv, double* __restrict__ ab,
         double* __restrict__ tau) {
   extern __shared__ double sm[];
-  __shared__ double red[NT / 32];
-  __shared__ double s_tau[2];   // by the parity of j: a warp may still read step j's while warp 0 writes j+1's
+  constexpr int NW = NT / 32;
+  __shared__ double red[NW];
+  // v and tau by the parity of j: warp 0 builds reflector j+1 while the other
+  // warps still apply reflector j
+  __shared__ double s_tau[2];
   double* A = on_chip ? sm : hv;   // off chip the reflectors overwrite the columns they annihilated
-  double* v = sm + (on_chip ? (size_t)k * k : 0);
-  double* p = v + k;
+  double* vb = sm + (on_chip ? (size_t)k * k : 0);   // [2][k]
+  double* p = vb + 2 * k;
   double* part = p + k;            // [SY_GMAX][k]
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  for (int c = w; c < k; c += NT / 32)
+  for (int c = w; c < k; c += NW)
     for (int r = lane; r < k; r += 32) {
       const long e = r + (long)c * k;
       A[e] = (r == c) ? Ain[e] : 0.5 * (Ain[e] + Ain[c + (long)r * k]);
     }
   __syncthreads();
+  if (k > 2 && w == 0) sy_reflector(A, k, 0, hv, vb, ab, tau, &s_tau[0], lane);
+  __syncthreads();
   for (int j = 0; j + 2 < k; ++j) {
     const int L = k - j - 1;   // order of the trailing block
     double* A22 = A + (j + 1) + (long)(j + 1) * k;
-    if (w == 0) {
-      const double* x = A + (j + 1) + (long)j * k;
-      const double alpha = x[0];   // read by every lane before lane 0 overwrites it (off chip)
-      double sig = 0.0;
-      for (int i = 1 + lane; i < L; i += 32) sig += x[i] * x[i];
-      sig = psc_warp_sum(sig);
-      double t = 0.0, beta = alpha, scal = 0.0;
-      if (sig > 0.0) {
-        beta = -copysign(sqrt(alpha * alpha + sig), alpha);
-        t = (beta - alpha) / beta;
-        scal = 1.0 / (alpha - beta);
-      }
-      double* hj = hv + (j + 1) + (long)j * k;
-      for (int i = lane; i < L; i += 32) {
-        const double vi = i == 0 ? 1.0 : x[i] * scal;
-        v[i] = vi;
-        hj[i] = vi;
-      }
-      if (lane == 0) {
-        ab[2 * j] = A[j + (long)j * k];
-        ab[2 * j + 1] = beta;
-        tau[j] = t;
-        s_tau[j & 1] = t;
-      }
-    }
-    __syncthreads();
+    const double* v = vb + (j & 1) * k;
+    double* vn = vb + ((j + 1) & 1) * k;
+    const bool next = j + 3 < k;   // reflector j+1 exists
     const double t = s_tau[j & 1];
-    if (t == 0.0) continue;   // H_j = I (the same branch in every thread)
-    // partial products sum_{c = g mod G} A22[i, c] v[c]
-    const int R = min(NT, (L + 31) & ~31);
-    const int G = min(SY_GMAX, NT / R);
-    {
-      const int r0 = tid % R, g = tid / R;
-      if (g < G)
-        for (int i = r0; i < L; i += R) {
-          double s = 0.0;
-          for (int c = g; c < L; c += G) s += A22[i + (long)c * k] * v[c];
-          part[g * k + i] = s;
-        }
-    }
-    __syncthreads();
-    double q = 0.0;
-    for (int i = tid; i < L; i += NT) {
-      double s = 0.0;
-      for (int g = 0; g < G; ++g) s += part[g * k + i];
-      s *= t;
-      p[i] = s;
-      q += s * v[i];
-    }
-    q = psc_warp_sum(q);
-    if (lane == 0) red[w] = q;
-    __syncthreads();
-    double pv = 0.0;
-    for (int i = 0; i < NT / 32; ++i) pv += red[i];
-    const double K = 0.5 * t * pv;
-    for (int c = w; c < L; c += NT / 32) {
-      const double vc = v[c], wc = p[c] - K * vc;
-      double* col = A22 + (long)c * k;
-      for (int r = lane; r < L; r += 32) {
-        const double vr = v[r];
-        col[r] -= vr * wc + (p[r] - K * vr) * vc;
+    if (t != 0.0) {   // the same branch in every thread
+      // partial products sum_{c = g mod G} A22[i, c] v[c]
+      const int R = min(NT, (L + 31) & ~31);
+      const int G = min(SY_GMAX, NT / R);
+      {
+        const int r0 = tid % R, g = tid / R;
+        if (g < G)
+          for (int i = r0; i < L; i += R) {
+            double s = 0.0;
+            for (int c = g; c < L; c += G) s += A22[i + (long)c * k] * v[c];
+            part[g * k + i] = s;
+          }
       }
+      __syncthreads();
+      double q = 0.0;
+      for (int i = tid; i < L; i += NT) {
+        double s = 0.0;
+        for (int g = 0; g < G; ++g) s += part[g * k + i];
+        s *= t;
+        p[i] = s;
+        q += s * v[i];
+      }
+      q = psc_warp_sum(q);
+      if (lane == 0) red[w] = q;
+      __syncthreads();
+      double pv = 0.0;
+      for (int i = 0; i < NW; ++i) pv += red[i];
+      const double K = 0.5 * t * pv;
+      // rank-2 update; warp 0 takes column 0 (column j+1 of A) first and
+      // builds reflector j+1 from it before its other columns
+      for (int c = w; c < L; c += NW) {
+        const double vc = v[c], wc = p[c] - K * vc;
+        double* col = A22 + (long)c * k;
+        for (int r = lane; r < L; r += 32) {
+          const double vr = v[r];
+          col[r] -= vr * wc + (p[r] - K * vr) * vc;
+        }
+        if (c == 0 && next) {
+          __syncwarp();
+          sy_reflector(A, k, j + 1, hv, vn, ab, tau, &s_tau[(j + 1) & 1], lane);
+        }
+      }
+    } else if (w == 0 && next) {   // H_j = I: column j+1 is unchanged
+      sy_reflector(A, k, j + 1, hv, vn, ab, tau, &s_tau[(j + 1) & 1], lane);
     }
     __syncthreads();
   }
@@ -323,29 +428,48 @@ k_sytrd(const double* __restrict__ Ain, int k, int on_chip, double* __restrict__
   }
 }
 
-// out = H_0 H_1 ... H_{k-3} Z, one warp per column of Z (k x k, ld k)
-template <int NW>
-__global__ void __launch_bounds__(NW * 32)
+// out = H_0 H_1 ... H_{k-3} Z (Z k x k, ld k).  A CTA owns OR_NW columns, one
+// warp each; the whole CTA stages the reflectors OR_CH at a time in shared
+// memory (one round of independent L2 loads per chunk instead of two
+// dependent ones per reflector), then every warp applies them to its column.
+constexpr int OR_NW = 8, OR_CH = 16;
+
+static size_t ormtr_smem_bytes(int k) { return (size_t)(OR_NW + OR_CH) * k * sizeof(double); }
+
+__global__ void __launch_bounds__(OR_NW * 32)
 k_ormtr(const double* __restrict__ hv, const double* __restrict__ tau, int k, const double* __restrict__ Z,
         double* __restrict__ out) {
-  extern __shared__ double zs[];
+  extern __shared__ double sm[];
+  __shared__ double ts[OR_CH];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int col = blockIdx.x * NW + w;
-  if (col >= k) return;
-  double* z = zs + (size_t)w * k;
-  for (int i = lane; i < k; i += 32) z[i] = Z[i + (long)col * k];
-  __syncwarp();
-  for (int j = k - 3; j >= 0; --j) {
-    const double t = tau[j];
-    if (t == 0.0) continue;
-    const double* vj = hv + (long)j * k;   // rows j+1..k-1
-    double s = 0.0;
-    for (int i = j + 1 + lane; i < k; i += 32) s += vj[i] * z[i];
-    s = psc_warp_sum(s) * t;
-    for (int i = j + 1 + lane; i < k; i += 32) z[i] -= s * vj[i];
-    __syncwarp();
+  const int col = blockIdx.x * OR_NW + w;
+  double* z = sm + (size_t)w * k;
+  double* vs = sm + (size_t)OR_NW * k;   // [OR_CH][k]
+  if (col < k)
+    for (int i = lane; i < k; i += 32) z[i] = Z[i + (long)col * k];
+  for (int j1 = k - 3; j1 >= 0; j1 -= OR_CH) {
+    const int j0 = max(0, j1 - OR_CH + 1);
+    __syncthreads();   // the previous chunk is consumed
+    for (int c = w; c <= j1 - j0; c += OR_NW) {
+      const int j = j0 + c;
+      for (int i = j + 1 + lane; i < k; i += 32) vs[(size_t)c * k + i] = hv[i + (long)j * k];
+      if (lane == 0) ts[c] = tau[j];
+    }
+    __syncthreads();
+    if (col < k)
+      for (int j = j1; j >= j0; --j) {
+        const double t = ts[j - j0];
+        if (t == 0.0) continue;
+        const double* vj = vs + (size_t)(j - j0) * k;   // rows j+1..k-1
+        double s = 0.0;
+        for (int i = j + 1 + lane; i < k; i += 32) s += vj[i] * z[i];
+        s = psc_warp_sum(s) * t;
+        for (int i = j + 1 + lane; i < k; i += 32) z[i] -= s * vj[i];
+        __syncwarp();
+      }
   }
-  for (int i = lane; i < k; i += 32) out[i + (long)col * k] = z[i];
+  if (col < k)
+    for (int i = lane; i < k; i += 32) out[i + (long)col * k] = z[i];
 }
 
 int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, cudaStream_t st) {
@@ -371,7 +495,10 @@ int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, 
   PSC_LAUNCH_CHECK(ctx);
   int rc = psc_tridiag_eig_impl(ctx, ab, k, k, evals, Z, k, 1e-3, st);
   if (rc) return rc;
-  k_ormtr<4><<<psc_div_up(k, 4), 128, 4 * (size_t)k * sizeof(double), st>>>(hv, tau, k, Z, evecs);
+  const size_t dyn2 = ormtr_smem_bytes(k);
+  if (dyn2 > 48 * 1024)
+    PSC_CUDA(ctx, cudaFuncSetAttribute(k_ormtr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn2));
+  k_ormtr<<<psc_div_up(k, OR_NW), OR_NW * 32, dyn2, st>>>(hv, tau, k, Z, evecs);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }
@@ -396,10 +523,8 @@ extern "C" int psc_orthonormalize(psc_ctx* ctx, int dtype, void* W, void* T, lon
   for (int p = 0; p < passes; ++p) {
     int rc = psc_gram_impl(ctx, dtype, buf[cur], ld, buf[cur], ld, k, ctx->gram, 2, st);
     if (rc) return rc;
-    k_cholesky<<<1, 1024, 0, st>>>(ctx->gram, k, ctx->dev_status);
-    PSC_LAUNCH_CHECK(ctx);
-    k_triu_inv<<<psc_div_up(k, 128), 128, 0, st>>>(ctx->gram, k, ctx->tri);
-    PSC_LAUNCH_CHECK(ctx);
+    rc = psc_chol_inv_dev(ctx, ctx->gram, k, ctx->tri, st);
+    if (rc) return rc;
     rc = psc_gemm_nn_impl(ctx, dtype, buf[cur], ld, k, ctx->tri, k, buf[cur ^ 1], ld, st);
     if (rc) return rc;
     cur ^= 1;
@@ -423,16 +548,4 @@ extern "C" int psc_rayleigh_ritz(psc_ctx* ctx, int dtype, const void* W, void* V
   rc = psc_syev_impl(ctx, ctx->gram, k, ritz_dev, ctx->evec, st);
   if (rc) return rc;
   return psc_gemm_nn_impl(ctx, dtype, W, ld, k, ctx->evec, k, V, ld, st);
-}
-
-int psc_cholesky_dev(psc_ctx* ctx, double* A, int k, cudaStream_t st) {
-  k_cholesky<<<1, 1024, 0, st>>>(A, k, ctx->dev_status);
-  PSC_LAUNCH_CHECK(ctx);
-  return 0;
-}
-
-int psc_triu_inv_dev(psc_ctx* ctx, const double* R, int k, double* X, cudaStream_t st) {
-  k_triu_inv<<<psc_div_up(k, 128), 128, 0, st>>>(R, k, X);
-  PSC_LAUNCH_CHECK(ctx);
-  return 0;
 }

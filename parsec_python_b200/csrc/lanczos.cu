@@ -150,9 +150,11 @@ extern "C" int psc_lanczos_run(psc_ctx* ctx, const double* v_start, unsigned lon
 //
 // Eigenvalues: the Sturm count c(x) (negative pivots of the LDL^T factors of
 // T - x I) is the number of eigenvalues below x.  One warp finds eigenvalue i
-// by multisection of the Gershgorin interval: its 32 lanes evaluate c at 32
-// interior points, a ballot keeps the sub-interval with c(lo) <= i < c(hi),
-// so every round gains five bits (at most 16 rounds).
+// by multisection of the Gershgorin interval: each of its 32 lanes evaluates
+// c at P = PSC_TRI_POINTS interior points (32 P in all, the P recurrences of
+// a lane interleaved so that their divisions overlap), a ballot keeps the
+// sub-interval with c(lo) <= i < c(hi), so every round gains log2(32 P + 1)
+// bits (at most 16 rounds).
 //
 // Eigenvectors: inverse iteration, (T - lambda I) x_new = x, three times from
 // a pseudo-random start, with Gaussian elimination with partial pivoting of
@@ -197,19 +199,34 @@ __device__ __forceinline__ void tri_load(const double* __restrict__ ab, int k, d
   __syncthreads();
 }
 
-__device__ __forceinline__ int sturm_count(const double* a, const double* e, int k, double x, double pivmin) {
-  double q = a[0] - x;
-  if (fabs(q) < pivmin) q = -pivmin;
-  int c = q < 0.0;
-  for (int i = 1; i < k; ++i) {
-    q = (a[i] - x) - (e[i - 1] * e[i - 1]) / q;
-    if (fabs(q) < pivmin) q = -pivmin;
-    c += q < 0.0;
+#ifndef PSC_TRI_POINTS
+#define PSC_TRI_POINTS 1   // Sturm counts per lane and multisection round (2 and 4 measured slower)
+#endif
+
+// Sturm counts at P points, the P recurrences interleaved so that their
+// divisions overlap
+template <int P>
+__device__ __forceinline__ void sturm_counts(const double* a, const double* e, int k, const double (&x)[P],
+                                             double pivmin, int (&c)[P]) {
+  double q[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    q[p] = a[0] - x[p];
+    if (fabs(q[p]) < pivmin) q[p] = -pivmin;
+    c[p] = q[p] < 0.0;
   }
-  return c;
+  for (int i = 1; i < k; ++i) {
+    const double ai = a[i], e2 = e[i - 1] * e[i - 1];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      q[p] = (ai - x[p]) - e2 / q[p];
+      if (fabs(q[p]) < pivmin) q[p] = -pivmin;
+      c[p] += q[p] < 0.0;
+    }
+  }
 }
 
-template <int NT>
+template <int NT, int P>
 __global__ void __launch_bounds__(NT) k_tri_bisect(const double* __restrict__ ab, int k, double* __restrict__ evals) {
   extern __shared__ double tri_sm[];
   __shared__ double red[64];
@@ -223,20 +240,38 @@ __global__ void __launch_bounds__(NT) k_tri_bisect(const double* __restrict__ ab
   const double tnorm = fmax(fabs(s_lo), fabs(s_hi));
   const double pivmin = DBL_MIN * fmax(1.0, tnorm * tnorm);
   const double pad = 4.0 * DBL_EPSILON * tnorm * k + 4.0 * pivmin;
+  const double step = 1.0 / (32.0 * P + 1.0);
   double lo = s_lo - pad, hi = s_hi + pad;
   for (int round = 0; round < 16; ++round) {
     if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin) break;
-    const double x = lo + (hi - lo) * (double)(lane + 1) / 33.0;
-    const int c = sturm_count(a, e, k, x, pivmin);
-    const unsigned m = __ballot_sync(0xffffffffu, c > i);
+    // point t = lane P + p of 32 P interior points; counts rise with t
+    double x[P];
+    int c[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) x[p] = lo + (hi - lo) * ((double)(lane * P + p + 1) * step);
+    sturm_counts<P>(a, e, k, x, pivmin, c);
+    int pf = P;   // this lane's first point with more than i eigenvalues below it
+    double xhi = 0.0, xlo = 0.0;
+#pragma unroll
+    for (int p = P - 1; p >= 0; --p)
+      if (c[p] > i) {
+        pf = p;
+        xhi = x[p];
+        xlo = p > 0 ? x[p - 1] : 0.0;
+      }
+    const unsigned m = __ballot_sync(0xffffffffu, pf < P);
+    const double xlast = x[P - 1];
     if (m == 0) {
-      lo = __shfl_sync(0xffffffffu, x, 31);
+      lo = __shfl_sync(0xffffffffu, xlast, 31);
     } else {
       const int f = __ffs(m) - 1;
-      const double xf = __shfl_sync(0xffffffffu, x, f);
-      const double xp = __shfl_sync(0xffffffffu, x, f > 0 ? f - 1 : 0);
-      hi = xf;
-      if (f > 0) lo = xp;
+      const int pff = __shfl_sync(0xffffffffu, pf, f);
+      const double h = __shfl_sync(0xffffffffu, xhi, f);
+      const double l_in = __shfl_sync(0xffffffffu, xlo, f);
+      const double l_prev = __shfl_sync(0xffffffffu, xlast, f > 0 ? f - 1 : 0);
+      hi = h;
+      if (pff > 0) lo = l_in;
+      else if (f > 0) lo = l_prev;
     }
   }
   if (lane == 0) evals[i] = 0.5 * (lo + hi);
@@ -378,8 +413,16 @@ int psc_tridiag_eig_impl(psc_ctx* ctx, const double* ab, int k, int nvec, double
   PSC_REQUIRE(ctx, ab && evals && k >= 1 && k <= TRI_MAX_K, "tridiag_eig: k out of range");
   PSC_REQUIRE(ctx, nvec >= 0 && nvec <= k && (nvec == 0 || (Z && ldz >= k)), "tridiag_eig: bad eigenvector block");
   const size_t smem = 2 * (size_t)k * sizeof(double);
-  if (tri_smem(ctx, (const void*)k_tri_bisect<256>, smem)) return 1;
-  k_tri_bisect<256><<<psc_div_up(k, 8), 256, smem, st>>>(ab, k, evals);
+  // up to k = 512 one warp per CTA, so that the latency-bound warps get an SM
+  // scheduler each; beyond, eight warps share each copy of T in shared memory
+  const bool solo = k <= 512;
+  if (solo) {
+    if (tri_smem(ctx, (const void*)k_tri_bisect<32, PSC_TRI_POINTS>, smem)) return 1;
+    k_tri_bisect<32, PSC_TRI_POINTS><<<k, 32, smem, st>>>(ab, k, evals);
+  } else {
+    if (tri_smem(ctx, (const void*)k_tri_bisect<256, PSC_TRI_POINTS>, smem)) return 1;
+    k_tri_bisect<256, PSC_TRI_POINTS><<<psc_div_up(k, 8), 256, smem, st>>>(ab, k, evals);
+  }
   PSC_LAUNCH_CHECK(ctx);
   if (nvec == 0) return 0;
   const size_t need = 5 * (size_t)k * nvec;
@@ -390,8 +433,13 @@ int psc_tridiag_eig_impl(psc_ctx* ctx, const double* ab, int k, int nvec, double
     PSC_CUDA(ctx, psc_dmalloc(&ctx->tri_work, need * sizeof(double)));
     ctx->tri_work_doubles = need;
   }
-  if (tri_smem(ctx, (const void*)k_tri_invit<128>, smem)) return 1;
-  k_tri_invit<128><<<psc_div_up(nvec, 4), 128, smem, st>>>(ab, k, evals, nvec, Z, ldz, crel, ctx->tri_work);
+  if (solo) {
+    if (tri_smem(ctx, (const void*)k_tri_invit<32>, smem)) return 1;
+    k_tri_invit<32><<<nvec, 32, smem, st>>>(ab, k, evals, nvec, Z, ldz, crel, ctx->tri_work);
+  } else {
+    if (tri_smem(ctx, (const void*)k_tri_invit<128>, smem)) return 1;
+    k_tri_invit<128><<<psc_div_up(nvec, 4), 128, smem, st>>>(ab, k, evals, nvec, Z, ldz, crel, ctx->tri_work);
+  }
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }

@@ -188,8 +188,7 @@ __global__ void k_small_mm(const double* __restrict__ A, const double* __restric
 }
 
 // dense.cu
-int psc_cholesky_dev(psc_ctx* ctx, double* A, int k, cudaStream_t st);
-int psc_triu_inv_dev(psc_ctx* ctx, const double* R, int k, double* X, cudaStream_t st);
+int psc_chol_inv_dev(psc_ctx* ctx, double* S, int k, double* X, cudaStream_t st);
 
 int psc_gemm_tall(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Tm, int kout, void* O,
                   long ldo, cudaStream_t st) {
@@ -260,9 +259,7 @@ extern "C" int psc_subspace_rr(psc_ctx* ctx, int dtype, const void* W, void* V, 
   double* Y = ctx->evec;
   rc = gram_pair(ctx, dtype, W, V, ld, k, S, K, st);
   if (rc) return rc;
-  rc = psc_cholesky_dev(ctx, S, k, st);
-  if (rc) return rc;
-  rc = psc_triu_inv_dev(ctx, S, k, Ri, st);
+  rc = psc_chol_inv_dev(ctx, S, k, Ri, st);
   if (rc) return rc;
   const long kk = (long)k * k;
   const int nb = std::max(1, (int)std::min<long>(592, (kk + 127) / 128));

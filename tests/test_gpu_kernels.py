@@ -158,7 +158,7 @@ def test_dense_building_blocks():
     dom = {"nx": 20, "ny": 20, "nz": 20, "h": 0.5, "radius": 4.75}
     ctx = gpu.GridContext(dom, 8)
     rng = np.random.default_rng(6)
-    for k in (6, 27, 55, 130):
+    for k in (6, 27, 55, 130, 151, 200):  # Cholesky + inverse on chip up to 151, two kernels beyond
         W = rng.standard_normal((ctx.n, k))
         V = rng.standard_normal((ctx.n, k))
         g = ctx.empty(k, k)
@@ -191,6 +191,20 @@ def test_dense_building_blocks():
         Qd = torch.from_numpy(Qm.ravel(order="F").copy()).to(DEV)
         ctx.call("psc_gemm_nn", F64, gpu._p(Wd), ctx.n, k, gpu._p(Qd), k, gpu._p(out), ctx.n, gpu._stream())
         assert rel(host(out), W @ Qm) < 1e-13
+
+
+@pytest.mark.parametrize("k", [8, 160])
+def test_cholesky_flags_rank_deficient_block(k):
+    """A zero column makes its Cholesky pivot exactly 0: status word 1 names
+    it (column 3 -> 4), on chip (k = 8) and in the two-kernel form (k = 160)."""
+    dom = {"nx": 20, "ny": 20, "nz": 20, "h": 0.5, "radius": 4.75}
+    ctx = gpu.GridContext(dom, 8)
+    W = np.random.default_rng(k).standard_normal((ctx.n, k))
+    W[:, 3] = 0.0
+    Wd = block(W)
+    ctx.status(clear=True)
+    gpu.orthonormalize(ctx, Wd, torch.empty_like(Wd), passes=1)
+    assert ctx.status()[1] == 4
 
 
 @pytest.mark.parametrize("k,kind", [(1, "rand"), (2, "rand"), (3, "rand"), (7, "rand"), (55, "diag"),
