@@ -17,8 +17,8 @@ sample (setup, first filter step, two more SCF iterations; extrapolated to
 the run's iteration count).
 
 --impl reference times that CPU implementation of the path alone (the
-reference is pure Python and does not run on the GPU box; its port, the
-oracle, does), one SCF iteration per step.  Multi-GPU runs are independent
+reference is pure Python and is not shipped with this repository; its port,
+the oracle, is), one SCF iteration per step.  Multi-GPU runs are independent
 replicas (the SCF of one molecule does not shard in this implementation).
 """
 from __future__ import annotations

@@ -1,6 +1,6 @@
 """CPU oracle for the real-space Kohn-Sham SCF hot path (TEST INFRASTRUCTURE).
 
-This module is the checker, never the product.  Only ``tests/``,
+This module checks the product and is never part of it.  Only ``tests/``,
 ``__graft_entry__.smoke()`` and the CPU-baseline legs of ``bench.py`` may import
 it.  The product path (``parsec_python_b200``) runs on the GPU through
 ``libpsc.so`` and never calls into this file.

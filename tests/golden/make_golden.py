@@ -3,8 +3,9 @@
 Runs PARSEC.py's own CPU code (zeyizhang-berkeley/parsec_python, ``src/``)
 in this container -- it needs only numpy, scipy and pandas plus a stub for the
 unused ``matplotlib`` import -- on small seeded inputs, and writes the outputs
-to ``tests/golden/ref_*.npz`` and ``tests/golden/ref_meta.json``.  The GPU box
-has no copy of the reference, so the tests read only these files.
+to ``tests/golden/ref_*.npz`` and ``tests/golden/ref_meta.json``.  Machines
+that run the tests need no copy of the reference: the tests read only these
+files.
 
 Usage: python tests/golden/make_golden.py [reference src dir]
 """

@@ -1,6 +1,6 @@
 """Whole-SCF parity on the GPU against the reference's own SCF results.
 
-The bar (stated in the north star of this build): total energy and
+The bar: total energy and
 eigenvalues within 1e-5 Ha of the reference CPU path on the same input,
 integrated |delta rho| within 1e-4 electrons.  Energies are compared in Ry
 (1e-5 Ha = 2e-5 Ry).  The GPU and the reference draw different random
