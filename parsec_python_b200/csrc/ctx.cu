@@ -110,7 +110,7 @@ extern "C" int psc_ctx_destroy(psc_ctx* ctx) {
   psc_dfree(ctx->gram_partial); psc_dfree(ctx->lz_v); psc_dfree(ctx->cg_r); psc_dfree(ctx->cg_p);
   psc_dfree(ctx->cg_ap); psc_dfree(ctx->cg_part); psc_dfree(ctx->mix_dx); psc_dfree(ctx->mix_df);
   psc_dfree(ctx->mix_nv); psc_dfree(ctx->mix_tmp); psc_dfree(ctx->mix_coef); psc_dfree(ctx->mix_partial);
-  psc_dfree(ctx->cg_x); psc_dfree(ctx->jac_v); psc_dfree(ctx->cg_p2); psc_dfree(ctx->cg_ro); psc_dfree(ctx->cg_bar);
+  psc_dfree(ctx->cg_x); psc_dfree(ctx->eig_work); psc_dfree(ctx->cg_p2); psc_dfree(ctx->cg_ro); psc_dfree(ctx->cg_bar);
   psc_dfree(ctx->tc_part); psc_dfree(ctx->tc_pairs); psc_dfree(ctx->tri_work);
   for (auto& e : ctx->st_sched) psc_dfree(e.dev);
   for (int a = 0; a < 3; ++a) { psc_dfree(ctx->spec_S[a]); psc_dfree(ctx->spec_lam[a]); }

@@ -91,11 +91,11 @@ int psc_ensure_dense(psc_ctx* ctx, int k) {
   PSC_REQUIRE(ctx, k >= 1 && k <= PSC_MAX_K, "subspace width out of range");
   if (k <= ctx->dense_cap) return 0;
   psc_dfree(ctx->gram); psc_dfree(ctx->gram2); psc_dfree(ctx->evec); psc_dfree(ctx->tri); psc_dfree(ctx->gram_partial);
-  psc_dfree(ctx->jac_v);
+  psc_dfree(ctx->eig_work);
   const int cap = std::max(k, 64);
   const size_t kk = (size_t)cap * cap;
   // eigensolver scratch: reflectors, tridiagonal eigenvectors, T and tau (>= 2 k^2 + 3 k)
-  PSC_CUDA(ctx, psc_dmalloc(&ctx->jac_v, 2 * (size_t)(cap + 2) * (cap + 2) * sizeof(double)));
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->eig_work, 2 * (size_t)(cap + 2) * (cap + 2) * sizeof(double)));
   PSC_CUDA(ctx, psc_dmalloc(&ctx->gram, kk * sizeof(double)));
   PSC_CUDA(ctx, psc_dmalloc(&ctx->gram2, kk * sizeof(double)));
   PSC_CUDA(ctx, psc_dmalloc(&ctx->evec, kk * sizeof(double)));
@@ -476,7 +476,7 @@ int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, 
   PSC_REQUIRE(ctx, k >= 1 && k <= PSC_MAX_K, "syev: k out of range");
   if (psc_ensure_dense(ctx, k)) return 1;
   const size_t kk = (size_t)k * k;
-  double* hv = ctx->jac_v;   // reflectors (and the matrix itself when it is not on chip)
+  double* hv = ctx->eig_work;   // reflectors (and the matrix itself when it is not on chip)
   double* Z = hv + kk;       // eigenvectors of T
   double* ab = Z + kk;       // T: diagonal ab[2i], off-diagonal ab[2i+1]
   double* tau = ab + 2 * k;

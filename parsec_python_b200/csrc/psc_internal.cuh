@@ -93,7 +93,7 @@ struct psc_ctx {
   double* gram2 = nullptr;       // [cap*cap]
   double* evec = nullptr;        // [cap*cap]
   double* tri = nullptr;         // [cap*cap]
-  double* jac_v = nullptr;       // [2 (cap+2)^2] eigensolver scratch: reflectors, eigenvectors of T, T, tau
+  double* eig_work = nullptr;    // [2 (cap+2)^2] eigensolver scratch: reflectors, eigenvectors of T, T, tau
   double* gram_partial = nullptr;// [gram_blocks][cap*cap] Gram partial sums
   int gram_blocks = 0;
   int* dev_status = nullptr;     // device-side error flags [8]
