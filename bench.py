@@ -229,6 +229,63 @@ def stencil_roofline(reps: int = 40, dtype: str = "f64") -> dict:
     return {"seconds": t, "bytes": bytes_, "gbs": bytes_ / t / 1e9, "gflops": flops / t / 1e9, "n": n, "k": k}
 
 
+def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 20) -> list:
+    """H.X microbenchmark on the real grids of C10H8 (78^3) and Si87H76 (90^3):
+    one Chebyshev step Out = a H In + b In + g Prev on k random columns, FP64
+    and FP32, first with the stencil and local potential alone (one kernel),
+    then with the Kleinman-Bylander projectors of the molecule added (two
+    more kernels).  Algorithmic bytes per step: (3 k + 1) n s for the stencil
+    part, plus sum_a n_a (4 + 3 s) for the projector tables (s = 8 or 4);
+    CUDA-event time per step over `reps` steps, inputs larger than L2."""
+    import torch
+
+    from parsec_python_b200 import gpu
+    from parsec_python_b200._lib import F32, F64
+    from parsec_python_b200.inputs import pseudo_tables
+
+    out = []
+    for name in names:
+        prob, elem, _ = gpu_problem("fp64", 0, name=name)
+        for with_nl in (False, True):
+            ctx = gpu.GridContext(prob.domain, 8)
+            n = ctx.n
+            pot = torch.randn(n, dtype=torch.float64, device="cuda")
+            gpu.Hamiltonian(ctx, pot)
+            if with_nl:
+                gpu.projector_setup(ctx, prob.input_data.atoms, elem, pseudo_tables())
+            nl_points = ctx.info()["nl_points"] if with_nl else 0
+            st = gpu._stream()
+            for k in widths:
+                for dtype in ("f64", "f32"):
+                    tdt, code, size = (torch.float64, F64, 8) if dtype == "f64" else (torch.float32, F32, 4)
+                    X = torch.randn(k, n, dtype=tdt, device="cuda")
+                    Y = torch.randn(k, n, dtype=tdt, device="cuda")
+
+                    def step(a, b):
+                        ctx.call("psc_apply_h_axpby", code, gpu._p(a), n, gpu._p(b), n, gpu._p(b), n, k, 0.1,
+                                 -0.3, -0.5, st)
+
+                    for _ in range(3):
+                        step(X, Y)
+                        step(Y, X)
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    for i in range(reps):
+                        step(X, Y) if i % 2 == 0 else step(Y, X)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    t = e0.elapsed_time(e1) / 1000.0 / reps
+                    bytes_ = (3 * k + 1) * n * size + nl_points * (4 + 3 * size)
+                    out.append({"system": name, "n": n, "k": k, "dtype": dtype, "projectors": with_nl,
+                                "nl_points": nl_points, "us": t * 1e6, "bytes": bytes_, "gbs": bytes_ / t / 1e9})
+                    del X, Y
+            ctx.check_status()
+            del ctx
+            torch.cuda.empty_cache()
+    return out
+
+
 def syev_timing(cases: str = "55_rand,55_near,143_near,307_near", reps: int = 20) -> dict:
     """The FP64 symmetric eigensolver of the Rayleigh-Ritz step (psc_syev:
     Householder tridiagonalisation, bisection, inverse iteration,
@@ -601,6 +658,8 @@ def main():
                     help="only time the Hartree solve and its spectral preconditioner on the C10H8 grid")
     ap.add_argument("--stencil", choices=["f64", "f32"], default=None,
                     help="only time the fused stencil step (k = 55, C10H8 grid) for kernel profiling")
+    ap.add_argument("--hx", action="store_true",
+                    help="only run the H.X microbenchmark (C10H8 and Si87H76 grids, k = 27/55/143/307, FP64/FP32)")
     ap.add_argument("--syev", nargs="?", const="55_rand,55_near,143_near,307_near", default=None,
                     help="only time the k x k symmetric eigensolver (comma-separated <k>_<rand|near> cases)")
     args = ap.parse_args()
@@ -629,6 +688,10 @@ def main():
         return
     if args.syev:
         print(json.dumps(syev_timing(args.syev)))
+        return
+    if args.hx:
+        for r in hx_sweep(reps=max(1, args.steps) * 4):
+            print(json.dumps(r), flush=True)
         return
     rank, local, world = dist_init()
     try:
