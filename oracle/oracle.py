@@ -313,14 +313,102 @@ def nonlocal_csr(projs: list, n: int) -> sp.csr_matrix:
     return vnl.tocsr()
 
 
-def nonlocal_apply(projs: list, x: np.ndarray) -> np.ndarray:
-    """Factored V_nl @ x = sum_a sum_m u_m (u_m . x[idx]) / xint."""
-    y = np.zeros_like(x)
+def nonlocal_apply(projs: list, x: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+    """Factored V_nl @ x = sum_a sum_m u_m (u_m . x[idx]) / xint, added to
+    `out` when given (pseudoNL_original.py:187-206 without forming the
+    n x n matrix)."""
+    y = np.zeros_like(x) if out is None else out
     for pr in projs:
         idx, u = pr["idx"], pr["u"]
         proj = u @ x[idx]                      # (3, k)
         y[idx] += (u.T @ proj) / pr["xint"]
     return y
+
+
+_FD_LIB = None
+
+
+def _fd_lib():
+    """oracle/liboracle_fd.so (oracle/fd_apply.c), built on first use."""
+    global _FD_LIB
+    if _FD_LIB is None:
+        import ctypes
+
+        from oracle import build_oracle
+
+        lib = ctypes.CDLL(str(build_oracle.build()))
+        lib.oracle_fd_apply.restype = ctypes.c_int
+        lib.oracle_fd_apply.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
+                                        ctypes.c_void_p, ctypes.c_long, ctypes.c_long, ctypes.c_int]
+        _FD_LIB = lib
+    return _FD_LIB
+
+
+def fd_apply(domain: dict, order: int, x: np.ndarray, scale: float, pot: np.ndarray | None = None) -> np.ndarray:
+    """scale * (fd3d @ x) + pot * x, matrix-free (oracle/fd_apply.c), for a
+    vector (n,) or a block (n, k) in C or Fortran order; the result has the
+    layout of x.  The same stencil as fd3d (Laplacian/fd3d.py:34-106) with
+    the sums in a different order."""
+    import ctypes
+
+    nx, ny, nz = domain["nx"], domain["ny"], domain["nz"]
+    n = nx * ny * nz
+    c0, cs = fd_stencil(order)
+    w = np.ascontiguousarray([c0] + list(cs), dtype=np.float64)
+    x = np.asarray(x, dtype=np.float64)
+    if x.shape[0] != n:
+        raise ValueError(f"operand has {x.shape[0]} rows, the grid {n} points")
+    if x.ndim == 1 or x.flags.f_contiguous:
+        layout = 0
+    elif x.flags.c_contiguous:
+        layout = 1
+    else:
+        x = np.ascontiguousarray(x)
+        layout = 1
+    k = 1 if x.ndim == 1 else x.shape[1]
+    y = np.empty_like(x)
+    p = None if pot is None else np.ascontiguousarray(pot, dtype=np.float64)
+    vp = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    st = _fd_lib().oracle_fd_apply(nx, ny, nz, len(cs), vp(w), float(scale), vp(p), vp(x), n, vp(y), n, k, layout)
+    if st != 0:
+        raise ValueError("oracle_fd_apply: invalid argument")
+    return y
+
+
+class StencilLaplacian:
+    """A = (1/h^2) fd3d (rsdft_solver.py:186) as an operator: A @ x and
+    A.dot(x) give the CSR product of laplacian() up to the order of sums."""
+
+    def __init__(self, domain: dict, order: int):
+        self.domain, self.order = domain, order
+        n = domain["nx"] * domain["ny"] * domain["nz"]
+        self.shape = (n, n)
+
+    def dot(self, x):
+        return fd_apply(self.domain, self.order, x, 1.0 / self.domain["h"] ** 2)
+
+    __matmul__ = dot
+
+
+class StencilHamiltonian:
+    """B = 0.5 A + V_nl + diag(pot) (rsdft_solver.py:263,285) as an
+    operator: the stencil and the local potential in one C pass, then the
+    factored projectors.  The same numbers as the assembled CSR B up to the
+    order of sums; used for the largest configurations, whose CSR products
+    take minutes per block on the host."""
+
+    def __init__(self, domain: dict, order: int, projs: list, pot: np.ndarray):
+        self.domain, self.order, self.projs = domain, order, projs
+        self.pot = np.ascontiguousarray(pot, dtype=np.float64)
+        n = self.pot.size
+        self.shape = (n, n)
+
+    def dot(self, x):
+        y = fd_apply(self.domain, self.order, x, 0.5 / self.domain["h"] ** 2, self.pot)
+        return nonlocal_apply(self.projs, np.asarray(x, dtype=np.float64), out=y)
+
+    __matmul__ = dot
 
 
 def nuclear(atoms: list, elements: dict) -> float:
@@ -901,8 +989,12 @@ class OracleSCF:
 
     def __init__(self, domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
                  maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, z_charge: float = 0.0,
-                 elements=None, tables=None, diagmeth: int = 3, density_method: str = "sad", density=None):
+                 elements=None, tables=None, diagmeth: int = 3, density_method: str = "sad", density=None,
+                 operator: str = "csr"):
+        if operator not in ("csr", "stencil"):
+            raise ValueError(f"operator must be 'csr' or 'stencil', not {operator!r}")
         self.domain, self.atoms, self.nev, self.poldeg, self.tol = domain, atoms, nev, poldeg, tol
+        self.operator = operator
         self.diagmeth = diagmeth
         self.density_method, self.density = density_method, density
         self.maxits, self.fd_order, self.fermi_temp, self.z_charge = maxits, fd_order, fermi_temp, z_charge
@@ -917,7 +1009,7 @@ class OracleSCF:
 
         t0 = time.perf_counter()
         d, h = self.domain, self.domain["h"]
-        self.A = laplacian(d, self.fd_order)
+        self.A = laplacian(d, self.fd_order) if self.operator == "csr" else StencilLaplacian(d, self.fd_order)
         n = self.n = self.A.shape[0]
         self.Hpot = np.zeros(n)
         self.err = 10.0 + self.tol
@@ -932,13 +1024,14 @@ class OracleSCF:
                                                                       self.atoms, self.elements, self.tables)
         projs = projectors(ml_grid(d) if dm in ("ml", "sad_ml_grid") else d, self.atoms, self.elements,
                            self.tables)
-        vnl = nonlocal_csr(projs, n)
+        self.projs = projs
+        vnl = nonlocal_csr(projs, n) if self.operator == "csr" else None
         xcpot, self.exc = exc_nspn(h, self.rho0 / h ** 3)
         self.XCpot = xcpot
         self.nelec = nelectrons(self.atoms, self.elements) - self.z_charge
         self.pot = self.ppot + self.hpot0 + 0.5 * xcpot
         self.mixer = MSecant1()
-        self.half_a_plus_vnl = 0.5 * self.A + vnl
+        self.half_a_plus_vnl = 0.5 * self.A + vnl if self.operator == "csr" else None
         self.W = self.lam = None
         self.rho = np.zeros(n)
         self.t_setup = time.perf_counter() - t0
@@ -952,7 +1045,10 @@ class OracleSCF:
         t0 = time.perf_counter()
         n, h, nev = self.n, self.domain["h"], self.nev
         self.its += 1
-        B = (self.half_a_plus_vnl + sp.diags(self.pot, 0, shape=(n, n))).tocsr()
+        if self.operator == "csr":
+            B = (self.half_a_plus_vnl + sp.diags(self.pot, 0, shape=(n, n))).tocsr()
+        else:
+            B = StencilHamiltonian(self.domain, self.fd_order, self.projs, self.pot)
         dm = self.diagmeth
         if dm == 1 or (self.its == 1 and dm == 0):
             # rsdft_solver.py:63-68 (CPU vector) and :47-49 (nev + 500 steps)
@@ -992,14 +1088,14 @@ class OracleSCF:
 def run_scf(domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
             maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, seed: int | None = None,
             z_charge: float = 0.0, elements=None, tables=None, log=None, diagmeth: int = 3,
-            density_method: str = "sad", density=None) -> dict:
+            density_method: str = "sad", density=None, operator: str = "csr") -> dict:
     """Run OracleSCF to convergence; with a seed, numpy's global generator is
     seeded first so the random draws match a reference run with that seed."""
     if seed is not None:
         np.random.seed(seed)
     scf = OracleSCF(domain, atoms, nev=nev, poldeg=poldeg, tol=tol, maxits=maxits, fd_order=fd_order,
                     fermi_temp=fermi_temp, z_charge=z_charge, elements=elements, tables=tables, diagmeth=diagmeth,
-                    density_method=density_method, density=density)
+                    density_method=density_method, density=density, operator=operator)
     scf.setup()
     while not scf.done():
         rec = scf.step()

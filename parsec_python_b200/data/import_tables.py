@@ -11,6 +11,7 @@ need the reference tree at run time.
 
 Usage: python parsec_python_b200/data/import_tables.py <reference src dir>
 """
+import os
 import sys
 from pathlib import Path
 
@@ -33,4 +34,9 @@ def main(src_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    elif os.environ.get("PARSEC_REF_SRC"):
+        main(os.environ["PARSEC_REF_SRC"])
+    else:
+        sys.exit(f"usage: python {sys.argv[0]} <reference src directory> (or set PARSEC_REF_SRC)")

@@ -233,4 +233,9 @@ def main(src: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    elif os.environ.get("PARSEC_REF_SRC"):
+        main(os.environ["PARSEC_REF_SRC"])
+    else:
+        sys.exit(f"usage: python {sys.argv[0]} <reference src directory> (or set PARSEC_REF_SRC)")

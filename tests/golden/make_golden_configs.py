@@ -85,4 +85,7 @@ def main(name: str, src: str, tol: float | None = None) -> None:
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--tol")]
     tols = [float(a.split("=", 1)[1]) for a in sys.argv[1:] if a.startswith("--tol=")]
-    main(args[0], args[1] if len(args) > 1 else "/root/reference/src", tols[0] if tols else None)
+    src = args[1] if len(args) > 1 else os.environ.get("PARSEC_REF_SRC")
+    if not args or not src:
+        sys.exit(f"usage: python {sys.argv[0]} NAME <reference src directory> [--tol=T] (or set PARSEC_REF_SRC)")
+    main(args[0], src, tols[0] if tols else None)
