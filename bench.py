@@ -1,25 +1,39 @@
-"""Benchmark: SCF time-to-solution of the C10H8 configuration on the GPU.
+"""Benchmark: SCF time-to-1e-5 Ha of the Si87H76 configuration on one B200.
 
-One step = one complete SCF solve (SAD setup, projector setup, first filter,
-Chebyshev-filtered subspace iterations, Hartree CG, LDA XC, mixing) of the
-planar naphthalene molecule (sphere radius 7 A, spacing 0.18 A -> 78^3 =
-474,552 grid points, nev 40 -> 55 subspace columns, poldeg 12, tol 1e-6),
-started from the atom coordinates with the pseudopotential tables already in
-device memory.  The step's device work is timed with CUDA events on the
-launching stream; the SCF working set (two 474,552 x 55 FP64 blocks = 418 MB
-plus the mixer history) is larger than the 126 MB L2, so no flush is needed.
+Workload (the largest configuration, on which the metric is quoted): the
+H-passivated silicon cluster Si87H76 (diamond lattice a = 5.43 A, 7 distance
+shells around an atom-centred Si, Si-H 1.48 A), sphere radius 11 A, spacing
+0.25 A -> 90^3 = 729,000 grid points, nev 292 -> 307 subspace columns,
+poldeg 16 (the first filter clamps it to 10, Eigensolvers/first_filt.py:22-23),
+fd_order 8, LDA, msecant1 mixing, tol 1e-6.  One step = one complete SCF
+solve from the atom coordinates (SAD / learned start, projector setup, first
+filter, Chebyshev-filtered subspace iterations, Hartree solve, XC, mixing)
+that stops at the reference's test err <= tol once the total energy is within
+1e-5 Ha of E*, the oracle's converged energy at tol 1e-8
+(tests/golden/ref_si87h76_tol8.json).
+
+`value` is the chosen form: mixed precision (FP32 filter and H.X, tcgen05
+Gram and block products, FP64 Cholesky / eigensolver / energies, FP64 blocks
+once the SCF error is below 1e-4), the preconditioned Hartree solve
+(cg_prec = 1) and the learned initial density.  The legs beside it run the
+same input and bar as plain FP64 (the reference's method: cg_prec = 0, SAD),
+FP64 with cg_prec = 1, and mixed precision from SAD; `speedup_vs_fp64_plain`
+is the metric's ratio.  Device work is timed with CUDA events on the
+launching stream; the working set (several 0.9-1.8 GB blocks) exceeds the
+126 MB L2, so no flush is needed.
 
 Extra keys: `e2e` times the public entry (input file -> .out log + density
 .npy files on the host) with host<->device copies inside; `roofline` times
-the fused H.X stencil (one Chebyshev step, FP64, k = 55) against the
-measured HBM copy bandwidth; `cpu_baseline` times the CPU oracle on a bounded
-sample (setup, first filter step, two more SCF iterations; extrapolated to
-the run's iteration count).
+the dominant kernel of the chosen form (the FP32 Chebyshev step of the
+filter, k = 307) against the measured HBM copy bandwidth; `cpu_baseline`
+times the CPU oracle on a bounded sample (setup, one block H.X, one
+Rayleigh-Ritz, one Hartree CG, XC) extrapolated to the oracle's own
+iteration count.
 
 --impl reference times that CPU implementation of the path alone (the
 reference is pure Python and is not shipped with this repository; its port,
-the oracle, is), one SCF iteration per step.  Multi-GPU runs are independent
-replicas (the SCF of one molecule does not shard in this implementation).
+the oracle, is), one block H.X per step.  Multi-GPU runs are independent
+replicas (one SCF per GPU).
 """
 from __future__ import annotations
 
@@ -39,16 +53,28 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-CFG_NAME = "c10h8"
+CFG_NAME = "si87h76"
 METRIC = "SCF time-to-1e-5 Ha: mixed-prec+learned init vs plain FP64 GPU; H\u00b7X GB/s"
 HA_TOL = 1e-5          # energy bar, Hartree
 
 
-def workload_config(precision: str) -> dict:
-    return {"workload": "C10H8 naphthalene SCF: sphere radius 7 A, h 0.18 A, 78^3 = 474,552 points, nev 40 "
-                        "(k = 55), poldeg 12, fd_order 8, tol 1e-6, LDA, SAD init, msecant1 mixing",
-            "precision": precision, "init": "sad", "global_batch": 1, "parallelism": "replicas",
-            "l2": "working set (2 x 209 MB subspace blocks + mixer history) > 126 MB L2; no flush"}
+# The SCF variants timed on the workload: precision, Hartree preconditioner,
+# initial density
+FORMS = {
+    "chosen": {"precision": "mixed", "cg_prec": 1, "init": "learned"},
+    "fp64_plain": {"precision": "fp64", "cg_prec": 0, "init": "sad"},
+    "fp64_prec": {"precision": "fp64", "cg_prec": 1, "init": "sad"},
+    "mixed_sad": {"precision": "mixed", "cg_prec": 1, "init": "sad"},
+}
+
+
+def workload_config(form: str = "chosen") -> dict:
+    f = FORMS[form]
+    return {"workload": "Si87H76 SCF: sphere radius 11 A, h 0.25 A, 90^3 = 729,000 points, nev 292 (k = 307), "
+                        "poldeg 16, fd_order 8, tol 1e-6, LDA, msecant1 mixing",
+            "precision": f["precision"], "cg_prec": f["cg_prec"], "init": f["init"], "global_batch": 1,
+            "parallelism": "replicas",
+            "l2": "working set (0.9-1.8 GB subspace blocks) > 126 MB L2; no flush"}
 
 
 # ---------------------------------------------------------------------------
@@ -146,15 +172,15 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def gpu_problem(precision: str, seed: int, name: str = CFG_NAME, cg_prec: int = 0):
+def gpu_problem(precision: str, seed: int, name: str = CFG_NAME, cg_prec: int = 0, init: str = "sad"):
     from parsec_python_b200 import workloads
     from parsec_python_b200.inputs import ElementTable
     from parsec_python_b200.models import SolverSettings
     from parsec_python_b200.system import system_from_atoms
 
     cfg = workloads.config_system(name)
-    s = SolverSettings(tol=cfg["tol"], poldeg=cfg["poldeg"], maxits=60, precision=precision, seed=seed,
-                       cg_prec=cg_prec)
+    s = SolverSettings(tol=cfg["tol"], poldeg=cfg["poldeg"], maxits=80, precision=precision, seed=seed,
+                       cg_prec=cg_prec, init=init)
     s.normalize()
     elem = ElementTable()
     prob = system_from_atoms(cfg["atoms"], h=cfg["h"], radius=cfg["radius"], nev=cfg["nev"], settings=s, elem=elem)
@@ -162,14 +188,17 @@ def gpu_problem(precision: str, seed: int, name: str = CFG_NAME, cg_prec: int = 
 
 
 def reference_energy(name: str = CFG_NAME):
-    """Converged total energy (Ry) of the reference CPU path run to tol 1e-8
-    (its tol-1e-6 energies scatter by 2e-5 Ha between random starts, more
-    than the bar), and the reference's iteration count at the config's tol."""
+    """Converged total energy (Ry) of the reference CPU path (the oracle for
+    Si87H76) run to tol 1e-8 -- at tol 1e-6 the energies of different random
+    starts scatter by about the bar -- and that run's iteration count at the
+    configuration's tol 1e-6."""
     e_star, its = None, None
     f8 = ROOT / "tests" / "golden" / f"ref_{name}_tol8.json"
     f6 = ROOT / "tests" / "golden" / f"ref_{name}.json"
     if f8.exists():
-        e_star = json.loads(f8.read_text())["total_ry"]
+        m = json.loads(f8.read_text())
+        e_star = m["total_ry"]
+        its = m.get("iterations_to_1e-6")
     if f6.exists():
         m = json.loads(f6.read_text())
         its = m["iterations"]
@@ -178,31 +207,61 @@ def reference_energy(name: str = CFG_NAME):
     return e_star, its
 
 
-def solve_once(precision: str, seed: int, energy_target=None, cg_prec: int = 0):
+def solve_once(form: str, seed: int, energy_target=None, name: str = CFG_NAME):
     """One SCF; returns (result, backend) so that the caller releases the
     device context (cudaFree) outside its timed region."""
     from parsec_python_b200.backend import select_solver_backend
     from parsec_python_b200.solver import run_rsdft_calculation
 
-    prob, elem, s = gpu_problem(precision, seed, cg_prec=cg_prec)
+    f = FORMS[form]
+    prob, elem, s = gpu_problem(f["precision"], seed, name=name, cg_prec=f["cg_prec"], init=f["init"])
     backend = select_solver_backend(s)
     res = run_rsdft_calculation(prob, elem, len(elem), backend, verbose=False, energy_target=energy_target)
     return res, backend
 
 
-def stencil_roofline(reps: int = 40, dtype: str = "f64") -> dict:
+def timed_form(form: str, target, seeds, name: str = CFG_NAME) -> dict:
+    """CUDA-event times of whole SCF solves of one form (one warm-up solve
+    first), with iterations, FP32 iterations and |E - E*|."""
+    import torch
+
+    res, be = solve_once(form, 90_000 + seeds[0], target, name)
+    del res, be
+    times, its, f32, errs = [], [], [], []
+    for sd in seeds:
+        gc.collect()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res, be = solve_once(form, sd, target, name)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1000.0)
+        its.append(res.iterations)
+        f32.append(sum(1 for h in res.history if h.get("block_dtype") == "f32"))
+        if target is not None:
+            errs.append(abs(res.history[-1]["total_ry"] - target[0]) / 2.0)
+        del res, be
+    return {"value": float(np.mean(times)), "unit": "s", "step_times_s": times, "iterations": its,
+            "fp32_iterations": f32, "energy_error_ha_vs_reference": max(errs) if errs else None,
+            **FORMS[form]}
+
+
+def stencil_roofline(reps: int = 40, dtype: str = "f32", name: str = CFG_NAME, k: int | None = None) -> dict:
     """Time the fused stencil (one Chebyshev step Out = a H In + b In + g Prev,
-    k = 55, no projectors so that only the stencil kernel launches) on the
-    C10H8 grid; algorithmic bytes = read In + read Prev + write Out + read pot
-    = (3 k + 1) n s, s = 8 (FP64) or 4 (FP32, the mixed-precision filter)."""
+    no projectors so that only the stencil kernel launches) on a
+    configuration's grid, k = nev + 15 columns by default; algorithmic bytes
+    = read In + read Prev + write Out + read pot = (3 k + 1) n s, s = 4 (FP32,
+    the chosen form's filter) or 8 (FP64)."""
     import torch
 
     from parsec_python_b200 import gpu
     from parsec_python_b200._lib import F32, F64
 
-    prob, _, _ = gpu_problem("fp64", 0)
+    prob, _, _ = gpu_problem("fp64", 0, name=name)
     ctx = gpu.GridContext(prob.domain, 8)
-    n, k = ctx.n, prob.nev + 15
+    n = ctx.n
+    k = k or prob.nev + 15
     tdt, code, size = (torch.float64, F64, 8) if dtype == "f64" else (torch.float32, F32, 4)
     pot = torch.randn(n, dtype=torch.float64, device="cuda")
     gpu.Hamiltonian(ctx, pot)
@@ -226,17 +285,23 @@ def stencil_roofline(reps: int = 40, dtype: str = "f64") -> dict:
     t = e0.elapsed_time(e1) / 1000.0 / reps
     bytes_ = (3 * k + 1) * n * size
     flops = n * k * (2 * (3 * 8 + 1) + 2 + 4)
-    return {"seconds": t, "bytes": bytes_, "gbs": bytes_ / t / 1e9, "gflops": flops / t / 1e9, "n": n, "k": k}
+    ctx.check_status()
+    return {"seconds": t, "bytes": bytes_, "gbs": bytes_ / t / 1e9, "gflops": flops / t / 1e9, "n": n, "k": k,
+            "dtype": dtype, "grid": name}
 
 
-def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 20) -> list:
+def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 20,
+             masks=("cube", "sphere"), impls=(0,)) -> list:
     """H.X microbenchmark on the real grids of C10H8 (78^3) and Si87H76 (90^3):
     one Chebyshev step Out = a H In + b In + g Prev on k random columns, FP64
     and FP32, first with the stencil and local potential alone (one kernel),
     then with the Kleinman-Bylander projectors of the molecule added (two
-    more kernels).  Algorithmic bytes per step: (3 k + 1) n s for the stencil
-    part, plus sum_a n_a (4 + 3 s) for the projector tables (s = 8 or 4);
-    CUDA-event time per step over `reps` steps, inputs larger than L2."""
+    more kernels); on the cube and with the sphere mask (only the points
+    inside the inscribed sphere are produced and counted).  Algorithmic bytes
+    per step: (3 k + 1) n s for the stencil part, n the points produced, plus
+    sum_a n_a (4 + 3 s) for the projector tables (s = 8 or 4); CUDA-event
+    time per step over `reps` steps, inputs larger than L2.  impls: stencil
+    implementations to time (0 default, 2 four-point FP32 runs)."""
     import torch
 
     from parsec_python_b200 import gpu
@@ -246,43 +311,52 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
     out = []
     for name in names:
         prob, elem, _ = gpu_problem("fp64", 0, name=name)
-        for with_nl in (False, True):
-            ctx = gpu.GridContext(prob.domain, 8)
-            n = ctx.n
-            pot = torch.randn(n, dtype=torch.float64, device="cuda")
-            gpu.Hamiltonian(ctx, pot)
-            if with_nl:
-                gpu.projector_setup(ctx, prob.input_data.atoms, elem, pseudo_tables())
-            nl_points = ctx.info()["nl_points"] if with_nl else 0
-            st = gpu._stream()
-            for k in widths:
-                for dtype in ("f64", "f32"):
-                    tdt, code, size = (torch.float64, F64, 8) if dtype == "f64" else (torch.float32, F32, 4)
-                    X = torch.randn(k, n, dtype=tdt, device="cuda")
-                    Y = torch.randn(k, n, dtype=tdt, device="cuda")
+        for mask in masks:
+            for with_nl in (False, True):
+                ctx = gpu.GridContext(prob.domain, 8)
+                if mask == "sphere":
+                    ctx.set_sphere_mask(ctx.radius)
+                n = ctx.n
+                n_out = ctx.inside_count()
+                pot = torch.randn(n, dtype=torch.float64, device="cuda")
+                gpu.Hamiltonian(ctx, pot)
+                if with_nl:
+                    gpu.projector_setup(ctx, prob.input_data.atoms, elem, pseudo_tables())
+                nl_points = ctx.info()["nl_points"] if with_nl else 0
+                st = gpu._stream()
+                for impl in impls:
+                    ctx.call("psc_set_stencil_impl", impl)
+                    for k in widths:
+                        for dtype in ("f64", "f32"):
+                            if impl == 2 and dtype == "f64":
+                                continue
+                            tdt, code, size = (torch.float64, F64, 8) if dtype == "f64" else (torch.float32, F32, 4)
+                            X = ctx.mask_block(torch.randn(k, n, dtype=tdt, device="cuda"))
+                            Y = ctx.mask_block(torch.randn(k, n, dtype=tdt, device="cuda"))
 
-                    def step(a, b):
-                        ctx.call("psc_apply_h_axpby", code, gpu._p(a), n, gpu._p(b), n, gpu._p(b), n, k, 0.1,
-                                 -0.3, -0.5, st)
+                            def step(a, b):
+                                ctx.call("psc_apply_h_axpby", code, gpu._p(a), n, gpu._p(b), n, gpu._p(b), n, k,
+                                         0.1, -0.3, -0.5, st)
 
-                    for _ in range(3):
-                        step(X, Y)
-                        step(Y, X)
-                    torch.cuda.synchronize()
-                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    e0.record()
-                    for i in range(reps):
-                        step(X, Y) if i % 2 == 0 else step(Y, X)
-                    e1.record()
-                    torch.cuda.synchronize()
-                    t = e0.elapsed_time(e1) / 1000.0 / reps
-                    bytes_ = (3 * k + 1) * n * size + nl_points * (4 + 3 * size)
-                    out.append({"system": name, "n": n, "k": k, "dtype": dtype, "projectors": with_nl,
-                                "nl_points": nl_points, "us": t * 1e6, "bytes": bytes_, "gbs": bytes_ / t / 1e9})
-                    del X, Y
-            ctx.check_status()
-            del ctx
-            torch.cuda.empty_cache()
+                            for _ in range(3):
+                                step(X, Y)
+                                step(Y, X)
+                            torch.cuda.synchronize()
+                            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                            e0.record()
+                            for i in range(reps):
+                                step(X, Y) if i % 2 == 0 else step(Y, X)
+                            e1.record()
+                            torch.cuda.synchronize()
+                            t = e0.elapsed_time(e1) / 1000.0 / reps
+                            bytes_ = (3 * k + 1) * n_out * size + nl_points * (4 + 3 * size)
+                            out.append({"system": name, "mask": mask, "impl": impl, "n": n, "n_produced": n_out,
+                                        "k": k, "dtype": dtype, "projectors": with_nl, "nl_points": nl_points,
+                                        "us": t * 1e6, "bytes": bytes_, "gbs": bytes_ / t / 1e9})
+                            del X, Y
+                ctx.check_status()
+                del ctx
+                torch.cuda.empty_cache()
     return out
 
 
@@ -340,7 +414,7 @@ def hartree_timing(reps: int = 20) -> dict:
 
     from parsec_python_b200 import gpu
 
-    prob, _, _ = gpu_problem("fp64", 0)
+    prob, _, _ = gpu_problem("fp64", 0, name="c10h8")
     ctx = gpu.GridContext(prob.domain, 8)
     n = ctx.n
     nx, ny, nz = ctx.nx, ctx.ny, ctx.nz
@@ -376,52 +450,6 @@ def hartree_timing(reps: int = 20) -> dict:
     return out
 
 
-def mixed_leg(target, steps: int = 3, cg_prec: int = 0) -> dict:
-    """The same C10H8 solve in mixed precision: FP32 filter and subspace
-    blocks, tensor-core (3xTF32) Gram pairs, FP64 small dense work, energies
-    and the last iterations (FP64 blocks once the SCF error is below 1e-4);
-    stopped on the same energy bar.  cg_prec = 1 adds the spectrally
-    preconditioned Hartree solve (the chosen form)."""
-    import torch
-
-    res, be = solve_once("mixed", seed=7, energy_target=target, cg_prec=cg_prec)   # warm-up
-    del res, be
-    gc.collect()
-    times, its, errs, f32_its = [], [], [], []
-    for s in range(steps):
-        gc.collect()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        res, be = solve_once("mixed", seed=2000 + s, energy_target=target, cg_prec=cg_prec)
-        e1.record()
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1) / 1000.0)
-        its.append(res.iterations)
-        f32_its.append(sum(1 for h in res.history if h.get("block_dtype") == "f32"))
-        if target is not None:
-            errs.append(abs(res.history[-1]["total_ry"] - target[0]) / 2.0)
-        del res, be
-    return {"value": float(np.mean(times)), "unit": "s", "step_times_s": times, "iterations": its,
-            "fp32_iterations": f32_its, "energy_error_ha_vs_reference": max(errs) if errs else None}
-
-
-def learned_leg(seeds=(512, 513, 514, 515)) -> dict | None:
-    """Learned initial density on held-out water clusters (the network is
-    trained on geometries 0..511): SCF iterations and time to 1e-5 Ha of the
-    geometry's tol-1e-8 energy, from SAD and from the network's density;
-    None when no trained weights are present."""
-    from parsec_python_b200 import learned
-
-    if learned.load_weights() is None:
-        return None
-    learned.run_scf(seeds[0])   # warm-up of the water grid
-    summ = learned.evaluate(seeds, learned.DEFAULT_WEIGHTS, log=lambda *a: None)
-    summ.pop("rows", None)
-    summ["workload"] = "(H2O)n, n in 2..8, held-out seeds %d-%d, h 0.2 A, sphere radius 9 A" % (seeds[0], seeds[-1])
-    return summ
-
-
 def measured_peak() -> tuple[float, str]:
     f = ROOT / "MEASURED_PEAKS.json"
     if f.exists():
@@ -432,13 +460,14 @@ def measured_peak() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def stencil_traffic():
-    """ncu DRAM bytes (read + write) of one stencil launch of this workload."""
+def stencil_traffic(key: str):
+    """ncu DRAM bytes (read + write) of one stencil launch of a workload, from
+    profiles/stencil_traffic.txt (key = value lines)."""
     f = ROOT / "profiles" / "stencil_traffic.txt"
     try:
         for line in f.read_text().splitlines():
-            if line.startswith("dram_bytes_per_launch_c10h8"):
-                return int(line.split("=")[1])
+            if line.startswith(key + " ") or line.startswith(key + "="):
+                return int(float(line.split("=")[1]))
     except (OSError, ValueError):
         pass
     return None
@@ -451,95 +480,147 @@ $system
 $settings
 unit = Angstrom
 density_method = sad
-grid_spacing = 0.180000
-sphere_radius = 7.000000
-tol = 1e-06
+grid_spacing = {h:.6f}
+sphere_radius = {radius:.6f}
+tol = {tol:g}
 Fermi_temp = 500
-maxits = 60
+maxits = 80
 fd_order = 8
-poldeg = 12
+poldeg = {poldeg}
 diagmeth = 3
-nev = 40
+nev = {nev}
 recenter_atoms = 0
 precision = {precision}
+cg_prec = {cg_prec}
+init = {init}
 $settings
 """
 
 
-def e2e_once(precision: str, workdir: Path) -> tuple[float, int, int]:
-    """Public entry: write an input file, run it, read the outputs from disk."""
+def e2e_once(form: str, workdir: Path, name: str = CFG_NAME) -> tuple[float, int, int, int]:
+    """Public entry: write an input file, run it (python -m parsec_python_b200
+    semantics, in process), read the converged density back from disk."""
     import torch
 
     from parsec_python_b200 import __main__ as cli
     from parsec_python_b200 import workloads
+    from parsec_python_b200.inputs import pseudo_tables
 
-    atoms = workloads.CONFIGS[CFG_NAME]["atoms"]()
+    cfg = workloads.CONFIGS[name]
+    f = FORMS[form]
+    atoms = cfg["atoms"]()
     lines = "\n".join(f"{a['typ']} {x:.8f} {y:.8f} {z:.8f}" for a in atoms for x, y, z in a["coord"])
-    inp = workdir / "c10h8.in"
-    inp.write_text(E2E_INPUT.format(atoms=lines, precision=precision))
+    inp = workdir / f"{name}.in"
+    inp.write_text(E2E_INPUT.format(atoms=lines, h=cfg["h"], radius=cfg["radius"], tol=cfg["tol"],
+                                    poldeg=cfg["poldeg"], nev=cfg["nev"], **f))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     res = cli.main([str(inp)])
-    rho = np.load(workdir / "c10h8_conv_rho_grid.npy")
+    rho = np.load(workdir / f"{name}_conv_rho_grid.npy")
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     n = rho.size
-    k = 55
-    # host->device: species tables (5 splines x 4 arrays per species) + atoms + potential-free setup
-    from parsec_python_b200.inputs import pseudo_tables
-
+    k = cfg["nev"] + 15
+    # host->device: species tables (5 splines x 4 arrays per species) + atom coordinates and species ids
     tabs = pseudo_tables()
-    h2d = sum(5 * 4 * tabs[s].shape[0] * 8 for s in ("C", "H")) + 18 * (3 * 8 + 4) * 2
+    species = {a["typ"] for a in atoms}
+    n_atoms = sum(len(a["coord"]) for a in atoms)
+    h2d = sum(5 * 4 * tabs[sp].shape[0] * 8 for sp in species) + n_atoms * (3 * 8 + 4) * 2
     # device->host: init/conv densities (n doubles each), per-iteration log block, CG/mixer scalars
     d2h = 2 * n * 8 + res.iterations * ((2 * k + 8) * 8 + 16 * 8)
-    return dt, h2d, d2h
+    return dt, h2d, d2h, res.iterations
 
 
-def cpu_sample(n_extra: int = 2, steps_total: int | None = None) -> dict:
-    """Oracle SCF on the host cores: setup, first iteration, n_extra more."""
+def cpu_components(name: str = CFG_NAME, reps_hx: int = 1) -> dict:
+    """The oracle on the host cores, timed by component on the workload
+    (matrix-free operator, NumPy/SciPy with all BLAS threads): setup
+    (local potential, SAD, projector tables), one block H.X of k columns, one
+    Rayleigh-Ritz (Householder QR, H W, the Gram, eigh, W Q), one Hartree CG
+    (200 iterations at most) and one XC evaluation."""
     from oracle import oracle as O
     from parsec_python_b200 import workloads
 
-    cfg = workloads.config_system(CFG_NAME)
+    cfg = workloads.config_system(name)
     atoms = cfg["atoms"]
     dom = O.build_system(atoms, h=cfg["h"], radius=cfg["radius"])
     np.random.seed(0)
-    scf = O.OracleSCF(dom, atoms, nev=cfg["nev"], poldeg=cfg["poldeg"], tol=cfg["tol"], maxits=60)
+    scf = O.OracleSCF(dom, atoms, nev=cfg["nev"], poldeg=cfg["poldeg"], tol=cfg["tol"], maxits=80,
+                      operator="stencil")
     scf.setup()
-    t_first = scf.step()["wall"]
-    walls = [scf.step()["wall"] for _ in range(n_extra)]
-    return {"t_setup": scf.t_setup, "t_first": t_first, "t_iter": float(np.mean(walls)), "walls": walls,
-            "scf": scf}
+    n, k = scf.n, cfg["nev"] + 15
+    B = O.StencilHamiltonian(dom, 8, scf.projs, scf.pot)
+    X = np.random.rand(n, k)
+    t_hx = []
+    for _ in range(reps_hx):
+        t0 = time.perf_counter()
+        Y = B @ X
+        t_hx.append(time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    W, _ = O.scipy.linalg.qr(Y, mode="economic", pivoting=False)
+    V = B @ W
+    G = O._gram_upper(V, W)
+    _, Q = O.scipy.linalg.eigh(G)
+    W = W @ Q
+    t_rr = time.perf_counter() - t0
+    h = dom["h"]
+    rho = (W[:, :cfg["nev"]] ** 2) @ np.full(cfg["nev"], 2.0)
+    t0 = time.perf_counter()
+    O.pcg(scf.A, (4 * np.pi / h ** 3) * (rho - scf.rho0), np.zeros(n), 200, 1e-5)
+    t_cg = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.exc_nspn(h, rho / h ** 3)
+    t_xc = time.perf_counter() - t0
+    return {"t_setup": scf.t_setup, "t_hx": float(np.mean(t_hx)), "t_rr": t_rr, "t_cg": t_cg, "t_xc": t_xc,
+            "deg": cfg["poldeg"], "n": n, "k": k}
+
+
+def cpu_estimate(c: dict, its: int, first_rounds: int = 4) -> float:
+    """SCF time of the oracle from its components: the first step is
+    `first_rounds` rounds of the slim filter (polm 10: 10 H.X) plus a
+    Rayleigh-Ritz (1 H.X), later steps the scaled filter (deg H.X) plus a
+    Rayleigh-Ritz; every step adds a Hartree CG and an XC evaluation."""
+    step = c["t_cg"] + c["t_xc"]
+    first = first_rounds * (10 * c["t_hx"] + c["t_rr"]) + step
+    later = c["deg"] * c["t_hx"] + c["t_rr"] + step
+    return c["t_setup"] + first + (its - 1) * later
 
 
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
-    from oracle import oracle as Orc
+    _, ref_its = reference_energy()
+    its = ref_its or 30
+    c = cpu_components(reps_hx=1)
+    from oracle import oracle as O
     from parsec_python_b200 import workloads
 
-    _, ref_its = reference_energy()
     cfg = workloads.config_system(CFG_NAME)
-    atoms = cfg["atoms"]
-    dom = Orc.build_system(atoms, h=cfg["h"], radius=cfg["radius"])
-    np.random.seed(0)
-    scf = Orc.OracleSCF(dom, atoms, nev=cfg["nev"], poldeg=cfg["poldeg"], tol=cfg["tol"], maxits=60)
+    dom = O.build_system(cfg["atoms"], h=cfg["h"], radius=cfg["radius"])
+    np.random.seed(1)
+    scf = O.OracleSCF(dom, cfg["atoms"], nev=cfg["nev"], poldeg=cfg["poldeg"], tol=cfg["tol"], operator="stencil")
     scf.setup()
-    t_first = scf.step()["wall"]
+    B = O.StencilHamiltonian(dom, 8, scf.projs, scf.pot)
+    X = np.random.rand(scf.n, c["k"])
     for _ in range(args.warmup):
-        scf.step()
-    walls = [scf.step()["wall"] for _ in range(args.steps)]
-    its = ref_its or 23
-    value = scf.t_setup + t_first + (its - 1) * float(np.mean(walls))
+        B @ X
+    walls = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        B @ X
+        walls.append(time.perf_counter() - t0)
+    c["t_hx"] = float(np.mean(walls))
+    value = cpu_estimate(c, its)
     cores = os.cpu_count()
-    sample = (f"oracle (NumPy/SciPy port of the reference CPU path) on {cores} host threads: setup "
-              f"{scf.t_setup:.1f}s + first SCF iteration {t_first:.1f}s + {args.steps} timed SCF iterations "
-              f"(mean {np.mean(walls):.2f}s) extrapolated to {its} iterations")
+    sample = (f"oracle (NumPy/SciPy port of the reference CPU path, matrix-free H.X in C/OpenMP) on {cores} host "
+              f"threads: setup {c['t_setup']:.1f}s, block H.X {c['t_hx']:.2f}s (mean of {args.steps} timed steps, "
+              f"k = {c['k']}), Rayleigh-Ritz {c['t_rr']:.1f}s, Hartree CG {c['t_cg']:.1f}s, XC {c['t_xc']:.2f}s; "
+              f"extrapolated to {its} SCF iterations (the oracle's own count at tol 1e-6) with a 4-round first "
+              f"filter and {c['deg']} H.X per later filter")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(walls)) * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic C10H8 geometry; the reference's pseudopotential tables",
-            "config": workload_config("fp64"),
+            "data": "synthetic Si87H76 geometry; the reference's pseudopotential tables",
+            "config": workload_config("fp64_plain"),
             "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -548,20 +629,20 @@ def run_reference_arm(args, rank, world):
 def run_gpu_arm(args, rank, local, world):
     import torch
 
-    from parsec_python_b200 import _lib
+    from parsec_python_b200 import _lib, learned, workloads
 
     torch.cuda.set_device(local)
     lib = _lib.load()
-    prec = args.precision
+    form = args.form
     e_ref, ref_its = reference_energy()
     target = None if e_ref is None else (e_ref, 2.0 * HA_TOL)   # 1e-5 Ha = 2e-5 Ry
     for w in range(args.warmup):
-        res, be = solve_once(prec, seed=100 + w, energy_target=target)
+        res, be = solve_once(form, seed=100 + w, energy_target=target)
         del res, be
     gc.collect()
     torch.cuda.synchronize()
     barrier(world)
-    times, energies, iters, setups = [], [], [], []
+    times, energies, iters, setups, f32its = [], [], [], [], []
     launches0 = lib.psc_launch_count()
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
@@ -571,74 +652,80 @@ def run_gpu_arm(args, rank, local, world):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            res, be = solve_once(prec, seed=1000 * rank + s, energy_target=target)
+            res, be = solve_once(form, seed=1000 * rank + s, energy_target=target)
             e1.record()
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1000.0)
             energies.append(res.history[-1]["total_ry"])
             iters.append(res.iterations)
+            f32its.append(sum(1 for h in res.history if h.get("block_dtype") == "f32"))
             setups.append(res.timings.get("setup_total", 0.0))
             del res, be
         torch.cuda.synchronize()
         barrier(world)
     launches = (lib.psc_launch_count() - launches0) // max(1, args.steps)
     clocks = clk.summary()
+    t_step = allmax(float(np.mean(times)), world)
     if args.scf_only:
         if rank == 0:
-            print(json.dumps({"scf_only": True, "step_times_s": times, "iterations": iters}), flush=True)
+            print(json.dumps({"scf_only": True, "form": form, "step_times_s": times, "iterations": iters}), flush=True)
         return
-    t_step = allmax(float(np.mean(times)), world)
-    mixed = mixed_leg(target) if not args.scf_only else None
-    chosen = mixed_leg(target, cg_prec=1) if not args.scf_only else None
-    learned_res = learned_leg() if rank == 0 else None
-    roof = stencil_roofline()
-    roof32 = stencil_roofline(dtype="f32")
+    legs = {}
+    if rank == 0:
+        for leg in ("fp64_plain", "fp64_prec", "mixed_sad"):
+            if leg != form:
+                legs[leg] = timed_form(leg, target, seeds=(2000, 2001))
+    roof = stencil_roofline(dtype="f32") if rank == 0 else None
+    roof64 = stencil_roofline(dtype="f64") if rank == 0 else None
     peak, peak_kind = measured_peak()
     err_ha = None if e_ref is None else max(abs(e - e_ref) for e in energies) / 2.0
     within = None if err_ha is None else bool(err_ha <= HA_TOL)
-    e2e_t = h2d = d2h = None
+    e2e_t = h2d = d2h = e2e_its = None
     if rank == 0:
         with tempfile.TemporaryDirectory() as td:
-            e2e_once(prec, Path(td))  # warm the public path once
-            e2e_t, h2d, d2h = e2e_once(prec, Path(td))
+            e2e_once(form, Path(td))  # warm the public path once
+            e2e_t, h2d, d2h, e2e_its = e2e_once(form, Path(td))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cs = cpu_sample(2)
-        its = int(np.median(iters))
-        v = cs["t_setup"] + cs["t_first"] + (its - 1) * cs["t_iter"]
+        c = cpu_components()
+        its = ref_its or int(np.median(iters))
+        v = cpu_estimate(c, its)
         cpu = {"value": v, "unit": "s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"oracle on {os.cpu_count()} host threads: setup {cs['t_setup']:.1f}s + first SCF "
-                         f"iteration {cs['t_first']:.1f}s + 2 iterations (mean {cs['t_iter']:.2f}s), extrapolated "
-                         f"to the GPU run's {its} iterations"}
+               "sample": f"oracle (matrix-free H.X in C/OpenMP, NumPy/SciPy BLAS) on {os.cpu_count()} host threads: "
+                         f"setup {c['t_setup']:.1f}s, one block H.X {c['t_hx']:.2f}s (k = {c['k']}), one "
+                         f"Rayleigh-Ritz {c['t_rr']:.1f}s, one Hartree CG {c['t_cg']:.1f}s, XC {c['t_xc']:.2f}s, "
+                         f"extrapolated to {its} SCF iterations (the oracle's own count at tol 1e-6)"}
     if rank != 0:
         return
+    plain = legs.get("fp64_plain")
+    weights = learned.weights_for(workloads.config_system(CFG_NAME)["atoms"])
     line = {"metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32+f64",
-            "data": "synthetic C10H8 geometry; the reference's pseudopotential tables",
-            "config": workload_config(prec),
-            "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "vs_baseline": None, "dtype": "f64" if FORMS[form]["precision"] == "fp64" else "f32+f64",
+            "data": "synthetic Si87H76 geometry; the reference's pseudopotential tables",
+            "config": workload_config(form),
+            "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "iterations": e2e_its},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": roof["gbs"], "peak": peak, "unit": "GB/s",
-                         "frac": roof["gbs"] / peak, "traffic": stencil_traffic(),
-                         "kernel": "k_stencil_tma<double,4> (one FP64 Chebyshev step, k=55, C10H8 grid)",
-                         "peak_kind": peak_kind, "launch_s": roof["seconds"],
-                         "algorithmic_bytes": roof["bytes"]},
+                         "frac": roof["gbs"] / peak, "traffic": stencil_traffic("dram_bytes_per_launch_si87h76_f32_k307"),
+                         "kernel": "k_stencil_tma<float,4> (one FP32 Chebyshev step of the filter, k=307, "
+                                   "Si87H76 90^3 grid)",
+                         "peak_kind": peak_kind, "launch_s": roof["seconds"], "algorithmic_bytes": roof["bytes"]},
             "hx_gbs": roof["gbs"], "hx_gflops": roof["gflops"],
-            "roofline_f32": {"bound": "hbm", "achieved": roof32["gbs"], "peak": peak, "unit": "GB/s",
-                             "frac": roof32["gbs"] / peak, "peak_kind": peak_kind, "launch_s": roof32["seconds"],
-                             "algorithmic_bytes": roof32["bytes"],
-                             "kernel": "k_stencil_tma<float,4> (one FP32 Chebyshev step of the mixed-precision "
-                                       "filter, k=55, C10H8 grid)"},
+            "roofline_f64": {"bound": "hbm", "achieved": roof64["gbs"], "peak": peak, "unit": "GB/s",
+                             "frac": roof64["gbs"] / peak, "peak_kind": peak_kind, "launch_s": roof64["seconds"],
+                             "algorithmic_bytes": roof64["bytes"],
+                             "kernel": "k_stencil_tma<double,4> (one FP64 Chebyshev step, k=307, Si87H76 grid)"},
             "cpu_baseline": cpu, "clocks": clocks,
-            "iterations": int(np.median(iters)), "energy_error_ha_vs_reference": err_ha,
-            "energy_within_1e-5_ha": within, "reference_energy_ry": e_ref,
+            "iterations": int(np.median(iters)), "fp32_iterations": int(np.median(f32its)),
+            "energy_error_ha_vs_reference": err_ha, "energy_within_1e-5_ha": within, "reference_energy_ry": e_ref,
+            "reference": "oracle (NumPy/SciPy port of the reference CPU path), tol 1e-8",
             "setup_s": float(np.mean(setups)), "reference_iterations": ref_its, "step_times_s": times,
-            "step_iterations": iters, "mixed_precision": mixed,
-            "mixed_speedup_vs_fp64": (t_step / mixed["value"]) if mixed else None,
-            "chosen_form": chosen,
-            "chosen_form_speedup_vs_fp64": (t_step / chosen["value"]) if chosen else None,
-            "learned_init": learned_res}
+            "step_iterations": iters, "learned_weights": weights.name if weights.exists() else None,
+            "legs": legs,
+            "speedup_vs_fp64_plain": (plain["value"] / t_step) if plain else None,
+            "speedup_vs_fp64_prec": (legs["fp64_prec"]["value"] / t_step) if "fp64_prec" in legs else None}
     print(json.dumps(line), flush=True)
 
 
@@ -648,7 +735,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--form", choices=sorted(FORMS), default="chosen",
+                    help="SCF variant of the timed steps (default: the chosen form)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scf-only", action="store_true",
                     help="run only the warm-up and timed SCF solves (for launch-list profiling)")
@@ -657,9 +745,13 @@ def main():
     ap.add_argument("--hartree", action="store_true",
                     help="only time the Hartree solve and its spectral preconditioner on the C10H8 grid")
     ap.add_argument("--stencil", choices=["f64", "f32"], default=None,
-                    help="only time the fused stencil step (k = 55, C10H8 grid) for kernel profiling")
+                    help="only time the fused stencil step (default: Si87H76 grid, k = 307) for kernel profiling")
+    ap.add_argument("--grid", default=None, help="configuration whose grid --stencil uses (h2o, c10h8, si35h36, si87h76)")
+    ap.add_argument("--k", type=int, default=None, help="columns of the --stencil step (default nev + 15)")
     ap.add_argument("--hx", action="store_true",
-                    help="only run the H.X microbenchmark (C10H8 and Si87H76 grids, k = 27/55/143/307, FP64/FP32)")
+                    help="only run the H.X microbenchmark (C10H8 and Si87H76 grids, cube and sphere mask, FP64/FP32)")
+    ap.add_argument("--hx-widths", default="27,55,143,307", help="column counts of --hx")
+    ap.add_argument("--hx-impls", default="0", help="stencil implementations of --hx (0 default, 2 four-point FP32)")
     ap.add_argument("--syev", nargs="?", const="55_rand,55_near,143_near,307_near", default=None,
                     help="only time the k x k symmetric eigensolver (comma-separated <k>_<rand|near> cases)")
     args = ap.parse_args()
@@ -684,13 +776,16 @@ def main():
         print(json.dumps(hartree_timing(reps=max(1, args.steps))))
         return
     if args.stencil:
-        print(json.dumps(stencil_roofline(reps=max(1, args.steps), dtype=args.stencil)))
+        name = args.grid or CFG_NAME
+        print(json.dumps(stencil_roofline(reps=max(1, args.steps), dtype=args.stencil, name=name, k=args.k)))
         return
     if args.syev:
         print(json.dumps(syev_timing(args.syev)))
         return
     if args.hx:
-        for r in hx_sweep(reps=max(1, args.steps) * 4):
+        widths = tuple(int(x) for x in args.hx_widths.split(","))
+        impls = tuple(int(x) for x in args.hx_impls.split(","))
+        for r in hx_sweep(widths=widths, reps=max(1, args.steps) * 4, impls=impls):
             print(json.dumps(r), flush=True)
         return
     rank, local, world = dist_init()

@@ -45,8 +45,14 @@ int psc_ctx_info(const psc_ctx* ctx, long* out);
 /* host flags[8] of device-side checks: [0] filter bounds inverted, [1]
  * Cholesky pivot <= 0 at column flags[1]-1, [3] TMA stencil wait timed out,
  * [4] persistent CG grid barrier timed out, [5] tensor-core Gram pipeline
- * wait timed out; [2] and [6] reserved.  clear != 0 resets */
+ * wait timed out, [6] tensor-core block product pipeline wait timed out;
+ * [2] reserved.  clear != 0 resets */
 int psc_status(psc_ctx* ctx, int* host_flags, int clear, void* stream);
+/* Polls of every bounded device-side wait (status words 3-6) before the CTA
+ * gives up, records its status word and returns; polls < 0 restores the
+ * default (2^24; the CG grid barrier waits 4x as long).  0 makes every wait
+ * run out at once (failure-path tests).  No counterpart in the reference. */
+int psc_set_wait_limit(psc_ctx* ctx, long polls);
 
 /* ---- ionic setup ------------------------------------------------------ */
 /* Radial tables of one species: row-major nknots x 7 (radius, charge,
@@ -97,8 +103,20 @@ int psc_apply_h(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long 
 int psc_apply_h_axpby(psc_ctx* ctx, int dtype, const void* X, long ldx, const void* P, long ldp, void* Y, long ldy,
                       int k, double alpha, double beta, double gamma, void* stream);
 /* Stencil implementation: 0 = TMA-fed pipeline where the bulk-copy alignment
- * rules hold (default), 1 = register-queue kernel everywhere. */
+ * rules hold (default; FP32 blocks take 2-point runs when nx is even but not
+ * a multiple of 4), 1 = register-queue kernel everywhere, 2 = the TMA
+ * pipeline with 4-point FP32 runs in every case. */
 int psc_set_stencil_impl(psc_ctx* ctx, int impl);
+/* Sphere-masked Hamiltonian (no counterpart in the reference, which solves
+ * on the whole cube): with radius > 0 (bohr) every H X returns zero at the
+ * points farther than radius from the cube's centre, the projector tables
+ * lose their points there, and the TMA stencil reads nothing for the planes
+ * of a slab that hold no point inside (it only writes their zeros).  On
+ * blocks that vanish outside the sphere this is P H P.  radius <= 0 restores
+ * the cube.  Synchronises the stream. */
+int psc_set_sphere_mask(psc_ctx* ctx, double radius, void* stream);
+/* Zero the points outside the sphere mask in k columns (no-op without one). */
+int psc_mask_block(psc_ctx* ctx, int dtype, void* X, long ld, int k, void* stream);
 /* Y = A X with A = -Lap_h (Laplacian/fd3d.py:34-106 scaled by 1/h^2). */
 int psc_laplacian_apply(psc_ctx* ctx, const double* x, double* y, int k, long ld, void* stream);
 
@@ -172,7 +190,10 @@ int psc_syev(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, void*
 int psc_occupations(psc_ctx* ctx, const double* lam_dev, int n, double temp, double nelec, double tol,
                     double* ef_dev, double* occ_dev, void* stream);
 /* rho = sum_i W_i^2 (2 f_i) / h^3 and hrhs = fourpi_h3 (h^3 rho - rho0)
- * (rsdft_solver.py:324-328); hrhs may be NULL. */
+ * (rsdft_solver.py:324-328); hrhs may be NULL.  For FP32 blocks each
+ * orbital's weight is divided by its exact (FP64-summed) squared norm, so
+ * that the electron count does not inherit the block's column-scale
+ * rounding. */
 int psc_density(psc_ctx* ctx, int dtype, const void* W, long ld, int nev, const double* occ_dev,
                 const double* rho0, double fourpi_h3, double h3, double* rho, double* hrhs, void* stream);
 
@@ -198,7 +219,8 @@ int psc_poisson_precond(psc_ctx* ctx, const double* r, double* z, void* stream);
  * the host.  All modes compute the same iterates. */
 int psc_set_use_graphs(psc_ctx* ctx, int mode);
 /* LDA (Ceperley-Alder / Perdew-Zunger), V_xc/exc_nspn.py:8-103.
- * out_dev = [exc, max rho, min rho]. */
+ * out_dev = [exc, max rho, min rho]; max and min propagate NaN as numpy's
+ * max and min do (rsdft_solver.py logs them). */
 int psc_lda_xc(psc_ctx* ctx, const double* rho, double* vxc, double h3, double* out_dev, void* stream);
 /* LDA exchange-correlation like psc_lda_xc, for callers that cannot allocate
  * device memory (inside a CUDA stream capture, or under a host that owns all
@@ -206,9 +228,12 @@ int psc_lda_xc(psc_ctx* ctx, const double* rho, double* vxc, double h3, double* 
  * exists for those callers.  Needs no context and allocates nothing: its
  * per-CTA partials live in a fixed 96 KiB device array of the library.  rho,
  * vxc: n device doubles, 1 <= n <= 33554432 (larger n is rejected with
- * status 2); out_dev = [exc, max rho, min rho].  The first call on a device
- * looks up that array's address and should come before any stream capture;
- * concurrent calls share the array and race, so serialise them. */
+ * status 2); out_dev = [exc, max rho, min rho] (max and min propagate NaN,
+ * as in psc_lda_xc).  The first call on a device looks up that array's
+ * address and must come before any stream capture (a first call made during
+ * a capture is refused with status 2); the address is kept for the process,
+ * so do not call this entry point after cudaDeviceReset.  Concurrent calls
+ * share the array and race, so serialise them. */
 int psc_lda_xc_noalloc(const double* rho, double* vxc, long n, double h3, double* out_dev, void* stream);
 /* pot_new = ppot + 0.5 vxc + hpot + hpot0, f = pot_new - pot (may be NULL),
  * out_dev = [|f|^2, |pot_new|^2, sum rho(hpot+hpot0), sum rho vxc]
@@ -238,6 +263,11 @@ int psc_dot(psc_ctx* ctx, const double* a, const double* b, long n, double* out_
  * split-precision TF32 (1, default) or on CUDA cores with FP64 accumulation
  * (0).  No counterpart in the reference (its GPU path is cuBLAS FP32). */
 int psc_set_gram_impl(psc_ctx* ctx, int tensor_cores);
+/* Block products W T of FP32 blocks (the W Q of Rayleighritz.py:4-30 and
+ * chefsi1.py:64-67, here W R^{-1} Y) on tcgen05 tensor cores with
+ * split-precision TF32 and FP32 accumulation (1, default) or on CUDA cores
+ * (0).  No counterpart in the reference (its GPU path is cuBLAS FP32). */
+int psc_set_gemm_impl(psc_ctx* ctx, int tensor_cores);
 /* S = W^T W and K = W^T V for n x k blocks (leading dimension ld), k x k
  * column-major FP64 results on the device (the Gram and projected-Hamiltonian
  * products of Rayleighritz.py:4-30). */

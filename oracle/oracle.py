@@ -981,7 +981,8 @@ def build_system(atoms: list, *, h: float, radius: float, elements: dict | None 
 
 class OracleSCF:
     """The SCF of rsdft_solver.run_rsdft_calculation (rsdft_solver.py:156-462)
-    for density_method = sad, adaptive_scheme = 0, cg_prec = 0, any diagmeth
+    for density_method = sad, adaptive_scheme = 0, cg_prec = 0 or 1 (the
+    spectral preconditioner), any diagmeth
     (rsdft_solver.py:287-317: 3 first_filt, 2 chsubsp, 0 lanczos, then chefsi1;
     1 lanczos at every iteration),
     split into setup() and step() so that a bounded number of iterations can
@@ -990,11 +991,12 @@ class OracleSCF:
     def __init__(self, domain: dict, atoms: list, *, nev: int, poldeg: int = 10, tol: float = 2e-4,
                  maxits: int = 40, fd_order: int = 8, fermi_temp: float = 500.0, z_charge: float = 0.0,
                  elements=None, tables=None, diagmeth: int = 3, density_method: str = "sad", density=None,
-                 operator: str = "csr"):
+                 operator: str = "csr", cg_prec: int = 0):
         if operator not in ("csr", "stencil"):
             raise ValueError(f"operator must be 'csr' or 'stencil', not {operator!r}")
         self.domain, self.atoms, self.nev, self.poldeg, self.tol = domain, atoms, nev, poldeg, tol
         self.operator = operator
+        self.cg_prec = cg_prec
         self.diagmeth = diagmeth
         self.density_method, self.density = density_method, density
         self.maxits, self.fd_order, self.fermi_temp, self.z_charge = maxits, fd_order, fermi_temp, z_charge
@@ -1063,7 +1065,15 @@ class OracleSCF:
         rho = (self.W[:, :nev] ** 2) @ (2 * occ)
         hrhs = (4 * np.pi / h ** 3) * (rho - self.rho0)
         self.rho = rho / h ** 3
-        self.Hpot, cg_its = pcg(self.A, hrhs, self.Hpot, 200, 1e-5)
+        if self.cg_prec:
+            # rsdft_solver.py:336-342 with the preconditioned branch of pcg.py;
+            # the preconditioner is the spectral inverse of the stencil (the
+            # reference's own ILU path cannot run, see pcg_prec)
+            if getattr(self, "_prec", None) is None:
+                self._prec = spectral_preconditioner(self.domain, self.fd_order)
+            self.Hpot, cg_its = pcg_prec(self.A, hrhs, self.Hpot, 200, 1e-5, self._prec)
+        else:
+            self.Hpot, cg_its = pcg(self.A, hrhs, self.Hpot, 200, 1e-5)
         self.XCpot, self.exc = exc_nspn(h, self.rho)
         pot_new = self.ppot + 0.5 * self.XCpot + self.Hpot + self.hpot0
         self.err = float(np.linalg.norm(pot_new - self.pot) / np.linalg.norm(pot_new))

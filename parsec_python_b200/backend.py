@@ -27,6 +27,9 @@ class GpuRuntime:
     def context(self, domain: dict) -> gpu.GridContext:
         if self.ctx is None or not self.ctx.matches(domain, self.settings.fd_order):
             self.ctx = gpu.GridContext(domain, self.settings.fd_order, seed=self.settings.seed)
+            if self.settings.mask == "sphere":
+                # the sphere inscribed in the cube: radius = the domain's half-width
+                self.ctx.set_sphere_mask(self.ctx.radius)
         return self.ctx
 
     # -- reference entry points ------------------------------------------------
@@ -55,7 +58,9 @@ class GpuRuntime:
         return (rho1, hpot1, ppot, info) if return_info else (rho1, hpot1, ppot)
 
     def first_filt(self, nev, H, polm=10):
-        return gpu.first_filt(nev, H, polm, dtype=self.block_dtype)
+        s = self.settings
+        return gpu.first_filt(nev, H, polm, dtype=self.block_dtype, energ_tol=s.first_tol,
+                              max_iter=s.first_rounds or None)
 
     def chefsi1(self, W, ritzv, deg, nev, H):
         return gpu.chefsi1(W, ritzv, deg, nev, H)

@@ -111,7 +111,7 @@ extern "C" int psc_ctx_destroy(psc_ctx* ctx) {
   psc_dfree(ctx->cg_ap); psc_dfree(ctx->cg_part); psc_dfree(ctx->mix_dx); psc_dfree(ctx->mix_df);
   psc_dfree(ctx->mix_nv); psc_dfree(ctx->mix_tmp); psc_dfree(ctx->mix_coef); psc_dfree(ctx->mix_partial);
   psc_dfree(ctx->cg_x); psc_dfree(ctx->eig_work); psc_dfree(ctx->cg_p2); psc_dfree(ctx->cg_ro); psc_dfree(ctx->cg_bar);
-  psc_dfree(ctx->tc_part); psc_dfree(ctx->tc_pairs); psc_dfree(ctx->tri_work);
+  psc_dfree(ctx->tc_part); psc_dfree(ctx->tc_pairs); psc_dfree(ctx->tri_work); psc_dfree(ctx->col_norm_part); psc_dfree(ctx->tsplit);
   for (auto& e : ctx->st_sched) psc_dfree(e.dev);
   for (int a = 0; a < 3; ++a) { psc_dfree(ctx->spec_S[a]); psc_dfree(ctx->spec_lam[a]); }
   psc_dfree(ctx->spec_tmp); psc_dfree(ctx->lz_basis);
@@ -376,6 +376,17 @@ extern "C" int psc_status(psc_ctx* ctx, int* host_flags /* [8] */, int clear, vo
   PSC_CUDA(ctx, cudaMemcpyAsync(host_flags, ctx->dev_status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
   PSC_CUDA(ctx, cudaStreamSynchronize(st));
   if (clear) PSC_CUDA(ctx, cudaMemsetAsync(ctx->dev_status, 0, 8 * sizeof(int), st));
+  return 0;
+}
+
+// Polls of every bounded device-side wait (stencil bulk-copy pipeline,
+// tensor-core Gram and block-product pipelines; the CG grid barrier waits 4x
+// as long) before the CTA gives up and records its status word.  polls < 0
+// restores the default.  A test can set 0 to make every wait run out at once
+// and check that the failure is reported and the context stays usable.
+extern "C" int psc_set_wait_limit(psc_ctx* ctx, long polls) {
+  if (!ctx) return 2;
+  ctx->wait_limit = polls < 0 ? PSC_WAIT_DEFAULT : polls;
   return 0;
 }
 

@@ -6,9 +6,12 @@
 // Eigensolvers/chefsi1.py:43 and first_filt.py:43) and Rayleigh-Ritz
 // (chefsi1.py:46-67, first_filt.py:44-63).  Small k x k work is FP64.
 #include "psc_internal.cuh"
+#include <cooperative_groups.h>
 #include "../../include/psc.h"
 
 #include <algorithm>
+
+namespace cg = cooperative_groups;
 #include <cmath>
 
 // ---------------------------------------------------------------------------
@@ -160,53 +163,15 @@ extern "C" int psc_gemm_nn(psc_ctx* ctx, int dtype, const void* W, long ldw, int
 }
 
 // ---------------------------------------------------------------------------
-// Cholesky (upper, G = R^T R, in place, one CTA) and upper-triangular inverse
+// Cholesky S = R^T R (upper R) and R^{-1}
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_cholesky(double* A, int k, int* status) {
-  for (int j = 0; j < k; ++j) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const double d = A[j + (long)j * k];
-      if (!(d > 0.0)) status[1] = j + 1;  // not positive definite
-      A[j + (long)j * k] = d > 0.0 ? sqrt(d) : 1.0;
-    }
-    __syncthreads();
-    const double rjj = A[j + (long)j * k];
-    for (int c = j + 1 + threadIdx.x; c < k; c += blockDim.x) A[j + (long)c * k] /= rjj;
-    __syncthreads();
-    const int m = k - j - 1;
-    for (long e = threadIdx.x; e < (long)m * m; e += blockDim.x) {
-      const int r = j + 1 + (int)(e % m), c = j + 1 + (int)(e / m);
-      if (r <= c) A[r + (long)c * k] -= A[j + (long)r * k] * A[j + (long)c * k];
-    }
-  }
-  __syncthreads();
-  for (long e = threadIdx.x; e < (long)k * k; e += blockDim.x) {
-    const int r = (int)(e % k), c = (int)(e / k);
-    if (r > c) A[e] = 0.0;
-  }
-}
-
-__global__ void k_triu_inv(const double* __restrict__ R, int k, double* __restrict__ X) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x) {
-    double* xj = X + (long)j * k;
-    for (int i = j + 1; i < k; ++i) xj[i] = 0.0;
-    xj[j] = 1.0 / R[j + (long)j * k];
-    for (int i = j - 1; i >= 0; --i) {
-      double s = 0.0;
-      for (int l = i + 1; l <= j; ++l) s += R[i + (long)l * k] * xj[l];
-      xj[i] = -s / R[i + (long)i * k];
-    }
-  }
-}
-
 // Cholesky and inverse in one CTA with the matrix in shared memory (k up to
 // 150): S = R^T R (R upper, written back in place with zeros below) and
 // X = R^{-1}.
 //   column j: every thread reads d = S[j,j] and takes r_jj = sqrt(d) (1, and
 //   status word 1 = j + 1, if d <= 0); row j right of the diagonal divided by
 //   r_jj goes to u; barrier; the trailing upper triangle loses u_r u_c;
-//   barrier.  The same operations as k_cholesky, two barriers per column.
+//   barrier.  Two barriers per column.
 //   R^{-1}: one warp per column j, right-looking substitution on b = e_j:
 //   x_i = b_i / r_ii, then b_r -= R[r, i] x_i for r < i.
 constexpr int CI_NT = 512;
@@ -263,6 +228,162 @@ __global__ void __launch_bounds__(CI_NT) k_chol_inv(double* __restrict__ S, int 
   }
 }
 
+// Blocked right-looking Cholesky for matrices that do not fit one CTA's
+// shared memory (k > 151): block columns of CB.  Per block step j0:
+//   k_potrf_diag    one CTA factors the CB x CB diagonal block in shared
+//                   memory (the k_chol_inv column loop) and writes R11 and
+//                   R11^{-T} (the latter into scratch D);
+//   k_potrf_panel   R12 = R11^{-T} A12, 64 columns per CTA;
+//   k_potrf_update  A22 -= R12^T R12 on the upper triangle, 64 x 64 tiles.
+// Then k_trtri_warp forms R^{-1}: one warp per column, the right-looking
+// substitution of k_chol_inv with R read from global memory (L2-resident).
+constexpr int CB = 64;
+
+__global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int k, int j0, double* __restrict__ D,
+                                                    int* status) {
+  __shared__ double a[CB][CB + 1];   // a[c][r] = A[j0 + r, j0 + c]
+  __shared__ double u[CB], dg[CB];
+  const int nb = min(CB, k - j0);
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int e = tid; e < nb * nb; e += 256) {
+    const int r = e % nb, c = e / nb;
+    a[c][r] = A[(j0 + r) + (long)(j0 + c) * k];
+  }
+  __syncthreads();
+  for (int j = 0; j < nb; ++j) {
+    const double d = a[j][j];
+    const double rjj = d > 0.0 ? sqrt(d) : 1.0;
+    if (tid == 0) {
+      dg[j] = rjj;
+      if (!(d > 0.0) && status[1] == 0) status[1] = j0 + j + 1;   // not positive definite
+    }
+    for (int c = j + 1 + tid; c < nb; c += 256) {
+      const double v = a[c][j] / rjj;
+      u[c] = v;
+      a[c][j] = v;
+    }
+    __syncthreads();
+    for (int c = j + 1 + w; c < nb; c += 8) {
+      const double uc = u[c];
+      for (int r = j + 1 + lane; r <= c; r += 32) a[c][r] -= u[r] * uc;
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < nb * nb; e += 256) {
+    const int r = e % nb, c = e / nb;
+    A[(j0 + r) + (long)(j0 + c) * k] = r < c ? a[c][r] : (r == c ? dg[c] : 0.0);
+  }
+  // D = R11^{-T} (lower triangular, column-major nb x nb): column j of R11^{-1}
+  // by right-looking substitution, one warp per column, stored transposed
+  __shared__ double b[8][CB];
+  for (int j = w; j < nb; j += 8) {
+    for (int r = lane; r < nb; r += 32) b[w][r] = r == j ? 1.0 : 0.0;
+    __syncwarp();
+    for (int i = j; i >= 0; --i) {
+      const double xi = b[w][i] / dg[i];
+      for (int r = lane; r < i; r += 32) b[w][r] -= a[i][r] * xi;
+      if (lane == 0) b[w][i] = xi;
+      __syncwarp();
+    }
+    for (int r = lane; r < nb; r += 32) D[j + (long)r * CB] = r <= j ? b[w][r] : 0.0;   // D[j, r] = Rinv[r, j]
+    __syncwarp();
+  }
+}
+
+// R12 (rows j0..j0+nb, columns c >= j0+nb) = D A12 with D = R11^{-T}
+__global__ void __launch_bounds__(256) k_potrf_panel(double* __restrict__ A, int k, int j0,
+                                                     const double* __restrict__ D) {
+  extern __shared__ double psm[];
+  double (*d)[CB + 1] = reinterpret_cast<double (*)[CB + 1]>(psm);               // d[l][i] = D[i, l]
+  double (*x)[CB + 1] = reinterpret_cast<double (*)[CB + 1]>(psm + CB * (CB + 1));  // 64 columns of A12
+  const int nb = min(CB, k - j0);
+  const int c0 = j0 + nb + blockIdx.x * 64;
+  const int nc = min(64, k - c0);
+  for (int e = threadIdx.x; e < nb * nb; e += 256) d[e / nb][e % nb] = D[(e % nb) + (long)(e / nb) * CB];
+  for (int e = threadIdx.x; e < nb * nc; e += 256) {
+    const int r = e % nb, c = e / nb;
+    x[c][r] = A[(j0 + r) + (long)(c0 + c) * k];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nb * nc; e += 256) {
+    const int i = e % nb, c = e / nb;
+    double s = 0.0;
+    for (int l = 0; l <= i; ++l) s += d[l][i] * x[c][l];
+    A[(j0 + i) + (long)(c0 + c) * k] = s;
+  }
+}
+
+// A22[r, c] -= sum_l R12[l, r] R12[l, c] for j0+nb <= r <= c (upper triangle)
+__global__ void __launch_bounds__(256) k_potrf_update(double* __restrict__ A, int k, int j0) {
+  const int nb = min(CB, k - j0);
+  const int b0 = j0 + nb;
+  const int tr = blockIdx.x, tc = blockIdx.y;
+  if (tr > tc) return;
+  extern __shared__ double usm[];
+  double (*pr)[64 + 1] = reinterpret_cast<double (*)[64 + 1]>(usm);                // pr[l][i] = R12[l, r0 + i]
+  double (*pc)[64 + 1] = reinterpret_cast<double (*)[64 + 1]>(usm + CB * (64 + 1));
+  const int r0 = b0 + tr * 64, cc0 = b0 + tc * 64;
+  for (int e = threadIdx.x; e < nb * 64; e += 256) {
+    const int l = e % nb, i = e / nb;
+    pr[l][i] = (r0 + i < k) ? A[(j0 + l) + (long)(r0 + i) * k] : 0.0;
+    pc[l][i] = (cc0 + i < k) ? A[(j0 + l) + (long)(cc0 + i) * k] : 0.0;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+  for (int l = 0; l < nb; ++l) {
+    double ra[4], cq[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) ra[a] = pr[l][tx + 16 * a];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cq[q] = pc[l][ty + 16 * q];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[a][q] += ra[a] * cq[q];
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = r0 + tx + 16 * a, c = cc0 + ty + 16 * q;
+      if (r < k && c < k && r <= c) A[r + (long)c * k] -= acc[a][q];
+    }
+}
+
+__global__ void k_tril_zero(double* A, int k) {
+  const long kk = (long)k * k;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < kk; e += (long)gridDim.x * blockDim.x)
+    if ((int)(e % k) > (int)(e / k)) A[e] = 0.0;
+}
+
+// X = R^{-1}, one warp per column: b = e_j, then for i = j .. 0: x_i = b_i / r_ii,
+// b_r -= R[r, i] x_i (r < i); columns of R come from global memory
+__global__ void __launch_bounds__(256) k_trtri_warp(const double* __restrict__ R, int k, double* __restrict__ X) {
+  extern __shared__ double bs[];   // [8][k]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int j = blockIdx.x * 8 + w;
+  if (j >= k) return;
+  double* b = bs + (long)w * k;
+  double* xj = X + (long)j * k;
+  for (int r = lane; r < k; r += 32) {
+    if (r <= j) b[r] = r == j ? 1.0 : 0.0;
+    else xj[r] = 0.0;
+  }
+  __syncwarp();
+  for (int i = j; i >= 0; --i) {
+    const double* ri = R + (long)i * k;
+    const double xi = b[i] / ri[i];
+    for (int r = lane; r < i; r += 32) b[r] -= ri[r] * xi;
+    if (lane == 0) xj[i] = xi;
+    __syncwarp();
+  }
+}
+
 // R and R^{-1} of S = R^T R (S overwritten by R)
 int psc_chol_inv_dev(psc_ctx* ctx, double* S, int k, double* X, cudaStream_t st) {
   const size_t dyn = chol_inv_smem_doubles(k) * sizeof(double);
@@ -273,9 +394,29 @@ int psc_chol_inv_dev(psc_ctx* ctx, double* S, int k, double* X, cudaStream_t st)
     PSC_LAUNCH_CHECK(ctx);
     return 0;
   }
-  k_cholesky<<<1, 1024, 0, st>>>(S, k, ctx->dev_status);
+  double* D = X;   // R11^{-T} of the current block step, in the first CB x CB of X (overwritten below)
+  const int psmem = (CB + 64) * (CB + 1) * (int)sizeof(double);
+  const int usmem = 2 * CB * (64 + 1) * (int)sizeof(double);
+  PSC_CUDA(ctx, cudaFuncSetAttribute(k_potrf_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
+  PSC_CUDA(ctx, cudaFuncSetAttribute(k_potrf_update, cudaFuncAttributeMaxDynamicSharedMemorySize, usmem));
+  for (int j0 = 0; j0 < k; j0 += CB) {
+    const int nb = std::min(CB, k - j0);
+    k_potrf_diag<<<1, 256, 0, st>>>(S, k, j0, D, ctx->dev_status);
+    PSC_LAUNCH_CHECK(ctx);
+    const int m = k - j0 - nb;
+    if (m <= 0) break;
+    k_potrf_panel<<<psc_div_up(m, 64), 256, psmem, st>>>(S, k, j0, D);
+    PSC_LAUNCH_CHECK(ctx);
+    const int t = psc_div_up(m, 64);
+    k_potrf_update<<<dim3(t, t), 256, usmem, st>>>(S, k, j0);
+    PSC_LAUNCH_CHECK(ctx);
+  }
+  k_tril_zero<<<std::max(1, std::min(592, psc_div_up((long)k * k, 256))), 256, 0, st>>>(S, k);
   PSC_LAUNCH_CHECK(ctx);
-  k_triu_inv<<<psc_div_up(k, 128), 128, 0, st>>>(S, k, X);
+  const size_t tdyn = 8 * (size_t)k * sizeof(double);
+  if (tdyn > 48 * 1024)
+    PSC_CUDA(ctx, cudaFuncSetAttribute(k_trtri_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tdyn));
+  k_trtri_warp<<<psc_div_up(k, 8), 256, tdyn, st>>>(S, k, X);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }
@@ -428,6 +569,137 @@ k_sytrd(const double* __restrict__ Ain, int k, int on_chip, double* __restrict__
   }
 }
 
+// The same reduction for matrices too large for one CTA's shared memory
+// (153 < k <= ~420): a cluster of SY_CL CTAs holds the symmetrised matrix in
+// their shared memory, column c in CTA c mod SY_CL (cyclic, so the trailing
+// block stays spread over all of them).  Step j:
+//   the owner of column j builds reflector j (one warp, as sy_reflector) and
+//   writes it to hv / ab / tau;                               cluster barrier
+//   every CTA copies v and tau from the owner's shared memory, and forms the
+//   partial products of its columns, part = sum_c A[:, c] v_c; cluster barrier
+//   every CTA sums the SY_CL partials in rank order (distributed shared
+//   memory, the same order everywhere), p = tau part, K = tau (p.v) / 2, and
+//   applies the rank-2 update A -= v w^T + w v^T (w = p - K v) to its columns.
+// Two cluster barriers per step instead of three block barriers over L2.
+constexpr int SY_CL = 8;
+constexpr int SY_CNT = 512;
+
+static size_t sytrd_cl_smem_doubles(int k) {
+  return (size_t)((k + SY_CL - 1) / SY_CL) * k + 3 * (size_t)k;
+}
+
+__global__ void __cluster_dims__(SY_CL, 1, 1) __launch_bounds__(SY_CNT)
+k_sytrd_cl(const double* __restrict__ Ain, int k, double* __restrict__ hv, double* __restrict__ ab,
+           double* __restrict__ tau) {
+  extern __shared__ double sm[];
+  __shared__ double red[SY_CNT / 32];
+  __shared__ double s_t;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int ncl = (k + SY_CL - 1) / SY_CL;
+  double* A = sm;                        // [ncl][k]: local column lc is global column rank + SY_CL lc
+  double* vb = A + (size_t)ncl * k;      // reflector, entry i = row j+1+i
+  double* part = vb + k;                 // this CTA's partial products (row j+1+i at i)
+  double* pf = part + k;                 // p
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int lc = w; lc < ncl; lc += SY_CNT / 32) {
+    const int c = rank + SY_CL * lc;
+    if (c >= k) continue;
+    for (int r = lane; r < k; r += 32)
+      A[(long)lc * k + r] = (r == c) ? Ain[r + (long)c * k] : 0.5 * (Ain[r + (long)c * k] + Ain[c + (long)r * k]);
+  }
+  __syncthreads();
+  for (int j = 0; j + 2 < k; ++j) {
+    const int L = k - j - 1;
+    const int owner = j % SY_CL;
+    if (rank == owner && w == 0) {
+      // reflector j from column j below the diagonal
+      const double* x = A + (long)(j / SY_CL) * k + (j + 1);
+      const double alpha = x[0];
+      double sig = 0.0;
+      for (int i = 1 + lane; i < L; i += 32) sig += x[i] * x[i];
+      sig = psc_warp_sum(sig);
+      double t = 0.0, beta = alpha, scal = 0.0;
+      if (sig > 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + sig), alpha);
+        t = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      for (int i = lane; i < L; i += 32) {
+        const double vi = i == 0 ? 1.0 : x[i] * scal;
+        vb[i] = vi;
+        hv[(j + 1 + i) + (long)j * k] = vi;
+      }
+      if (lane == 0) {
+        ab[2 * j] = A[(long)(j / SY_CL) * k + j];
+        ab[2 * j + 1] = beta;
+        tau[j] = t;
+        s_t = t;
+      }
+    }
+    cl.sync();
+    const double t = *cl.map_shared_rank(&s_t, owner);
+    if (rank != owner) {
+      const double* rv = cl.map_shared_rank(vb, owner);
+      for (int i = tid; i < L; i += SY_CNT) vb[i] = rv[i];
+    }
+    __syncthreads();
+    const int lc0 = (j + 1 - rank + SY_CL - 1) / SY_CL;   // first local column with c >= j+1
+    if (t != 0.0) {
+      for (int i = tid; i < L; i += SY_CNT) {
+        double acc = 0.0;
+        for (int lc = lc0; lc < ncl; ++lc) {
+          const int c = rank + SY_CL * lc;
+          if (c >= k) break;
+          acc += A[(long)lc * k + (j + 1 + i)] * vb[c - (j + 1)];
+        }
+        part[i] = acc;
+      }
+    }
+    cl.sync();
+    if (t != 0.0) {
+      double q = 0.0;
+      for (int i = tid; i < L; i += SY_CNT) {
+        double acc = 0.0;
+        for (int r = 0; r < SY_CL; ++r) acc += cl.map_shared_rank(part, r)[i];
+        const double pi = t * acc;
+        pf[i] = pi;
+        q += pi * vb[i];
+      }
+      q = psc_warp_sum(q);
+      if (lane == 0) red[w] = q;
+      __syncthreads();
+      double pv = 0.0;
+      for (int i = 0; i < SY_CNT / 32; ++i) pv += red[i];
+      const double K = 0.5 * t * pv;
+      for (int lc = lc0 + w; lc < ncl; lc += SY_CNT / 32) {
+        const int c = rank + SY_CL * lc;
+        if (c >= k) continue;
+        const int ci = c - (j + 1);
+        const double vc = vb[ci], wc = pf[ci] - K * vc;
+        double* col = A + (long)lc * k + (j + 1);
+        for (int r = lane; r < L; r += 32) {
+          const double vr = vb[r];
+          col[r] -= vr * wc + (pf[r] - K * vr) * vc;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // the last 2 x 2 block
+  if (tid == 0 && k >= 2) {
+    if (rank == (k - 2) % SY_CL) {
+      ab[2 * (k - 2)] = A[(long)((k - 2) / SY_CL) * k + (k - 2)];
+      ab[2 * (k - 2) + 1] = A[(long)((k - 2) / SY_CL) * k + (k - 1)];
+    }
+    if (rank == (k - 1) % SY_CL) {
+      ab[2 * (k - 1)] = A[(long)((k - 1) / SY_CL) * k + (k - 1)];
+      ab[2 * (k - 1) + 1] = 0.0;
+    }
+  }
+  cl.sync();   // no CTA leaves while others may still read its shared memory
+}
+
 // out = H_0 H_1 ... H_{k-3} Z (Z k x k, ld k).  A CTA owns OR_NW columns, one
 // warp each; the whole CTA stages the reflectors OR_CH at a time in shared
 // memory (one round of independent L2 loads per chunk instead of two
@@ -481,6 +753,8 @@ int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, 
   double* ab = Z + kk;       // T: diagonal ab[2i], off-diagonal ab[2i+1]
   double* tau = ab + 2 * k;
   const bool on_chip = sytrd_smem_doubles(k, true) * sizeof(double) <= 200 * 1024;
+  const size_t dyn_cl = sytrd_cl_smem_doubles(k) * sizeof(double);
+  const bool clustered = !on_chip && k >= 3 && dyn_cl <= 200 * 1024;
   const size_t dyn = sytrd_smem_doubles(k, on_chip) * sizeof(double);
 #define PSC_SYTRD(NTH)                                                                                      \
   {                                                                                                         \
@@ -488,7 +762,10 @@ int psc_syev_impl(psc_ctx* ctx, double* A, int k, double* evals, double* evecs, 
       PSC_CUDA(ctx, cudaFuncSetAttribute(k_sytrd<NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)); \
     k_sytrd<NTH><<<1, NTH, dyn, st>>>(A, k, on_chip ? 1 : 0, hv, ab, tau);                                  \
   }
-  if (!on_chip) PSC_SYTRD(1024)
+  if (clustered) {
+    PSC_CUDA(ctx, cudaFuncSetAttribute(k_sytrd_cl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_cl));
+    k_sytrd_cl<<<SY_CL, SY_CNT, dyn_cl, st>>>(A, k, hv, ab, tau);
+  } else if (!on_chip) PSC_SYTRD(1024)
   else if (k <= 96) PSC_SYTRD(256)
   else PSC_SYTRD(512)
 #undef PSC_SYTRD

@@ -9,12 +9,20 @@
 //
 // Grid: (chunk of the n rows) x (pair of 128-column tiles, upper triangle).
 // Each CTA streams its rows through a two-deep shared-memory ring, 32 rows
-// (one 128-byte swizzle row of FP32) per stage; its threads load and split
+// (one 128-byte swizzle row of FP32) per stage, the next stage's loads in
+// flight in registers while the current one is stored; its threads load and split
 // the tiles into hi/lo copies in the canonical K-major 128-byte-swizzled
 // layout, one elected thread issues the MMAs (M = 128, N = tile width,
 // K = 8 per instruction) and commits them to an mbarrier.  Partial FP32
 // tiles go to global memory and are summed over the chunks in FP64.
-// Every wait is bounded; on a timeout the kernel records status word 5.
+// The tensor cores' FP32 accumulation rounds toward zero, so a long chunk
+// biases every entry towards zero (about 1e-4 relative at 7,000 rows).  The
+// diagonal entries (column norms and Rayleigh quotients, which set the
+// density's normalisation and the eigenvalue sum) are therefore recomputed
+// exactly: the CTAs of diagonal tile pairs sum w_j^2 and w_j v_j in FP64
+// from the same FP32 registers they split, and the final kernel uses those.
+// Every wait is bounded by the context's wait limit; on a timeout the kernel
+// drains the MMAs it issued and records status word 5.
 #include "psc_internal.cuh"
 #include "../../include/psc.h"
 
@@ -28,7 +36,6 @@ constexpr int TILE_BYTES = TROWS * 128;  // 16 KB
 constexpr int NTILES = 6;                // A hi/lo, BS hi/lo, BK hi/lo
 constexpr int BUF_BYTES = NTILES * TILE_BYTES;
 constexpr int TMEM_COLS = 256;           // S accumulator at column 0, K at column 128
-constexpr long WAIT_LIMIT = 1L << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -64,8 +71,8 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b
       "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (long i = 0; i < WAIT_LIMIT; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long limit) {
+  for (long i = 0; i < limit; ++i) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -132,7 +139,8 @@ __device__ __forceinline__ void tile_store_split(const TileLoad& t, int nrows, u
 
 __global__ void __launch_bounds__(TC_NT, 1)
 k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int k, long n, long chunk,
-          const int2* __restrict__ pairs, float* __restrict__ part, int* status) {
+          const int2* __restrict__ pairs, float* __restrict__ part, double* __restrict__ dpart, long wait_limit,
+          int* status) {
   extern __shared__ unsigned char smraw[];
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t s_tmem;
@@ -168,7 +176,21 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
   const uint32_t tmem_s = tmem, tmem_k = tmem + 128;
+  // exact FP64 diagonal sums of a diagonal tile pair: this thread's columns
+  // are col_a + (threadIdx.x >> 3) + 32 u, u < PER
+  double dsum_s[PER], dsum_k[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) dsum_s[u] = dsum_k[u] = 0.0;
 
+  int last_commit = -1;   // thread 0: stage of the last MMA commit
+  // the tiles of stage s+1 are loaded into registers while stage s is split,
+  // stored and multiplied, so the HBM latency overlaps the tensor-core work
+  TileLoad ta, tb, tk;
+  if (nstage > 0) {
+    tile_load(W, ld, col_a, valid_a, TROWS, n_begin, n_end, vec, ta);
+    if (!same) tile_load(W, ld, col_b, valid_b, N, n_begin, n_end, vec, tb);
+    tile_load(V, ld, col_b, valid_b, N, n_begin, n_end, vec, tk);
+  }
   for (int s = 0; s < nstage; ++s) {
     const int b = s & 1;
     unsigned char* buf = sm + b * BUF_BYTES;
@@ -178,21 +200,36 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
     unsigned char* bs_lo = same ? a_lo : buf + 3 * TILE_BYTES;
     unsigned char* bk_hi = buf + 4 * TILE_BYTES;
     unsigned char* bk_lo = buf + 5 * TILE_BYTES;
-    if (s >= 2) {
+    if (s >= 2 && threadIdx.x == 0) {
       // the MMAs of stage s-2 read this buffer: wait for their commit
-      if (!mbar_wait(smem_u32(&mbar[b]), (uint32_t)(((s - 2) >> 1) & 1))) s_fail = 1;
+      if (!mbar_wait(smem_u32(&mbar[b]), (uint32_t)(((s - 2) >> 1) & 1), wait_limit)) s_fail = 1;
     }
     __syncthreads();
     if (s_fail) break;
-    const long n0 = n_begin + (long)s * KSTAGE;
     {
-      TileLoad ta, tb, tk;
-      tile_load(W, ld, col_a, valid_a, TROWS, n0, n_end, vec, ta);
-      if (!same) tile_load(W, ld, col_b, valid_b, N, n0, n_end, vec, tb);
-      tile_load(V, ld, col_b, valid_b, N, n0, n_end, vec, tk);
+      if (same) {
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const float4 a = ta.v[u], v = tk.v[u];
+          dsum_s[u] = fma((double)a.x, (double)a.x, dsum_s[u]);
+          dsum_s[u] = fma((double)a.y, (double)a.y, dsum_s[u]);
+          dsum_s[u] = fma((double)a.z, (double)a.z, dsum_s[u]);
+          dsum_s[u] = fma((double)a.w, (double)a.w, dsum_s[u]);
+          dsum_k[u] = fma((double)a.x, (double)v.x, dsum_k[u]);
+          dsum_k[u] = fma((double)a.y, (double)v.y, dsum_k[u]);
+          dsum_k[u] = fma((double)a.z, (double)v.z, dsum_k[u]);
+          dsum_k[u] = fma((double)a.w, (double)v.w, dsum_k[u]);
+        }
+      }
       tile_store_split(ta, TROWS, a_hi, a_lo);
       if (!same) tile_store_split(tb, N, bs_hi, bs_lo);
       tile_store_split(tk, N, bk_hi, bk_lo);
+      if (s + 1 < nstage) {
+        const long n1 = n_begin + (long)(s + 1) * KSTAGE;
+        tile_load(W, ld, col_a, valid_a, TROWS, n1, n_end, vec, ta);
+        if (!same) tile_load(W, ld, col_b, valid_b, N, n1, n_end, vec, tb);
+        tile_load(V, ld, col_b, valid_b, N, n1, n_end, vec, tk);
+      }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -215,15 +252,35 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(&mbar[b]))
                    : "memory");
+      last_commit = s;
     }
   }
-  // the last commit covers every MMA issued before it
-  if (nstage > 0 && !s_fail) {
-    const int sl = nstage - 1;
-    if (!mbar_wait(smem_u32(&mbar[sl & 1]), (uint32_t)((sl >> 1) & 1))) s_fail = 1;
+  // the last commit covers every MMA issued before it; after a failed wait
+  // the MMAs still in flight are drained before tensor memory is released
+  if (threadIdx.x == 0 && last_commit >= 0) {
+    const uint32_t bar = smem_u32(&mbar[last_commit & 1]), par = (uint32_t)((last_commit >> 1) & 1);
+    if (s_fail || !mbar_wait(bar, par, wait_limit)) {
+      s_fail = 1;
+      mbar_wait(bar, par, PSC_DRAIN_WAIT);
+    }
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (same && !s_fail && nstage > 0) {
+    // the 8 lanes that share a column (equal lane >> 3) sum their parts
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      for (int o = 1; o < 8; o <<= 1) {
+        dsum_s[u] += __shfl_xor_sync(0xffffffffu, dsum_s[u], o);
+        dsum_k[u] += __shfl_xor_sync(0xffffffffu, dsum_k[u], o);
+      }
+      const int row = (threadIdx.x >> 3) + u * (TC_NT / 8);
+      if ((threadIdx.x & 7) == 0 && row < valid_a) {
+        dpart[((long)blockIdx.x * 2 + 0) * k + col_a + row] = dsum_s[u];
+        dpart[((long)blockIdx.x * 2 + 1) * k + col_a + row] = dsum_k[u];
+      }
+    }
+  }
   if (s_fail) {
     if (threadIdx.x == 0) atomicExch(&status[5], 1);
   } else if (nstage > 0 && warp < 4) {
@@ -258,9 +315,11 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
 // S, K (k x k, column-major FP64) = sums over the chunks, one warp per entry
 // (lanes take every 32nd chunk, then a fixed shuffle tree).  Diagonal tiles
 // are symmetrised as 0.5 (X + X^T) (as the CUDA-core path does); off-diagonal
-// tiles are computed above the diagonal only and mirrored.
-__global__ void k_gram_tc_final(const float* __restrict__ part, int nchunk, int npair, const int2* __restrict__ pairs,
-                                int k, double* __restrict__ S, double* __restrict__ K) {
+// tiles are computed above the diagonal only and mirrored.  Diagonal entries
+// come from the exact FP64 chunk sums in dpart.
+__global__ void k_gram_tc_final(const float* __restrict__ part, const double* __restrict__ dpart, int nchunk,
+                                int npair, const int2* __restrict__ pairs, int k, double* __restrict__ S,
+                                double* __restrict__ K) {
   const int lane = threadIdx.x & 31;
   const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
   const long total = (long)npair * TROWS * TROWS;
@@ -273,6 +332,19 @@ __global__ void k_gram_tc_final(const float* __restrict__ part, int nchunk, int 
     const bool diag = pairs[p].x == pairs[p].y;
     const int cr = c * TROWS + r;
     double s = 0.0, kv = 0.0, st = 0.0, kt = 0.0;
+    if (i == j) {
+      for (int ch = lane; ch < nchunk; ch += 32) {
+        s += dpart[((long)ch * 2 + 0) * k + i];
+        kv += dpart[((long)ch * 2 + 1) * k + i];
+      }
+      s = psc_warp_sum(s);
+      kv = psc_warp_sum(kv);
+      if (lane == 0) {
+        S[i + (long)i * k] = s;
+        K[i + (long)i * k] = kv;
+      }
+      continue;
+    }
     for (int ch = lane; ch < nchunk; ch += 32) {
       const float* ps = part + (((long)ch * npair + p) * 2) * (TROWS * TROWS);
       s += (double)ps[rc];
@@ -313,7 +385,8 @@ int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int 
   int nchunk = std::max(1, 4 * 148 / npair);
   long chunk = ((n + nchunk - 1) / nchunk + KSTAGE - 1) / KSTAGE * KSTAGE;
   nchunk = (int)((n + chunk - 1) / chunk);
-  const size_t part_floats = (size_t)nchunk * npair * 2 * TROWS * TROWS;
+  const size_t tile_floats = (size_t)nchunk * npair * 2 * TROWS * TROWS;   // even, so dpart is 8-byte aligned
+  const size_t part_floats = tile_floats + (size_t)nchunk * 2 * k * 2;    // + nchunk x 2 x k doubles
   if (ctx->tc_part_floats < part_floats) {
     psc_dfree(ctx->tc_part);
     ctx->tc_part = nullptr;
@@ -332,12 +405,13 @@ int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int 
   }
   const size_t smem = 2 * (size_t)BUF_BYTES + 1024;
   PSC_CUDA(ctx, cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  double* dpart = reinterpret_cast<double*>(ctx->tc_part + tile_floats);
   k_gram_tc<<<dim3(nchunk, npair), TC_NT, smem, st>>>(W, V, ld, k, n, chunk, (const int2*)ctx->tc_pairs,
-                                                      ctx->tc_part, ctx->dev_status);
+                                                      ctx->tc_part, dpart, ctx->wait_limit, ctx->dev_status);
   PSC_LAUNCH_CHECK(ctx);
   const long total = (long)npair * TROWS * TROWS;
   k_gram_tc_final<<<std::max(1, (int)std::min<long>(148 * 8, (total + 7) / 8)), 256, 0, st>>>(
-      ctx->tc_part, nchunk, npair, (const int2*)ctx->tc_pairs, k, S, K);
+      ctx->tc_part, dpart, nchunk, npair, (const int2*)ctx->tc_pairs, k, S, K);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }

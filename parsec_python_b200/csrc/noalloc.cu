@@ -11,7 +11,11 @@
 //
 // Set-up: the first call on a device looks up the device address of
 // g_xc_scratch with cudaGetSymbolAddress (with that device current) and
-// caches it; make that first call before any stream capture.  Every call
+// caches it; make that first call before any stream capture (a first call
+// made during a capture is refused with status 2).  The cached address
+// belongs to the device's primary context: a process that resets the device
+// (cudaDeviceReset) must not call this entry point afterwards.  The minimum
+// and maximum density propagate NaN, as numpy's max and min do.  Every call
 // shares the one array, so calls that overlap on the GPU (two streams, or two
 // host threads) race on it and must be serialised by the caller.  Each call
 // writes every partial it later reads, so nothing has to be cleared between
@@ -31,36 +35,6 @@ namespace {
 std::mutex g_mu;
 double* g_scratch_dev[64] = {nullptr};  // device address of g_xc_scratch, per device
 
-// Ceperley-Alder / Perdew-Zunger LDA of one density value (V_xc/exc_nspn.py:73-91):
-// returns v_xc (Ry) and adds this point's energy density to e.
-__device__ __forceinline__ double lda_point(double r, double& e) {
-  const double g = -0.2846, b1 = 1.0529, b2 = 0.3334;
-  const double c1 = 0.0622, c2 = 0.096, c3 = 0.004, c4 = 0.0232, c5 = 0.0192;
-  const double third = 1.0 / 3.0;
-  const double pi = 3.141592653589793;
-  const double a0 = pow(4.0 / (9.0 * pi), third);
-  const double twovpia0 = 2.0 / (pi * a0);
-  const double p75vpi = 0.75 / pi;
-  double v = 0.0;
-  if (r > 0.0) {
-    const double rs = pow(p75vpi / r, third);
-    v = -twovpia0 / rs;
-    double ec;
-    e += 0.75 * r * v;
-    if (rs >= 1.0) {
-      const double sq = sqrt(rs);
-      ec = g / (1.0 + b1 * sq + b2 * rs);
-      v += (ec * ec) * (1.0 + 3.5 * b1 * sq * third + 4.0 * b2 * rs * third) / g;
-    } else {
-      const double al = log(rs);
-      ec = c1 * al - c2 + (c3 * al - c4) * rs;
-      v += ec - (c1 + (c3 * al - c5) * rs) * third;
-    }
-    e += r * ec;
-  }
-  return v;
-}
-
 }  // namespace
 
 // one CTA per chunk of PSC_XC_NOALLOC_CHUNK points
@@ -73,20 +47,20 @@ k_xc_noalloc(const double* __restrict__ rho, double* __restrict__ vxc, long n, d
   double e = 0.0, mx = -1e300, mn = 1e300;
   for (long i = lo + threadIdx.x; i < hi; i += 256) {
     const double r = rho[i];
-    mx = fmax(mx, r);
-    mn = fmin(mn, r);
-    vxc[i] = lda_point(r, e);
+    mx = psc_nanmax(mx, r);
+    mn = psc_nanmin(mn, r);
+    vxc[i] = psc_lda_point(r, e);
   }
   e = psc_block_sum<double, 256>(e, sh);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = psc_nanmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mn = psc_nanmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
   }
   if ((threadIdx.x & 31) == 0) { smx[threadIdx.x >> 5] = mx; smn[threadIdx.x >> 5] = mn; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < 8; ++w) { mx = fmax(mx, smx[w]); mn = fmin(mn, smn[w]); }
+    for (int w = 1; w < 8; ++w) { mx = psc_nanmax(mx, smx[w]); mn = psc_nanmin(mn, smn[w]); }
     scratch[blockIdx.x] = e;
     scratch[PSC_XC_NOALLOC_MAX_CTAS + blockIdx.x] = mx;
     scratch[2 * PSC_XC_NOALLOC_MAX_CTAS + blockIdx.x] = mn;
@@ -101,8 +75,8 @@ __global__ void k_xc_noalloc_final(const double* __restrict__ scratch, int nblk,
   if (threadIdx.x == 0) {
     double mx = -1e300, mn = 1e300;
     for (int i = 0; i < nblk; ++i) {
-      mx = fmax(mx, scratch[PSC_XC_NOALLOC_MAX_CTAS + i]);
-      mn = fmin(mn, scratch[2 * PSC_XC_NOALLOC_MAX_CTAS + i]);
+      mx = psc_nanmax(mx, scratch[PSC_XC_NOALLOC_MAX_CTAS + i]);
+      mn = psc_nanmin(mn, scratch[2 * PSC_XC_NOALLOC_MAX_CTAS + i]);
     }
     out[0] = s * h3;
     out[1] = mx;
@@ -127,10 +101,20 @@ extern "C" int psc_lda_xc_noalloc(const double* rho, double* vxc, long n, double
     psc_set_error(nullptr, std::string("psc_lda_xc_noalloc: no usable current device: ") + cudaGetErrorString(e));
     return 1;
   }
+  cudaStream_t st = (cudaStream_t)stream;
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_scratch_dev[dev]) {
+      // the address lookup may load the module: it must not happen inside a
+      // stream capture
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      e = cudaStreamIsCapturing(st, &cs);
+      if (e != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        psc_set_error(nullptr, "psc_lda_xc_noalloc: the first call on a device sets up the scratch address and "
+                               "must come before any stream capture");
+        return 2;
+      }
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_xc_scratch);
       if (e != cudaSuccess || !p) {
@@ -142,7 +126,6 @@ extern "C" int psc_lda_xc_noalloc(const double* rho, double* vxc, long n, double
     }
     scratch = g_scratch_dev[dev];
   }
-  cudaStream_t st = (cudaStream_t)stream;
   const int nblk = (int)((n + PSC_XC_NOALLOC_CHUNK - 1) / PSC_XC_NOALLOC_CHUNK);
   k_xc_noalloc<<<nblk, 256, 0, st>>>(rho, vxc, n, scratch);
   PSC_LAUNCH_CHECK((psc_ctx*)nullptr);

@@ -4,10 +4,10 @@
 // is applied as  Y[idx] += alpha * sum_a sum_m u_am * (w_a * u_am . X[idx]),
 // w_a = 1/xint_a = h^3 / Zvalue_a, never forming the n_a x n_a blocks.
 //   project: one CTA per (atom, column group) reduces w_a * U_a^T X (3 values
-//            per column) with a fixed-order block reduction;
-//   scatter: one thread per (touched grid point, column) adds the sum over
-//            the balls covering that point, in atom order.  No atomics, so the
-//            result is bitwise reproducible.
+//            per column) with warp shuffles and one fixed-order block sum;
+//   scatter: one thread per (touched grid point, group of 8 columns) adds the
+//            sum over the balls covering that point, in atom order.  No
+//            atomics, so the result is bitwise reproducible.
 #include "psc_internal.cuh"
 #include "../../include/psc.h"
 
@@ -22,8 +22,8 @@ __global__ void __launch_bounds__(128)
 k_nl_project(const T* __restrict__ X, long ldx, int k, const int* __restrict__ atom_off,
              const int* __restrict__ idx, const T* __restrict__ u, long npts, const double* __restrict__ w,
              double* __restrict__ proj) {
-  constexpr int NT = 128;
-  __shared__ double sh[NT / 32];
+  constexpr int NT = 128, NW = NT / 32;
+  __shared__ double sh[NW][3 * NL_KC];
   const int a = blockIdx.x;
   const int c0 = blockIdx.y * NL_KC;
   const int lo = atom_off[a], hi = atom_off[a + 1];
@@ -45,35 +45,59 @@ k_nl_project(const T* __restrict__ X, long ldx, int k, const int* __restrict__ a
       }
     }
   }
-  const double wa = w[a];
+  // all 3 x NL_KC sums at once: a shuffle tree per warp, then warp 0 adds
+  // the NW warp partials in warp order (fixed, so the result is reproducible)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int m = 0; m < 3; ++m)
 #pragma unroll
     for (int c = 0; c < NL_KC; ++c) {
-      double s = psc_block_sum<double, NT>(acc[m][c], sh);
-      if (threadIdx.x == 0 && c0 + c < k) proj[((long)a * 3 + m) * k + c0 + c] = wa * s;
+      const double v = psc_warp_sum(acc[m][c]);
+      if (lane == 0) sh[wid][m * NL_KC + c] = v;
     }
+  __syncthreads();
+  if (threadIdx.x < 3 * NL_KC) {
+    const int m = threadIdx.x / NL_KC, c = threadIdx.x % NL_KC;
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < NW; ++q) s += sh[q][threadIdx.x];
+    if (c0 + c < k) proj[((long)a * 3 + m) * k + c0 + c] = w[a] * s;
+  }
 }
 
+// One thread per (touched grid point, group of NL_SC columns): the entries
+// covering the point and their u values are read once and used for every
+// column of the group; each column's sum runs over the entries in atom
+// order (no atomics, so the result is bitwise reproducible).
+constexpr int NL_SC = 8;
 template <typename T>
 __global__ void k_nl_scatter(T* Y, long ldy, int k, long ntouched, const int* __restrict__ t_idx,
                              const int* __restrict__ t_off, const int* __restrict__ t_ent,
                              const int* __restrict__ pt_atom, const T* __restrict__ u, long npts,
                              const double* __restrict__ proj, const double* __restrict__ coef, double ha) {
   const double alpha = coef ? coef[0] : ha;
-  const long total = ntouched * (long)k;
+  const int ngrp = (k + NL_SC - 1) / NL_SC;
+  const long total = ntouched * (long)ngrp;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
     const long pt = t % ntouched;
-    const int c = (int)(t / ntouched);
-    double s = 0.0;
+    const int c0 = (int)(t / ntouched) * NL_SC;
+    const int nc = min(NL_SC, k - c0);
+    double s[NL_SC];
+#pragma unroll
+    for (int c = 0; c < NL_SC; ++c) s[c] = 0.0;
     for (int e = t_off[pt]; e < t_off[pt + 1]; ++e) {
       const int p = t_ent[e];
       const int a = pt_atom[p];
-      const double* pr = proj + (long)a * 3 * k + c;
-      s += (double)u[p] * pr[0] + (double)u[npts + p] * pr[k] + (double)u[2 * npts + p] * pr[2 * k];
+      const double u0 = (double)u[p], u1 = (double)u[npts + p], u2 = (double)u[2 * npts + p];
+      const double* pr = proj + (long)a * 3 * k + c0;
+#pragma unroll
+      for (int c = 0; c < NL_SC; ++c)
+        if (c < nc) s[c] += u0 * pr[c] + u1 * pr[k + c] + u2 * pr[2 * k + c];
     }
-    T* yp = Y + (long)t_idx[pt] + (long)c * ldy;
-    *yp = (T)((double)*yp + alpha * s);
+    T* yp = Y + (long)t_idx[pt] + (long)c0 * ldy;
+#pragma unroll
+    for (int c = 0; c < NL_SC; ++c)
+      if (c < nc) yp[(long)c * ldy] = (T)((double)yp[(long)c * ldy] + alpha * s[c]);
   }
 }
 
@@ -103,7 +127,7 @@ int psc_nl_project(psc_ctx* ctx, int dtype, const void* X, long ldx, int k, cuda
 
 int psc_nl_scatter(psc_ctx* ctx, int dtype, void* Y, long ldy, int k, const double* coef, double a,
                    cudaStream_t st) {
-  const long total = ctx->nl_touched * (long)k;
+  const long total = ctx->nl_touched * (long)((k + NL_SC - 1) / NL_SC);
   const int nb = (int)std::min<long>(148L * 16, (total + 255) / 256);
   if (dtype == PSC_F64)
     k_nl_scatter<double><<<nb, 256, 0, st>>>((double*)Y, ldy, k, ctx->nl_touched, ctx->nl_t_idx,
@@ -126,6 +150,8 @@ void psc_free_projectors(psc_ctx* ctx) {
   ctx->nl_proj_bytes = 0;
   ctx->nl_atoms = 0; ctx->nl_points = 0; ctx->nl_touched = 0;
 }
+
+int psc_nl_apply_mask(psc_ctx* ctx, cudaStream_t st);
 
 // setup.cu
 int psc_nl_box_distances(psc_ctx* ctx, int nbox, const int* box_dev /* [nbox][8] */, const double* xyz_dev,
@@ -261,10 +287,36 @@ extern "C" int psc_projector_setup(psc_ctx* ctx, int natoms, const int* species,
   PSC_CUDA(ctx, cudaMemcpyAsync(pt_orig_d, pt_orig.data(), npts * sizeof(int), cudaMemcpyHostToDevice, st));
   int rc = psc_nl_eval_u(ctx, npts, ctx->nl_idx, pt_orig_d, asp_d, xyz_d, radius, ctx->nl_u64, st);
   if (!rc) rc = psc_cast(ctx, PSC_F32, ctx->nl_u64, ctx->nl_u32, 3 * npts, st);
+  if (!rc) rc = psc_nl_apply_mask(ctx, st);
   PSC_CUDA(ctx, cudaStreamSynchronize(st));
   psc_dfree(pt_orig_d);
   cleanup();
   return rc;
+}
+
+// Sphere mask: the projector functions vanish at ball points outside the
+// sphere (their rows and columns of V_nl are those of masked points).
+__global__ void k_nl_mask(double* u64, float* u32, const int* __restrict__ idx, long npts, int nx, int ny, double h,
+                          double cx, double cy, double cz, double r2) {
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npts; p += (long)gridDim.x * blockDim.x) {
+    const long g = idx[p];
+    const double x = (g % nx) * h - cx, y = ((g / nx) % ny) * h - cy, z = (g / ((long)nx * ny)) * h - cz;
+    if (x * x + y * y + z * z > r2)
+      for (int m = 0; m < 3; ++m) {
+        u64[m * npts + p] = 0.0;
+        u32[m * npts + p] = 0.0f;
+      }
+  }
+}
+
+int psc_nl_apply_mask(psc_ctx* ctx, cudaStream_t st) {
+  if (ctx->mask_r2 <= 0.0 || ctx->nl_points == 0) return 0;
+  const long npts = ctx->nl_points;
+  k_nl_mask<<<(int)std::min<long>(148L * 8, (npts + 255) / 256), 256, 0, st>>>(
+      ctx->nl_u64, ctx->nl_u32, ctx->nl_idx, npts, ctx->nx, ctx->ny, ctx->h, ctx->mask_c[0], ctx->mask_c[1],
+      ctx->mask_c[2], ctx->mask_r2);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
 }
 
 // Copy the projector tables out (for checks against the reference's V_nl).

@@ -23,8 +23,8 @@
 //   C  ro1 from all partials; the stop decision and beta are then identical
 //      in every CTA.
 // The grid barrier is a monotone arrival counter with a bounded spin: a CTA
-// that waits more than 2^26 polls records status[4] and stops waiting, so a
-// fault can never hang the GPU.  Every CTA takes the same number of barriers.
+// that waits more than 4x the context's wait limit (2^26 polls by default)
+// records status[4] and stops waiting, so a fault can never hang the GPU.  Every CTA takes the same number of barriers.
 #include "psc_internal.cuh"
 #include "../../include/psc.h"
 
@@ -32,9 +32,9 @@
 
 namespace {
 constexpr int PNT = 1024;
-constexpr long BAR_LIMIT = 1L << 26;
 
-__device__ __forceinline__ void grid_barrier(unsigned int* ctr, unsigned int target, int* status, bool& failed) {
+__device__ __forceinline__ void grid_barrier(unsigned int* ctr, unsigned int target, int* status, bool& failed,
+                                             long limit) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -45,7 +45,7 @@ __device__ __forceinline__ void grid_barrier(unsigned int* ctr, unsigned int tar
         unsigned int v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
         if (v >= target) break;
-        if (++spins > BAR_LIMIT) {
+        if (++spins > limit) {
           failed = true;
           atomicExch(&status[4], 1);
           break;
@@ -76,7 +76,7 @@ template <int R>
 __global__ void __launch_bounds__(PNT, 1)
 k_cg_persistent(const double* __restrict__ rhs, double* __restrict__ xg, double* rg, int nx, int ny, int nz,
                 double c0, double4 cw, int chunk, double* part, unsigned int* bar, int* status, double tol,
-                int maxit, double* out) {
+                int maxit, double* out, long bar_limit) {
   extern __shared__ double sm[];
   __shared__ double sh[PNT / 32];
   __shared__ double bc[2];
@@ -150,7 +150,7 @@ k_cg_persistent(const double* __restrict__ rhs, double* __restrict__ xg, double*
   }
   rr = psc_block_sum<double, PNT>(rr, sh);
   if (threadIdx.x == 0) part[G + blockIdx.x] = rr;
-  grid_barrier(bar, (++nbar) * G, status, failed);
+  grid_barrier(bar, (++nbar) * G, status, failed, bar_limit);
   double ro = grid_sum(part + G, G, &bc[0]);
   const double tol1 = tol * tol * ro;
   int it = 0;
@@ -175,7 +175,7 @@ k_cg_persistent(const double* __restrict__ rhs, double* __restrict__ xg, double*
     }
     pap = psc_block_sum<double, PNT>(pap, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = pap;
-    grid_barrier(bar, (++nbar) * G, status, failed);
+    grid_barrier(bar, (++nbar) * G, status, failed, bar_limit);
     pap = grid_sum(part, G, &bc[0]);
     // B: alpha, updates, partial of r.r
     const double alp = ro / pap;
@@ -189,7 +189,7 @@ k_cg_persistent(const double* __restrict__ rhs, double* __restrict__ xg, double*
     }
     rr = psc_block_sum<double, PNT>(rr, sh);
     if (threadIdx.x == 0) part[G + blockIdx.x] = rr;
-    grid_barrier(bar, (++nbar) * G, status, failed);
+    grid_barrier(bar, (++nbar) * G, status, failed, bar_limit);
     // C: stop test and beta, identical in every CTA
     const double ro1 = grid_sum(part + G, G, &bc[1]);
     beta = ro1 / ro;
@@ -254,8 +254,10 @@ int psc_pcg_persistent(psc_ctx* ctx, const double* rhs, double* x, int maxit, do
   double c0 = ctx->lap_c0;
   int chunk_i = (int)chunk;
   double* part = ctx->cg_part;
+  long bar_limit = 4 * ctx->wait_limit;   // grid barriers wait 4x longer than the mbarrier pipelines
   void* args[] = {(void*)&rhs, (void*)&x, (void*)&rg, (void*)&nx, (void*)&ny, (void*)&nz, (void*)&c0, (void*)&cw,
-                  (void*)&chunk_i, (void*)&part, (void*)&bar, (void*)&status, (void*)&tol, (void*)&maxit, (void*)&out};
+                  (void*)&chunk_i, (void*)&part, (void*)&bar, (void*)&status, (void*)&tol, (void*)&maxit, (void*)&out,
+                  (void*)&bar_limit};
   PSC_CUDA(ctx, cudaLaunchCooperativeKernel(fn, dim3(G), dim3(PNT), args, smem, st));
   PSC_LAUNCH_CHECK(ctx);
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->host_scalars + 80, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));

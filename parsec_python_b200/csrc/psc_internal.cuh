@@ -19,6 +19,9 @@
 #define PSC_MAX_K 1024        // widest subspace block accepted
 #define PSC_RED_BLOCKS 592    // fixed partial-sum count of the deterministic reductions (4 x 148 SMs)
 #define PSC_RED_SLOTS 16      // simultaneous dot products per reduction launch
+#define PSC_NORM_CHUNKS 32    // row chunks of the column-norm partial sums
+#define PSC_WAIT_DEFAULT (1L << 24)  // polls of a bounded device-side wait before it gives up
+#define PSC_DRAIN_WAIT (1L << 24)    // polls spent, after a failed wait, on copies and MMAs already issued
 
 enum { PSC_F64 = 0, PSC_F32 = 1 };
 
@@ -103,6 +106,19 @@ struct psc_ctx {
   size_t tc_part_floats = 0;
   void* tc_pairs = nullptr;      // int2 tile pairs (upper triangle)
   int tc_pairs_k = 0;
+  // tensor-core block product W T (mixed precision Rayleigh-Ritz)
+  int gemm_tc = 1;               // 1: FP32 W T on tcgen05 (3xTF32), 0: CUDA cores
+  float* tsplit = nullptr;       // T split into TF32 hi/lo B tiles
+  size_t tsplit_floats = 0;
+  // sphere mask of the Hamiltonian (0: the whole cube): H X is zero at
+  // points farther than sqrt(mask_r2) from mask_c (the cube's centre)
+  double mask_r2 = 0.0;
+  double mask_c[3] = {0.0, 0.0, 0.0};
+  // polls of every bounded device-side wait before it gives up (status words 3-6)
+  long wait_limit = PSC_WAIT_DEFAULT;
+  // exact squared column norms of FP32 blocks (density normalisation)
+  double* col_norm_part = nullptr;  // [cap][PSC_NORM_CHUNKS]
+  int col_norm_cap = 0;
 
   // TMA stencil work tables (column, slab, z range per CTA), one per launch shape
   struct StencilSched {
@@ -235,6 +251,43 @@ __device__ __forceinline__ T psc_block_sum(T v, T* sh /* >= NT/32 */) {
   return r;
 }
 
+// Ceperley-Alder / Perdew-Zunger LDA of one density value r (electrons per
+// bohr^3), V_xc/exc_nspn.py:73-91: returns v_xc (Ry) and adds the point's
+// energy density 0.75 r v_x + r eps_c to e.  Points with r <= 0 give 0.
+// Shared by k_xc (scf.cu) and k_xc_noalloc (noalloc.cu).
+__device__ __forceinline__ double psc_lda_point(double r, double& e) {
+  const double g = -0.2846, b1 = 1.0529, b2 = 0.3334;
+  const double c1 = 0.0622, c2 = 0.096, c3 = 0.004, c4 = 0.0232, c5 = 0.0192;
+  const double third = 1.0 / 3.0;
+  const double pi = 3.141592653589793;
+  const double a0 = pow(4.0 / (9.0 * pi), third);
+  const double twovpia0 = 2.0 / (pi * a0);
+  const double p75vpi = 0.75 / pi;
+  double v = 0.0;
+  if (r > 0.0) {
+    const double rs = pow(p75vpi / r, third);
+    v = -twovpia0 / rs;
+    double ec;
+    e += 0.75 * r * v;
+    if (rs >= 1.0) {
+      const double sq = sqrt(rs);
+      ec = g / (1.0 + b1 * sq + b2 * rs);
+      v += (ec * ec) * (1.0 + 3.5 * b1 * sq * third + 4.0 * b2 * rs * third) / g;
+    } else {
+      const double al = log(rs);
+      ec = c1 * al - c2 + (c3 * al - c4) * rs;
+      v += ec - (c1 + (c3 * al - c5) * rs) * third;
+    }
+    e += r * ec;
+  }
+  return v;
+}
+
+// max / min that propagate NaN, as numpy.max / numpy.min do (fmax / fmin
+// would drop it)
+__device__ __forceinline__ double psc_nanmax(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
+__device__ __forceinline__ double psc_nanmin(double a, double b) { return (a != a || b != b) ? a + b : fmin(a, b); }
+
 // ---------------------------------------------------------------------------
 // cross-unit host entry points used internally
 // ---------------------------------------------------------------------------
@@ -258,6 +311,11 @@ int psc_laplacian_fused(psc_ctx* ctx, const double* x, const double* prev, doubl
                         double g, double* dot_partial, int* nblocks, cudaStream_t st);
 int psc_random_impl(psc_ctx* ctx, int dtype, int dist, unsigned long long seed, void* out, long ld,
                     long rows, int cols, cudaStream_t st);
+// zero the points outside the sphere mask in k columns (no-op without a mask)
+int psc_mask_block_impl(psc_ctx* ctx, int dtype, void* X, long ld, int k, cudaStream_t st);
+// FP32 block product W T on tensor cores; -1 when it does not apply
+int psc_gemm_tall_tc(psc_ctx* ctx, const float* W, long ld, int k, const double* Tm, int kout, float* O, long ldo,
+                     cudaStream_t st);
 // FP32 Gram pair on tensor cores; -1 when it does not apply
 int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int k, double* S, double* K,
                      cudaStream_t st);

@@ -239,10 +239,18 @@ extern "C" int psc_occupations(psc_ctx* ctx, const double* lam_dev, int n, doubl
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_density(const T* __restrict__ W, long ld, int nev, const double* __restrict__ occ,
-                          const double* __restrict__ rho0, double* __restrict__ rho, double* __restrict__ hrhs,
-                          long n, double fourpi_h3, double h3) {
+                          const double* __restrict__ norm_part, const double* __restrict__ rho0,
+                          double* __restrict__ rho, double* __restrict__ hrhs, long n, double fourpi_h3, double h3) {
   __shared__ double f2[1024];
-  for (int i = threadIdx.x; i < nev; i += blockDim.x) f2[i] = 2 * occ[i];
+  for (int i = threadIdx.x; i < nev; i += blockDim.x) {
+    double w = 2 * occ[i];
+    if (norm_part) {
+      double nn = 0.0;
+      for (int c = 0; c < PSC_NORM_CHUNKS; ++c) nn += norm_part[(long)i * PSC_NORM_CHUNKS + c];
+      w /= nn;
+    }
+    f2[i] = w;
+  }
   __syncthreads();
   for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     double s = 0.0;
@@ -255,17 +263,54 @@ __global__ void k_density(const T* __restrict__ W, long ld, int nev, const doubl
   }
 }
 
+// Exact FP64 squared norms of the columns of an FP32 block, as
+// PSC_NORM_CHUNKS partial sums per column (summed in a fixed order by the
+// consumer).  FP32 blocks carry a small column-scale error (the tensor cores'
+// FP32 accumulation rounds toward zero, FP32 storage rounds each entry);
+// the density divides each orbital's weight by its measured norm so that the
+// electron count stays exact.
+__global__ void __launch_bounds__(256)
+k_colnorm_part(const float* __restrict__ W, long ld, long n, long chunk, double* __restrict__ part) {
+  __shared__ double sh[8];
+  const int col = blockIdx.y;
+  const long r0 = (long)blockIdx.x * chunk;
+  const long r1 = min(n, r0 + chunk);
+  const float* w = W + (long)col * ld;
+  double s = 0.0;
+  for (long p = r0 + threadIdx.x; p < r1; p += 256) {
+    const double v = (double)w[p];
+    s = fma(v, v, s);
+  }
+  s = psc_block_sum<double, 256>(s, sh);
+  if (threadIdx.x == 0) part[(long)col * PSC_NORM_CHUNKS + blockIdx.x] = s;
+}
+
 extern "C" int psc_density(psc_ctx* ctx, int dtype, const void* W, long ld, int nev, const double* occ_dev,
                            const double* rho0, double fourpi_h3, double h3, double* rho, double* hrhs,
                            void* stream) {
   if (!ctx) return 2;
   PSC_REQUIRE(ctx, nev >= 1 && nev <= 1024, "density: nev out of range");
+  PSC_REQUIRE(ctx, W && occ_dev && rho && ld >= ctx->n && (!hrhs || rho0), "density: bad arguments");
   cudaStream_t st = (cudaStream_t)stream;
   const int nb = 148 * 8;
-  if (dtype == PSC_F64)
-    k_density<double><<<nb, 256, 0, st>>>((const double*)W, ld, nev, occ_dev, rho0, rho, hrhs, ctx->n, fourpi_h3, h3);
-  else
-    k_density<float><<<nb, 256, 0, st>>>((const float*)W, ld, nev, occ_dev, rho0, rho, hrhs, ctx->n, fourpi_h3, h3);
+  if (dtype == PSC_F64) {
+    k_density<double><<<nb, 256, 0, st>>>((const double*)W, ld, nev, occ_dev, nullptr, rho0, rho, hrhs, ctx->n,
+                                          fourpi_h3, h3);
+  } else {
+    if (ctx->col_norm_cap < nev) {
+      psc_dfree(ctx->col_norm_part);
+      ctx->col_norm_part = nullptr;
+      ctx->col_norm_cap = 0;
+      PSC_CUDA(ctx, psc_dmalloc(&ctx->col_norm_part, (size_t)1024 * PSC_NORM_CHUNKS * sizeof(double)));
+      ctx->col_norm_cap = 1024;
+    }
+    const long chunk = (ctx->n + PSC_NORM_CHUNKS - 1) / PSC_NORM_CHUNKS;
+    k_colnorm_part<<<dim3(PSC_NORM_CHUNKS, nev), 256, 0, st>>>((const float*)W, ld, ctx->n, chunk,
+                                                               ctx->col_norm_part);
+    PSC_LAUNCH_CHECK(ctx);
+    k_density<float><<<nb, 256, 0, st>>>((const float*)W, ld, nev, occ_dev, ctx->col_norm_part, rho0, rho, hrhs,
+                                         ctx->n, fourpi_h3, h3);
+  }
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }
@@ -276,37 +321,13 @@ extern "C" int psc_density(psc_ctx* ctx, int dtype, const void* W, long ld, int 
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 k_xc(const double* __restrict__ rho, double* __restrict__ vxc, long n, double* __restrict__ partial) {
-  const double g = -0.2846, b1 = 1.0529, b2 = 0.3334;
-  const double c1 = 0.0622, c2 = 0.096, c3 = 0.004, c4 = 0.0232, c5 = 0.0192;
-  const double third = 1.0 / 3.0;
-  const double pi = 3.141592653589793;
-  const double a0 = pow(4.0 / (9.0 * pi), third);
-  const double twovpia0 = 2.0 / (pi * a0);
-  const double p75vpi = 0.75 / pi;
   __shared__ double sh[8];
   double e = 0.0, mx = -1e300, mn = 1e300;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     const double r = rho[i];
-    mx = fmax(mx, r);
-    mn = fmin(mn, r);
-    double v = 0.0;
-    if (r > 0.0) {
-      const double rs = pow(p75vpi / r, third);
-      v = -twovpia0 / rs;
-      double ec;
-      e += 0.75 * r * v;
-      if (rs >= 1.0) {
-        const double sq = sqrt(rs);
-        ec = g / (1.0 + b1 * sq + b2 * rs);
-        v += (ec * ec) * (1.0 + 3.5 * b1 * sq * third + 4.0 * b2 * rs * third) / g;
-      } else {
-        const double al = log(rs);
-        ec = c1 * al - c2 + (c3 * al - c4) * rs;
-        v += ec - (c1 + (c3 * al - c5) * rs) * third;
-      }
-      e += r * ec;
-    }
-    vxc[i] = v;
+    mx = psc_nanmax(mx, r);
+    mn = psc_nanmin(mn, r);
+    vxc[i] = psc_lda_point(r, e);
   }
   e = psc_block_sum<double, 256>(e, sh);
   if (threadIdx.x == 0) partial[blockIdx.x] = e;
@@ -314,13 +335,13 @@ k_xc(const double* __restrict__ rho, double* __restrict__ vxc, long n, double* _
   __shared__ double smx[8], smn[8];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = psc_nanmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mn = psc_nanmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
   }
   if ((threadIdx.x & 31) == 0) { smx[threadIdx.x >> 5] = mx; smn[threadIdx.x >> 5] = mn; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < 8; ++w) { mx = fmax(mx, smx[w]); mn = fmin(mn, smn[w]); }
+    for (int w = 1; w < 8; ++w) { mx = psc_nanmax(mx, smx[w]); mn = psc_nanmin(mn, smn[w]); }
     partial[PSC_RED_BLOCKS + blockIdx.x] = mx;
     partial[2 * PSC_RED_BLOCKS + blockIdx.x] = mn;
   }
@@ -334,8 +355,8 @@ __global__ void k_xc_final(const double* partial, double h3, double* out) {
   if (threadIdx.x == 0) {
     double mx = -1e300, mn = 1e300;
     for (int i = 0; i < PSC_RED_BLOCKS; ++i) {
-      mx = fmax(mx, partial[PSC_RED_BLOCKS + i]);
-      mn = fmin(mn, partial[2 * PSC_RED_BLOCKS + i]);
+      mx = psc_nanmax(mx, partial[PSC_RED_BLOCKS + i]);
+      mn = psc_nanmin(mn, partial[2 * PSC_RED_BLOCKS + i]);
     }
     out[0] = s * h3;
     out[1] = mx;
@@ -344,7 +365,11 @@ __global__ void k_xc_final(const double* partial, double h3, double* out) {
 }
 
 extern "C" int psc_lda_xc(psc_ctx* ctx, const double* rho, double* vxc, double h3, double* out_dev, void* stream) {
-  if (!ctx) return 2;
+  if (!ctx) {
+    psc_set_error(nullptr, "psc_lda_xc: NULL context");
+    return 2;
+  }
+  PSC_REQUIRE(ctx, rho && vxc && out_dev, "psc_lda_xc: NULL pointer argument");
   cudaStream_t st = (cudaStream_t)stream;
   k_xc<<<PSC_RED_BLOCKS, 256, 0, st>>>(rho, vxc, ctx->n, ctx->red_partial);
   PSC_LAUNCH_CHECK(ctx);

@@ -166,17 +166,53 @@ static int launch_stencil_t(psc_ctx* ctx, const StencilPlan& p, const T* X, long
 
 template <typename T>
 int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy, const T* pot,
-                    const double* w, const double* coef, double a, double b, double g, cudaStream_t st);
+                    const double* w, const double* coef, double a, double b, double g, bool masked,
+                    cudaStream_t st);
+
+// Sphere mask: zero every point of k columns farther than sqrt(mask_r2)
+// from the cube's centre.
+template <typename T>
+__global__ void k_apply_mask(T* X, long ld, int k, int nx, int ny, long n, double h, double cx, double cy, double cz,
+                             double r2) {
+  const long total = n * (long)k;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long p = e % n;
+    const int c = (int)(e / n);
+    const double x = (p % nx) * h - cx, y = ((p / nx) % ny) * h - cy, z = (p / ((long)nx * ny)) * h - cz;
+    if (x * x + y * y + z * z > r2) X[p + (long)c * ld] = T(0);
+  }
+}
+
+int psc_mask_block_impl(psc_ctx* ctx, int dtype, void* X, long ld, int k, cudaStream_t st) {
+  if (ctx->mask_r2 <= 0.0 || k < 1) return 0;
+  const long total = ctx->n * (long)k;
+  const int nb = (int)std::min<long>(148L * 16, (total + 255) / 256);
+  if (dtype == PSC_F64)
+    k_apply_mask<double><<<nb, 256, 0, st>>>((double*)X, ld, k, ctx->nx, ctx->ny, ctx->n, ctx->h, ctx->mask_c[0],
+                                             ctx->mask_c[1], ctx->mask_c[2], ctx->mask_r2);
+  else
+    k_apply_mask<float><<<nb, 256, 0, st>>>((float*)X, ld, k, ctx->nx, ctx->ny, ctx->n, ctx->h, ctx->mask_c[0],
+                                            ctx->mask_c[1], ctx->mask_c[2], ctx->mask_r2);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
 
 template <typename T>
 static int launch_stencil(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy,
                           const T* pot, const double* c0c, const double* coef, double a, double b,
-                          double g, double* dot_partial, int* nblocks_out, cudaStream_t st) {
+                          double g, double* dot_partial, int* nblocks_out, cudaStream_t st, bool masked = false) {
   // the TMA pipeline serves every launch that needs no fused dot product and
   // meets the bulk-copy alignment rules; the register-queue kernel the rest
+  // (followed by a masking pass when the Hamiltonian is sphere-masked)
   if (!dot_partial && ctx->stencil_impl == 0) {
-    const int rc = psc_stencil_tma<T>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, c0c, coef, a, b, g, st);
+    const int rc = psc_stencil_tma<T>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, c0c, coef, a, b, g, masked, st);
     if (rc >= 0) return rc;
+  }
+  if (masked && ctx->mask_r2 > 0.0) {
+    const int rc = launch_stencil<T>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, c0c, coef, a, b, g, dot_partial,
+                                     nblocks_out, st, false);
+    if (rc) return rc;
+    return psc_mask_block_impl(ctx, sizeof(T) == 8 ? PSC_F64 : PSC_F32, Y, ldy, k, st);
   }
   StencilPlan p = plan_stencil(ctx, k, sizeof(T));
   if (nblocks_out) *nblocks_out = (int)(p.grid.x * p.grid.y * p.grid.z);
@@ -229,10 +265,10 @@ int psc_apply_h_impl(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, 
   int rc;
   if (dtype == PSC_F64)
     rc = launch_stencil<double>(ctx, k, (const double*)X, ldx, (const double*)P, ldp, (double*)Y, ldy,
-                                ctx->pot64, w, coef_dev, a, b, g, nullptr, nullptr, st);
+                                ctx->pot64, w, coef_dev, a, b, g, nullptr, nullptr, st, true);
   else
     rc = launch_stencil<float>(ctx, k, (const float*)X, ldx, (const float*)P, ldp, (float*)Y, ldy,
-                               ctx->pot32, w, coef_dev, a, b, g, nullptr, nullptr, st);
+                               ctx->pot32, w, coef_dev, a, b, g, nullptr, nullptr, st, true);
   if (rc) return rc;
   if (ctx->nl_atoms > 0) return psc_nl_scatter(ctx, dtype, Y, ldy, k, coef_dev, a, st);
   return 0;
@@ -329,9 +365,35 @@ extern "C" int psc_cheb_filter(psc_ctx* ctx, int dtype, int mode, int deg, const
 }
 
 // 0: TMA pipeline wherever it applies (default), 1: register-queue kernel only.
+// Sphere-masked Hamiltonian: H X = P (0.5 A + V_nl + diag(pot)) X with P
+// zeroing the points farther than `radius` (bohr) from the cube's centre;
+// radius <= 0 restores the cube.  The projector tables lose their points
+// outside the sphere.  Meant for blocks that vanish outside the sphere (the
+// solver masks its random start); there the masked operator is P H P.
+int psc_nl_apply_mask(psc_ctx* ctx, cudaStream_t st);
+extern "C" int psc_set_sphere_mask(psc_ctx* ctx, double radius, void* stream) {
+  if (!ctx) return 2;
+  ctx->mask_r2 = radius > 0.0 ? radius * radius : 0.0;
+  ctx->mask_c[0] = 0.5 * ctx->h * (ctx->nx - 1);
+  ctx->mask_c[1] = 0.5 * ctx->h * (ctx->ny - 1);
+  ctx->mask_c[2] = 0.5 * ctx->h * (ctx->nz - 1);
+  // masked work tables depend on the radius: drop the cached ones once the
+  // launches that may still read them have finished
+  PSC_CUDA(ctx, cudaStreamSynchronize((cudaStream_t)stream));
+  for (auto& e : ctx->st_sched) psc_dfree(e.dev);
+  ctx->st_sched.clear();
+  return psc_nl_apply_mask(ctx, (cudaStream_t)stream);
+}
+
+extern "C" int psc_mask_block(psc_ctx* ctx, int dtype, void* X, long ld, int k, void* stream) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, X && ld >= ctx->n && k >= 0, "mask_block: bad arguments");
+  return psc_mask_block_impl(ctx, dtype, X, ld, k, (cudaStream_t)stream);
+}
+
 extern "C" int psc_set_stencil_impl(psc_ctx* ctx, int impl) {
   if (!ctx) return 2;
-  PSC_REQUIRE(ctx, impl == 0 || impl == 1, "stencil impl must be 0 or 1");
+  PSC_REQUIRE(ctx, impl >= 0 && impl <= 2, "stencil impl must be 0, 1 or 2");
   ctx->stencil_impl = impl;
   return 0;
 }

@@ -19,13 +19,15 @@
 // each thread reads back itself (no block-wide handshake).  D planes of X are
 // in flight per CTA at all times, which is what keeps HBM busy.
 //
-// Every mbarrier wait is bounded: on timeout the CTA records the failure in
-// status[3] and carries on without waiting (results are then garbage but the
-// GPU is never hung).  Every bulk copy issued is waited for before the CTA
-// exits.
+// Every mbarrier wait is bounded by the context's wait limit: on timeout the
+// CTA records the failure in status[3], stops issuing copies and carries on
+// without waiting (results are then garbage but the GPU is never hung).
+// Every bulk copy issued is waited for before the CTA exits.
 #include "psc_internal.cuh"
 #include "../../include/psc.h"
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <functional>
@@ -61,7 +63,6 @@ constexpr int PP_SLOTS = PSC_STENCIL_PP_SLOTS;  // Prev/pot slots: the plane in 
 #define PSC_STENCIL_SYNC_EVERY 2
 #endif
 constexpr int SYNC_EVERY = PSC_STENCIL_SYNC_EVERY;  // planes between block barriers
-constexpr long WAIT_LIMIT = 1L << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -87,15 +88,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // bounded wait; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long i = 0; i < WAIT_LIMIT; ++i)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long limit) {
+  for (long i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
 
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
@@ -108,45 +106,48 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
-// 16-byte vectors: two FP64 or four FP32 points per thread
-template <typename T>
+// Points per thread: 16-byte vectors (two FP64 or four FP32 points), or
+// 8-byte vectors of two FP32 points when nx is only even (the runs then never
+// cross a row, so the x terms need no per-point masks).
+template <typename T, int VW>
 struct VecOf;
 template <>
-struct VecOf<double> {
+struct VecOf<double, 2> {
   using type = double2;
-  static constexpr int W = 2;
 };
 template <>
-struct VecOf<float> {
+struct VecOf<float, 4> {
   using type = float4;
-  static constexpr int W = 4;
+};
+template <>
+struct VecOf<float, 2> {
+  using type = float2;
 };
 
-template <typename T>
+template <int VW, typename T>
 __device__ __forceinline__ void vload(const T* p, T* out) {
-  using V = typename VecOf<T>::type;
+  using V = typename VecOf<T, VW>::type;
   const V v = *reinterpret_cast<const V*>(p);
   const T* e = reinterpret_cast<const T*>(&v);
 #pragma unroll
-  for (int j = 0; j < VecOf<T>::W; ++j) out[j] = e[j];
+  for (int j = 0; j < VW; ++j) out[j] = e[j];
 }
 
-template <typename T>
+template <int VW, typename T>
 __device__ __forceinline__ void vstore(T* p, const T* in) {
-  using V = typename VecOf<T>::type;
+  using V = typename VecOf<T, VW>::type;
   V v;
   T* e = reinterpret_cast<T*>(&v);
 #pragma unroll
-  for (int j = 0; j < VecOf<T>::W; ++j) e[j] = in[j];
+  for (int j = 0; j < VW; ++j) e[j] = in[j];
   *reinterpret_cast<V*>(p) = v;
 }
 
 // load VW consecutive values from an address aligned to A elements (A | VW)
-template <typename T, int A>
+template <typename T, int A, int VW>
 __device__ __forceinline__ void vload_a(const T* p, T* out) {
-  constexpr int VW = VecOf<T>::W;
   if constexpr (A == VW) {
-    vload(p, out);
+    vload<VW>(p, out);
   } else if constexpr (A == 2) {
     using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
 #pragma unroll
@@ -161,9 +162,18 @@ __device__ __forceinline__ void vload_a(const T* p, T* out) {
   }
 }
 
-template <typename T>
+// per-thread asynchronous copy of one run (VW points) into shared memory
+template <int BYTES>
+__device__ __forceinline__ void cp_async_run(void* dst, const void* src) {
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+template <int VW>
 __host__ __device__ constexpr int slab_points() {
-  return VecOf<T>::W * TNT;
+  return VW * TNT;
 }
 
 template <typename T>
@@ -180,6 +190,10 @@ struct TmaArgs {
   T c0, c[4];
   const double* coef;
   double a, b, g;
+  long wait_limit;    // polls of each mbarrier wait before the CTA gives up
+  // sphere mask: outputs at points with (i h - cx)^2 + (j h - cy)^2 +
+  // (l h - cz)^2 > mask_r2 are zero (mask_r2 = 0: the whole cube)
+  double mask_r2, h, cx, cy, cz;
   int* status;
 };
 
@@ -187,11 +201,10 @@ struct TmaArgs {
 
 // YA: alignment (in elements) of the y-neighbour rows, the largest of VW, 2, 1
 // that divides nx; their loads are split to match.
-template <typename T, int R, int YA>
+template <typename T, int R, int YA, int VW>
 __global__ void __launch_bounds__(TNT)
 k_stencil_tma(TmaArgs<T> A) {
-  constexpr int VW = VecOf<T>::W;          // points per thread
-  constexpr int TS = slab_points<T>();     // points per slab
+  constexpr int TS = slab_points<VW>();    // points per slab (VW per thread)
   constexpr int NBUF = R + 1 + prefetch_depth<T>();   // X plane windows resident
   constexpr int NS = PP_SLOTS;
   constexpr int Q = 2 * R + 1;             // z queue length
@@ -214,6 +227,19 @@ k_stencil_tma(TmaArgs<T> A) {
   const int slab0 = work.y * TS;
   const int z0 = work.z;
   const int z1 = work.w;
+  if (work.x < 0) {
+    // sphere mask: planes of this slab that hold no point inside the sphere;
+    // the output is zero there and nothing is read
+    const int loc0 = VW * threadIdx.x;
+    if (loc0 < min(TS, nxy - slab0)) {
+      T zv[VW];
+#pragma unroll
+      for (int j = 0; j < VW; ++j) zv[j] = T(0);
+      T* Yz = A.Y + (long)(-1 - work.x) * A.ldy + slab0 + loc0;
+      for (int z = z0; z < z1; ++z) vstore<VW>(Yz + (long)z * nxy, zv);
+    }
+    return;
+  }
   const int zlast = min(nz, z1 + R);  // X planes needed: [z0 - R, z1 + R) within [0, nz)
   const long col = work.x;
   const T* Xc = A.X + col * A.ldx;
@@ -275,8 +301,8 @@ k_stencil_tma(TmaArgs<T> A) {
   auto copy_pp = [&](int z) {
     if (own && z < z1) {
       T* d = pring + (size_t)((z - z0) % NS) * 2 * TS + loc;
-      if (Pc) cp_async16(d, Pc + (long)z * nxy + q);
-      if (has_pot) cp_async16(d + TS, A.pot + (long)z * nxy + q);
+      if (Pc) cp_async_run<VW * sizeof(T)>(d, Pc + (long)z * nxy + q);
+      if (has_pot) cp_async_run<VW * sizeof(T)>(d + TS, A.pot + (long)z * nxy + q);
     }
     cp_async_commit();
   };
@@ -292,21 +318,25 @@ k_stencil_tma(TmaArgs<T> A) {
     for (int j = 0; j < VW; ++j) zq[j][i] = T(0);
     if (zz < z0 && own && zz >= 0) {
       T v[VW];
-      vload(Xc + (long)zz * nxy + q, v);
+      vload<VW>(Xc + (long)zz * nxy + q, v);
 #pragma unroll
       for (int j = 0; j < VW; ++j) zq[j][i] = v[j];
     }
   }
   bool fail = false;
+  int fail_plane = zlast;   // first plane whose wait this thread gave up on
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     const int p = z0 + i;
     if (p < nz) {
       const int s = (p - z0) % NBUF;
-      if (!fail && !mbar_wait(&bars[s], ((p - z0) / NBUF) & 1)) fail = true;
+      if (!fail && !mbar_wait(&bars[s], ((p - z0) / NBUF) & 1, A.wait_limit)) {
+        fail = true;
+        fail_plane = p;
+      }
       if (own) {
         T v[VW];
-        vload(ring + (size_t)s * WS + s_c, v);
+        vload<VW>(ring + (size_t)s * WS + s_c, v);
 #pragma unroll
         for (int j = 0; j < VW; ++j) zq[j][R + i] = v[j];
       }
@@ -333,6 +363,14 @@ k_stencil_tma(TmaArgs<T> A) {
     el[j] = min(R, xj);
     er[j] = min(R, nx - 1 - xj);
   }
+  const bool masked = A.mask_r2 > 0.0;
+  double mxy[VW];   // (x^2 + y^2) of the run's points, for the sphere mask
+#pragma unroll
+  for (int j = 0; j < VW; ++j) {
+    const int qq = own ? q + j : 0;
+    const double xm = (qq % nx) * A.h - A.cx, ym = (qq / nx) * A.h - A.cy;
+    mxy[j] = xm * xm + ym * ym;
+  }
   const T c0 = A.c0;
   // z loop unrolled by Q so the register queue rotates by renaming:
   // at unrolled position u, plane z - R + i lives in zq[.][(u + i) % Q]
@@ -350,8 +388,11 @@ k_stencil_tma(TmaArgs<T> A) {
         for (int j = 0; j < VW; ++j) f[j] = T(0);
         if (pf < nz) {
           const int s = (pf - z0) % NBUF;
-          if (!fail && !mbar_wait(&bars[s], ((pf - z0) / NBUF) & 1)) fail = true;
-          if (own) vload(ring + (size_t)s * WS + s_c, f);
+          if (!fail && !mbar_wait(&bars[s], ((pf - z0) / NBUF) & 1, A.wait_limit)) {
+            fail = true;
+            fail_plane = pf;
+          }
+          if (own) vload<VW>(ring + (size_t)s * WS + s_c, f);
         }
 #pragma unroll
         for (int j = 0; j < VW; ++j) zq[j][(u + 2 * R) % Q] = f[j];
@@ -364,8 +405,8 @@ k_stencil_tma(TmaArgs<T> A) {
         cp_async_wait<NS - 1>();
         if (own) {
           const T* pp = pring + (size_t)((z - z0) % NS) * 2 * TS + loc;
-          if (Pc) vload(pp, pvv);
-          if (has_pot) vload(pp + TS, pov);
+          if (Pc) vload<VW>(pp, pvv);
+          if (has_pot) vload<VW>(pp + TS, pov);
         }
       }
       const T* pl = ring + (size_t)((z - z0) % NBUF) * WS;
@@ -377,7 +418,7 @@ k_stencil_tma(TmaArgs<T> A) {
 #pragma unroll
             for (int j = 0; j < VW; ++j) xs[v * VW + j] = zq[j][(u + R) % Q];
           } else {
-            vload(pl + xo[v], xs + v * VW);
+            vload<VW>(pl + xo[v], xs + v * VW);
           }
         }
         const T* pc = pl + s_c;
@@ -387,8 +428,8 @@ k_stencil_tma(TmaArgs<T> A) {
 #pragma unroll
         for (int d = 1; d <= R; ++d) {
           T ym[VW], yp[VW];
-          vload(pc - d * nx, ym);
-          vload(pc + d * nx, yp);
+          vload<VW>(pc - d * nx, ym);
+          vload<VW>(pc + d * nx, yp);
           const T cd = A.c[d - 1];
 #pragma unroll
           for (int j = 0; j < VW; ++j) {
@@ -406,7 +447,13 @@ k_stencil_tma(TmaArgs<T> A) {
           o[j] = ca * a + cb * xc;
           if (Pc) o[j] += cg * pvv[j];
         }
-        vstore(Yc + (long)z * nxy + q, o);
+        if (masked) {
+          const double zm = z * A.h - A.cz;
+#pragma unroll
+          for (int j = 0; j < VW; ++j)
+            if (mxy[j] + zm * zm > A.mask_r2) o[j] = T(0);
+        }
+        vstore<VW>(Yc + (long)z * nxy + q, o);
       } else if (own) {
         // x neighbours: the aligned vectors around the run; the run itself is the queue's centre
         T xs[NPV * VW];
@@ -416,7 +463,7 @@ k_stencil_tma(TmaArgs<T> A) {
 #pragma unroll
             for (int j = 0; j < VW; ++j) xs[v * VW + j] = zq[j][(u + R) % Q];
           } else {
-            vload(pl + s_c - OFF + v * VW, xs + v * VW);
+            vload<VW>(pl + s_c - OFF + v * VW, xs + v * VW);
           }
         }
         // two partial sums per point: y + z terms, x terms
@@ -430,8 +477,8 @@ k_stencil_tma(TmaArgs<T> A) {
         for (int d = 1; d <= R; ++d) {
           // rows outside the plane are zero in the window, so y needs no test
           T ym[VW], yp[VW];
-          vload_a<T, YA>(pl + s_c - d * nx, ym);
-          vload_a<T, YA>(pl + s_c + d * nx, yp);
+          vload_a<T, YA, VW>(pl + s_c - d * nx, ym);
+          vload_a<T, YA, VW>(pl + s_c + d * nx, yp);
           const T cd = A.c[d - 1];
 #pragma unroll
           for (int j = 0; j < VW; ++j) {
@@ -450,19 +497,31 @@ k_stencil_tma(TmaArgs<T> A) {
           o[j] = ca * a + cb * xc;
           if (Pc) o[j] += cg * pvv[j];
         }
-        vstore(Yc + (long)z * nxy + q, o);
+        if (masked) {
+          const double zm = z * A.h - A.cz;
+#pragma unroll
+          for (int j = 0; j < VW; ++j)
+            if (mxy[j] + zm * zm > A.mask_r2) o[j] = T(0);
+        }
+        vstore<VW>(Yc + (long)z * nxy + q, o);
       }
       // every SYNC_EVERY planes (and after the last): the slots of all
       // planes <= z are free, so the ring is topped up to plane z + NBUF.
       // The queue front z + R stays covered while SYNC_EVERY <= NBUF - R.
       if ((z - z0) % SYNC_EVERY == SYNC_EVERY - 1 || z == z1 - 1) {
         __syncthreads();
-        if (threadIdx.x == 0)
+        if (threadIdx.x == 0 && !fail)
           for (; issued < zlast && issued <= z + NBUF; ++issued) issue_x(issued);
       }
     }
   }
   if (fail) s_fail = 1;
+  // Thread 0 issues every copy and waits for the planes in order; once it
+  // has given up it issues no more, so the planes fail_plane .. issued-1 sit
+  // in distinct slots.  Their copies are drained before the CTA exits.
+  if (threadIdx.x == 0 && fail)
+    for (int p = fail_plane; p < issued; ++p)
+      mbar_wait(&bars[(p - z0) % NBUF], ((p - z0) / NBUF) & 1, PSC_DRAIN_WAIT);
   __syncthreads();
   if (threadIdx.x == 0 && s_fail) atomicExch(&A.status[3], 1);
 }
@@ -545,10 +604,56 @@ static std::vector<int4> stencil_schedule(int nslab, int nz, int k, int fill, in
   return out;
 }
 
-// Cached per context: the table of a (k, slab count, fill) combination is
-// built and uploaded once.
-static const int4* stencil_sched(psc_ctx* ctx, int nslab, int k, int fill, int slots, int* n, cudaStream_t st) {
-  const long long key = ((long long)k << 32) | ((long long)nslab << 16) | ((long long)fill << 8) | (slots & 0xff);
+// Masked launches (sphere mode): per slab, the planes [zlo, zhi) that hold a
+// point inside the sphere (one plane of margin each side) are computed, the
+// rest only zero-filled.  Compute items are cut into chunks of at most lc
+// planes and sorted longest first; the zero items (column stored as
+// -1 - column) follow, at about a third of a plane's cost each.
+static std::vector<int4> stencil_schedule_masked(const psc_ctx* ctx, int ts, int nslab, int k, int slots) {
+  const int nx = ctx->nx, nxy = ctx->nx * ctx->ny, nz = ctx->nz;
+  std::vector<int2> zr(nslab);
+  long work = 0;
+  for (int sl = 0; sl < nslab; ++sl) {
+    double d2 = 1e300;
+    for (int q = sl * ts; q < std::min(nxy, (sl + 1) * ts); ++q) {
+      const double x = (q % nx) * ctx->h - ctx->mask_c[0], y = (q / nx) * ctx->h - ctx->mask_c[1];
+      d2 = std::min(d2, x * x + y * y);
+    }
+    int lo = nz, hi = 0;
+    if (d2 <= ctx->mask_r2) {
+      const double half = std::sqrt(ctx->mask_r2 - d2);
+      lo = std::max(0, (int)std::floor((ctx->mask_c[2] - half) / ctx->h) - 1);
+      hi = std::min(nz, (int)std::ceil((ctx->mask_c[2] + half) / ctx->h) + 2);
+    }
+    zr[sl] = make_int2(lo, hi);
+    if (hi > lo) work += hi - lo;
+  }
+  const int lc = std::max(8, (int)std::min<long>(nz, (work * (long)k + 2L * slots - 1) / (2L * slots)));
+  std::vector<int4> comp, zero;
+  for (int col = 0; col < k; ++col)
+    for (int sl = 0; sl < nslab; ++sl) {
+      const int lo = zr[sl].x, hi = zr[sl].y;
+      if (hi > lo) {
+        const int nch = (hi - lo + lc - 1) / lc;
+        const int len = (hi - lo + nch - 1) / nch;
+        for (int z = lo; z < hi; z += len) comp.push_back(make_int4(col, sl, z, std::min(hi, z + len)));
+        if (lo > 0) zero.push_back(make_int4(-1 - col, sl, 0, lo));
+        if (hi < nz) zero.push_back(make_int4(-1 - col, sl, hi, nz));
+      } else {
+        zero.push_back(make_int4(-1 - col, sl, 0, nz));
+      }
+    }
+  std::stable_sort(comp.begin(), comp.end(), [](const int4& a, const int4& b) { return a.w - a.z > b.w - b.z; });
+  comp.insert(comp.end(), zero.begin(), zero.end());
+  return comp;
+}
+
+// Cached per context: the table of a (k, slab count, fill, mask) combination
+// is built and uploaded once.
+static const int4* stencil_sched(psc_ctx* ctx, int nslab, int k, int fill, int slots, bool masked, int ts, int* n,
+                                 cudaStream_t st) {
+  const long long key = ((long long)k << 32) | ((long long)nslab << 16) | ((long long)fill << 8) | (slots & 0x7f) |
+                        (masked ? 0x80 : 0);
   for (auto& e : ctx->st_sched)
     if (e.key == key) {
       *n = e.n;
@@ -556,7 +661,8 @@ static const int4* stencil_sched(psc_ctx* ctx, int nslab, int k, int fill, int s
     }
   psc_ctx::StencilSched e;
   e.key = key;
-  std::vector<int4> tab = stencil_schedule(nslab, ctx->nz, k, fill, slots);
+  std::vector<int4> tab = masked ? stencil_schedule_masked(ctx, ts, nslab, k, slots)
+                                 : stencil_schedule(nslab, ctx->nz, k, fill, slots);
   e.n = (int)tab.size();
   e.host.resize(4 * tab.size());
   std::memcpy(e.host.data(), tab.data(), tab.size() * sizeof(int4));
@@ -569,12 +675,12 @@ static const int4* stencil_sched(psc_ctx* ctx, int nslab, int k, int fill, int s
   return reinterpret_cast<const int4*>(b.dev);
 }
 
-template <typename T, int R>
+template <typename T, int R, int VW>
 static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy,
                         const T* pot, const double* w, const double* coef, double a, double b, double g,
-                        cudaStream_t st) {
+                        bool masked, cudaStream_t st) {
   const int nxy = ctx->nx * ctx->ny;
-  constexpr int TS = slab_points<T>();
+  constexpr int TS = slab_points<VW>();
   const int nslab = (nxy + TS - 1) / TS;
   // each CTA pays a pipeline fill of about R + D planes; two CTAs per SM
   // are resident (registers and shared memory)
@@ -583,16 +689,16 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   const int slots = PSC_STENCIL_CTAS_PER_SM * sms;
   const int fill = R + prefetch_depth<T>() + 2;
   int nwork = 0;
-  const int4* sched = stencil_sched(ctx, nslab, k, fill, slots, &nwork, st);
+  masked = masked && ctx->mask_r2 > 0.0;
+  const int4* sched = stencil_sched(ctx, nslab, k, fill, slots, masked, TS, &nwork, st);
   PSC_REQUIRE(ctx, sched != nullptr, "stencil: work table allocation failed");
   constexpr int NBUF = R + 1 + prefetch_depth<T>();
-  const size_t win = TS + 2 * (size_t)R * ctx->nx + VecOf<T>::W;   // window + zero pad vector
+  const size_t win = TS + 2 * (size_t)R * ctx->nx + VW;   // window + zero pad vector
   const size_t smem = (NBUF * win + (size_t)PP_SLOTS * 2 * TS) * sizeof(T) + NBUF * sizeof(uint64_t);
   if (smem > 220 * 1024) return -1;  // window too wide: the register-queue kernel takes it
-  constexpr int VW = VecOf<T>::W;
-  auto kern = (ctx->nx % VW == 0) ? k_stencil_tma<T, R, VW>
-              : (ctx->nx % 2 == 0) ? k_stencil_tma<T, R, (VW >= 2 ? 2 : 1)>
-                                   : k_stencil_tma<T, R, 1>;
+  auto kern = (ctx->nx % VW == 0) ? k_stencil_tma<T, R, VW, VW>
+              : (ctx->nx % 2 == 0) ? k_stencil_tma<T, R, (VW >= 2 ? 2 : 1), VW>
+                                   : k_stencil_tma<T, R, 1, VW>;
   PSC_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   TmaArgs<T> A;
   A.X = X; A.ldx = ldx; A.P = P; A.ldp = ldp; A.Y = Y; A.ldy = ldy; A.pot = pot;
@@ -600,6 +706,10 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   A.c0 = (T)w[0];
   for (int i = 0; i < 4; ++i) A.c[i] = (T)w[1 + i];
   A.coef = coef; A.a = a; A.b = b; A.g = g; A.status = ctx->dev_status;
+  A.wait_limit = ctx->wait_limit;
+  A.mask_r2 = masked ? ctx->mask_r2 : 0.0;
+  A.h = ctx->h;
+  A.cx = ctx->mask_c[0]; A.cy = ctx->mask_c[1]; A.cz = ctx->mask_c[2];
   kern<<<nwork, TNT, smem, st>>>(A);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
@@ -608,20 +718,33 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
 // Returns -1 if the TMA path does not apply (caller uses the register kernel).
 template <typename T>
 int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy, const T* pot,
-                    const double* w, const double* coef, double a, double b, double g, cudaStream_t st) {
+                    const double* w, const double* coef, double a, double b, double g, bool masked,
+                    cudaStream_t st) {
   if (!tma_ok<T>(ctx, X, ldx, P, ldp, Y, ldy)) return -1;
+  // FP32 takes 2-point runs when nx is even but not a multiple of 4 (the
+  // aligned, mask-free x terms), unless stencil_impl 2 asks for 4-point runs
+  const bool narrow = sizeof(T) == 4 && ctx->nx % 4 != 0 && ctx->nx % 2 == 0 && ctx->stencil_impl != 2;
+#define PSC_TMA_R(RR)                                                                                         \
+  case RR:                                                                                                    \
+    if constexpr (sizeof(T) == 8)                                                                             \
+      return launch_tma_t<T, RR, 2>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st);       \
+    else if (narrow)                                                                                          \
+      return launch_tma_t<T, RR, 2>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st);       \
+    else                                                                                                      \
+      return launch_tma_t<T, RR, 4>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st);
   switch (ctx->radius) {
-    case 1: return launch_tma_t<T, 1>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, st);
-    case 2: return launch_tma_t<T, 2>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, st);
-    case 3: return launch_tma_t<T, 3>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, st);
-    case 4: return launch_tma_t<T, 4>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, st);
+    PSC_TMA_R(1)
+    PSC_TMA_R(2)
+    PSC_TMA_R(3)
+    PSC_TMA_R(4)
   }
+#undef PSC_TMA_R
   return -1;
 }
 
 template int psc_stencil_tma<double>(psc_ctx*, int, const double*, long, const double*, long, double*, long,
-                                     const double*, const double*, const double*, double, double, double,
+                                     const double*, const double*, const double*, double, double, double, bool,
                                      cudaStream_t);
 template int psc_stencil_tma<float>(psc_ctx*, int, const float*, long, const float*, long, float*, long,
-                                    const float*, const double*, const double*, double, double, double,
+                                    const float*, const double*, const double*, double, double, double, bool,
                                     cudaStream_t);

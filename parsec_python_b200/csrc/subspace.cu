@@ -15,7 +15,7 @@
 //                8 x 8 register tile per thread, rows staged in shared memory)
 //   k_gemm_tall  Out = W T for n x k by k x kout (128 rows x 64 columns per
 //                CTA, 4 x 8 register tile per thread)
-//   k_small_mm   C = op(A) B for k x k matrices
+//   k_small_mm   C = op(A) B for k x k matrices (64 x 64 shared-memory tiles)
 #include "psc_internal.cuh"
 #include "../../include/psc.h"
 
@@ -172,19 +172,55 @@ k_gemm_tall(const T* __restrict__ W, long ldw, int k, const double* __restrict__
   }
 }
 
-// C (k x k) = op(A) B, op = transpose if ta; column-major k x k
-__global__ void k_small_mm(const double* __restrict__ A, const double* __restrict__ B, int k, int ta,
-                           double* __restrict__ C) {
-  const long kk = (long)k * k;
-  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < kk; e += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(e % k), j = (int)(e / k);
-    double s = 0.0;
-    for (int l = 0; l < k; ++l) {
-      const double a = ta ? A[l + (long)i * k] : A[i + (long)l * k];
-      s += a * B[l + (long)j * k];
+// C (k x k) = op(A) B, op = transpose if ta; column-major k x k.  64 x 64
+// output tile per CTA, 4 x 4 per thread, the reduction staged 16 at a time
+// in shared memory; every output is summed over l in increasing order (the
+// order of a plain dot product).
+constexpr int SM_T = 64, SM_K = 16;
+__global__ void __launch_bounds__(256)
+k_small_mm(const double* __restrict__ A, const double* __restrict__ B, int k, int ta, double* __restrict__ C) {
+  __shared__ double As[SM_K][SM_T + 1];   // As[l][i] = op(A)[i0 + i, l0 + l]
+  __shared__ double Bs[SM_K][SM_T + 1];   // Bs[l][j] = B[l0 + l, j0 + j]
+  const int i0 = blockIdx.x * SM_T, j0 = blockIdx.y * SM_T;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // outputs i0 + tx + 16 a, j0 + ty + 16 b
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int l0 = 0; l0 < k; l0 += SM_K) {
+    for (int e = threadIdx.x; e < SM_K * SM_T; e += 256) {
+      // A: for ta the reduction index is A's row (contiguous): e -> (l fastest)
+      int l, i;
+      if (ta) { l = e % SM_K; i = e / SM_K; } else { i = e % SM_T; l = e / SM_T; }
+      const int gi = i0 + i, gl = l0 + l;
+      As[l][i] = (gi < k && gl < k) ? (ta ? A[gl + (long)gi * k] : A[gi + (long)gl * k]) : 0.0;
+      const int bl = e % SM_K, bj = e / SM_K;
+      const int gbl = l0 + bl, gj = j0 + bj;
+      Bs[bl][bj] = (gbl < k && gj < k) ? B[gbl + (long)gj * k] : 0.0;
     }
-    C[e] = s;
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < SM_K; ++l) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) av[a] = As[l][tx + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bv[b] = Bs[l][ty + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+    }
+    __syncthreads();
   }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = i0 + tx + 16 * a, j = j0 + ty + 16 * b;
+      if (i < k && j < k) C[i + (long)j * k] = acc[a][b];
+    }
 }
 
 // dense.cu
@@ -193,6 +229,10 @@ int psc_chol_inv_dev(psc_ctx* ctx, double* S, int k, double* X, cudaStream_t st)
 int psc_gemm_tall(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Tm, int kout, void* O,
                   long ldo, cudaStream_t st) {
   PSC_REQUIRE(ctx, W != O, "gemm: output must not alias input");
+  if (dtype == PSC_F32) {
+    const int rc = psc_gemm_tall_tc(ctx, (const float*)W, ldw, k, Tm, kout, (float*)O, ldo, st);
+    if (rc >= 0) return rc;
+  }
   dim3 grid(psc_div_up(ctx->n, 128), psc_div_up(kout, 64));
   if (dtype == PSC_F64)
     k_gemm_tall<double><<<grid, 256, 0, st>>>((const double*)W, ldw, k, Tm, kout, (double*)O, ldo, ctx->n);
@@ -261,17 +301,16 @@ extern "C" int psc_subspace_rr(psc_ctx* ctx, int dtype, const void* W, void* V, 
   if (rc) return rc;
   rc = psc_chol_inv_dev(ctx, S, k, Ri, st);
   if (rc) return rc;
-  const long kk = (long)k * k;
-  const int nb = std::max(1, (int)std::min<long>(592, (kk + 127) / 128));
+  const dim3 gmm(psc_div_up(k, SM_T), psc_div_up(k, SM_T));
   // S <- K R^{-1}; K <- R^{-T} S  (M, symmetric up to rounding)
-  k_small_mm<<<nb, 128, 0, st>>>(K, Ri, k, 0, S);
+  k_small_mm<<<gmm, 256, 0, st>>>(K, Ri, k, 0, S);
   PSC_LAUNCH_CHECK(ctx);
-  k_small_mm<<<nb, 128, 0, st>>>(Ri, S, k, 1, K);
+  k_small_mm<<<gmm, 256, 0, st>>>(Ri, S, k, 1, K);
   PSC_LAUNCH_CHECK(ctx);
   rc = psc_syev_impl(ctx, K, k, ritz_dev, Y, st);
   if (rc) return rc;
   // S <- R^{-1} Y
-  k_small_mm<<<nb, 128, 0, st>>>(Ri, Y, k, 0, S);
+  k_small_mm<<<gmm, 256, 0, st>>>(Ri, Y, k, 0, S);
   PSC_LAUNCH_CHECK(ctx);
   return psc_gemm_tall(ctx, dtype, W, ld, k, S, k, V, ld, st);
 }

@@ -57,6 +57,7 @@ class GridContext:
         self.species: dict[str, int] = {}
         self._seed = itertools.count(int(seed) * 1_000_003 + 17)
         self.projectors = None
+        self.mask_radius = 0.0
 
     def __del__(self):
         try:
@@ -73,6 +74,30 @@ class GridContext:
 
     def call(self, name: str, *args) -> None:
         call(name, self.ptr, *args, ctx=self.ptr)
+
+    def set_sphere_mask(self, radius: float) -> None:
+        """H X is zero outside the sphere of this radius (bohr) around the
+        cube's centre; 0 restores the cube (psc_set_sphere_mask)."""
+        self.call("psc_set_sphere_mask", float(radius), _stream())
+        self.mask_radius = float(radius) if radius > 0 else 0.0
+
+    def mask_block(self, X: torch.Tensor) -> torch.Tensor:
+        """Zero X (a (k, n) block or an n-vector) outside the sphere mask, in place."""
+        if self.mask_radius > 0:
+            k = 1 if X.dim() == 1 else X.shape[0]
+            self.call("psc_mask_block", _dtype_code(X), _p(X), self.n, k, _stream())
+        return X
+
+    def inside_count(self) -> int:
+        """Grid points the Hamiltonian produces: inside the sphere mask, or all."""
+        if self.mask_radius <= 0:
+            return self.n
+        c = 0.5 * self.h * (np.array([self.nx, self.ny, self.nz]) - 1)
+        x = np.arange(self.nx) * self.h - c[0]
+        y = np.arange(self.ny) * self.h - c[1]
+        z = np.arange(self.nz) * self.h - c[2]
+        d2 = (z[:, None, None] ** 2 + y[None, :, None] ** 2) + x[None, None, :] ** 2
+        return int(np.count_nonzero(d2 <= self.mask_radius ** 2))
 
     def next_seed(self) -> int:
         return next(self._seed)
@@ -121,6 +146,8 @@ class GridContext:
             raise PscError("persistent CG grid barrier timed out")
         if f[5]:
             raise PscError("tensor-core Gram pipeline wait timed out")
+        if f[6]:
+            raise PscError("tensor-core block product pipeline wait timed out")
 
     def info(self) -> dict:
         out = (c_long * 8)()
@@ -228,19 +255,25 @@ def lanczos_bound(ctx: GridContext, mode: int) -> torch.Tensor:
     return out
 
 
-def first_filt(nev: int, H: Hamiltonian, polm: int = 10, dtype=torch.float64, log_trace=None):
+def first_filt(nev: int, H: Hamiltonian, polm: int = 10, dtype=torch.float64, log_trace=None,
+               energ_tol: float = 0.08, max_iter: int | None = None):
     """First SCF step (Eigensolvers/first_filt.py:6-75): Lanczos bounds,
     random block, up to max_iter rounds of slim filter + orthonormalisation +
-    Rayleigh-Ritz, stop when the Ritz trace moves by <= 8%."""
+    Rayleigh-Ritz, stop when the Ritz trace moves by <= energ_tol (8 % and
+    max(min(60 / polm, 5), 3) rounds in the reference; a start whose
+    potential is already close to self-consistent, such as the learned one,
+    can ask for a converged first subspace instead)."""
     ctx = H.ctx
     if polm < 10 or polm > 15:
         polm = 10
-    max_iter = max(min(int(60 / polm), 5), 3)
+    if not max_iter:
+        max_iter = max(min(int(60 / polm), 5), 3)
     lz = lanczos_bound(ctx, 0)                       # [uppbnd, ritz_0..5]
     bounds = ctx.empty(3)
     ctx.call("psc_filter_bounds", 1, _p(lz[1:7]), 6, _p(lz[0:1]), _p(bounds), _stream())
     W = ctx.empty(nev, ctx.n, dtype=dtype)
     ctx.call("psc_random", _dtype_code(W), 0, ctx.next_seed(), _p(W), ctx.n, ctx.n, nev, _stream())
+    ctx.mask_block(W)
     T = torch.empty_like(W)
     ritz = ctx.empty(nev)
     tr0 = None
@@ -254,7 +287,7 @@ def first_filt(nev: int, H: Hamiltonian, polm: int = 10, dtype=torch.float64, lo
         if it == 1:
             tr0 = tr
         else:
-            if abs(tr - tr0) <= 0.08 * abs(tr0):
+            if abs(tr - tr0) <= energ_tol * abs(tr0):
                 break
             tr0 = tr
     ctx.check_status()
@@ -317,6 +350,12 @@ def lanczos_krylov(H: Hamiltonian, nev: int, m: int, test: int, v=None, tol: flo
     ab = ctx.zeros(2 * m)
     evals = ctx.empty(m)
     v0 = _start_vector(ctx, v)
+    if v0 is None and ctx.mask_radius > 0:
+        # a start that vanishes outside the sphere keeps the Krylov basis there
+        v0 = ctx.empty(n)
+        ctx.call("psc_random", F64, 1, ctx.next_seed(), _p(v0), n, n, 1, _stream())
+    if v0 is not None and ctx.mask_radius > 0:
+        v0 = ctx.mask_block(v0.clone())
     seed = ctx.next_seed()
     if not test:
         ctx.call("psc_lanczos_run", _p(v0), seed, 0, m, _p(VV), n, _p(ab), _stream())
@@ -360,6 +399,7 @@ def _krylov_ritz(H: Hamiltonian, VV: torch.Tensor, ab: torch.Tensor, k: int, rr:
         # as many directions as the reference's QR returns: fresh random
         # columns after the kept ones, then the whole block orthonormalised
         ctx.call("psc_random", F64, 1, ctx.next_seed(), _p(B[r:]), n, n, nev - r, _stream())
+        ctx.mask_block(B[r:nev])
         B, S = orthonormalize(ctx, B[:nev], S[:nev])
         r = nev
     V = S[:r]

@@ -46,6 +46,7 @@ from .models import A0_ANG, SolverSettings
 
 DATA_DIR = Path(__file__).resolve().parent / "data"
 DEFAULT_WEIGHTS = DATA_DIR / "learned_init_water.npz"
+SIH_WEIGHTS = DATA_DIR / "learned_init_sih.npz"
 
 
 @dataclass(frozen=True)
@@ -271,26 +272,50 @@ def load_weights(path: Path | str = DEFAULT_WEIGHTS) -> dict | None:
             "meta": json.loads(str(z["meta"]))}
 
 
+# Networks built for a grid shape, reused by later SCFs on the same grid: the
+# weights are uploaded once per process, not once per SCF.  Each entry keeps
+# the grid context it was built with alive (kernel calls need a context; the
+# network's own buffers do not depend on which SCF is running).
+_NET_CACHE: dict = {}
+
+
+def cached_net(ctx: gpu.GridContext, params: dict) -> "UNet3D":
+    key = (ctx.device.index, ctx.nx, ctx.ny, ctx.nz, id(params["w"]))
+    hit = _NET_CACHE.get(key)
+    if hit is None:
+        if len(_NET_CACHE) >= 4:
+            _NET_CACHE.pop(next(iter(_NET_CACHE)))
+        # the entry keeps the weight array alive, so its id cannot be reused
+        hit = (UNet3D(ctx, params=params), params["w"])
+        _NET_CACHE[key] = hit
+    return hit[0]
+
+
 class LearnedInit:
     """init_density callback for solver.run_rsdft_calculation: SAD density ->
     network correction -> clamp, renormalise, Hartree potential of the
     difference from SAD (pseudoDiag_ML4Den_poisson.py:448-538).  Returns
     (rho1, dh); the solver uses them for the first potential and as the
-    Hartree CG's starting point."""
+    Hartree CG's starting point.  dh is solved with the spectrally
+    preconditioned CG (2-3 iterations to tol 1e-5; the reference's plain
+    200-iteration CG stops short of its tolerance at these grid sizes).
+    `last` records the CUDA-event times of the three stages."""
 
     def __init__(self, params: dict):
         if params["w"].size != n_params():
             raise ValueError("weights do not match the network")
         self.params = params
-        self.net = None
         self.last = {}
 
     def __call__(self, ctx: gpu.GridContext, rho0, hpot0, ppot, A):
-        if self.net is None or self.net.ctx is not ctx:
-            self.net = UNet3D(ctx, params=self.params)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
+        net = cached_net(ctx, self.params)
+        ev[1].record()
         h3 = ctx.h ** 3
         rho_b = rho0 / h3
-        delta = self.net.predict_delta(rho_b, ppot)
+        delta = net.predict_delta(rho_b, ppot)
+        ev[2].record()
         if not bool(torch.isfinite(delta).all()):
             self.last = {"fallback": "non-finite prediction"}
             return rho0, torch.zeros_like(rho0)
@@ -298,8 +323,11 @@ class LearnedInit:
         zsum = gpu.numpy_sum(ctx, rho0)
         rho1 = rho1 * (zsum / gpu.numpy_sum(ctx, rho1))
         hrhs = (4 * np.pi / h3) * (rho1 - rho0)
-        dh, its = gpu.pcg(A, hrhs, torch.zeros_like(hrhs), 200, 1e-5)
-        self.last = {"cg_its": its, "rho_start": rho1}
+        dh, its = gpu.pcg(A, hrhs, torch.zeros_like(hrhs), 200, 1e-5, "spectral", "precLU")
+        ev[3].record()
+        torch.cuda.synchronize()
+        self.last = {"cg_its": its, "rho_start": rho1, "net_s": ev[0].elapsed_time(ev[1]) / 1e3,
+                     "forward_s": ev[1].elapsed_time(ev[2]) / 1e3, "hartree_s": ev[2].elapsed_time(ev[3]) / 1e3}
         return rho1, dh
 
 
@@ -310,28 +338,61 @@ WATER_H_ANG = 0.2
 WATER_RADIUS_ANG = 9.0   # clusters live in a 6 A ball; 3 A margin for the density tails
 
 
-def water_system(seed: int, settings: SolverSettings):
+def _water_nev(counts: dict) -> int:
+    return 4 * counts.get("O", 0) + 4
+
+
+def _sih_nev(counts: dict) -> int:
+    occ = (4 * counts.get("Si", 0) + counts.get("H", 0)) // 2
+    return occ + max(8, int(round(0.45 * occ)))
+
+
+# Training families: geometry generator, grid, number of states, weights file.
+#   water  (H2O)n, n in 2..8 (workloads.water_cluster), h 0.2 A, 9 A sphere
+#   sih    Si(5..35) H-capped clusters (workloads.sih_random_cluster), h 0.25 A
+#          (the Si-H configurations' spacing), 10 A sphere (extents up to 8 A)
+FAMILIES = {
+    "water": {"build": workloads.water_cluster, "h_ang": WATER_H_ANG, "radius_ang": WATER_RADIUS_ANG,
+              "nev": _water_nev, "weights": DEFAULT_WEIGHTS},
+    "sih": {"build": workloads.sih_random_cluster, "h_ang": 0.25, "radius_ang": 10.0, "nev": _sih_nev,
+            "weights": SIH_WEIGHTS},
+}
+
+
+def weights_for(atoms) -> Path:
+    """The trained network for a system: the Si-H one when the system holds
+    silicon, else the water one."""
+    species = {a["typ"] for a in atoms}
+    return SIH_WEIGHTS if "Si" in species else DEFAULT_WEIGHTS
+
+
+def family_system(family: str, seed: int, settings: SolverSettings):
     from .inputs import ElementTable
     from .system import system_from_atoms
 
-    atoms = workloads.water_cluster(seed)
+    fam = FAMILIES[family]
+    atoms = fam["build"](seed)
     f = 1.0 / A0_ANG
     atoms = [{"typ": a["typ"], "coord": np.asarray(a["coord"], dtype=float).reshape(-1, 3) * f} for a in atoms]
-    nmol = sum(np.asarray(a["coord"]).reshape(-1, 3).shape[0] for a in atoms if a["typ"] == "O")
-    nev = 4 * nmol + 4
+    nev = fam["nev"](workloads.count(atoms))
     elem = ElementTable()
-    prob = system_from_atoms(atoms, h=WATER_H_ANG * f, radius=WATER_RADIUS_ANG * f, nev=nev, settings=settings,
+    prob = system_from_atoms(atoms, h=fam["h_ang"] * f, radius=fam["radius_ang"] * f, nev=nev, settings=settings,
                              elem=elem)
     return prob, elem
 
 
-def run_scf(seed: int, init=None, tol: float = 1e-6, scf_seed: int = 0, energy_target=None):
+def water_system(seed: int, settings: SolverSettings):
+    return family_system("water", seed, settings)
+
+
+def run_scf(seed: int, init=None, tol: float = 1e-6, scf_seed: int = 0, energy_target=None, family: str = "water",
+            cg_prec: int = 0, precision: str = "fp64"):
     from .backend import select_solver_backend
     from .solver import run_rsdft_calculation
 
-    s = SolverSettings(tol=tol, poldeg=10, maxits=80, seed=scf_seed)
+    s = SolverSettings(tol=tol, poldeg=10, maxits=80, seed=scf_seed, cg_prec=cg_prec, precision=precision)
     s.normalize()
-    prob, elem = water_system(seed, s)
+    prob, elem = family_system(family, seed, s)
     backend = select_solver_backend(s)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -341,11 +402,14 @@ def run_scf(seed: int, init=None, tol: float = 1e-6, scf_seed: int = 0, energy_t
     return res, time.perf_counter() - t0, backend
 
 
-def make_sample(seed: int):
-    """(SAD density e/bohr^3, V_loc, converged - SAD density) on the water grid."""
-    res, _, backend = run_scf(seed)
+def make_sample(seed: int, family: str = "water"):
+    """(SAD density e/bohr^3, V_loc, converged - SAD density) on the family's
+    grid; the converged density of the FP64 SCF (preconditioned Hartree solve
+    for the Si-H family, whose larger grids leave the plain CG short of its
+    tolerance)."""
+    res, _, backend = run_scf(seed, family=family, cg_prec=1 if family == "sih" else 0)
     rt = backend.runtime
-    prob, elem = water_system(seed, rt.settings)
+    prob, elem = family_system(family, seed, rt.settings)
     ctx = rt.context(prob.domain)
     rho0, _, ppot, _ = backend.pseudo_diag(prob.domain, prob.input_data.atoms, elem, len(elem), return_info=True)
     h3 = ctx.h ** 3
@@ -356,7 +420,8 @@ def make_sample(seed: int):
 TRAIN_SEEDS = 512        # geometries 0..511 train the network; 512.. are held out
 
 
-def train(n_train: int, epochs: int, out: Path, lr: float = 2e-4, seed: int = 0, log=print) -> dict:
+def train(n_train: int, epochs: int, out: Path, lr: float = 2e-4, seed: int = 0, log=print,
+          family: str = "water") -> dict:
     t_data = time.perf_counter()
     samples = []
     ctx0 = None
@@ -364,7 +429,7 @@ def train(n_train: int, epochs: int, out: Path, lr: float = 2e-4, seed: int = 0,
     sd = 0
     while len(samples) < n_train and sd < TRAIN_SEEDS:
         try:
-            ctx, rs, vl, dt, res = make_sample(sd)
+            ctx, rs, vl, dt, res = make_sample(sd, family)
         except ValueError as exc:   # e.g. the reference's "Bounds are incorrect" stop in chefsi1
             skipped.append(sd)
             log(f"  seed {sd} skipped: {exc}")
@@ -411,13 +476,13 @@ def train(n_train: int, epochs: int, out: Path, lr: float = 2e-4, seed: int = 0,
     t_train = time.perf_counter() - t_train
     meta = {"n_train": n_train, "epochs": epochs, "lr": lr, "seed": seed, "losses": losses,
             "seeds_used": [0, sd], "seeds_skipped": skipped,
-            "data_seconds": t_data, "train_seconds": t_train, "grid": list(net.grid["in"]),
-            "h_ang": WATER_H_ANG, "radius_ang": WATER_RADIUS_ANG, "params": n_params()}
+            "data_seconds": t_data, "train_seconds": t_train, "grid": list(net.grid["in"]), "family": family,
+            "h_ang": FAMILIES[family]["h_ang"], "radius_ang": FAMILIES[family]["radius_ang"], "params": n_params()}
     net.save(out, meta)
     return meta
 
 
-def evaluate(seeds, weights: Path, log=print) -> dict:
+def evaluate(seeds, weights: Path, log=print, family: str = "water") -> dict:
     """SCF time-to-1e-5 Ha from SAD and from the learned density on each
     geometry: E* is the SAD-initialised run driven to tol 1e-8; both timed
     runs stop at the reference test (err <= 1e-6) once their energy is within
@@ -429,16 +494,16 @@ def evaluate(seeds, weights: Path, log=print) -> dict:
     skipped = []
     for sd in seeds:
         try:
-            r_ref, _, _ = run_scf(sd, tol=1e-8)
+            r_ref, _, _ = run_scf(sd, tol=1e-8, family=family)
             if not r_ref.converged:
                 skipped.append(sd)
                 log(f"  seed {sd} skipped: the tol-1e-8 SCF did not converge")
                 continue
             e_star = r_ref.history[-1]["total_ry"]
             target = (e_star, 2e-5)   # 1e-5 Ha
-            r_sad, t_sad, _ = run_scf(sd, energy_target=target)
+            r_sad, t_sad, _ = run_scf(sd, energy_target=target, family=family)
             init = LearnedInit(params)
-            r_ml, t_ml, backend = run_scf(sd, init=init, energy_target=target)
+            r_ml, t_ml, backend = run_scf(sd, init=init, energy_target=target, family=family)
         except ValueError as exc:
             skipped.append(sd)
             log(f"  seed {sd} skipped: {exc}")
@@ -446,7 +511,7 @@ def evaluate(seeds, weights: Path, log=print) -> dict:
         e_sad, e_ml = r_sad.history[-1]["total_ry"], r_ml.history[-1]["total_ry"]
         # distance of each starting density from the converged one, in electrons: h^3 sum |rho_start - rho|
         rt = backend.runtime
-        prob, elem = water_system(sd, rt.settings)
+        prob, elem = family_system(family, sd, rt.settings)
         ctx = rt.context(prob.domain)
         rho0, _, _, _ = backend.pseudo_diag(prob.domain, prob.input_data.atoms, elem, len(elem), return_info=True)
         h3 = ctx.h ** 3
@@ -482,21 +547,24 @@ def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m parsec_python_b200.learned")
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
+    t.add_argument("--family", choices=sorted(FAMILIES), default="water")
     t.add_argument("--n-train", type=int, default=512)
     t.add_argument("--epochs", type=int, default=12)
     t.add_argument("--lr", type=float, default=2e-4)
-    t.add_argument("--out", type=Path, default=DEFAULT_WEIGHTS)
+    t.add_argument("--out", type=Path, default=None)
     e = sub.add_parser("eval")
+    e.add_argument("--family", choices=sorted(FAMILIES), default="water")
     e.add_argument("--first", type=int, default=512)
     e.add_argument("--count", type=int, default=64)
-    e.add_argument("--weights", type=Path, default=DEFAULT_WEIGHTS)
+    e.add_argument("--weights", type=Path, default=None)
     e.add_argument("--json", type=Path, default=None)
     a = ap.parse_args(argv)
     if a.cmd == "train":
-        meta = train(a.n_train, a.epochs, a.out, lr=a.lr)
+        meta = train(a.n_train, a.epochs, a.out or FAMILIES[a.family]["weights"], lr=a.lr, family=a.family)
         print(json.dumps({k: v for k, v in meta.items() if k != "losses"} | {"final_loss": meta["losses"][-1]}))
     else:
-        summ = evaluate(range(a.first, a.first + a.count), a.weights)
+        summ = evaluate(range(a.first, a.first + a.count), a.weights or FAMILIES[a.family]["weights"],
+                        family=a.family)
         if a.json:
             a.json.write_text(json.dumps(summ, indent=1))
         print(json.dumps({k: v for k, v in summ.items() if k != "rows"}))

@@ -55,6 +55,9 @@ class SolverSettings:
     init: str = "sad"            # sad | learned
     seed: int = 0
     mixed_switch: float = 1e-4   # mixed precision: FP64 subspace blocks once the SCF error is below this
+    mask: str = "cube"           # cube (the reference's domain) | sphere (H zero outside the inscribed sphere)
+    first_tol: float = 0.08      # first_filt: stop when the Ritz trace moves by <= this fraction (first_filt.py:14)
+    first_rounds: int = 0        # first_filt: most filter rounds; 0 = the reference's max(min(60 / polm, 5), 3)
 
     _KEYS = {
         "fd_order": ("fd_order", int), "maxits": ("maxits", int), "tol": ("tol", _parse_tol),
@@ -65,6 +68,7 @@ class SolverSettings:
         "gpu": ("use_gpu", _parse_bool), "recenter_atoms": ("recenter_atoms", _parse_bool),
         "recenter": ("recenter_atoms", _parse_bool), "precision": ("precision", str),
         "init": ("init", str), "seed": ("seed", int), "mixed_switch": ("mixed_switch", float),
+        "mask": ("mask", str), "first_tol": ("first_tol", float), "first_rounds": ("first_rounds", int),
     }
 
     def normalize(self) -> None:
@@ -88,6 +92,11 @@ class SolverSettings:
         if self.init not in ("sad", "learned"):
             self.init = "sad"
         self.mixed_switch = float(self.mixed_switch)
+        self.first_tol = float(self.first_tol)
+        self.first_rounds = max(0, int(self.first_rounds))
+        self.mask = str(self.mask).lower()
+        if self.mask not in ("cube", "sphere"):
+            self.mask = "cube"
 
     def apply_overrides(self, overrides: dict[str, Any] | None) -> dict[str, Any]:
         """Apply known keys (case-insensitive), drop unknown ones, return what changed."""

@@ -98,7 +98,7 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
     if init_density is None and s.init == "learned":
         from . import learned
 
-        params = learned.load_weights()
+        params = learned.load_weights(learned.weights_for(problem.input_data.atoms))
         if params is not None:
             init_density = learned.LearnedInit(params)
         else:

@@ -8,6 +8,8 @@ No public dataset is involved; every structure is generated:
                            first `shells` neighbour-distance shells of an
                            atom-centred Si (4 -> Si35H36, 7 -> Si87H76), every
                            dangling bond capped by H at 1.48 along the bond
+  sih_random_cluster(seed) Si(n)H(m), n ~ U{5..35}, grown on the same lattice
+                           from an atom-centred Si, H-capped, default_rng(seed)
   water_cluster(seed)      (H2O)n, n ~ U{2..8}, rigid O-H 0.957 / 104.5 deg,
                            random positions in a 6 A ball with O-O >= 2.6,
                            random orientations, numpy default_rng(seed)
@@ -81,6 +83,43 @@ def sih_cluster(shells: int, a: float = 5.43, sih: float = 1.48):
     for p, s in zip(si, si_sub):
         for b in bond * (1.0 if s == 0 else -1.0):
             if tuple(np.round(p + b, 6)) not in si_set:
+                hs.append(p + sih * b / np.linalg.norm(b))
+    return group(["Si"] * len(si) + ["H"] * len(hs), list(si) + hs)
+
+
+def sih_random_cluster(seed: int, nmin: int = 5, nmax: int = 35, a: float = 5.43, sih: float = 1.48):
+    """Seeded hydrogen-passivated silicon cluster of n ~ U{nmin..nmax} Si
+    atoms: the diamond lattice (a = 5.43) grown from an atom-centred Si by
+    adding, one at a time, a random lattice site bonded to the cluster (drawn
+    with weight bonds^2 exp(-|r| / 0.8 A), so the clusters stay compact),
+    then every dangling bond capped by H at 1.48 along the bond.  The
+    training set of the learned start for the Si-H configurations."""
+    rng = np.random.default_rng(seed)
+    n_si = int(rng.integers(nmin, nmax + 1))
+    bond = np.array([[1, 1, 1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], dtype=float) * (a / 4)
+    key = lambda p: tuple(np.round(p, 6))  # noqa: E731
+    si = [np.zeros(3)]
+    sub = [0]
+    have = {key(si[0])}
+    while len(si) < n_si:
+        cand: dict = {}
+        for p, s in zip(si, sub):
+            for b in bond * (1.0 if s == 0 else -1.0):
+                q = p + b
+                kq = key(q)
+                if kq not in have:
+                    c = cand.setdefault(kq, [q, 1 - s, 0])
+                    c[2] += 1
+        keys = sorted(cand)
+        w = np.array([cand[k][2] ** 2 * np.exp(-np.linalg.norm(cand[k][0]) / 0.8) for k in keys], dtype=float)
+        pick = cand[keys[int(rng.choice(len(keys), p=w / w.sum()))]]
+        si.append(pick[0])
+        sub.append(pick[1])
+        have.add(key(pick[0]))
+    hs = []
+    for p, s in zip(si, sub):
+        for b in bond * (1.0 if s == 0 else -1.0):
+            if key(p + b) not in have:
                 hs.append(p + sih * b / np.linalg.norm(b))
     return group(["Si"] * len(si) + ["H"] * len(hs), list(si) + hs)
 

@@ -10,7 +10,13 @@ seed 0, to the given tolerance.  It writes tests/golden/ref_<name>_tol<e>.json
 and .npz in the layout of make_golden_configs.py, with "source" set to
 "oracle".
 
-Usage: python tests/golden/make_golden_oracle_configs.py NAME [--tol=1e-8] [--maxits=80]
+The SCF fixed point does not depend on the Hartree solver (at convergence
+the warm-started CG converges the potential either way); --cg_prec=1 reaches
+it in fewer iterations (the oracle's spectral preconditioner) and keeps the
+msecant1 mixer away from the history blow-ups a long plain-CG run meets at
+this size.
+
+Usage: python tests/golden/make_golden_oracle_configs.py NAME [--tol=1e-8] [--maxits=80] [--cg_prec=1]
 """
 from __future__ import annotations
 
@@ -26,7 +32,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 
 
-def main(name: str, tol: float, maxits: int) -> None:
+def main(name: str, tol: float, maxits: int, cg_prec: int = 0) -> None:
     from oracle import oracle as O
     from parsec_python_b200 import workloads as w
 
@@ -35,7 +41,7 @@ def main(name: str, tol: float, maxits: int) -> None:
     tag = f"{name}_tol{int(round(-np.log10(tol)))}"
     np.random.seed(0)
     scf = O.OracleSCF(dom, cfg["atoms"], nev=cfg["nev"], poldeg=cfg["poldeg"], tol=tol, maxits=maxits,
-                      operator="stencil")
+                      operator="stencil", cg_prec=cg_prec)
     t0 = time.time()
     scf.setup()
     print(f"setup {scf.t_setup:.1f} s, n = {scf.n}", flush=True)
@@ -53,11 +59,13 @@ def main(name: str, tol: float, maxits: int) -> None:
                         eigen_sum_ry=np.array(fin["eigen_sum_ry"]), hartree_ry=np.array(fin["hartree_ry"]),
                         xc_ry=np.array(fin["xc_ry"]), ion_ry=np.array(fin["ion_ry"]), log_total_ry=np.array(hist),
                         log_err=np.array(errs))
-    meta = {"name": name, "source": "oracle", "operator": "stencil", "domain": dom, "nev": cfg["nev"],
+    meta = {"name": name, "source": "oracle", "operator": "stencil", "cg_prec": cg_prec, "domain": dom,
+            "nev": cfg["nev"],
             "poldeg": cfg["poldeg"], "tol": tol, "seed": 0, "iterations": res["iterations"],
             "error": float(res["error"]), "converged": bool(res["converged"]), "wall_s": wall,
             "total_ry": fin["total_ry"], "cpu": os.cpu_count(),
-            "iterations_to_1e-6": next((i + 1 for i, e in enumerate(errs) if e <= 1e-6), None)}
+            "iterations_to_1e-6": next((i + 1 for i, e in enumerate(errs) if e <= 1e-6), None),
+            "log_err": errs}
     (HERE / f"ref_{tag}.json").write_text(json.dumps(meta, indent=1))
     print(json.dumps(meta), flush=True)
 
@@ -67,4 +75,4 @@ if __name__ == "__main__":
     opts = dict(a[2:].split("=", 1) for a in sys.argv[1:] if a.startswith("--") and "=" in a)
     if not args:
         sys.exit(f"usage: python {sys.argv[0]} NAME [--tol=1e-8] [--maxits=80]")
-    main(args[0], float(opts.get("tol", 1e-8)), int(opts.get("maxits", 80)))
+    main(args[0], float(opts.get("tol", 1e-8)), int(opts.get("maxits", 80)), int(opts.get("cg_prec", 0)))

@@ -158,7 +158,7 @@ def test_dense_building_blocks():
     dom = {"nx": 20, "ny": 20, "nz": 20, "h": 0.5, "radius": 4.75}
     ctx = gpu.GridContext(dom, 8)
     rng = np.random.default_rng(6)
-    for k in (6, 27, 55, 130, 151, 200):  # Cholesky + inverse on chip up to 151, two kernels beyond
+    for k in (6, 27, 55, 130, 151, 200, 307):  # Cholesky + inverse on chip up to 151, blocked beyond
         W = rng.standard_normal((ctx.n, k))
         V = rng.standard_normal((ctx.n, k))
         g = ctx.empty(k, k)
@@ -196,7 +196,7 @@ def test_dense_building_blocks():
 @pytest.mark.parametrize("k", [8, 160])
 def test_cholesky_flags_rank_deficient_block(k):
     """A zero column makes its Cholesky pivot exactly 0: status word 1 names
-    it (column 3 -> 4), on chip (k = 8) and in the two-kernel form (k = 160)."""
+    it (column 3 -> 4), on chip (k = 8) and in the blocked form (k = 160)."""
     dom = {"nx": 20, "ny": 20, "nz": 20, "h": 0.5, "radius": 4.75}
     ctx = gpu.GridContext(dom, 8)
     W = np.random.default_rng(k).standard_normal((ctx.n, k))
@@ -212,9 +212,10 @@ def test_cholesky_flags_rank_deficient_block(k):
                                     (200, "neardiag"), (307, "rand"), (1024, "neardiag")])
 def test_syev_edge_cases(k, kind):
     """Householder + bisection + inverse iteration eigensolver: orders with
-    no reflector (1, 2) and one (3), the three CTA sizes (256 threads up to
-    k = 96, 512 up to 153 with the matrix on chip, 1024 with it in global
-    scratch beyond), the widest block (1024), an input that is already
+    no reflector (1, 2) and one (3), the four reductions (one CTA of 256
+    threads up to k = 96, of 512 up to 153 with the matrix on chip, a cluster
+    of 8 CTAs holding it in their shared memory up to about k = 420 (200,
+    307), one CTA with it in global scratch beyond), the widest block (1024), an input that is already
     diagonal (every reflector the identity), eigenvalues of multiplicity 14
     and 28 (one inverse-iteration cluster each), the zero matrix, nearly
     diagonal RR matrices."""
@@ -284,6 +285,41 @@ def test_gram_pair_tensor_cores_match_fp64(shape, k):
         assert np.abs(S - S_ref).max() <= tol * np.abs(S_ref).max(), impl
         assert np.abs(K - (K_tc if impl == 1 else K_sym)).max() <= tol * np.abs(K_ref).max(), impl
         assert np.array_equal(S, S.T) and np.array_equal(K, K.T)
+        # the diagonals (column norms, Rayleigh quotients) are FP64 sums on
+        # both paths: no bias from the tensor cores' FP32 accumulation
+        assert rel(np.diag(S), np.diag(S_ref)) < 1e-13, impl
+        assert np.abs(np.diag(K) - np.diag(K_ref)).max() < 1e-13 * np.abs(K_ref).max(), impl
+
+
+@pytest.mark.parametrize("shape,k,kout", [((30, 28, 26), 27, 27), ((40, 40, 40), 55, 55), ((24, 24, 24), 143, 143),
+                                          ((40, 40, 40), 307, 307), ((21, 20, 19), 300, 260),
+                                          ((16, 16, 16), 64, 30), ((12, 12, 12), 5, 3), ((33, 31, 29), 55, 40)])
+def test_block_product_tensor_cores_match_fp64(shape, k, kout):
+    """FP32 block product Out = W T (the Rayleigh-Ritz W R^{-1} Y) on tcgen05
+    (3xTF32, FP32 accumulation over k) and on CUDA cores (FP64 arithmetic),
+    against the FP64 product of the same FP32 W and FP64 T.  kout > 256 uses
+    the second accumulator; an odd n (33 x 31 x 29) takes the CUDA-core path.
+    Bound 2e-5 of the largest entry for the tensor cores (the FP32
+    accumulation over k terms), FP32 rounding of the result for the CUDA
+    cores."""
+    nx, ny, nz = shape
+    ctx = gpu.GridContext({"nx": nx, "ny": ny, "nz": nz, "h": 0.4, "radius": 0.2 * (nx - 1)}, 8)
+    n = ctx.n
+    rng = np.random.default_rng(k + kout)
+    W = rng.standard_normal((k, n)).astype(np.float32)
+    T = rng.standard_normal((k, kout)) / np.sqrt(k)
+    Wd = torch.from_numpy(W).to(DEV)
+    Td = torch.from_numpy(np.ascontiguousarray(T.T)).to(DEV)        # column-major k x kout, ld k
+    ref = W.astype(np.float64).T @ T                                # n x kout
+    for impl, tol in ((1, 2e-5), (0, 1.2e-7)):
+        ctx.call("psc_set_gemm_impl", impl)
+        out = torch.full((kout, n), np.nan, dtype=torch.float32, device=DEV)
+        for _ in range(2):   # twice: the second call reuses the split T buffer
+            ctx.call("psc_gemm_nn", F32, gpu._p(Wd), n, k, gpu._p(Td), kout, gpu._p(out), n, gpu._stream())
+        got = out.cpu().numpy().T.astype(np.float64)
+        assert np.isfinite(got).all(), impl
+        assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), (impl, np.abs(got - ref).max() / np.abs(ref).max())
+    assert ctx.status()[6] == 0
 
 
 def test_occupations_match_reference(golden_dir):

@@ -1,0 +1,116 @@
+"""Sphere-masked Hamiltonian (mask = sphere): H X is zero outside the sphere
+inscribed in the cube, and the TMA stencil reads nothing for the planes of a
+slab that hold no point inside.  The reference solves on the whole cube
+(Laplacian/fd3d.py:34-106), which stays the parity mode; these tests check
+the masked operator against the oracle's cube operator followed by the mask
+(P B X for blocks X that vanish outside), that every point outside comes out
+exactly zero whatever the output buffer held, and how far a masked SCF lands
+from the cube SCF."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - collected on CPU runs
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from parsec_python_b200 import gpu, workloads  # noqa: E402
+from parsec_python_b200._lib import F32, F64  # noqa: E402
+from parsec_python_b200.inputs import ElementTable, pseudo_tables  # noqa: E402
+
+DEV = torch.device("cuda", 0)
+A0 = O.A0_ANG
+
+
+def _h2o():
+    return [{"typ": "O", "coord": np.array([[0.0, 0.0, 0.0]]) / A0},
+            {"typ": "H", "coord": np.array([[0.757, 0.586, 0.0], [-0.757, 0.586, 0.0]]) / A0}]
+
+
+def _mask(dom):
+    nx, ny, nz, h = dom["nx"], dom["ny"], dom["nz"], dom["h"]
+    c = 0.5 * h * (np.array([nx, ny, nz]) - 1)
+    x = np.arange(nx) * h - c[0]
+    y = np.arange(ny) * h - c[1]
+    z = np.arange(nz) * h - c[2]
+    d2 = (x[None, None, :] ** 2 + y[None, :, None] ** 2) + z[:, None, None] ** 2
+    return (d2 <= dom["radius"] ** 2).ravel()
+
+
+@pytest.mark.parametrize("nx,k", [(32, 5), (40, 27), (26, 1)])
+def test_masked_hamiltonian_matches_masked_oracle(nx, k):
+    dom = O.build_system(_h2o(), h=0.5, radius=0.25 * (nx - 1))
+    assert dom["nx"] == nx
+    n = nx ** 3
+    E, T = O.load_elements(), O.load_tables()
+    projs = O.projectors(dom, _h2o(), E, T)
+    _, h0, pp, _ = O.pseudo_diag(dom, _h2o(), E, T)
+    pot = pp + h0
+    B = (0.5 * O.laplacian(dom, 8) + O.nonlocal_csr(projs, n) + sp.diags(pot, 0, shape=(n, n))).tocsr()
+    inside = _mask(dom)
+    X = np.random.default_rng(nx + k).standard_normal((n, k)) * inside[:, None]
+    ref = (B @ X) * inside[:, None]
+    ctx = gpu.GridContext(dom, 8)
+    gpu.projector_setup(ctx, _h2o(), ElementTable(), pseudo_tables())
+    ctx.set_sphere_mask(dom["radius"])
+    H = gpu.Hamiltonian(ctx, torch.from_numpy(pot).to(DEV))
+    for dt, tol in ((torch.float64, 1e-12), (torch.float32, 2e-6)):
+        Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(DEV, dt)
+        Y = (H @ Xd).double().cpu().numpy().T
+        assert np.abs(Y - ref).max() <= tol * np.abs(ref).max(), dt
+        assert not Y[~inside].any()
+    assert ctx.inside_count() == int(inside.sum())
+    ctx.check_status()
+
+
+@pytest.mark.parametrize("impl", [0, 1])
+def test_masked_output_outside_is_exact_zero(impl):
+    """Whatever the output buffer held (NaN here), points outside come out 0:
+    written as zeros by the zero-fill work items (TMA path) or by the masking
+    pass after the register-queue kernel."""
+    dom = O.build_system(_h2o(), h=0.5, radius=0.25 * 31)
+    ctx = gpu.GridContext(dom, 8)
+    ctx.call("psc_set_stencil_impl", impl)
+    ctx.set_sphere_mask(dom["radius"])
+    inside = torch.from_numpy(_mask(dom)).to(DEV)
+    H = gpu.Hamiltonian(ctx, torch.zeros(ctx.n, dtype=torch.float64, device=DEV))
+    X = torch.randn(6, ctx.n, dtype=torch.float64, device=DEV) * inside
+    Y = torch.full_like(X, float("nan"))
+    ctx.call("psc_apply_h", F64, gpu._p(X), ctx.n, gpu._p(Y), ctx.n, 6, gpu._stream())
+    torch.cuda.synchronize()
+    assert torch.isfinite(Y).all()
+    assert float(Y[:, ~inside].abs().max()) == 0.0
+    assert float(Y[:, inside].abs().max()) > 0.0
+
+
+def test_masked_scf_lands_near_the_cube_scf(capsys):
+    """H2O, the configuration's spacing (0.2 A) in a 5 A sphere: the SCF with
+    the sphere-masked Hamiltonian against the cube SCF at tol 1e-8; the
+    energy difference is reported (it is the cost of dropping the corners)."""
+    from parsec_python_b200.backend import select_solver_backend
+    from parsec_python_b200.models import SolverSettings
+    from parsec_python_b200.solver import run_rsdft_calculation
+    from parsec_python_b200.system import system_from_atoms
+
+    cfg = workloads.config_system("h2o")
+    out = {}
+    for mask in ("cube", "sphere"):
+        s = SolverSettings(tol=1e-8, poldeg=cfg["poldeg"], maxits=80, mask=mask, seed=4)
+        s.normalize()
+        elem = ElementTable()
+        prob = system_from_atoms(cfg["atoms"], h=cfg["h"], radius=cfg["radius"], nev=cfg["nev"], settings=s,
+                                 elem=elem)
+        res = run_rsdft_calculation(prob, elem, len(elem), select_solver_backend(s), verbose=False)
+        assert res.converged, mask
+        out[mask] = res
+    de = abs(out["sphere"].history[-1]["total_ry"] - out["cube"].history[-1]["total_ry"]) / 2
+    nocc = int(np.count_nonzero(out["cube"].occupations > 1e-6))
+    dlam = float(np.abs(out["sphere"].eigenvalues[:nocc] - out["cube"].eigenvalues[:nocc]).max())
+    with capsys.disabled():
+        print(f"\nH2O sphere vs cube: |dE| {de:.2e} Ha, max |d lambda| (occupied) {dlam:.2e} Ha, "
+              f"{out['sphere'].iterations} vs {out['cube'].iterations} iterations")
+    assert de < 2e-5 and dlam < 2e-5

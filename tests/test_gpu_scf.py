@@ -37,12 +37,20 @@ def run_gpu(atoms_bohr, h, radius, nev, poldeg, tol, precision="fp64", seed=0, m
     return prob, run_rsdft_calculation(prob, elem, len(elem), backend, verbose=False)
 
 
+def occupied(ref, nev):
+    """States the reference occupies (f > 1e-6): their eigenvalues converge
+    with the density.  The empty states at the top of the nev window converge
+    only as fast as the filter reaches them, differently in every run."""
+    return int(np.count_nonzero(np.asarray(ref["occupations"])[:nev] > 1e-6))
+
+
 def check(prob, res, ref, nev):
     h = prob.domain["h"]
     e = res.history[-1]["total_ry"]
     assert res.converged
     assert abs(e - float(ref["total_ry"])) < E_TOL_RY, (e, float(ref["total_ry"]))
-    assert np.abs(res.eigenvalues[:nev] - ref["eigenvalues"][:nev]).max() < 1e-5
+    nocc = occupied(ref, nev)
+    assert np.abs(res.eigenvalues[:nocc] - ref["eigenvalues"][:nocc]).max() < 1e-5
     drho = np.abs(res.rho.cpu().numpy() - ref["rho"].astype(np.float64)).sum() * h ** 3
     assert drho < RHO_TOL, drho
     return e, drho
@@ -73,8 +81,11 @@ def test_scf_is_deterministic():
 # H2O converges to the same fixed point at the configuration's tol 1e-6 (the
 # reference's own seed-to-seed spread there is ~1e-6 Ha).  For C10H8 the
 # reference's seed-to-seed spread at tol 1e-6 is 2.2e-5 Ha, above the bar, so
-# both sides are compared at tol 1e-8.
-@pytest.mark.parametrize("name,tag", [("h2o", "h2o"), ("c10h8", "c10h8_tol8")])
+# both sides are compared at tol 1e-8; likewise Si35H36 (the reference's own
+# SCF) and Si87H76 (the oracle with its matrix-free operator: the reference's
+# CSR SCF would take many hours at 729,000 points and 292 states).
+@pytest.mark.parametrize("name,tag", [("h2o", "h2o"), ("c10h8", "c10h8_tol8"), ("si35h36", "si35h36_tol8"),
+                                      ("si87h76", "si87h76_tol8")])
 def test_benchmark_config_matches_reference(golden_dir, name, tag):
     f = golden_dir / f"ref_{tag}.npz"
     if not f.exists():
@@ -85,3 +96,37 @@ def test_benchmark_config_matches_reference(golden_dir, name, tag):
     prob, res = run_gpu(cfg["atoms"], cfg["h"], cfg["radius"], cfg["nev"], cfg["poldeg"], meta["tol"], maxits=80)
     assert prob.domain["nx"] == meta["domain"]["nx"]
     check(prob, res, ref, cfg["nev"])
+
+
+def _mixed_vs_reference(golden_dir, name, tag, switch):
+    f = golden_dir / f"ref_{tag}.npz"
+    if not f.exists():
+        pytest.skip(f"{f.name} not generated")
+    ref = np.load(f)
+    cfg = workloads.config_system(name)
+    s = SolverSettings(tol=1e-8, poldeg=cfg["poldeg"], maxits=80, precision="mixed", cg_prec=1, seed=2)
+    s.mixed_switch = switch
+    s.normalize()
+    elem = ElementTable()
+    prob = system_from_atoms(cfg["atoms"], h=cfg["h"], radius=cfg["radius"], nev=cfg["nev"], settings=s, elem=elem)
+    res = run_rsdft_calculation(prob, elem, len(elem), select_solver_backend(s), verbose=False)
+    nev, h = cfg["nev"], prob.domain["h"]
+    nocc = occupied(ref, nev)
+    de_ha = abs(res.history[-1]["total_ry"] - float(ref["total_ry"])) / HA
+    dlam_ha = float(np.abs(res.eigenvalues[:nocc] - ref["eigenvalues"][:nocc]).max())
+    drho = float(np.abs(res.rho.cpu().numpy() - ref["rho"].astype(np.float64)).sum() * h ** 3)
+    f32_its = sum(1 for r in res.history if r["block_dtype"] == "f32")
+    print(f"{name} mixed (switch {switch}): {res.iterations} its ({f32_its} FP32), |dE| {de_ha:.2e} Ha, "
+          f"max |d lambda| (occupied) {dlam_ha:.2e} Ha, int |d rho| {drho:.2e} e")
+    return res, de_ha, dlam_ha, drho
+
+
+@pytest.mark.parametrize("name,tag", [("si35h36", "si35h36_tol8"), ("si87h76", "si87h76_tol8")])
+def test_mixed_precision_matches_reference(golden_dir, name, tag):
+    """The chosen form (FP32 filter and tensor-core Rayleigh-Ritz products,
+    FP64 finish, preconditioned Hartree solve) driven to tol 1e-8 reaches the
+    reference's FP64 fixed point: energy and every occupied eigenvalue within
+    1e-5 Ha, integrated |delta rho| within 1e-4 e."""
+    res, de, dlam, drho = _mixed_vs_reference(golden_dir, name, tag, 1e-4)
+    assert res.converged
+    assert de < 1e-5 and dlam < 1e-5 and drho < RHO_TOL

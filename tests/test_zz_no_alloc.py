@@ -6,7 +6,9 @@ context, because creating one allocates.  This entry point needs no context:
 its scratch is a fixed device array inside the library.  The test calls it
 through the C ABI twice in a row, on different densities, and compares each
 result with the context-based psc_lda_xc at the tolerance of the other XC
-test (1e-13 relative on v_xc, 1e-12 on E_xc).  The file name sorts last so
+test (1e-13 relative on v_xc, 1e-12 on E_xc); it also checks the entry point
+against the reference's own exc_nspn fixture and that a call leaves the
+device's free memory unchanged.  The file name sorts last so
 that a run stopping at the first failure has already run every other test.
 """
 import ctypes
@@ -55,6 +57,52 @@ def test_noalloc_xc_matches_context_xc_on_two_calls():
         oa, ob = out_a.cpu().numpy(), out_b.cpu().numpy()
         assert abs(oa[0] - ob[0]) <= 1e-12 * abs(ob[0])
         assert oa[1] == ob[1] and oa[2] == ob[2]
+
+
+def test_noalloc_xc_matches_reference_fixture(golden_dir):
+    """Against the reference's own exc_nspn output (tests/golden/ref_xc.npz,
+    made by running V_xc/exc_nspn.py), the same bars as the context path's
+    test: 1e-13 on v_xc, 1e-12 on E_xc, exact max and min."""
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    xc = np.load(golden_dir / "ref_xc.npz")
+    rho = torch.from_numpy(xc["rho"]).to(dev)
+    vxc = torch.empty_like(rho)
+    out = torch.empty(3, dtype=torch.float64, device=dev)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert lib.psc_lda_xc_noalloc(_p(rho), _p(vxc), rho.numel(), 0.37 ** 3, _p(out), st) == 0
+    torch.cuda.synchronize()
+    v = vxc.cpu().numpy()
+    assert np.abs(v - xc["vxc"]).max() <= 1e-13 * np.abs(xc["vxc"]).max()
+    o = out.cpu().numpy()
+    assert abs(o[0] - float(xc["exc"])) <= 1e-12 * abs(float(xc["exc"]))
+    assert o[1] == xc["rho"].max() and o[2] == xc["rho"].min()
+
+
+def test_noalloc_xc_allocates_nothing_and_propagates_nan():
+    """After the first call (which may load the module), a call leaves the
+    device's free memory unchanged.  A NaN density makes the logged maximum
+    and minimum NaN on both entry points, as numpy's max and min do."""
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    n = 50_000
+    rho = torch.from_numpy(_densities(n, 3)).to(dev)
+    vxc = torch.empty_like(rho)
+    out = torch.empty(3, dtype=torch.float64, device=dev)
+    assert lib.psc_lda_xc_noalloc(_p(rho), _p(vxc), n, 1.0, _p(out), st) == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    assert lib.psc_lda_xc_noalloc(_p(rho), _p(vxc), n, 1.0, _p(out), st) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(dev)[0] == free0
+    rho[n // 3] = float("nan")
+    assert lib.psc_lda_xc_noalloc(_p(rho), _p(vxc), n, 1.0, _p(out), st) == 0
+    ctx = gpu.GridContext({"nx": n, "ny": 1, "nz": 1, "h": 1.0, "radius": 1.0}, 8)
+    _, out_b = gpu.lda_xc(ctx, rho)
+    torch.cuda.synchronize()
+    for o in (out.cpu().numpy(), out_b.cpu().numpy()):
+        assert np.isnan(o[1]) and np.isnan(o[2])
 
 
 def test_noalloc_xc_rejects_sizes_beyond_its_scratch():
