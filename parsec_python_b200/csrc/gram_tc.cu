@@ -7,7 +7,7 @@
 // Replaces the dense products of Rayleighritz.py:4-30 / chefsi1.py:43-67 in
 // the mixed-precision path; the FP64 path keeps the CUDA-core kernels.
 //
-// Grid: (chunk of the n rows) x (pair of 128-column tiles, upper triangle).
+// Grid: (pair of 128-column tiles, upper triangle) x (chunk of the n rows).
 // Each CTA streams its rows through a two-deep shared-memory ring, 32 rows
 // (one 128-byte swizzle row of FP32) per stage, the next stage's loads in
 // flight in registers while the current one is stored; its threads load and split
@@ -147,13 +147,15 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
   __shared__ int s_fail;
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5;
-  const int2 pr = pairs[blockIdx.y];
+  // blockIdx.x = tile pair, blockIdx.y = row chunk: the pairs of one chunk
+  // run side by side and stream the same rows, which they share through L2
+  const int2 pr = pairs[blockIdx.x];
   const int mt = pr.x, nt = pr.y;
   const int col_a = mt * TROWS, col_b = nt * TROWS;
   const int valid_a = min(TROWS, k - col_a), valid_b = min(TROWS, k - col_b);
   const int N = (valid_b + 15) & ~15;   // MMA N: multiple of 16 for M = 128
   const bool same = mt == nt;
-  const long n_begin = (long)blockIdx.x * chunk;
+  const long n_begin = (long)blockIdx.y * chunk;
   const long n_end = min(n, n_begin + chunk);
   const int nstage = (int)((max(0L, n_end - n_begin) + KSTAGE - 1) / KSTAGE);
   const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(W) & 15) == 0) &&
@@ -276,8 +278,8 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
       }
       const int row = (threadIdx.x >> 3) + u * (TC_NT / 8);
       if ((threadIdx.x & 7) == 0 && row < valid_a) {
-        dpart[((long)blockIdx.x * 2 + 0) * k + col_a + row] = dsum_s[u];
-        dpart[((long)blockIdx.x * 2 + 1) * k + col_a + row] = dsum_k[u];
+        dpart[((long)blockIdx.y * 2 + 0) * k + col_a + row] = dsum_s[u];
+        dpart[((long)blockIdx.y * 2 + 1) * k + col_a + row] = dsum_k[u];
       }
     }
   }
@@ -286,7 +288,7 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
   } else if (nstage > 0 && warp < 4) {
     // epilogue: warp w (< 4) owns TMEM lanes (= rows) 32w .. 32w+31
     const int row = warp * 32 + (threadIdx.x & 31);
-    float* ps = part + (((long)blockIdx.x * gridDim.y + blockIdx.y) * 2) * (TROWS * TROWS);
+    float* ps = part + (((long)blockIdx.y * gridDim.x + blockIdx.x) * 2) * (TROWS * TROWS);
     float* pk = ps + TROWS * TROWS;
     for (int which = 0; which < 2; ++which) {
       const uint32_t base = (which == 0 ? tmem_s : tmem_k) + ((uint32_t)(warp * 32) << 16);
@@ -406,7 +408,7 @@ int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int 
   const size_t smem = 2 * (size_t)BUF_BYTES + 1024;
   PSC_CUDA(ctx, cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   double* dpart = reinterpret_cast<double*>(ctx->tc_part + tile_floats);
-  k_gram_tc<<<dim3(nchunk, npair), TC_NT, smem, st>>>(W, V, ld, k, n, chunk, (const int2*)ctx->tc_pairs,
+  k_gram_tc<<<dim3(npair, nchunk), TC_NT, smem, st>>>(W, V, ld, k, n, chunk, (const int2*)ctx->tc_pairs,
                                                       ctx->tc_part, dpart, ctx->wait_limit, ctx->dev_status);
   PSC_LAUNCH_CHECK(ctx);
   const long total = (long)npair * TROWS * TROWS;

@@ -217,7 +217,10 @@ k_stencil_tma(TmaArgs<T> A) {
   const int nxy = nx * ny;
   const int H = R * nx;
   const int WIN = TS + 2 * H;
-  const int WS = WIN + VW;  // slot stride: the window and one zero vector
+  // slot stride: the window and one zero vector, rounded up to 16 bytes so
+  // that every slot starts where a bulk copy may write
+  constexpr int Q16 = 16 / (int)sizeof(T);
+  const int WS = (WIN + VW + Q16 - 1) / Q16 * Q16;
   T* ring = reinterpret_cast<T*>(smem_raw);                                   // [NBUF][WS]
   T* pring = ring + (size_t)NBUF * WS;                                        // [NS][2][TS]: Prev, pot
   uint64_t* bars = reinterpret_cast<uint64_t*>(pring + (size_t)NS * 2 * TS);  // [NBUF]
@@ -693,7 +696,8 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   const int4* sched = stencil_sched(ctx, nslab, k, fill, slots, masked, TS, &nwork, st);
   PSC_REQUIRE(ctx, sched != nullptr, "stencil: work table allocation failed");
   constexpr int NBUF = R + 1 + prefetch_depth<T>();
-  const size_t win = TS + 2 * (size_t)R * ctx->nx + VW;   // window + zero pad vector
+  constexpr size_t Q16 = 16 / sizeof(T);
+  const size_t win = (TS + 2 * (size_t)R * ctx->nx + VW + Q16 - 1) / Q16 * Q16;   // window + zero pad, 16-byte slots
   const size_t smem = (NBUF * win + (size_t)PP_SLOTS * 2 * TS) * sizeof(T) + NBUF * sizeof(uint64_t);
   if (smem > 220 * 1024) return -1;  // window too wide: the register-queue kernel takes it
   auto kern = (ctx->nx % VW == 0) ? k_stencil_tma<T, R, VW, VW>
