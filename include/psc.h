@@ -97,6 +97,9 @@ int psc_numpy_sum(psc_ctx* ctx, const double* x, long n, double* out_dev, void* 
 /* Diagonal potential (Hartree, device, n): B = 0.5A + V_nl + diag(pot) at
  * rsdft_solver.py:285 without assembling B. */
 int psc_set_potential(psc_ctx* ctx, const double* pot, void* stream);
+/* Y = V_nl X alone: the factored form of the matrix pseudoNL returns
+ * (V_ion/pseudoNL_original.py:187-206). */
+int psc_apply_nonlocal(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long ldy, int k, void* stream);
 /* Y = H X for k columns (the SpMM `H @ X` in the Eigensolvers package). */
 int psc_apply_h(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long ldy, int k, void* stream);
 /* Y = alpha H X + beta X + gamma P (P may be NULL or alias Y). */
@@ -131,6 +134,10 @@ int psc_cheb_filter(psc_ctx* ctx, int dtype, int mode, int deg, const double* bo
  * out = [uppbnd, ritz_0..ritz_5]; mode 1: Eigensolvers/lanczosForChefsi1.py:5-99,
  * out = [bound].  The start vector is drawn from `seed`. */
 int psc_lanczos_bound(psc_ctx* ctx, int mode, unsigned long long seed, double* out_dev, void* stream);
+/* The same from the caller's start vector v_start (device, n doubles): the
+ * vector lancz_uppbnd.py:22 draws (mode 0) or the one chefsi1.py:29 passes to
+ * lanczosForChefsi1 (mode 1). */
+int psc_lanczos_bound_v(psc_ctx* ctx, int mode, const double* v_start, double* out_dev, void* stream);
 /* Lanczos with a kept basis (Eigensolvers/lanczosForChsubsp.py:33-119 and
  * lanczos.py:38-139, no reorthogonalisation): runs steps k0 .. k1-1 of
  * w = H v_j - beta_{j-1} v_{j-1}, alpha_j = v_j.w, w -= alpha_j v_j,

@@ -39,6 +39,8 @@ _SIGS = {
     "psc_laplacian_apply": ([_P, _P, _P, c_int, c_long, _P], c_int),
     "psc_cheb_filter": ([_P, c_int, c_int, c_int, _P, _P, _P, c_long, c_int, POINTER(c_int), _P], c_int),
     "psc_lanczos_bound": ([_P, c_int, c_ulonglong, _P, _P], c_int),
+    "psc_lanczos_bound_v": ([_P, c_int, _P, _P, _P], c_int),
+    "psc_apply_nonlocal": ([_P, c_int, _P, c_long, _P, c_long, c_int, _P], c_int),
     "psc_lanczos_run": ([_P, _P, c_ulonglong, c_int, c_int, _P, c_long, _P, _P], c_int),
     "psc_tridiag_eig": ([_P, _P, c_int, c_int, _P, _P, c_long, _P], c_int),
     "psc_orthonormalize_rank": ([_P, c_int, _P, _P, c_long, c_int, c_double, POINTER(c_int), POINTER(c_int), _P],

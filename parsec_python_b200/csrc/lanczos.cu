@@ -546,13 +546,14 @@ __global__ void k_lz_bound6(const double* __restrict__ ev, const double* __restr
   }
 }
 
-int psc_lanczos_bound_basis(psc_ctx* ctx, unsigned long long seed, double* out_dev, cudaStream_t st) {
+int psc_lanczos_bound_basis(psc_ctx* ctx, unsigned long long seed, const double* v_start, double* out_dev,
+                            cudaStream_t st) {
   constexpr int m = 6;
   const long n = ctx->n;
   if (!ctx->lz_basis) PSC_CUDA(ctx, psc_dmalloc(&ctx->lz_basis, (size_t)(m + 1) * n * sizeof(double)));
   double* ab = ctx->scalars + 160;  // [2m] alpha, beta
   double* ev = ctx->scalars + 176;  // [m]
-  int rc = psc_lanczos_run(ctx, nullptr, seed, 0, m, ctx->lz_basis, n, ab, st);
+  int rc = psc_lanczos_run(ctx, v_start, seed, 0, m, ctx->lz_basis, n, ab, st);
   if (rc) return rc;
   rc = psc_tridiag_eig(ctx, ab, m, 0, ev, nullptr, 0, st);
   if (rc) return rc;

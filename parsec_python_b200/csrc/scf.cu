@@ -73,14 +73,17 @@ __global__ void k_lz_bound(const double* sc, int m, const double* ritz, const do
 //           out = [uppbnd, ritz_0..ritz_5] (ritz ascending)
 //   mode 1: lanczosForChefsi1 (Eigensolvers/lanczosForChefsi1.py:5-99):
 //           normal start, out = [max|ritz| + beta_6]
-int psc_lanczos_bound_basis(psc_ctx* ctx, unsigned long long seed, double* out_dev, cudaStream_t st);
+int psc_lanczos_bound_basis(psc_ctx* ctx, unsigned long long seed, const double* v_start, double* out_dev,
+                            cudaStream_t st);
 
-extern "C" int psc_lanczos_bound(psc_ctx* ctx, int mode, unsigned long long seed, double* out_dev, void* stream) {
-  if (!ctx) return 2;
-  cudaStream_t st = (cudaStream_t)stream;
+// The six-step bounds; v_start (device, n, may be NULL) replaces the vector
+// drawn from `seed` (the reference draws np.random.rand for lancz_uppbnd and
+// np.random.randn for chefsi1's lanczosForChefsi1).
+static int lanczos_bound_impl(psc_ctx* ctx, int mode, unsigned long long seed, const double* v_start,
+                              double* out_dev, cudaStream_t st) {
   // mode 1 runs the three-term recurrence of psc_lanczos_run (the same steps,
   // fused, keeping a basis of 7 vectors) and bisection on T_6
-  if (mode != 0) return psc_lanczos_bound_basis(ctx, seed, out_dev, st);
+  if (mode != 0) return psc_lanczos_bound_basis(ctx, seed, v_start, out_dev, st);
   const long n = ctx->n;
   const int m = 6;
   if (psc_ensure_dense(ctx, m)) return 1;
@@ -89,8 +92,13 @@ extern "C" int psc_lanczos_bound(psc_ctx* ctx, int mode, unsigned long long seed
   double* f = ctx->lz_v + 2 * n;
   double* sc = ctx->scalars;  // [0..31]
   const int nb = 148 * 8;
-  int rc = psc_random_impl(ctx, PSC_F64, mode == 0 ? 0 : 1, seed, f, n, n, 1, st);
-  if (rc) return rc;
+  int rc = 0;
+  if (v_start) {
+    PSC_CUDA(ctx, cudaMemcpyAsync(f, v_start, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  } else {
+    rc = psc_random_impl(ctx, PSC_F64, mode == 0 ? 0 : 1, seed, f, n, n, 1, st);
+    if (rc) return rc;
+  }
   // v = f / ||f||
   const double* a1[1] = {f};
   rc = psc_dots(ctx, 1, a1, a1, n, sc + 2, st);
@@ -146,6 +154,17 @@ extern "C" int psc_lanczos_bound(psc_ctx* ctx, int mode, unsigned long long seed
     PSC_LAUNCH_CHECK(ctx);
   }
   return 0;
+}
+
+extern "C" int psc_lanczos_bound(psc_ctx* ctx, int mode, unsigned long long seed, double* out_dev, void* stream) {
+  if (!ctx) return 2;
+  return lanczos_bound_impl(ctx, mode, seed, nullptr, out_dev, (cudaStream_t)stream);
+}
+
+extern "C" int psc_lanczos_bound_v(psc_ctx* ctx, int mode, const double* v_start, double* out_dev, void* stream) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, v_start && out_dev, "lanczos_bound_v: NULL pointer argument");
+  return lanczos_bound_impl(ctx, mode, 0, v_start, out_dev, (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------

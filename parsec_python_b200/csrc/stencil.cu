@@ -274,6 +274,21 @@ int psc_apply_h_impl(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, 
   return 0;
 }
 
+// Y = V_nl X alone (the factored Kleinman-Bylander term), for checks against
+// the reference's V_nl matrix without the Laplacian around it.
+extern "C" int psc_apply_nonlocal(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long ldy, int k,
+                                  void* stream) {
+  if (!ctx) return 2;
+  cudaStream_t st = (cudaStream_t)stream;
+  PSC_REQUIRE(ctx, X && Y && X != Y && k >= 1 && ldx >= ctx->n && ldy >= ctx->n, "apply_nonlocal: bad arguments");
+  const size_t es = dtype == PSC_F64 ? sizeof(double) : sizeof(float);
+  PSC_CUDA(ctx, cudaMemset2DAsync(Y, ldy * es, 0, ctx->n * es, k, st));
+  if (ctx->nl_atoms == 0) return 0;
+  int rc = psc_nl_project(ctx, dtype, X, ldx, k, st);
+  if (rc) return rc;
+  return psc_nl_scatter(ctx, dtype, Y, ldy, k, nullptr, 1.0, st);
+}
+
 extern "C" int psc_apply_h(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long ldy, int k,
                            void* stream) {
   if (!ctx) return 2;

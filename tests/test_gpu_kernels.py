@@ -16,7 +16,7 @@ torch = pytest.importorskip("torch")
 if not torch.cuda.is_available():  # pragma: no cover - collected on CPU runs
     pytest.skip("needs a CUDA device", allow_module_level=True)
 
-from parsec_python_b200 import _lib, gpu  # noqa: E402
+from parsec_python_b200 import _lib, gpu, workloads  # noqa: E402
 from parsec_python_b200._lib import F32, F64  # noqa: E402
 from parsec_python_b200.inputs import ElementTable, pseudo_tables  # noqa: E402
 
@@ -118,12 +118,39 @@ def test_hamiltonian_fp64_matches_reference_operator(h2o_box, golden_dir):
         X = rng.standard_normal((ctx.n, k))
         Y = host(H @ block(X))
         assert rel(Y, B @ X) < 1e-12, k
-    # the reference's own V_nl (pseudoNL_original) through H - 0.5A - diag(pot)
+    # the reference's own V_nl (the pseudoNL_original matrix times vnl_x)
+    # against the projector apply alone
     ion = np.load(golden_dir / "ref_ion_h2o.npz")
-    X = ion["vnl_x"]
-    Hz = gpu.Hamiltonian(ctx, torch.zeros(ctx.n, dtype=torch.float64, device=DEV))
-    vnl = host(Hz @ block(X)) - 0.5 * (O.laplacian(mi["domain"], 8) @ X)
-    assert rel(vnl, ion["vnl_y"]) < 1e-9
+    X, ref = ion["vnl_x"], ion["vnl_y"]
+    Xd = block(X)
+    Yd = torch.full_like(Xd, float("nan"))
+    k = Xd.shape[0]
+    ctx.call("psc_apply_nonlocal", F64, gpu._p(Xd), ctx.n, gpu._p(Yd), ctx.n, k, gpu._stream())
+    vnl = host(Yd)
+    assert np.abs(vnl - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_hamiltonian_matches_reference_csr_on_h2o_grid(golden_dir):
+    """H X on the H2O configuration's own grid (52^3, 0.2 A, O-H projectors)
+    against the reference's assembled CSR B = 0.5 A + V_nl + diag(pot)
+    (rsdft_solver.py:263,285) applied to the same seeded columns, FP64, to
+    1e-12 of the largest entry; FP32 blocks to FP32 rounding."""
+    ref = np.load(golden_dir / "ref_hx_h2o.npz")
+    cfg = workloads.config_system("h2o")
+    dom = O.build_system(cfg["atoms"], h=cfg["h"], radius=cfg["radius"])
+    assert dom["nx"] == int(ref["nx"]) == 52 and abs(dom["h"] - float(ref["h"])) < 1e-15
+    ctx = gpu.GridContext(dom, 8)
+    gpu.projector_setup(ctx, cfg["atoms"], ElementTable(), pseudo_tables())
+    H = gpu.Hamiltonian(ctx, torch.from_numpy(ref["pot"]).to(DEV))
+    X = np.random.default_rng(11).standard_normal((ctx.n, 2))
+    y = ref["y"]
+    for impl in (0, 1):
+        ctx.call("psc_set_stencil_impl", impl)
+        got = host(H @ block(X))
+        assert np.abs(got - y).max() <= 1e-12 * np.abs(y).max(), impl
+        got32 = host(H @ block(X).float()).astype(np.float64)
+        assert np.abs(got32 - y).max() <= 2e-6 * np.abs(y).max(), impl
+    ctx.check_status()
 
 
 def test_hamiltonian_fp32(h2o_box, golden_dir):
@@ -360,6 +387,31 @@ def test_pcg_matches_reference(golden_dir):
                      200, 1e-5)
     assert abs(its - int(pc["its"])) <= 1
     assert rel(x.cpu().numpy(), pc["x"]) < 1e-9
+
+
+def test_lanczos_bounds_with_reference_start_vectors(h2o_box, golden_dir):
+    """The reference's bounds came from lancz_uppbnd after np.random.seed(7)
+    (its start vector is np.random.rand(n, 1), lancz_uppbnd.py:22) and from
+    lanczosForChefsi1 on np.random.randn(n, 1) after np.random.seed(8): the
+    same start vectors passed in give the same bound and Ritz values to
+    1e-12 (the recurrence is a handful of H products and dot products)."""
+    ctx, atoms, mi = h2o_box
+    gpu.projector_setup(ctx, atoms, ElementTable(), pseudo_tables())
+    ev = np.load(golden_dir / "ref_eigs.npz")
+    gpu.Hamiltonian(ctx, torch.from_numpy(ev["pot"]).to(DEV))
+    np.random.seed(7)
+    v0 = torch.from_numpy(np.random.rand(ctx.n)).to(DEV)
+    np.random.seed(8)
+    v1 = torch.from_numpy(np.random.randn(ctx.n)).to(DEV)
+    out = ctx.empty(8)
+    ctx.call("psc_lanczos_bound_v", 0, gpu._p(v0), gpu._p(out), gpu._stream())
+    b0 = out.cpu().numpy().copy()
+    ctx.call("psc_lanczos_bound_v", 1, gpu._p(v1), gpu._p(out), gpu._stream())
+    b1 = out.cpu().numpy().copy()
+    assert abs(b0[0] - float(ev["uppbnd"])) <= 1e-12 * abs(float(ev["uppbnd"]))
+    assert np.abs(b0[1:7] - ev["ritz"]).max() <= 1e-12 * np.abs(ev["ritz"]).max()
+    assert abs(b1[0] - float(ev["bound"])) <= 1e-12 * abs(float(ev["bound"]))
+    ctx.check_status()
 
 
 def test_lanczos_bounds_bracket_the_spectrum(h2o_box, golden_dir):

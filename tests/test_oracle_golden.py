@@ -75,6 +75,26 @@ def test_pseudo_diag_and_projectors(golden_dir, meta, tables):
     assert O.nuclear(atoms, elements) == mi["e_nuc"]
 
 
+def test_hamiltonian_on_h2o_grid_matches_reference_csr(golden_dir, tables):
+    """The oracle's B = 0.5 A + V_nl + diag(pot) on the H2O configuration's
+    52^3 grid against the reference's assembled CSR applied to the same two
+    seeded columns (tests/golden/make_golden_hx.py), CSR and matrix-free."""
+    from parsec_python_b200 import workloads
+
+    elements, tab = tables
+    ref = np.load(golden_dir / "ref_hx_h2o.npz")
+    cfg = workloads.config_system("h2o")
+    dom = O.build_system(cfg["atoms"], h=cfg["h"], radius=cfg["radius"])
+    n = dom["nx"] ** 3
+    projs = O.projectors(dom, cfg["atoms"], elements, tab)
+    B = (0.5 * O.laplacian(dom, 8) + O.nonlocal_csr(projs, n) + sp.diags(ref["pot"], 0, shape=(n, n))).tocsr()
+    X = np.random.default_rng(11).standard_normal((n, 2))
+    y = ref["y"]
+    assert np.abs(B @ X - y).max() <= 1e-13 * np.abs(y).max()
+    Hs = O.StencilHamiltonian(dom, 8, projs, ref["pot"])
+    assert np.abs(Hs @ X - y).max() <= 1e-12 * np.abs(y).max()
+
+
 def test_sample_h2o_sad_density_bit_exact(meta, tables):
     """Known-answer test: the shipped samples/h2o/*_init_rho_grid.npy."""
     elements, tab = tables
