@@ -25,9 +25,15 @@ FP32 accumulation; all kernels in csrc/unet.cu):
     u0  3^3  up(u1) + e0 -> 8   full
     out 1^3  8 -> 8 (channel 0 = correction), linear
 
-Training data come from this project's own FP64 GPU SCF on seeded water
-clusters; training runs on the GPU through psc_conv3d_fwd / psc_conv3d_bwd /
-psc_adam_step.
+Training data come from this project's own FP64 GPU SCF on seeded systems of
+two families (water clusters; hydrogen-capped silicon clusters).  `generate`
+writes a training set with one replica per GPU under torchrun (a strided
+share of the seeds per rank, no exchange but one host barrier); training
+runs on one GPU through psc_conv3d_fwd / psc_conv3d_bwd / psc_adam_step,
+from such a set or generating its samples itself.
+
+    torchrun --nproc-per-node 8 -m parsec_python_b200.learned generate --family sih --out DIR
+    python -m parsec_python_b200.learned train --family sih --data DIR
 """
 from __future__ import annotations
 
@@ -420,13 +426,116 @@ def make_sample(seed: int, family: str = "water"):
 TRAIN_SEEDS = 512        # geometries 0..511 train the network; 512.. are held out
 
 
+def partition_seeds(seeds, rank: int, world: int) -> list:
+    """The geometries one replica generates: every world-th seed from position
+    rank.  Cluster sizes are drawn independently per seed, so the strided
+    split balances the ranks' work without a schedule; the union over ranks is
+    every seed exactly once."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} outside a world of {world}")
+    return list(seeds)[rank::world]
+
+
+def sample_arrays(seed: int, family: str):
+    """One training sample as host arrays: SAD density (e/bohr^3), V_loc, the
+    converged - SAD density (all FP32, x fastest), the domain and the SCF's
+    iteration count."""
+    ctx, rs, vl, dt, res = make_sample(seed, family)
+    dom = {"nx": ctx.nx, "ny": ctx.ny, "nz": ctx.nz, "h": ctx.h, "radius": ctx.radius}
+    return (rs.float().cpu().numpy(), vl.float().cpu().numpy(), dt.float().cpu().numpy(), dom,
+            int(res.iterations))
+
+
+def generate(family: str, seeds, out_dir: Path, rank: int = 0, world: int = 1, sample_fn=None, log=print) -> dict:
+    """Training samples of one replica into out_dir/<family>_<seed>.npz.
+
+    Each rank runs its share of the seeds (partition_seeds) on its own GPU,
+    one SCF per geometry, with no exchange between ranks; a file already
+    present is kept, so an interrupted run resumes.  Seeds whose SCF stops
+    with ValueError (the reference's "Bounds are incorrect") are listed as
+    skipped.  The rank's record goes to out_dir/manifest_rank<r>.json;
+    merge_manifests joins them once every rank is done."""
+    sample_fn = sample_fn or sample_arrays
+    out_dir = Path(out_dir)
+    out_dir.mkdir(parents=True, exist_ok=True)
+    done, skipped, t0 = [], [], time.perf_counter()
+    for sd in partition_seeds(seeds, rank, world):
+        path = out_dir / f"{family}_{sd:05d}.npz"
+        if path.exists():
+            done.append(sd)
+            continue
+        try:
+            rs, vl, dt, dom, its = sample_fn(sd, family)
+        except ValueError as exc:
+            skipped.append(sd)
+            log(f"  rank {rank}: seed {sd} skipped: {exc}")
+            continue
+        tmp = path.with_name(path.stem + f".part{rank}.npz")
+        np.savez(tmp, rho_sad=rs, vloc=vl, delta=dt, domain=json.dumps(dom), iterations=np.array(its),
+                 seed=np.array(sd))
+        tmp.replace(path)
+        done.append(sd)
+    rec = {"rank": rank, "world": world, "family": family, "done": done, "skipped": skipped,
+           "seconds": time.perf_counter() - t0}
+    (out_dir / f"manifest_rank{rank}.json").write_text(json.dumps(rec))
+    return rec
+
+
+def merge_manifests(out_dir: Path, world: int) -> dict:
+    """Join the ranks' records into out_dir/manifest.json (seeds ascending).
+    Raises if a rank's record is missing or two ranks claim the same seed."""
+    out_dir = Path(out_dir)
+    recs = []
+    for r in range(world):
+        f = out_dir / f"manifest_rank{r}.json"
+        if not f.exists():
+            raise FileNotFoundError(f"rank {r} left no record in {out_dir}")
+        recs.append(json.loads(f.read_text()))
+    done = [sd for rec in recs for sd in rec["done"]]
+    if len(done) != len(set(done)):
+        raise ValueError("two ranks generated the same seed")
+    man = {"family": recs[0]["family"], "world": world, "seeds": sorted(done),
+           "skipped": sorted(sd for rec in recs for sd in rec["skipped"]),
+           "rank_seconds": [rec["seconds"] for rec in recs]}
+    (out_dir / "manifest.json").write_text(json.dumps(man))
+    return man
+
+
+def load_samples(data_dir: Path, n_train: int, device=None):
+    """The first n_train samples (ascending seed) of a generated set as
+    (domain, [(rho_sad, vloc, delta)], seeds): inputs FP64, targets FP32, on
+    device (host when None)."""
+    data_dir = Path(data_dir)
+    man = json.loads((data_dir / "manifest.json").read_text())
+    seeds = man["seeds"][:n_train]
+    out, dom = [], None
+    for sd in seeds:
+        with np.load(data_dir / f"{man['family']}_{sd:05d}.npz") as z:
+            d = json.loads(str(z["domain"]))
+            if dom is None:
+                dom = d
+            elif (d["nx"], d["ny"], d["nz"]) != (dom["nx"], dom["ny"], dom["nz"]):
+                raise ValueError(f"seed {sd}: grid {d} differs from {dom}")
+            out.append(tuple(torch.from_numpy(z[k]).to(device, dt) for k, dt in
+                             (("rho_sad", torch.float64), ("vloc", torch.float64), ("delta", torch.float32))))
+    return dom, out, seeds
+
+
 def train(n_train: int, epochs: int, out: Path, lr: float = 2e-4, seed: int = 0, log=print,
-          family: str = "water") -> dict:
+          family: str = "water", data_dir: Path | None = None) -> dict:
+    """Train the network on n_train geometries of the family: generated here
+    one after another, or read from data_dir (a set written by generate on
+    any number of replicas)."""
     t_data = time.perf_counter()
     samples = []
     ctx0 = None
     skipped = []
     sd = 0
+    if data_dir is not None:
+        dom, samples, used = load_samples(data_dir, n_train, torch.device("cuda", torch.cuda.current_device()))
+        ctx0 = gpu.GridContext(dom, 8)
+        skipped = json.loads((Path(data_dir) / "manifest.json").read_text())["skipped"]
+        sd = used[-1] + 1 if used else 0
     while len(samples) < n_train and sd < TRAIN_SEEDS:
         try:
             ctx, rs, vl, dt, res = make_sample(sd, family)
@@ -543,6 +652,34 @@ def evaluate(seeds, weights: Path, log=print, family: str = "water") -> dict:
     return summary
 
 
+def generate_distributed(family: str, seeds, out_dir: Path, sample_fn=None, timeout_s: float = 3600.0) -> dict:
+    """generate() on every rank of a torchrun launch (RANK / LOCAL_RANK /
+    WORLD_SIZE from the environment; one process per GPU, LOCAL_RANK picks
+    the device), then rank 0 merges the records.  The only exchange is one
+    host barrier on a gloo group (no data crosses it); without torchrun
+    variables it runs as a single replica."""
+    import os
+
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("gloo", timeout=timedelta(seconds=timeout_s))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    try:
+        rec = generate(family, seeds, out_dir, rank, world, sample_fn=sample_fn)
+        if world > 1:
+            dist.barrier()
+        return merge_manifests(out_dir, world) if rank == 0 else rec
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m parsec_python_b200.learned")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -552,6 +689,12 @@ def main(argv=None):
     t.add_argument("--epochs", type=int, default=12)
     t.add_argument("--lr", type=float, default=2e-4)
     t.add_argument("--out", type=Path, default=None)
+    t.add_argument("--data", type=Path, default=None, help="a set written by `generate` (else generated here)")
+    g = sub.add_parser("generate", help="training samples, one replica per GPU under torchrun")
+    g.add_argument("--family", choices=sorted(FAMILIES), default="water")
+    g.add_argument("--first", type=int, default=0)
+    g.add_argument("--count", type=int, default=TRAIN_SEEDS)
+    g.add_argument("--out", type=Path, required=True)
     e = sub.add_parser("eval")
     e.add_argument("--family", choices=sorted(FAMILIES), default="water")
     e.add_argument("--first", type=int, default=512)
@@ -560,8 +703,11 @@ def main(argv=None):
     e.add_argument("--json", type=Path, default=None)
     a = ap.parse_args(argv)
     if a.cmd == "train":
-        meta = train(a.n_train, a.epochs, a.out or FAMILIES[a.family]["weights"], lr=a.lr, family=a.family)
+        meta = train(a.n_train, a.epochs, a.out or FAMILIES[a.family]["weights"], lr=a.lr, family=a.family,
+                     data_dir=a.data)
         print(json.dumps({k: v for k, v in meta.items() if k != "losses"} | {"final_loss": meta["losses"][-1]}))
+    elif a.cmd == "generate":
+        print(json.dumps(generate_distributed(a.family, range(a.first, a.first + a.count), a.out)))
     else:
         summ = evaluate(range(a.first, a.first + a.count), a.weights or FAMILIES[a.family]["weights"],
                         family=a.family)
