@@ -291,7 +291,7 @@ def stencil_roofline(reps: int = 40, dtype: str = "f32", name: str = CFG_NAME, k
 
 
 def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 20,
-             masks=("cube", "sphere"), impls=(0,)) -> list:
+             masks=("cube", "sphere"), impls=(0,), dtypes=("f64", "f32"), nl=(False, True)) -> list:
     """H.X microbenchmark on the real grids of C10H8 (78^3) and Si87H76 (90^3):
     one Chebyshev step Out = a H In + b In + g Prev on k random columns, FP64
     and FP32, first with the stencil and local potential alone (one kernel),
@@ -301,7 +301,8 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
     per step: (3 k + 1) n s for the stencil part, n the points produced, plus
     sum_a n_a (4 + 3 s) for the projector tables (s = 8 or 4); CUDA-event
     time per step over `reps` steps, inputs larger than L2.  impls: stencil
-    implementations to time (0 default, 2 four-point FP32 runs)."""
+    implementations to time (0 default, 2 four-point FP32 runs, 3 / 4 the
+    same with packed FP32 pairs)."""
     import torch
 
     from parsec_python_b200 import gpu
@@ -312,7 +313,7 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
     for name in names:
         prob, elem, _ = gpu_problem("fp64", 0, name=name)
         for mask in masks:
-            for with_nl in (False, True):
+            for with_nl in nl:
                 ctx = gpu.GridContext(prob.domain, 8)
                 if mask == "sphere":
                     ctx.set_sphere_mask(ctx.radius)
@@ -327,8 +328,8 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
                 for impl in impls:
                     ctx.call("psc_set_stencil_impl", impl)
                     for k in widths:
-                        for dtype in ("f64", "f32"):
-                            if impl == 2 and dtype == "f64":
+                        for dtype in dtypes:
+                            if impl >= 2 and dtype == "f64":   # FP32-only variants
                                 continue
                             tdt, code, size = (torch.float64, F64, 8) if dtype == "f64" else (torch.float32, F32, 4)
                             X = ctx.mask_block(torch.randn(k, n, dtype=tdt, device="cuda"))
@@ -759,7 +760,12 @@ def main():
     ap.add_argument("--hx", action="store_true",
                     help="only run the H.X microbenchmark (C10H8 and Si87H76 grids, cube and sphere mask, FP64/FP32)")
     ap.add_argument("--hx-widths", default="27,55,143,307", help="column counts of --hx")
-    ap.add_argument("--hx-impls", default="0", help="stencil implementations of --hx (0 default, 2 four-point FP32)")
+    ap.add_argument("--hx-impls", default="0",
+                    help="stencil implementations of --hx (0 default, 2 four-point FP32, 3 / 4 packed FP32 pairs)")
+    ap.add_argument("--hx-systems", default="c10h8,si87h76", help="grids of --hx")
+    ap.add_argument("--hx-masks", default="cube,sphere", help="masks of --hx")
+    ap.add_argument("--hx-dtypes", default="f64,f32", help="block types of --hx")
+    ap.add_argument("--hx-nl", default="0,1", help="--hx without (0) and with (1) the projectors")
     ap.add_argument("--syev", nargs="?", const="55_rand,55_near,143_near,307_near", default=None,
                     help="only time the k x k symmetric eigensolver (comma-separated <k>_<rand|near> cases)")
     args = ap.parse_args()
@@ -793,7 +799,9 @@ def main():
     if args.hx:
         widths = tuple(int(x) for x in args.hx_widths.split(","))
         impls = tuple(int(x) for x in args.hx_impls.split(","))
-        for r in hx_sweep(widths=widths, reps=max(1, args.steps) * 4, impls=impls):
+        for r in hx_sweep(names=tuple(args.hx_systems.split(",")), widths=widths, reps=max(1, args.steps) * 4,
+                          masks=tuple(args.hx_masks.split(",")), impls=impls, dtypes=tuple(args.hx_dtypes.split(",")),
+                          nl=tuple(bool(int(x)) for x in args.hx_nl.split(","))):
             print(json.dumps(r), flush=True)
         return
     rank, local, world = dist_init()

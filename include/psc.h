@@ -108,8 +108,15 @@ int psc_apply_h_axpby(psc_ctx* ctx, int dtype, const void* X, long ldx, const vo
 /* Stencil implementation: 0 = TMA-fed pipeline where the bulk-copy alignment
  * rules hold (default; FP32 blocks take 2-point runs when nx is even but not
  * a multiple of 4), 1 = register-queue kernel everywhere, 2 = the TMA
- * pipeline with 4-point FP32 runs in every case. */
+ * pipeline with 4-point FP32 runs in every case, 3 / 4 = as 0 / 2 with the
+ * FP32 arithmetic on packed pairs of points (aligned runs). */
 int psc_set_stencil_impl(psc_ctx* ctx, int impl);
+/* FP32 weights of the TMA stencil: 1 (default) = each weight applied as its
+ * FP32 value plus its FP32 rounding error, so the FP32 operator is the FP64
+ * one up to unbiased arithmetic rounding; 0 = plain FP32 weights, whose
+ * rounding breaks the sum rule c0 + 6 sum c_d = 0 and shifts every
+ * eigenvalue by a constant of order 1e-7 Ha. */
+int psc_set_stencil_weights(psc_ctx* ctx, int compensated);
 /* Sphere-masked Hamiltonian (no counterpart in the reference, which solves
  * on the whole cube): with radius > 0 (bohr) every H X returns zero at the
  * points farther than radius from the cube's centre, the projector tables

@@ -36,6 +36,7 @@ _SIGS = {
     "psc_apply_h_axpby": ([_P, c_int, _P, c_long, _P, c_long, _P, c_long, c_int, c_double, c_double, c_double, _P],
                           c_int),
     "psc_set_stencil_impl": ([_P, c_int], c_int),
+    "psc_set_stencil_weights": ([_P, c_int], c_int),
     "psc_laplacian_apply": ([_P, _P, _P, c_int, c_long, _P], c_int),
     "psc_cheb_filter": ([_P, c_int, c_int, c_int, _P, _P, _P, c_long, c_int, POINTER(c_int), _P], c_int),
     "psc_lanczos_bound": ([_P, c_int, c_ulonglong, _P, _P], c_int),

@@ -204,7 +204,7 @@ static int launch_stencil(psc_ctx* ctx, int k, const T* X, long ldx, const T* P,
   // the TMA pipeline serves every launch that needs no fused dot product and
   // meets the bulk-copy alignment rules; the register-queue kernel the rest
   // (followed by a masking pass when the Hamiltonian is sphere-masked)
-  if (!dot_partial && ctx->stencil_impl == 0) {
+  if (!dot_partial && ctx->stencil_impl != 1) {
     const int rc = psc_stencil_tma<T>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, c0c, coef, a, b, g, masked, st);
     if (rc >= 0) return rc;
   }
@@ -406,9 +406,16 @@ extern "C" int psc_mask_block(psc_ctx* ctx, int dtype, void* X, long ld, int k, 
   return psc_mask_block_impl(ctx, dtype, X, ld, k, (cudaStream_t)stream);
 }
 
+extern "C" int psc_set_stencil_weights(psc_ctx* ctx, int compensated) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, compensated == 0 || compensated == 1, "stencil weights mode must be 0 or 1");
+  ctx->stencil_comp = compensated;
+  return 0;
+}
+
 extern "C" int psc_set_stencil_impl(psc_ctx* ctx, int impl) {
   if (!ctx) return 2;
-  PSC_REQUIRE(ctx, impl >= 0 && impl <= 2, "stencil impl must be 0, 1 or 2");
+  PSC_REQUIRE(ctx, impl >= 0 && impl <= 4, "stencil impl must be 0 .. 4");
   ctx->stencil_impl = impl;
   return 0;
 }

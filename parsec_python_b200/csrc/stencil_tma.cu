@@ -188,6 +188,7 @@ struct TmaArgs {
   int nx, ny, nz;
   const int4* sched;  // per CTA: column, slab, first plane, end plane
   T c0, c[4];
+  T c0lo, clo[4];     // FP32: the coefficients' rounding errors (c + clo = the FP64 value to 2^-48)
   const double* coef;
   double a, b, g;
   long wait_limit;    // polls of each mbarrier wait before the CTA gives up
@@ -200,10 +201,20 @@ struct TmaArgs {
 }  // namespace
 
 // YA: alignment (in elements) of the y-neighbour rows, the largest of VW, 2, 1
-// that divides nx; their loads are split to match.
-template <typename T, int R, int YA, int VW>
+// that divides nx; their loads are split to match.  MODE (FP32 only):
+// bit 0 = the arithmetic on packed pairs of points (YA == VW), bit 1 =
+// compensated coefficients: every weight is applied as c + clo, the FP32
+// value and its rounding error, so the operator is the FP64 one up to the
+// rounding of the arithmetic (which is unbiased).  With plain FP32 weights
+// the sum rule c0 + 6 sum_d c_d = 0 fails by a few 1e-8 Ha, a constant shift
+// of every eigenvalue that the band energy multiplies by the electron count.
+template <typename T, int R, int YA, int VW, int MODE>
 __global__ void __launch_bounds__(TNT)
 k_stencil_tma(TmaArgs<T> A) {
+  constexpr bool PK = (MODE & 1) != 0;
+  constexpr bool COMP = (MODE & 2) != 0;
+  static_assert(!PK || (sizeof(T) == 4 && YA == VW && VW % 2 == 0), "packed pairs need aligned FP32 runs");
+  static_assert(!COMP || sizeof(T) == 4, "compensated weights are for FP32");
   constexpr int TS = slab_points<VW>();    // points per slab (VW per thread)
   constexpr int NBUF = R + 1 + prefetch_depth<T>();   // X plane windows resident
   constexpr int NS = PP_SLOTS;
@@ -425,30 +436,81 @@ k_stencil_tma(TmaArgs<T> A) {
           }
         }
         const T* pc = pl + s_c;
-        T acc[VW];
+        T o[VW];
+        if constexpr (PK) {
+          // the same sums on pairs of points with the packed FP32 add / FMA
+          // (each lane rounds as the scalar instruction does): half the
+          // arithmetic instructions per point
+          constexpr int NP = VW / 2;
+          const float2 c02 = make_float2(c0, c0);
+          float2 acc[NP], alo[NP];
 #pragma unroll
-        for (int j = 0; j < VW; ++j) acc[j] = c0 * xs[OFF + j];
+          for (int h = 0; h < NP; ++h) {
+            const float2 xc = make_float2(xs[OFF + 2 * h], xs[OFF + 2 * h + 1]);
+            acc[h] = __fmul2_rn(c02, xc);
+            if constexpr (COMP) alo[h] = __fmul2_rn(make_float2(A.c0lo, A.c0lo), xc);
+          }
 #pragma unroll
-        for (int d = 1; d <= R; ++d) {
-          T ym[VW], yp[VW];
-          vload<VW>(pc - d * nx, ym);
-          vload<VW>(pc + d * nx, yp);
-          const T cd = A.c[d - 1];
+          for (int d = 1; d <= R; ++d) {
+            T ym[VW], yp[VW];
+            vload<VW>(pc - d * nx, ym);
+            vload<VW>(pc + d * nx, yp);
+            const float2 cd = make_float2(A.c[d - 1], A.c[d - 1]);
+            const int sm = (u + R - d) % Q, sp = (u + R + d) % Q;
+#pragma unroll
+            for (int h = 0; h < NP; ++h) {
+              const int j = 2 * h;
+              const float2 yy = __fadd2_rn(make_float2(ym[j], ym[j + 1]), make_float2(yp[j], yp[j + 1]));
+              const float2 zz = __fadd2_rn(make_float2(zq[j][sm], zq[j + 1][sm]), make_float2(zq[j][sp], zq[j + 1][sp]));
+              const float2 xx = __fadd2_rn(make_float2(xs[OFF + j - d], xs[OFF + j + 1 - d]),
+                                           make_float2(xs[OFF + j + d], xs[OFF + j + 1 + d]));
+              const float2 t = __fadd2_rn(__fadd2_rn(yy, zz), xx);
+              acc[h] = __ffma2_rn(cd, t, acc[h]);
+              if constexpr (COMP) alo[h] = __ffma2_rn(make_float2(A.clo[d - 1], A.clo[d - 1]), t, alo[h]);
+            }
+          }
+#pragma unroll
+          for (int h = 0; h < NP; ++h) {
+            const int j = 2 * h;
+            const float2 xc = make_float2(xs[OFF + j], xs[OFF + j + 1]);
+            float2 a = acc[h];
+            if constexpr (COMP) a = __fadd2_rn(a, alo[h]);
+            if (has_pot) a = __ffma2_rn(make_float2(pov[j], pov[j + 1]), xc, a);
+            float2 r = __ffma2_rn(make_float2(ca, ca), a, __fmul2_rn(make_float2(cb, cb), xc));
+            if (Pc) r = __ffma2_rn(make_float2(cg, cg), make_float2(pvv[j], pvv[j + 1]), r);
+            o[j] = r.x;
+            o[j + 1] = r.y;
+          }
+        } else {
+          T acc[VW], alo[VW];
 #pragma unroll
           for (int j = 0; j < VW; ++j) {
-            const T t = ((ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q])) +
-                        (xs[OFF + j - d] + xs[OFF + j + d]);
-            acc[j] += cd * t;
+            acc[j] = c0 * xs[OFF + j];
+            if constexpr (COMP) alo[j] = A.c0lo * xs[OFF + j];
           }
-        }
-        T o[VW];
 #pragma unroll
-        for (int j = 0; j < VW; ++j) {
-          const T xc = xs[OFF + j];
-          T a = acc[j];
-          if (has_pot) a += pov[j] * xc;
-          o[j] = ca * a + cb * xc;
-          if (Pc) o[j] += cg * pvv[j];
+          for (int d = 1; d <= R; ++d) {
+            T ym[VW], yp[VW];
+            vload<VW>(pc - d * nx, ym);
+            vload<VW>(pc + d * nx, yp);
+            const T cd = A.c[d - 1];
+#pragma unroll
+            for (int j = 0; j < VW; ++j) {
+              const T t = ((ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q])) +
+                          (xs[OFF + j - d] + xs[OFF + j + d]);
+              acc[j] += cd * t;
+              if constexpr (COMP) alo[j] += A.clo[d - 1] * t;
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < VW; ++j) {
+            const T xc = xs[OFF + j];
+            T a = acc[j];
+            if constexpr (COMP) a += alo[j];
+            if (has_pot) a += pov[j] * xc;
+            o[j] = ca * a + cb * xc;
+            if (Pc) o[j] += cg * pvv[j];
+          }
         }
         if (masked) {
           const double zm = z * A.h - A.cz;
@@ -474,7 +536,7 @@ k_stencil_tma(TmaArgs<T> A) {
 #pragma unroll
         for (int j = 0; j < VW; ++j) {
           acc[j] = c0 * xs[OFF + j];
-          ax[j] = T(0);
+          ax[j] = COMP ? A.c0lo * xs[OFF + j] : T(0);
         }
 #pragma unroll
         for (int d = 1; d <= R; ++d) {
@@ -489,6 +551,7 @@ k_stencil_tma(TmaArgs<T> A) {
             acc[j] += cd * t;
             const T xsum = (d <= el[j] ? xs[OFF + j - d] : T(0)) + (d <= er[j] ? xs[OFF + j + d] : T(0));
             ax[j] += cd * xsum;
+            if constexpr (COMP) ax[j] += A.clo[d - 1] * (t + xsum);
           }
         }
         T o[VW];
@@ -678,7 +741,7 @@ static const int4* stencil_sched(psc_ctx* ctx, int nslab, int k, int fill, int s
   return reinterpret_cast<const int4*>(b.dev);
 }
 
-template <typename T, int R, int VW>
+template <typename T, int R, int VW, int MODE>
 static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy,
                         const T* pot, const double* w, const double* coef, double a, double b, double g,
                         bool masked, cudaStream_t st) {
@@ -700,15 +763,21 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   const size_t win = (TS + 2 * (size_t)R * ctx->nx + VW + Q16 - 1) / Q16 * Q16;   // window + zero pad, 16-byte slots
   const size_t smem = (NBUF * win + (size_t)PP_SLOTS * 2 * TS) * sizeof(T) + NBUF * sizeof(uint64_t);
   if (smem > 220 * 1024) return -1;  // window too wide: the register-queue kernel takes it
-  auto kern = (ctx->nx % VW == 0) ? k_stencil_tma<T, R, VW, VW>
-              : (ctx->nx % 2 == 0) ? k_stencil_tma<T, R, (VW >= 2 ? 2 : 1), VW>
-                                   : k_stencil_tma<T, R, 1, VW>;
+  // packed pairs only where the runs are row-aligned (YA == VW)
+  constexpr int NOPK = MODE & 2;
+  auto kern = (ctx->nx % VW == 0) ? k_stencil_tma<T, R, VW, VW, MODE>
+              : (ctx->nx % 2 == 0) ? k_stencil_tma<T, R, (VW >= 2 ? 2 : 1), VW, (VW == 2 ? MODE : NOPK)>
+                                   : k_stencil_tma<T, R, 1, VW, NOPK>;
   PSC_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   TmaArgs<T> A;
   A.X = X; A.ldx = ldx; A.P = P; A.ldp = ldp; A.Y = Y; A.ldy = ldy; A.pot = pot;
   A.nx = ctx->nx; A.ny = ctx->ny; A.nz = ctx->nz; A.sched = sched;
   A.c0 = (T)w[0];
-  for (int i = 0; i < 4; ++i) A.c[i] = (T)w[1 + i];
+  A.c0lo = (T)(w[0] - (double)A.c0);
+  for (int i = 0; i < 4; ++i) {
+    A.c[i] = (T)w[1 + i];
+    A.clo[i] = (T)(w[1 + i] - (double)A.c[i]);
+  }
   A.coef = coef; A.a = a; A.b = b; A.g = g; A.status = ctx->dev_status;
   A.wait_limit = ctx->wait_limit;
   A.mask_r2 = masked ? ctx->mask_r2 : 0.0;
@@ -726,16 +795,31 @@ int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long 
                     cudaStream_t st) {
   if (!tma_ok<T>(ctx, X, ldx, P, ldp, Y, ldy)) return -1;
   // FP32 takes 2-point runs when nx is even but not a multiple of 4 (the
-  // aligned, mask-free x terms), unless stencil_impl 2 asks for 4-point runs
-  const bool narrow = sizeof(T) == 4 && ctx->nx % 4 != 0 && ctx->nx % 2 == 0 && ctx->stencil_impl != 2;
-#define PSC_TMA_R(RR)                                                                                         \
-  case RR:                                                                                                    \
+  // aligned, mask-free x terms), unless stencil_impl 2 / 4 asks for 4-point
+  // runs; impl 3 / 4 compute on packed pairs; compensated weights unless
+  // the context turned them off
+  const int impl = ctx->stencil_impl;
+  const bool narrow = sizeof(T) == 4 && ctx->nx % 4 != 0 && ctx->nx % 2 == 0 && impl != 2 && impl != 4;
+  const int mode = (impl == 3 || impl == 4 ? 1 : 0) | (ctx->stencil_comp ? 2 : 0);
+#define PSC_TMA_ARGS ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st
+#define PSC_TMA_MODES(VWW)                                                                                    \
+  switch (mode) {                                                                                             \
+    case 0: return launch_tma_t<T, RR, VWW, 0>(PSC_TMA_ARGS);                                                 \
+    case 1: return launch_tma_t<T, RR, VWW, 1>(PSC_TMA_ARGS);                                                 \
+    case 2: return launch_tma_t<T, RR, VWW, 2>(PSC_TMA_ARGS);                                                 \
+    default: return launch_tma_t<T, RR, VWW, 3>(PSC_TMA_ARGS);                                                \
+  }
+#define PSC_TMA_R(RRV)                                                                                        \
+  case RRV: {                                                                                                 \
+    constexpr int RR = RRV;                                                                                   \
     if constexpr (sizeof(T) == 8)                                                                             \
-      return launch_tma_t<T, RR, 2>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st);       \
-    else if (narrow)                                                                                          \
-      return launch_tma_t<T, RR, 2>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st);       \
-    else                                                                                                      \
-      return launch_tma_t<T, RR, 4>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st);
+      return launch_tma_t<T, RR, 2, 0>(PSC_TMA_ARGS);                                                         \
+    else if (narrow) {                                                                                        \
+      PSC_TMA_MODES(2)                                                                                        \
+    } else {                                                                                                  \
+      PSC_TMA_MODES(4)                                                                                        \
+    }                                                                                                         \
+  }
   switch (ctx->radius) {
     PSC_TMA_R(1)
     PSC_TMA_R(2)
@@ -743,6 +827,8 @@ int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long 
     PSC_TMA_R(4)
   }
 #undef PSC_TMA_R
+#undef PSC_TMA_MODES
+#undef PSC_TMA_ARGS
   return -1;
 }
 

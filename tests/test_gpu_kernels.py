@@ -445,14 +445,20 @@ def test_tma_stencil_matches_register_kernel(shape, order, dt):
     X = torch.randn(k, n, dtype=tdt, device=DEV, generator=g)
     P = torch.randn(k, n, dtype=tdt, device=DEV, generator=g)
     outs = []
-    for impl in (0, 1):
+    # 1: register-queue kernel; 0, 2: TMA pipeline (2- or 4-point FP32 runs);
+    # 3, 4: the same with the FP32 arithmetic on packed pairs
+    impls = (1, 0, 2, 3, 4) if dt == "f32" else (1, 0)
+    for impl in impls:
         ctx.call("psc_set_stencil_impl", impl)
         Y = P.clone()
         ctx.call("psc_apply_h_axpby", code, gpu._p(X), n, gpu._p(Y), n, gpu._p(Y), n, k, 0.7, -0.2, -0.9,
                  gpu._stream())
         outs.append(Y.double().cpu().numpy())
+    ctx.call("psc_set_stencil_impl", 0)
     tol = 1e-14 if dt == "f64" else 2e-6
-    assert rel(outs[0], outs[1]) < tol
+    for impl, o in zip(impls[1:], outs[1:]):
+        assert rel(o, outs[0]) < tol, impl
+    ctx.check_status()
 
 
 def test_pcg_graph_equals_direct_launches():
