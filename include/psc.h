@@ -106,10 +106,10 @@ int psc_apply_h(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long 
 int psc_apply_h_axpby(psc_ctx* ctx, int dtype, const void* X, long ldx, const void* P, long ldp, void* Y, long ldy,
                       int k, double alpha, double beta, double gamma, void* stream);
 /* Stencil implementation: 0 = TMA-fed pipeline where the bulk-copy alignment
- * rules hold (default; FP32 blocks take 2-point runs when nx is even but not
- * a multiple of 4), 1 = register-queue kernel everywhere, 2 = the TMA
- * pipeline with 4-point FP32 runs in every case, 3 / 4 = as 0 / 2 with the
- * FP32 arithmetic on packed pairs of points (aligned runs). */
+ * rules hold (default; 2-point FP64 and 4-point FP32 runs), 1 = register-queue
+ * kernel everywhere, 2 = the TMA pipeline with 2-point FP32 runs when nx is
+ * even but not a multiple of 4, 3 / 4 = as 2 / 0 with the FP32 arithmetic on
+ * packed pairs of points. */
 int psc_set_stencil_impl(psc_ctx* ctx, int impl);
 /* FP32 weights of the TMA stencil: 1 (default) = each weight applied as its
  * FP32 value plus its FP32 rounding error, so the FP32 operator is the FP64
@@ -277,6 +277,11 @@ int psc_dot(psc_ctx* ctx, const double* a, const double* b, long n, double* out_
  * split-precision TF32 (1, default) or on CUDA cores with FP64 accumulation
  * (0).  No counterpart in the reference (its GPU path is cuBLAS FP32). */
 int psc_set_gram_impl(psc_ctx* ctx, int tensor_cores);
+/* Rows per chunk of the tensor-core Gram pair (0 = automatic: four waves of
+ * CTAs).  Each chunk accumulates in FP32 tensor memory, which rounds toward
+ * zero; shorter chunks shrink that bias on the off-diagonal entries at the
+ * cost of more partial tiles (at most 2 GiB). */
+int psc_set_gram_chunk(psc_ctx* ctx, long rows);
 /* Block products W T of FP32 blocks (the W Q of Rayleighritz.py:4-30 and
  * chefsi1.py:64-67, here W R^{-1} Y) on tcgen05 tensor cores with
  * split-precision TF32 and FP32 accumulation (1, default) or on CUDA cores

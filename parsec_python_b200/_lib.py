@@ -62,6 +62,7 @@ _SIGS = {
     "psc_lda_xc": ([_P, _P, _P, c_double, _P, _P], c_int),
     "psc_lda_xc_noalloc": ([_P, _P, c_long, c_double, _P, _P], c_int),
     "psc_set_gram_impl": ([_P, c_int], c_int),
+    "psc_set_gram_chunk": ([_P, c_long], c_int),
     "psc_set_gemm_impl": ([_P, c_int], c_int),
     "psc_set_wait_limit": ([_P, c_long], c_int),
     "psc_set_sphere_mask": ([_P, c_double, _P], c_int),

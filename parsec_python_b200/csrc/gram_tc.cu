@@ -12,8 +12,11 @@
 // (one 128-byte swizzle row of FP32) per stage, the next stage's loads in
 // flight in registers while the current one is stored; its threads load and split
 // the tiles into hi/lo copies in the canonical K-major 128-byte-swizzled
-// layout, one elected thread issues the MMAs (M = 128, N = tile width,
-// K = 8 per instruction) and commits them to an mbarrier.  Partial FP32
+// layout, one elected thread issues the MMAs and commits them to an
+// mbarrier.  The W_b and V_b tiles of a stage sit next to each other in
+// shared memory, so one MMA of N = 2 x tile width (K = 8) yields the S and
+// K blocks side by side in tensor memory: three MMAs per K step (hi hi,
+// hi lo, lo hi), each reading its A tile once for both products.  Partial FP32
 // tiles go to global memory and are summed over the chunks in FP64.
 // The tensor cores' FP32 accumulation rounds toward zero, so a long chunk
 // biases every entry towards zero (about 1e-4 relative at 7,000 rows).  The
@@ -33,9 +36,9 @@ constexpr int TC_NT = 256;              // 8 warps: loads in flight; warps 0-3 a
 constexpr int TROWS = 128;               // tile rows (matrix columns), = MMA M
 constexpr int KSTAGE = 32;               // reduction rows per stage (128 bytes of FP32)
 constexpr int TILE_BYTES = TROWS * 128;  // 16 KB
-constexpr int NTILES = 6;                // A hi/lo, BS hi/lo, BK hi/lo
+constexpr int NTILES = 6;                // [W_b V_b] hi, [W_b V_b] lo, A hi, A lo
 constexpr int BUF_BYTES = NTILES * TILE_BYTES;
-constexpr int TMEM_COLS = 256;           // S accumulator at column 0, K at column 128
+constexpr int TMEM_COLS = 256;           // S accumulator at column 0, K at column N
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -160,7 +163,6 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
   const int nstage = (int)((max(0L, n_end - n_begin) + KSTAGE - 1) / KSTAGE);
   const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(W) & 15) == 0) &&
                    ((reinterpret_cast<uintptr_t>(V) & 15) == 0);
-  const uint32_t idesc = idesc_tf32(N);
 
   if (threadIdx.x == 0) {
     s_fail = 0;
@@ -177,7 +179,8 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
-  const uint32_t tmem_s = tmem, tmem_k = tmem + 128;
+  const uint32_t tmem_s = tmem, tmem_k = tmem + N;
+  const uint32_t idesc2 = idesc_tf32(2 * N);   // B = [W_b | V_b], D = [S | K]
   // exact FP64 diagonal sums of a diagonal tile pair: this thread's columns
   // are col_a + (threadIdx.x >> 3) + 32 u, u < PER
   double dsum_s[PER], dsum_k[PER];
@@ -196,12 +199,16 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
   for (int s = 0; s < nstage; ++s) {
     const int b = s & 1;
     unsigned char* buf = sm + b * BUF_BYTES;
-    unsigned char* a_hi = buf;
-    unsigned char* a_lo = buf + TILE_BYTES;
-    unsigned char* bs_hi = same ? a_hi : buf + 2 * TILE_BYTES;
-    unsigned char* bs_lo = same ? a_lo : buf + 3 * TILE_BYTES;
-    unsigned char* bk_hi = buf + 4 * TILE_BYTES;
-    unsigned char* bk_lo = buf + 5 * TILE_BYTES;
+    // N rows of W_b followed by N rows of V_b (N is a multiple of 16, so the
+    // V_b rows start on an 8-row swizzle group); a diagonal pair's A tile is
+    // its W_b rows (the MMA's rows beyond N read V_b and land in discarded
+    // accumulator rows)
+    unsigned char* bs_hi = buf;
+    unsigned char* bk_hi = buf + N * 128;
+    unsigned char* bs_lo = buf + 2 * TILE_BYTES;
+    unsigned char* bk_lo = bs_lo + N * 128;
+    unsigned char* a_hi = same ? bs_hi : buf + 4 * TILE_BYTES;
+    unsigned char* a_lo = same ? bs_lo : buf + 5 * TILE_BYTES;
     if (s >= 2 && threadIdx.x == 0) {
       // the MMAs of stage s-2 read this buffer: wait for their commit
       if (!mbar_wait(smem_u32(&mbar[b]), (uint32_t)(((s - 2) >> 1) & 1), wait_limit)) s_fail = 1;
@@ -223,8 +230,12 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
           dsum_k[u] = fma((double)a.w, (double)v.w, dsum_k[u]);
         }
       }
-      tile_store_split(ta, TROWS, a_hi, a_lo);
-      if (!same) tile_store_split(tb, N, bs_hi, bs_lo);
+      if (same) {
+        tile_store_split(ta, N, bs_hi, bs_lo);
+      } else {
+        tile_store_split(ta, TROWS, a_hi, a_lo);
+        tile_store_split(tb, N, bs_hi, bs_lo);
+      }
       tile_store_split(tk, N, bk_hi, bk_lo);
       if (s + 1 < nstage) {
         const long n1 = n_begin + (long)(s + 1) * KSTAGE;
@@ -238,18 +249,14 @@ k_gram_tc(const float* __restrict__ W, const float* __restrict__ V, long ld, int
     if (threadIdx.x == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo);
-      const uint32_t sh_ = smem_u32(bs_hi), sl = smem_u32(bs_lo);
-      const uint32_t kh = smem_u32(bk_hi), kl = smem_u32(bk_lo);
+      const uint32_t bh = smem_u32(bs_hi), bl = smem_u32(bs_lo);
 #pragma unroll
       for (int kk = 0; kk < KSTAGE / 8; ++kk) {
         const uint32_t o = kk * 32;   // 8 TF32 = 32 bytes along K inside the swizzled row
         const uint32_t acc = (s > 0 || kk > 0) ? 1u : 0u;
-        mma_tf32(tmem_s, sw128_desc(ah + o), sw128_desc(sh_ + o), idesc, acc);
-        mma_tf32(tmem_s, sw128_desc(ah + o), sw128_desc(sl + o), idesc, 1u);
-        mma_tf32(tmem_s, sw128_desc(al + o), sw128_desc(sh_ + o), idesc, 1u);
-        mma_tf32(tmem_k, sw128_desc(ah + o), sw128_desc(kh + o), idesc, acc);
-        mma_tf32(tmem_k, sw128_desc(ah + o), sw128_desc(kl + o), idesc, 1u);
-        mma_tf32(tmem_k, sw128_desc(al + o), sw128_desc(kh + o), idesc, 1u);
+        mma_tf32(tmem_s, sw128_desc(ah + o), sw128_desc(bh + o), idesc2, acc);
+        mma_tf32(tmem_s, sw128_desc(ah + o), sw128_desc(bl + o), idesc2, 1u);
+        mma_tf32(tmem_s, sw128_desc(al + o), sw128_desc(bh + o), idesc2, 1u);
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(&mbar[b]))
@@ -382,12 +389,16 @@ int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int 
   const long n = ctx->n;
   const int tiles = (k + TROWS - 1) / TROWS;
   const int npair = tiles * (tiles + 1) / 2;
-  // four waves of one CTA per SM: shorter chunks keep the FP32 accumulation
-  // in tensor memory short (its rounding error grows with the chunk length)
+  // four waves of one CTA per SM by default: shorter chunks keep the FP32
+  // accumulation in tensor memory short (its rounding error grows with the
+  // chunk length); psc_set_gram_chunk asks for a given chunk length
   int nchunk = std::max(1, 4 * 148 / npair);
   long chunk = ((n + nchunk - 1) / nchunk + KSTAGE - 1) / KSTAGE * KSTAGE;
+  if (ctx->gram_chunk > 0) chunk = (ctx->gram_chunk + KSTAGE - 1) / KSTAGE * KSTAGE;
   nchunk = (int)((n + chunk - 1) / chunk);
   const size_t tile_floats = (size_t)nchunk * npair * 2 * TROWS * TROWS;   // even, so dpart is 8-byte aligned
+  PSC_REQUIRE(ctx, tile_floats * sizeof(float) <= (size_t)1 << 31,
+              "gram_pair: the chunk length leaves more than 2 GiB of partial tiles");
   const size_t part_floats = tile_floats + (size_t)nchunk * 2 * k * 2;    // + nchunk x 2 x k doubles
   if (ctx->tc_part_floats < part_floats) {
     psc_dfree(ctx->tc_part);
@@ -415,6 +426,13 @@ int psc_gram_pair_tc(psc_ctx* ctx, const float* W, const float* V, long ld, int 
   k_gram_tc_final<<<std::max(1, (int)std::min<long>(148 * 8, (total + 7) / 8)), 256, 0, st>>>(
       ctx->tc_part, dpart, nchunk, npair, (const int2*)ctx->tc_pairs, k, S, K);
   PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
+
+extern "C" int psc_set_gram_chunk(psc_ctx* ctx, long rows) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, rows >= 0, "gram_chunk: rows < 0");
+  ctx->gram_chunk = rows;
   return 0;
 }
 

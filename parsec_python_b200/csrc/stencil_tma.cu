@@ -202,7 +202,7 @@ struct TmaArgs {
 
 // YA: alignment (in elements) of the y-neighbour rows, the largest of VW, 2, 1
 // that divides nx; their loads are split to match.  MODE (FP32 only):
-// bit 0 = the arithmetic on packed pairs of points (YA == VW), bit 1 =
+// bit 0 = the arithmetic on packed pairs of points, bit 1 =
 // compensated coefficients: every weight is applied as c + clo, the FP32
 // value and its rounding error, so the operator is the FP64 one up to the
 // rounding of the arithmetic (which is unbiased).  With plain FP32 weights
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(TNT)
 k_stencil_tma(TmaArgs<T> A) {
   constexpr bool PK = (MODE & 1) != 0;
   constexpr bool COMP = (MODE & 2) != 0;
-  static_assert(!PK || (sizeof(T) == 4 && YA == VW && VW % 2 == 0), "packed pairs need aligned FP32 runs");
+  static_assert(!PK || (sizeof(T) == 4 && VW % 2 == 0), "packed pairs need FP32 runs of an even length");
   static_assert(!COMP || sizeof(T) == 4, "compensated weights are for FP32");
   constexpr int TS = slab_points<VW>();    // points per slab (VW per thread)
   constexpr int NBUF = R + 1 + prefetch_depth<T>();   // X plane windows resident
@@ -532,36 +532,82 @@ k_stencil_tma(TmaArgs<T> A) {
           }
         }
         // two partial sums per point: y + z terms, x terms
-        T acc[VW], ax[VW];
+        T o[VW];
+        if constexpr (PK) {
+          // pairs of points on the packed FP32 add / FMA; the x neighbours
+          // are masked per point, then paired
+          constexpr int NP = VW / 2;
+          float2 acc[NP], ax[NP];
 #pragma unroll
-        for (int j = 0; j < VW; ++j) {
-          acc[j] = c0 * xs[OFF + j];
-          ax[j] = COMP ? A.c0lo * xs[OFF + j] : T(0);
-        }
+          for (int h = 0; h < NP; ++h) {
+            const float2 xc = make_float2(xs[OFF + 2 * h], xs[OFF + 2 * h + 1]);
+            acc[h] = __fmul2_rn(make_float2(c0, c0), xc);
+            ax[h] = COMP ? __fmul2_rn(make_float2(A.c0lo, A.c0lo), xc) : make_float2(0.f, 0.f);
+          }
 #pragma unroll
-        for (int d = 1; d <= R; ++d) {
-          // rows outside the plane are zero in the window, so y needs no test
-          T ym[VW], yp[VW];
-          vload_a<T, YA, VW>(pl + s_c - d * nx, ym);
-          vload_a<T, YA, VW>(pl + s_c + d * nx, yp);
-          const T cd = A.c[d - 1];
+          for (int d = 1; d <= R; ++d) {
+            T ym[VW], yp[VW];
+            vload_a<T, YA, VW>(pl + s_c - d * nx, ym);
+            vload_a<T, YA, VW>(pl + s_c + d * nx, yp);
+            const float2 cd = make_float2(A.c[d - 1], A.c[d - 1]);
+            const int sm = (u + R - d) % Q, sp = (u + R + d) % Q;
+#pragma unroll
+            for (int h = 0; h < NP; ++h) {
+              const int j = 2 * h;
+              const float2 yy = __fadd2_rn(make_float2(ym[j], ym[j + 1]), make_float2(yp[j], yp[j + 1]));
+              const float2 zz = __fadd2_rn(make_float2(zq[j][sm], zq[j + 1][sm]), make_float2(zq[j][sp], zq[j + 1][sp]));
+              const float2 t = __fadd2_rn(yy, zz);
+              acc[h] = __ffma2_rn(cd, t, acc[h]);
+              const float2 xl = make_float2(d <= el[j] ? xs[OFF + j - d] : 0.f, d <= el[j + 1] ? xs[OFF + j + 1 - d] : 0.f);
+              const float2 xr = make_float2(d <= er[j] ? xs[OFF + j + d] : 0.f, d <= er[j + 1] ? xs[OFF + j + 1 + d] : 0.f);
+              const float2 xx = __fadd2_rn(xl, xr);
+              ax[h] = __ffma2_rn(cd, xx, ax[h]);
+              if constexpr (COMP)
+                ax[h] = __ffma2_rn(make_float2(A.clo[d - 1], A.clo[d - 1]), __fadd2_rn(t, xx), ax[h]);
+            }
+          }
+#pragma unroll
+          for (int h = 0; h < NP; ++h) {
+            const int j = 2 * h;
+            const float2 xc = make_float2(xs[OFF + j], xs[OFF + j + 1]);
+            float2 a = __fadd2_rn(acc[h], ax[h]);
+            if (has_pot) a = __ffma2_rn(make_float2(pov[j], pov[j + 1]), xc, a);
+            float2 r = __ffma2_rn(make_float2(ca, ca), a, __fmul2_rn(make_float2(cb, cb), xc));
+            if (Pc) r = __ffma2_rn(make_float2(cg, cg), make_float2(pvv[j], pvv[j + 1]), r);
+            o[j] = r.x;
+            o[j + 1] = r.y;
+          }
+        } else {
+          T acc[VW], ax[VW];
 #pragma unroll
           for (int j = 0; j < VW; ++j) {
-            const T t = (ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q]);
-            acc[j] += cd * t;
-            const T xsum = (d <= el[j] ? xs[OFF + j - d] : T(0)) + (d <= er[j] ? xs[OFF + j + d] : T(0));
-            ax[j] += cd * xsum;
-            if constexpr (COMP) ax[j] += A.clo[d - 1] * (t + xsum);
+            acc[j] = c0 * xs[OFF + j];
+            ax[j] = COMP ? A.c0lo * xs[OFF + j] : T(0);
           }
-        }
-        T o[VW];
 #pragma unroll
-        for (int j = 0; j < VW; ++j) {
-          const T xc = xs[OFF + j];
-          T a = acc[j] + ax[j];
-          if (has_pot) a += pov[j] * xc;
-          o[j] = ca * a + cb * xc;
-          if (Pc) o[j] += cg * pvv[j];
+          for (int d = 1; d <= R; ++d) {
+            // rows outside the plane are zero in the window, so y needs no test
+            T ym[VW], yp[VW];
+            vload_a<T, YA, VW>(pl + s_c - d * nx, ym);
+            vload_a<T, YA, VW>(pl + s_c + d * nx, yp);
+            const T cd = A.c[d - 1];
+#pragma unroll
+            for (int j = 0; j < VW; ++j) {
+              const T t = (ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q]);
+              acc[j] += cd * t;
+              const T xsum = (d <= el[j] ? xs[OFF + j - d] : T(0)) + (d <= er[j] ? xs[OFF + j + d] : T(0));
+              ax[j] += cd * xsum;
+              if constexpr (COMP) ax[j] += A.clo[d - 1] * (t + xsum);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < VW; ++j) {
+            const T xc = xs[OFF + j];
+            T a = acc[j] + ax[j];
+            if (has_pot) a += pov[j] * xc;
+            o[j] = ca * a + cb * xc;
+            if (Pc) o[j] += cg * pvv[j];
+          }
         }
         if (masked) {
           const double zm = z * A.h - A.cz;
@@ -763,11 +809,9 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   const size_t win = (TS + 2 * (size_t)R * ctx->nx + VW + Q16 - 1) / Q16 * Q16;   // window + zero pad, 16-byte slots
   const size_t smem = (NBUF * win + (size_t)PP_SLOTS * 2 * TS) * sizeof(T) + NBUF * sizeof(uint64_t);
   if (smem > 220 * 1024) return -1;  // window too wide: the register-queue kernel takes it
-  // packed pairs only where the runs are row-aligned (YA == VW)
-  constexpr int NOPK = MODE & 2;
   auto kern = (ctx->nx % VW == 0) ? k_stencil_tma<T, R, VW, VW, MODE>
-              : (ctx->nx % 2 == 0) ? k_stencil_tma<T, R, (VW >= 2 ? 2 : 1), VW, (VW == 2 ? MODE : NOPK)>
-                                   : k_stencil_tma<T, R, 1, VW, NOPK>;
+              : (ctx->nx % 2 == 0) ? k_stencil_tma<T, R, (VW >= 2 ? 2 : 1), VW, MODE>
+                                   : k_stencil_tma<T, R, 1, VW, MODE>;
   PSC_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   TmaArgs<T> A;
   A.X = X; A.ldx = ldx; A.P = P; A.ldp = ldp; A.Y = Y; A.ldy = ldy; A.pot = pot;
@@ -794,12 +838,13 @@ int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long 
                     const double* w, const double* coef, double a, double b, double g, bool masked,
                     cudaStream_t st) {
   if (!tma_ok<T>(ctx, X, ldx, P, ldp, Y, ldy)) return -1;
-  // FP32 takes 2-point runs when nx is even but not a multiple of 4 (the
-  // aligned, mask-free x terms), unless stencil_impl 2 / 4 asks for 4-point
-  // runs; impl 3 / 4 compute on packed pairs; compensated weights unless
-  // the context turned them off
+  // FP32 takes 4-point runs (measured faster than 2-point runs even where
+  // nx is only 2-aligned and the x terms need per-point edge masks: 827
+  // against 1038 us per step at 90^3, k = 307); impl 2 / 3 ask for 2-point
+  // runs when nx is even but not a multiple of 4, impl 3 / 4 compute on
+  // packed pairs; compensated weights unless the context turned them off
   const int impl = ctx->stencil_impl;
-  const bool narrow = sizeof(T) == 4 && ctx->nx % 4 != 0 && ctx->nx % 2 == 0 && impl != 2 && impl != 4;
+  const bool narrow = sizeof(T) == 4 && ctx->nx % 4 != 0 && ctx->nx % 2 == 0 && (impl == 2 || impl == 3);
   const int mode = (impl == 3 || impl == 4 ? 1 : 0) | (ctx->stencil_comp ? 2 : 0);
 #define PSC_TMA_ARGS ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st
 #define PSC_TMA_MODES(VWW)                                                                                    \

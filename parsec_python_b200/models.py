@@ -54,7 +54,9 @@ class SolverSettings:
     precision: str = "fp64"      # fp64 | mixed
     init: str = "sad"            # sad | learned
     seed: int = 0
-    mixed_switch: float = 1e-4   # mixed precision: FP64 subspace blocks once the SCF error is below this
+    mixed_switch: float = 1e-4   # mixed precision: below this SCF error the block product W T leaves the tensor cores
+    mixed_finish: str = "fp64"   # fp64: the last iterations run on FP64 blocks | fp32: the run may end in FP32
+    mixed_fp64_at: float = 1e-6  # mixed_finish = fp64: FP64 blocks once the SCF error is below this (or stalls)
     mask: str = "cube"           # cube (the reference's domain) | sphere (H zero outside the inscribed sphere)
     first_tol: float = 0.08      # first_filt: stop when the Ritz trace moves by <= this fraction (first_filt.py:14)
     first_rounds: int = 0        # first_filt: most filter rounds; 0 = the reference's max(min(60 / polm, 5), 3)
@@ -68,6 +70,7 @@ class SolverSettings:
         "gpu": ("use_gpu", _parse_bool), "recenter_atoms": ("recenter_atoms", _parse_bool),
         "recenter": ("recenter_atoms", _parse_bool), "precision": ("precision", str),
         "init": ("init", str), "seed": ("seed", int), "mixed_switch": ("mixed_switch", float),
+        "mixed_finish": ("mixed_finish", str), "mixed_fp64_at": ("mixed_fp64_at", float),
         "mask": ("mask", str), "first_tol": ("first_tol", float), "first_rounds": ("first_rounds", int),
     }
 
@@ -92,6 +95,10 @@ class SolverSettings:
         if self.init not in ("sad", "learned"):
             self.init = "sad"
         self.mixed_switch = float(self.mixed_switch)
+        self.mixed_finish = str(self.mixed_finish).lower()
+        if self.mixed_finish not in ("fp32", "fp64"):
+            self.mixed_finish = "fp64"
+        self.mixed_fp64_at = float(self.mixed_fp64_at)
         self.first_tol = float(self.first_tol)
         self.first_rounds = max(0, int(self.first_rounds))
         self.mask = str(self.mask).lower()

@@ -172,10 +172,19 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
     history = []
     exc = float(xc0[0].item())
     host = torch.empty(2 * k + 8, dtype=torch.float64, pin_memory=True)
+    late, stall, best_late = False, 0, float("inf")
+
+    def fp32_blocks() -> bool:
+        return s.precision == "mixed" and (W is None or W.dtype == torch.float32)
+
+    if s.precision == "mixed":
+        ctx.call("psc_set_gemm_impl", 1)   # the context may come from an earlier run's late phase
     t_loop = time.perf_counter()
     def _done() -> bool:
         if err > s.tol:
             return False
+        if fp32_blocks() and s.mixed_finish == "fp64":
+            return False   # mixed precision ends on FP64 iterations
         if energy_target is None:
             return True
         return energies is not None and abs(energies.total_ry - energy_target[0]) <= energy_target[1]
@@ -185,9 +194,21 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         say(f"  Working ... SCF iter # {its} ... ")
         ev = _Events()
         H.set_potential(pot)
-        if W is not None and W.dtype == torch.float32 and err <= s.mixed_switch:
-            # mixed precision: the last iterations run with FP64 subspace blocks
-            W = W.double()
+        if fp32_blocks():
+            # mixed precision.  Late phase (error below mixed_switch): the
+            # block product W T leaves the tensor cores, whose truncating FP32
+            # accumulation holds the SCF error near 1e-6 and shakes the mixer,
+            # for the round-to-nearest path.  With mixed_finish = fp64 the
+            # blocks go to FP64 once the error is below mixed_fp64_at (or tol)
+            # or has not improved for three late iterations.
+            if err <= s.mixed_switch and not late:
+                late = True
+                ctx.call("psc_set_gemm_impl", 0)
+            if late:
+                stall = stall + 1 if err >= best_late else 0
+                best_late = min(best_late, err)
+            if late and s.mixed_finish == "fp64" and (err <= max(s.tol, s.mixed_fp64_at) or stall >= 3):
+                W = W.double()
         ev.mark("d0")
         deg = _scaled_poldeg(s.poldeg, deg_mod)
         if its == 1 and s.diagmeth == 3:
@@ -242,7 +263,7 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         rec = {"iter": its, "err": err, "total_ry": energies.total_ry, "eigen_sum_ry": energies.eigen_sum_ry,
                "hartree_ry": energies.hartree_ry, "xc_ry": energies.xc_ry, "lam": lam_h, "occ": occ_h,
                "cg_its": cg_its, "diag_s": diag_t, "hartree_s": hart_t, "iter_s": ev.seconds("d0", "end"),
-               "block_dtype": "f32" if W.dtype == torch.float32 else "f64"}
+               "block_dtype": "f32" if W.dtype == torch.float32 else "f64", "late": late}
         history.append(rec)
         if on_iteration:
             on_iteration(rec)

@@ -445,8 +445,8 @@ def test_tma_stencil_matches_register_kernel(shape, order, dt):
     X = torch.randn(k, n, dtype=tdt, device=DEV, generator=g)
     P = torch.randn(k, n, dtype=tdt, device=DEV, generator=g)
     outs = []
-    # 1: register-queue kernel; 0, 2: TMA pipeline (2- or 4-point FP32 runs);
-    # 3, 4: the same with the FP32 arithmetic on packed pairs
+    # 1: register-queue kernel; 0, 2: TMA pipeline (4- or 2-point FP32 runs);
+    # 3, 4: 2- / 4-point runs with the FP32 arithmetic on packed pairs
     impls = (1, 0, 2, 3, 4) if dt == "f32" else (1, 0)
     for impl in impls:
         ctx.call("psc_set_stencil_impl", impl)
