@@ -301,8 +301,8 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
     per step: (3 k + 1) n s for the stencil part, n the points produced, plus
     sum_a n_a (4 + 3 s) for the projector tables (s = 8 or 4); CUDA-event
     time per step over `reps` steps, inputs larger than L2.  impls: stencil
-    implementations to time (0 default, 2 two-point FP32 runs, 3 / 4 packed
-    FP32 pairs with two- / four-point runs)."""
+    implementations to time (0 default, 2 two-point FP32 runs, 3 / 4 scalar
+    FP32 arithmetic with two- / four-point runs)."""
     import torch
 
     from parsec_python_b200 import gpu
@@ -761,7 +761,7 @@ def main():
                     help="only run the H.X microbenchmark (C10H8 and Si87H76 grids, cube and sphere mask, FP64/FP32)")
     ap.add_argument("--hx-widths", default="27,55,143,307", help="column counts of --hx")
     ap.add_argument("--hx-impls", default="0",
-                    help="stencil implementations of --hx (0 default, 2 two-point FP32, 3 / 4 packed FP32 pairs)")
+                    help="stencil implementations of --hx (0 default, 2 two-point FP32, 3 / 4 scalar FP32 arithmetic)")
     ap.add_argument("--hx-systems", default="c10h8,si87h76", help="grids of --hx")
     ap.add_argument("--hx-masks", default="cube,sphere", help="masks of --hx")
     ap.add_argument("--hx-dtypes", default="f64,f32", help="block types of --hx")

@@ -106,10 +106,10 @@ int psc_apply_h(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, long 
 int psc_apply_h_axpby(psc_ctx* ctx, int dtype, const void* X, long ldx, const void* P, long ldp, void* Y, long ldy,
                       int k, double alpha, double beta, double gamma, void* stream);
 /* Stencil implementation: 0 = TMA-fed pipeline where the bulk-copy alignment
- * rules hold (default; 2-point FP64 and 4-point FP32 runs), 1 = register-queue
- * kernel everywhere, 2 = the TMA pipeline with 2-point FP32 runs when nx is
- * even but not a multiple of 4, 3 / 4 = as 2 / 0 with the FP32 arithmetic on
- * packed pairs of points. */
+ * rules hold (default; 2-point FP64 runs, 4-point FP32 runs with the
+ * arithmetic on packed pairs of points), 1 = register-queue kernel
+ * everywhere, 2 = the TMA pipeline with 2-point FP32 runs when nx is even but
+ * not a multiple of 4, 3 / 4 = as 2 / 0 with scalar FP32 arithmetic. */
 int psc_set_stencil_impl(psc_ctx* ctx, int impl);
 /* FP32 weights of the TMA stencil: 1 (default) = each weight applied as its
  * FP32 value plus its FP32 rounding error, so the FP32 operator is the FP64

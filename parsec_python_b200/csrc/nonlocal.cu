@@ -32,16 +32,33 @@ k_nl_project(const T* __restrict__ X, long ldx, int k, const int* __restrict__ a
   for (int m = 0; m < 3; ++m)
 #pragma unroll
     for (int c = 0; c < NL_KC; ++c) acc[m][c] = 0.0;
-  for (int p = lo + threadIdx.x; p < hi; p += NT) {
-    const long gi = idx[p];
+  // two ball points per trip: all 2 x NL_KC gathers are issued before the
+  // first is used (the sums still run over p, p + NT, p + 2 NT, ... in order)
+  for (int p = lo + threadIdx.x; p < hi; p += 2 * NT) {
+    const int p1 = p + NT;
+    const bool two = p1 < hi;
+    const long g0 = idx[p], g1 = two ? idx[p1] : g0;
+    double x0[NL_KC], x1[NL_KC];
+#pragma unroll
+    for (int c = 0; c < NL_KC; ++c) {
+      const bool in = c0 + c < k;
+      x0[c] = in ? (double)X[g0 + (long)(c0 + c) * ldx] : 0.0;
+      x1[c] = (in && two) ? (double)X[g1 + (long)(c0 + c) * ldx] : 0.0;
+    }
     const double u0 = u[p], u1 = u[npts + p], u2 = u[2 * npts + p];
 #pragma unroll
     for (int c = 0; c < NL_KC; ++c) {
-      if (c0 + c < k) {
-        const double xv = (double)X[gi + (long)(c0 + c) * ldx];
-        acc[0][c] += u0 * xv;
-        acc[1][c] += u1 * xv;
-        acc[2][c] += u2 * xv;
+      acc[0][c] += u0 * x0[c];
+      acc[1][c] += u1 * x0[c];
+      acc[2][c] += u2 * x0[c];
+    }
+    if (two) {
+      const double v0 = u[p1], v1 = u[npts + p1], v2 = u[2 * npts + p1];
+#pragma unroll
+      for (int c = 0; c < NL_KC; ++c) {
+        acc[0][c] += v0 * x1[c];
+        acc[1][c] += v1 * x1[c];
+        acc[2][c] += v2 * x1[c];
       }
     }
   }
@@ -68,37 +85,44 @@ k_nl_project(const T* __restrict__ X, long ldx, int k, const int* __restrict__ a
 // One thread per (touched grid point, group of NL_SC columns): the entries
 // covering the point and their u values are read once and used for every
 // column of the group; each column's sum runs over the entries in atom
-// order (no atomics, so the result is bitwise reproducible).
+// order (no atomics, so the result is bitwise reproducible).  The group's Y
+// values are all loaded before the sums and stored after them, so the
+// read-modify-writes of the NL_SC columns overlap instead of waiting on one
+// another.
 constexpr int NL_SC = 8;
 template <typename T>
-__global__ void k_nl_scatter(T* Y, long ldy, int k, long ntouched, const int* __restrict__ t_idx,
-                             const int* __restrict__ t_off, const int* __restrict__ t_ent,
-                             const int* __restrict__ pt_atom, const T* __restrict__ u, long npts,
-                             const double* __restrict__ proj, const double* __restrict__ coef, double ha) {
-  const double alpha = coef ? coef[0] : ha;
+__global__ void __launch_bounds__(256)
+k_nl_scatter(T* __restrict__ Y, long ldy, int k, long ntouched, const int* __restrict__ t_idx,
+             const int* __restrict__ t_off, const int* __restrict__ t_ent, const int* __restrict__ pt_atom,
+             const T* __restrict__ u, long npts, const double* __restrict__ proj, const double* __restrict__ coef,
+             double ha) {
   const int ngrp = (k + NL_SC - 1) / NL_SC;
   const long total = ntouched * (long)ngrp;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const long pt = t % ntouched;
-    const int c0 = (int)(t / ntouched) * NL_SC;
-    const int nc = min(NL_SC, k - c0);
-    double s[NL_SC];
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const double alpha = coef ? coef[0] : ha;
+  const long pt = t % ntouched;
+  const int c0 = (int)(t / ntouched) * NL_SC;
+  const int nc = min(NL_SC, k - c0);
+  T* yp = Y + (long)t_idx[pt] + (long)c0 * ldy;
+  T yv[NL_SC];
 #pragma unroll
-    for (int c = 0; c < NL_SC; ++c) s[c] = 0.0;
-    for (int e = t_off[pt]; e < t_off[pt + 1]; ++e) {
-      const int p = t_ent[e];
-      const int a = pt_atom[p];
-      const double u0 = (double)u[p], u1 = (double)u[npts + p], u2 = (double)u[2 * npts + p];
-      const double* pr = proj + (long)a * 3 * k + c0;
+  for (int c = 0; c < NL_SC; ++c) yv[c] = c < nc ? yp[(long)c * ldy] : T(0);
+  double s[NL_SC];
 #pragma unroll
-      for (int c = 0; c < NL_SC; ++c)
-        if (c < nc) s[c] += u0 * pr[c] + u1 * pr[k + c] + u2 * pr[2 * k + c];
-    }
-    T* yp = Y + (long)t_idx[pt] + (long)c0 * ldy;
+  for (int c = 0; c < NL_SC; ++c) s[c] = 0.0;
+  for (int e = t_off[pt]; e < t_off[pt + 1]; ++e) {
+    const int p = t_ent[e];
+    const int a = pt_atom[p];
+    const double u0 = (double)u[p], u1 = (double)u[npts + p], u2 = (double)u[2 * npts + p];
+    const double* pr = proj + (long)a * 3 * k + c0;
 #pragma unroll
     for (int c = 0; c < NL_SC; ++c)
-      if (c < nc) yp[(long)c * ldy] = (T)((double)yp[(long)c * ldy] + alpha * s[c]);
+      if (c < nc) s[c] += u0 * pr[c] + u1 * pr[k + c] + u2 * pr[2 * k + c];
   }
+#pragma unroll
+  for (int c = 0; c < NL_SC; ++c)
+    if (c < nc) yp[(long)c * ldy] = (T)((double)yv[c] + alpha * s[c]);
 }
 
 int psc_ensure_proj(psc_ctx* ctx, int k) {
@@ -128,7 +152,9 @@ int psc_nl_project(psc_ctx* ctx, int dtype, const void* X, long ldx, int k, cuda
 int psc_nl_scatter(psc_ctx* ctx, int dtype, void* Y, long ldy, int k, const double* coef, double a,
                    cudaStream_t st) {
   const long total = ctx->nl_touched * (long)((k + NL_SC - 1) / NL_SC);
-  const int nb = (int)std::min<long>(148L * 16, (total + 255) / 256);
+  if (total == 0) return 0;
+  PSC_REQUIRE(ctx, (total + 255) / 256 <= INT32_MAX, "nl_scatter: too many touched points x columns");
+  const int nb = (int)((total + 255) / 256);   // one (point, column group) per thread
   if (dtype == PSC_F64)
     k_nl_scatter<double><<<nb, 256, 0, st>>>((double*)Y, ldy, k, ctx->nl_touched, ctx->nl_t_idx,
                                               ctx->nl_t_off, ctx->nl_t_ent, ctx->nl_point_atom, ctx->nl_u64,

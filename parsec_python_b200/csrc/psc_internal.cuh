@@ -55,7 +55,7 @@ struct psc_ctx {
   int radius = 4;            // stencil half-width (fd_order/2, capped at 4)
   int stencil_comp = 1;      // FP32 TMA stencil: weights applied as FP32 value + rounding error
   int stencil_impl = 0;      // 0: TMA pipeline where it applies, 1: register-queue kernel only,
-                             // 2: TMA with 2-point FP32 runs, 3 / 4: as 2 / 0 with packed FP32 pairs
+                             // 2: TMA with 2-point FP32 runs, 3 / 4: as 2 / 0 with scalar FP32 arithmetic
   double lap_c0 = 0.0;       // centre weight of A = -Lap_h (1/h^2 folded in)
   double lap_c[4] = {0, 0, 0, 0};
   double ham_c0 = 0.0;       // 0.5 * A weights, as 0.5*(c*(1/(h*h)))

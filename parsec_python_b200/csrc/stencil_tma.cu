@@ -424,7 +424,11 @@ k_stencil_tma(TmaArgs<T> A) {
         }
       }
       const T* pl = ring + (size_t)((z - z0) % NBUF) * WS;
-      if (EXACT && own) {
+      if (own) {
+        // x neighbours: the aligned vectors around the run (the run itself is
+        // the queue's centre).  Row-aligned runs (EXACT) read the vectors
+        // outside the row from the slot's zero pad; otherwise each point
+        // masks its neighbours by its distances to the row edges.
         T xs[NPV * VW];
 #pragma unroll
         for (int v = 0; v < NPV; ++v) {
@@ -432,29 +436,34 @@ k_stencil_tma(TmaArgs<T> A) {
 #pragma unroll
             for (int j = 0; j < VW; ++j) xs[v * VW + j] = zq[j][(u + R) % Q];
           } else {
-            vload<VW>(pl + xo[v], xs + v * VW);
+            vload<VW>(pl + (EXACT ? xo[v] : s_c - OFF + v * VW), xs + v * VW);
           }
         }
-        const T* pc = pl + s_c;
+        auto xl = [&](int j, int d) -> T { return (EXACT || d <= el[j]) ? xs[OFF + j - d] : T(0); };
+        auto xr = [&](int j, int d) -> T { return (EXACT || d <= er[j]) ? xs[OFF + j + d] : T(0); };
+        // per point: acc = c0 x + sum_d c_d (((y-d + y+d) + (z-d + z+d)) + (x-d + x+d)),
+        // and with compensated weights the same sum over the weights'
+        // rounding errors in its own (small) accumulator.  FP32 sums the
+        // shells from d = R down to 1 and adds c0 x last: of the orders
+        // tried this leaves the smallest bias in the Rayleigh quotients of
+        // smooth fields (the low spectrum), about 3e-9 Ha.
+        constexpr bool REV = sizeof(T) == 4;
         T o[VW];
         if constexpr (PK) {
-          // the same sums on pairs of points with the packed FP32 add / FMA
-          // (each lane rounds as the scalar instruction does): half the
-          // arithmetic instructions per point
           constexpr int NP = VW / 2;
-          const float2 c02 = make_float2(c0, c0);
           float2 acc[NP], alo[NP];
 #pragma unroll
           for (int h = 0; h < NP; ++h) {
             const float2 xc = make_float2(xs[OFF + 2 * h], xs[OFF + 2 * h + 1]);
-            acc[h] = __fmul2_rn(c02, xc);
-            if constexpr (COMP) alo[h] = __fmul2_rn(make_float2(A.c0lo, A.c0lo), xc);
+            acc[h] = REV ? make_float2(0.f, 0.f) : __fmul2_rn(make_float2(c0, c0), xc);
+            alo[h] = (COMP && !REV) ? __fmul2_rn(make_float2(A.c0lo, A.c0lo), xc) : make_float2(0.f, 0.f);
           }
 #pragma unroll
-          for (int d = 1; d <= R; ++d) {
+          for (int dd = 0; dd < R; ++dd) {
+            const int d = REV ? R - dd : dd + 1;
             T ym[VW], yp[VW];
-            vload<VW>(pc - d * nx, ym);
-            vload<VW>(pc + d * nx, yp);
+            vload_a<T, YA, VW>(pl + s_c - d * nx, ym);
+            vload_a<T, YA, VW>(pl + s_c + d * nx, yp);
             const float2 cd = make_float2(A.c[d - 1], A.c[d - 1]);
             const int sm = (u + R - d) % Q, sp = (u + R + d) % Q;
 #pragma unroll
@@ -462,8 +471,7 @@ k_stencil_tma(TmaArgs<T> A) {
               const int j = 2 * h;
               const float2 yy = __fadd2_rn(make_float2(ym[j], ym[j + 1]), make_float2(yp[j], yp[j + 1]));
               const float2 zz = __fadd2_rn(make_float2(zq[j][sm], zq[j + 1][sm]), make_float2(zq[j][sp], zq[j + 1][sp]));
-              const float2 xx = __fadd2_rn(make_float2(xs[OFF + j - d], xs[OFF + j + 1 - d]),
-                                           make_float2(xs[OFF + j + d], xs[OFF + j + 1 + d]));
+              const float2 xx = __fadd2_rn(make_float2(xl(j, d), xl(j + 1, d)), make_float2(xr(j, d), xr(j + 1, d)));
               const float2 t = __fadd2_rn(__fadd2_rn(yy, zz), xx);
               acc[h] = __ffma2_rn(cd, t, acc[h]);
               if constexpr (COMP) alo[h] = __ffma2_rn(make_float2(A.clo[d - 1], A.clo[d - 1]), t, alo[h]);
@@ -474,6 +482,10 @@ k_stencil_tma(TmaArgs<T> A) {
             const int j = 2 * h;
             const float2 xc = make_float2(xs[OFF + j], xs[OFF + j + 1]);
             float2 a = acc[h];
+            if constexpr (REV) {
+              a = __ffma2_rn(make_float2(c0, c0), xc, a);
+              if constexpr (COMP) alo[h] = __ffma2_rn(make_float2(A.c0lo, A.c0lo), xc, alo[h]);
+            }
             if constexpr (COMP) a = __fadd2_rn(a, alo[h]);
             if (has_pot) a = __ffma2_rn(make_float2(pov[j], pov[j + 1]), xc, a);
             float2 r = __ffma2_rn(make_float2(ca, ca), a, __fmul2_rn(make_float2(cb, cb), xc));
@@ -485,19 +497,20 @@ k_stencil_tma(TmaArgs<T> A) {
           T acc[VW], alo[VW];
 #pragma unroll
           for (int j = 0; j < VW; ++j) {
-            acc[j] = c0 * xs[OFF + j];
-            if constexpr (COMP) alo[j] = A.c0lo * xs[OFF + j];
+            acc[j] = REV ? T(0) : c0 * xs[OFF + j];
+            alo[j] = (COMP && !REV) ? A.c0lo * xs[OFF + j] : T(0);
           }
 #pragma unroll
-          for (int d = 1; d <= R; ++d) {
+          for (int dd = 0; dd < R; ++dd) {
+            const int d = REV ? R - dd : dd + 1;
             T ym[VW], yp[VW];
-            vload<VW>(pc - d * nx, ym);
-            vload<VW>(pc + d * nx, yp);
+            vload_a<T, YA, VW>(pl + s_c - d * nx, ym);
+            vload_a<T, YA, VW>(pl + s_c + d * nx, yp);
             const T cd = A.c[d - 1];
 #pragma unroll
             for (int j = 0; j < VW; ++j) {
               const T t = ((ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q])) +
-                          (xs[OFF + j - d] + xs[OFF + j + d]);
+                          (xl(j, d) + xr(j, d));
               acc[j] += cd * t;
               if constexpr (COMP) alo[j] += A.clo[d - 1] * t;
             }
@@ -506,104 +519,11 @@ k_stencil_tma(TmaArgs<T> A) {
           for (int j = 0; j < VW; ++j) {
             const T xc = xs[OFF + j];
             T a = acc[j];
+            if constexpr (REV) {
+              a += c0 * xc;
+              if constexpr (COMP) alo[j] += A.c0lo * xc;
+            }
             if constexpr (COMP) a += alo[j];
-            if (has_pot) a += pov[j] * xc;
-            o[j] = ca * a + cb * xc;
-            if (Pc) o[j] += cg * pvv[j];
-          }
-        }
-        if (masked) {
-          const double zm = z * A.h - A.cz;
-#pragma unroll
-          for (int j = 0; j < VW; ++j)
-            if (mxy[j] + zm * zm > A.mask_r2) o[j] = T(0);
-        }
-        vstore<VW>(Yc + (long)z * nxy + q, o);
-      } else if (own) {
-        // x neighbours: the aligned vectors around the run; the run itself is the queue's centre
-        T xs[NPV * VW];
-#pragma unroll
-        for (int v = 0; v < NPV; ++v) {
-          if (v == HV) {
-#pragma unroll
-            for (int j = 0; j < VW; ++j) xs[v * VW + j] = zq[j][(u + R) % Q];
-          } else {
-            vload<VW>(pl + s_c - OFF + v * VW, xs + v * VW);
-          }
-        }
-        // two partial sums per point: y + z terms, x terms
-        T o[VW];
-        if constexpr (PK) {
-          // pairs of points on the packed FP32 add / FMA; the x neighbours
-          // are masked per point, then paired
-          constexpr int NP = VW / 2;
-          float2 acc[NP], ax[NP];
-#pragma unroll
-          for (int h = 0; h < NP; ++h) {
-            const float2 xc = make_float2(xs[OFF + 2 * h], xs[OFF + 2 * h + 1]);
-            acc[h] = __fmul2_rn(make_float2(c0, c0), xc);
-            ax[h] = COMP ? __fmul2_rn(make_float2(A.c0lo, A.c0lo), xc) : make_float2(0.f, 0.f);
-          }
-#pragma unroll
-          for (int d = 1; d <= R; ++d) {
-            T ym[VW], yp[VW];
-            vload_a<T, YA, VW>(pl + s_c - d * nx, ym);
-            vload_a<T, YA, VW>(pl + s_c + d * nx, yp);
-            const float2 cd = make_float2(A.c[d - 1], A.c[d - 1]);
-            const int sm = (u + R - d) % Q, sp = (u + R + d) % Q;
-#pragma unroll
-            for (int h = 0; h < NP; ++h) {
-              const int j = 2 * h;
-              const float2 yy = __fadd2_rn(make_float2(ym[j], ym[j + 1]), make_float2(yp[j], yp[j + 1]));
-              const float2 zz = __fadd2_rn(make_float2(zq[j][sm], zq[j + 1][sm]), make_float2(zq[j][sp], zq[j + 1][sp]));
-              const float2 t = __fadd2_rn(yy, zz);
-              acc[h] = __ffma2_rn(cd, t, acc[h]);
-              const float2 xl = make_float2(d <= el[j] ? xs[OFF + j - d] : 0.f, d <= el[j + 1] ? xs[OFF + j + 1 - d] : 0.f);
-              const float2 xr = make_float2(d <= er[j] ? xs[OFF + j + d] : 0.f, d <= er[j + 1] ? xs[OFF + j + 1 + d] : 0.f);
-              const float2 xx = __fadd2_rn(xl, xr);
-              ax[h] = __ffma2_rn(cd, xx, ax[h]);
-              if constexpr (COMP)
-                ax[h] = __ffma2_rn(make_float2(A.clo[d - 1], A.clo[d - 1]), __fadd2_rn(t, xx), ax[h]);
-            }
-          }
-#pragma unroll
-          for (int h = 0; h < NP; ++h) {
-            const int j = 2 * h;
-            const float2 xc = make_float2(xs[OFF + j], xs[OFF + j + 1]);
-            float2 a = __fadd2_rn(acc[h], ax[h]);
-            if (has_pot) a = __ffma2_rn(make_float2(pov[j], pov[j + 1]), xc, a);
-            float2 r = __ffma2_rn(make_float2(ca, ca), a, __fmul2_rn(make_float2(cb, cb), xc));
-            if (Pc) r = __ffma2_rn(make_float2(cg, cg), make_float2(pvv[j], pvv[j + 1]), r);
-            o[j] = r.x;
-            o[j + 1] = r.y;
-          }
-        } else {
-          T acc[VW], ax[VW];
-#pragma unroll
-          for (int j = 0; j < VW; ++j) {
-            acc[j] = c0 * xs[OFF + j];
-            ax[j] = COMP ? A.c0lo * xs[OFF + j] : T(0);
-          }
-#pragma unroll
-          for (int d = 1; d <= R; ++d) {
-            // rows outside the plane are zero in the window, so y needs no test
-            T ym[VW], yp[VW];
-            vload_a<T, YA, VW>(pl + s_c - d * nx, ym);
-            vload_a<T, YA, VW>(pl + s_c + d * nx, yp);
-            const T cd = A.c[d - 1];
-#pragma unroll
-            for (int j = 0; j < VW; ++j) {
-              const T t = (ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q]);
-              acc[j] += cd * t;
-              const T xsum = (d <= el[j] ? xs[OFF + j - d] : T(0)) + (d <= er[j] ? xs[OFF + j + d] : T(0));
-              ax[j] += cd * xsum;
-              if constexpr (COMP) ax[j] += A.clo[d - 1] * (t + xsum);
-            }
-          }
-#pragma unroll
-          for (int j = 0; j < VW; ++j) {
-            const T xc = xs[OFF + j];
-            T a = acc[j] + ax[j];
             if (has_pot) a += pov[j] * xc;
             o[j] = ca * a + cb * xc;
             if (Pc) o[j] += cg * pvv[j];
@@ -838,14 +758,15 @@ int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long 
                     const double* w, const double* coef, double a, double b, double g, bool masked,
                     cudaStream_t st) {
   if (!tma_ok<T>(ctx, X, ldx, P, ldp, Y, ldy)) return -1;
-  // FP32 takes 4-point runs (measured faster than 2-point runs even where
-  // nx is only 2-aligned and the x terms need per-point edge masks: 827
-  // against 1038 us per step at 90^3, k = 307); impl 2 / 3 ask for 2-point
-  // runs when nx is even but not a multiple of 4, impl 3 / 4 compute on
-  // packed pairs; compensated weights unless the context turned them off
+  // FP32 takes 4-point runs with the arithmetic on packed pairs (measured
+  // fastest, also where nx is only 2-aligned and the x terms need per-point
+  // edge masks: 818 us per step at 90^3, k = 307, against 995-1055 us for
+  // 2-point runs and 894 us for scalar arithmetic); impl 2 / 3 ask for
+  // 2-point runs when nx is even but not a multiple of 4, impl 3 / 4 for
+  // scalar arithmetic; compensated weights unless the context turned them off
   const int impl = ctx->stencil_impl;
   const bool narrow = sizeof(T) == 4 && ctx->nx % 4 != 0 && ctx->nx % 2 == 0 && (impl == 2 || impl == 3);
-  const int mode = (impl == 3 || impl == 4 ? 1 : 0) | (ctx->stencil_comp ? 2 : 0);
+  const int mode = (impl == 0 || impl == 2 ? 1 : 0) | (ctx->stencil_comp ? 2 : 0);
 #define PSC_TMA_ARGS ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st
 #define PSC_TMA_MODES(VWW)                                                                                    \
   switch (mode) {                                                                                             \

@@ -429,6 +429,61 @@ def test_lanczos_bounds_bracket_the_spectrum(h2o_box, golden_dir):
     assert np.all(np.diff(b0[1:7]) >= 0)
 
 
+def _smooth_block(nx, ny, nz):
+    """Three smooth fields vanishing at the faces (the low end of the
+    spectrum, where the occupied states live), as an (n, 3) array."""
+    i = (np.arange(nx) + 1.0) / (nx + 1)
+    j = (np.arange(ny) + 1.0) / (ny + 1)
+    l = (np.arange(nz) + 1.0) / (nz + 1)
+    cols = []
+    for a, b, c in ((1, 1, 1), (2, 1, 3), (3, 2, 2)):
+        f = np.sin(np.pi * a * l)[:, None, None] * np.sin(np.pi * b * j)[None, :, None] * \
+            np.sin(np.pi * c * i)[None, None, :]
+        cols.append(f.ravel())
+    return np.stack(cols, axis=1)
+
+
+@pytest.mark.parametrize("impl", [0, 2, 3, 4])
+def test_fp32_stencil_has_no_eigenvalue_offset(impl, capsys):
+    """The FP32 operator's Rayleigh quotients on smooth fields equal the
+    FP64 operator's to 5e-9 Ha with compensated weights (every occupied
+    eigenvalue of an FP32 SCF would otherwise move by the same constant,
+    which the band energy multiplies by the electron count).  With plain
+    FP32 weights the quotients move by the predicted sum-rule offset
+    dc0 + 6 sum_d dc_d (the weights' FP32 rounding errors), within 10 %.
+    Si87H76 grid (90^3, h = 0.4724 bohr), zero local potential."""
+    cfg = workloads.config_system("si87h76")
+    dom = O.build_system(cfg["atoms"], h=cfg["h"], radius=cfg["radius"])
+    ctx = gpu.GridContext(dom, 8)
+    gpu.Hamiltonian(ctx, torch.zeros(ctx.n, dtype=torch.float64, device=DEV))
+    W = _smooth_block(ctx.nx, ctx.ny, ctx.nz).astype(np.float32).astype(np.float64)
+    k = W.shape[1]
+    Wd = block(W)
+    ctx.call("psc_set_stencil_impl", impl)
+    Y64 = torch.empty_like(Wd)
+    ctx.call("psc_apply_h", F64, gpu._p(Wd), ctx.n, gpu._p(Y64), ctx.n, k, gpu._stream())
+    q64 = np.einsum("nk,nk->k", W, host(Y64)) / np.einsum("nk,nk->k", W, W)
+    W32 = Wd.float()
+    out = {}
+    for comp in (1, 0):
+        ctx.call("psc_set_stencil_weights", comp)
+        Y32 = torch.empty_like(W32)
+        ctx.call("psc_apply_h", F32, gpu._p(W32), ctx.n, gpu._p(Y32), ctx.n, k, gpu._stream())
+        out[comp] = np.einsum("nk,nk->k", W, host(Y32).astype(np.float64)) / np.einsum("nk,nk->k", W, W) - q64
+    ctx.call("psc_set_stencil_weights", 1)
+    ctx.call("psc_set_stencil_impl", 0)
+    h = dom["h"]
+    c0, c = 205.0 / 24.0, np.array([-8.0 / 5.0, 1.0 / 5.0, -8.0 / 315.0, 1.0 / 560.0])
+    w0, wd = 0.5 * (c0 / h ** 2), 0.5 * (c / h ** 2)
+    pred = (float(np.float32(w0)) - w0) + 6.0 * sum(float(np.float32(x)) - x for x in wd)
+    with capsys.disabled():
+        print(f"\nimpl {impl}: FP32 - FP64 Rayleigh quotients, compensated {out[1]}, plain {out[0]} "
+              f"(predicted plain offset {pred:.3e} Ha)")
+    assert np.abs(out[1]).max() < 5e-9
+    assert np.abs(out[0] - pred).max() < 0.1 * abs(pred)
+    ctx.check_status()
+
+
 @pytest.mark.parametrize("shape,order", [((78, 78, 78), 8), ((24, 24, 24), 8), ((20, 16, 12), 6), ((12, 10, 8), 4),
                                          ((10, 12, 14), 2), ((90, 90, 90), 8)])
 @pytest.mark.parametrize("dt", ["f64", "f32"])
@@ -445,8 +500,8 @@ def test_tma_stencil_matches_register_kernel(shape, order, dt):
     X = torch.randn(k, n, dtype=tdt, device=DEV, generator=g)
     P = torch.randn(k, n, dtype=tdt, device=DEV, generator=g)
     outs = []
-    # 1: register-queue kernel; 0, 2: TMA pipeline (4- or 2-point FP32 runs);
-    # 3, 4: 2- / 4-point runs with the FP32 arithmetic on packed pairs
+    # 1: register-queue kernel; 0, 2: TMA pipeline (4- or 2-point FP32 runs,
+    # packed-pair arithmetic); 3, 4: 2- / 4-point runs, scalar arithmetic
     impls = (1, 0, 2, 3, 4) if dt == "f32" else (1, 0)
     for impl in impls:
         ctx.call("psc_set_stencil_impl", impl)
