@@ -291,7 +291,7 @@ def stencil_roofline(reps: int = 40, dtype: str = "f32", name: str = CFG_NAME, k
 
 
 def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 20,
-             masks=("cube", "sphere"), impls=(0,), dtypes=("f64", "f32"), nl=(False, True)) -> list:
+             masks=("cube", "sphere"), impls=(0,), dtypes=("f64", "f32"), nl=(False, True), weights=(1,)) -> list:
     """H.X microbenchmark on the real grids of C10H8 (78^3) and Si87H76 (90^3):
     one Chebyshev step Out = a H In + b In + g Prev on k random columns, FP64
     and FP32, first with the stencil and local potential alone (one kernel),
@@ -302,7 +302,8 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
     sum_a n_a (4 + 3 s) for the projector tables (s = 8 or 4); CUDA-event
     time per step over `reps` steps, inputs larger than L2.  impls: stencil
     implementations to time (0 default, 2 two-point FP32 runs, 3 / 4 scalar
-    FP32 arithmetic with two- / four-point runs)."""
+    FP32 arithmetic with two- / four-point runs); weights: FP32 stencil
+    weights (1 compensated, the default; 0 plain FP32)."""
     import torch
 
     from parsec_python_b200 import gpu
@@ -325,11 +326,12 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
                     gpu.projector_setup(ctx, prob.input_data.atoms, elem, pseudo_tables())
                 nl_points = ctx.info()["nl_points"] if with_nl else 0
                 st = gpu._stream()
-                for impl in impls:
+                for impl, wmode in ((i, wm) for i in impls for wm in weights):
                     ctx.call("psc_set_stencil_impl", impl)
+                    ctx.call("psc_set_stencil_weights", wmode)
                     for k in widths:
                         for dtype in dtypes:
-                            if impl >= 2 and dtype == "f64":   # FP32-only variants
+                            if (impl >= 2 or wmode != 1) and dtype == "f64":   # FP32-only variants
                                 continue
                             tdt, code, size = (torch.float64, F64, 8) if dtype == "f64" else (torch.float32, F32, 4)
                             X = ctx.mask_block(torch.randn(k, n, dtype=tdt, device="cuda"))
@@ -351,7 +353,8 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
                             torch.cuda.synchronize()
                             t = e0.elapsed_time(e1) / 1000.0 / reps
                             bytes_ = (3 * k + 1) * n_out * size + nl_points * (4 + 3 * size)
-                            out.append({"system": name, "mask": mask, "impl": impl, "n": n, "n_produced": n_out,
+                            out.append({"system": name, "mask": mask, "impl": impl, "weights": wmode, "n": n,
+                                        "n_produced": n_out,
                                         "k": k, "dtype": dtype, "projectors": with_nl, "nl_points": nl_points,
                                         "us": t * 1e6, "bytes": bytes_, "gbs": bytes_ / t / 1e9})
                             del X, Y
@@ -766,6 +769,7 @@ def main():
     ap.add_argument("--hx-masks", default="cube,sphere", help="masks of --hx")
     ap.add_argument("--hx-dtypes", default="f64,f32", help="block types of --hx")
     ap.add_argument("--hx-nl", default="0,1", help="--hx without (0) and with (1) the projectors")
+    ap.add_argument("--hx-weights", default="1", help="FP32 stencil weights of --hx (1 compensated, 0 plain)")
     ap.add_argument("--syev", nargs="?", const="55_rand,55_near,143_near,307_near", default=None,
                     help="only time the k x k symmetric eigensolver (comma-separated <k>_<rand|near> cases)")
     args = ap.parse_args()
@@ -801,7 +805,8 @@ def main():
         impls = tuple(int(x) for x in args.hx_impls.split(","))
         for r in hx_sweep(names=tuple(args.hx_systems.split(",")), widths=widths, reps=max(1, args.steps) * 4,
                           masks=tuple(args.hx_masks.split(",")), impls=impls, dtypes=tuple(args.hx_dtypes.split(",")),
-                          nl=tuple(bool(int(x)) for x in args.hx_nl.split(","))):
+                          nl=tuple(bool(int(x)) for x in args.hx_nl.split(",")),
+                          weights=tuple(int(x) for x in args.hx_weights.split(","))):
             print(json.dumps(r), flush=True)
         return
     rank, local, world = dist_init()

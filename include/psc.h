@@ -117,6 +117,12 @@ int psc_set_stencil_impl(psc_ctx* ctx, int impl);
  * rounding breaks the sum rule c0 + 6 sum c_d = 0 and shifts every
  * eigenvalue by a constant of order 1e-7 Ha. */
 int psc_set_stencil_weights(psc_ctx* ctx, int compensated);
+/* Kleinman-Bylander projector terms of H X: 1 (default) = added in the TMA
+ * stencil pass's epilogue, at the points that balls cover, from the
+ * projections taken before it (no separate read-modify-write of Y); 0 = a
+ * separate scatter pass after the stencil (as the register-queue kernel
+ * always does). */
+int psc_set_projector_fusion(psc_ctx* ctx, int fused);
 /* Sphere-masked Hamiltonian (no counterpart in the reference, which solves
  * on the whole cube): with radius > 0 (bohr) every H X returns zero at the
  * points farther than radius from the cube's centre, the projector tables
@@ -274,8 +280,10 @@ int psc_axpby(psc_ctx* ctx, const double* x, const double* y, double a, double b
 int psc_dot(psc_ctx* ctx, const double* a, const double* b, long n, double* out_dev, void* stream);
 
 /* Gram pairs of FP32 blocks (mixed precision) on tcgen05 tensor cores with
- * split-precision TF32 (1, default) or on CUDA cores with FP64 accumulation
- * (0).  No counterpart in the reference (its GPU path is cuBLAS FP32). */
+ * split-precision TF32 and FP32 accumulation (1, default) or on the FP64
+ * tensor cores (DMMA) with exact products and FP64 accumulation (0, the path
+ * of FP64 blocks).  No counterpart in the reference (its GPU path is cuBLAS
+ * FP32). */
 int psc_set_gram_impl(psc_ctx* ctx, int tensor_cores);
 /* Rows per chunk of the tensor-core Gram pair (0 = automatic: four waves of
  * CTAs).  Each chunk accumulates in FP32 tensor memory, which rounds toward
@@ -284,8 +292,9 @@ int psc_set_gram_impl(psc_ctx* ctx, int tensor_cores);
 int psc_set_gram_chunk(psc_ctx* ctx, long rows);
 /* Block products W T of FP32 blocks (the W Q of Rayleighritz.py:4-30 and
  * chefsi1.py:64-67, here W R^{-1} Y) on tcgen05 tensor cores with
- * split-precision TF32 and FP32 accumulation (1, default) or on CUDA cores
- * (0).  No counterpart in the reference (its GPU path is cuBLAS FP32). */
+ * split-precision TF32 and FP32 accumulation (1, default) or on the FP64
+ * tensor cores (DMMA, FP64 products and sums, one rounding; 0).  No
+ * counterpart in the reference (its GPU path is cuBLAS FP32). */
 int psc_set_gemm_impl(psc_ctx* ctx, int tensor_cores);
 /* S = W^T W and K = W^T V for n x k blocks (leading dimension ld), k x k
  * column-major FP64 results on the device (the Gram and projected-Hamiltonian

@@ -145,8 +145,8 @@ extern "C" int psc_gram(psc_ctx* ctx, int dtype, const void* A, long lda, const 
 }
 
 // ---------------------------------------------------------------------------
-// Out (n x kout) = W (n x k) * Q (k x kout, FP64, column-major): k_gemm_tall
-// in subspace.cu
+// Out (n x kout) = W (n x k) * Q (k x kout, FP64, column-major): subspace.cu
+// (tcgen05 or DMMA)
 // ---------------------------------------------------------------------------
 int psc_gemm_tall(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Tm, int kout, void* O,
                   long ldo, cudaStream_t st);

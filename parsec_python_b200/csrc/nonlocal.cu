@@ -3,11 +3,12 @@
 // V_nl = sum_a sum_m u_am u_am^T / xint_a  (V_ion/pseudoNL_original.py:187-206)
 // is applied as  Y[idx] += alpha * sum_a sum_m u_am * (w_a * u_am . X[idx]),
 // w_a = 1/xint_a = h^3 / Zvalue_a, never forming the n_a x n_a blocks.
-//   project: one CTA per (atom, column group) reduces w_a * U_a^T X (3 values
-//            per column) with warp shuffles and one fixed-order block sum;
-//   scatter: one thread per (touched grid point, group of 8 columns) adds the
-//            sum over the balls covering that point, in atom order.  No
-//            atomics, so the result is bitwise reproducible.
+//   project: one warp per (atom, column) reduces w_a * U_a^T X (3 values)
+//            over the ball with a fixed shuffle tree;
+//   scatter: adds, at every touched grid point, the sum over the balls
+//            covering it in atom order (no atomics, so the result is
+//            bitwise reproducible): inside the TMA stencil's epilogue where
+//            that pass runs, else one thread per (point, column group).
 #include "psc_internal.cuh"
 #include "../../include/psc.h"
 
@@ -15,80 +16,74 @@
 #include <cmath>
 #include <numeric>
 
-constexpr int NL_KC = 8;  // columns per projection CTA
+// Projection: one CTA per (atom, group of NL_KC columns), one warp per
+// column.  The ball's grid indices and u values are staged in shared memory
+// NL_STAGE points at a time; lane l of a warp takes points l, l + 32, ...
+// (NL_UNROLL gathers in flight), then a fixed shuffle tree sums the lanes,
+// so the result is reproducible.  Many warps per SM keep enough gathers in
+// flight for HBM, which a few threads per ball point could not.
+constexpr int NL_KC = 16;       // columns (warps) per projection CTA
+constexpr int NL_STAGE = 1024;  // ball points staged per pass
+constexpr int NL_UNROLL = 4;
 
 template <typename T>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(NL_KC * 32)
 k_nl_project(const T* __restrict__ X, long ldx, int k, const int* __restrict__ atom_off,
              const int* __restrict__ idx, const T* __restrict__ u, long npts, const double* __restrict__ w,
              double* __restrict__ proj) {
-  constexpr int NT = 128, NW = NT / 32;
-  __shared__ double sh[NW][3 * NL_KC];
+  __shared__ int s_idx[NL_STAGE];
+  __shared__ T s_u[3][NL_STAGE];
   const int a = blockIdx.x;
-  const int c0 = blockIdx.y * NL_KC;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int c = blockIdx.y * NL_KC + wid;
   const int lo = atom_off[a], hi = atom_off[a + 1];
-  double acc[3][NL_KC];
-#pragma unroll
-  for (int m = 0; m < 3; ++m)
-#pragma unroll
-    for (int c = 0; c < NL_KC; ++c) acc[m][c] = 0.0;
-  // two ball points per trip: all 2 x NL_KC gathers are issued before the
-  // first is used (the sums still run over p, p + NT, p + 2 NT, ... in order)
-  for (int p = lo + threadIdx.x; p < hi; p += 2 * NT) {
-    const int p1 = p + NT;
-    const bool two = p1 < hi;
-    const long g0 = idx[p], g1 = two ? idx[p1] : g0;
-    double x0[NL_KC], x1[NL_KC];
-#pragma unroll
-    for (int c = 0; c < NL_KC; ++c) {
-      const bool in = c0 + c < k;
-      x0[c] = in ? (double)X[g0 + (long)(c0 + c) * ldx] : 0.0;
-      x1[c] = (in && two) ? (double)X[g1 + (long)(c0 + c) * ldx] : 0.0;
+  const T* Xc = X + (long)min(c, k - 1) * ldx;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int b = lo; b < hi; b += NL_STAGE) {
+    const int nb = min(NL_STAGE, hi - b);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += NL_KC * 32) {
+      s_idx[i] = idx[b + i];
+      s_u[0][i] = u[b + i];
+      s_u[1][i] = u[npts + b + i];
+      s_u[2][i] = u[2 * npts + b + i];
     }
-    const double u0 = u[p], u1 = u[npts + p], u2 = u[2 * npts + p];
+    __syncthreads();
+    for (int i0 = lane; i0 < nb; i0 += 32 * NL_UNROLL) {
+      double xv[NL_UNROLL];
 #pragma unroll
-    for (int c = 0; c < NL_KC; ++c) {
-      acc[0][c] += u0 * x0[c];
-      acc[1][c] += u1 * x0[c];
-      acc[2][c] += u2 * x0[c];
-    }
-    if (two) {
-      const double v0 = u[p1], v1 = u[npts + p1], v2 = u[2 * npts + p1];
+      for (int r = 0; r < NL_UNROLL; ++r) {
+        const int i = i0 + 32 * r;
+        xv[r] = i < nb ? (double)Xc[s_idx[i]] : 0.0;
+      }
 #pragma unroll
-      for (int c = 0; c < NL_KC; ++c) {
-        acc[0][c] += v0 * x1[c];
-        acc[1][c] += v1 * x1[c];
-        acc[2][c] += v2 * x1[c];
+      for (int r = 0; r < NL_UNROLL; ++r) {
+        const int i = i0 + 32 * r;
+        if (i < nb) {
+          s0 += (double)s_u[0][i] * xv[r];
+          s1 += (double)s_u[1][i] * xv[r];
+          s2 += (double)s_u[2][i] * xv[r];
+        }
       }
     }
   }
-  // all 3 x NL_KC sums at once: a shuffle tree per warp, then warp 0 adds
-  // the NW warp partials in warp order (fixed, so the result is reproducible)
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int m = 0; m < 3; ++m)
-#pragma unroll
-    for (int c = 0; c < NL_KC; ++c) {
-      const double v = psc_warp_sum(acc[m][c]);
-      if (lane == 0) sh[wid][m * NL_KC + c] = v;
-    }
-  __syncthreads();
-  if (threadIdx.x < 3 * NL_KC) {
-    const int m = threadIdx.x / NL_KC, c = threadIdx.x % NL_KC;
-    double s = 0.0;
-#pragma unroll
-    for (int q = 0; q < NW; ++q) s += sh[q][threadIdx.x];
-    if (c0 + c < k) proj[((long)a * 3 + m) * k + c0 + c] = w[a] * s;
+  s0 = psc_warp_sum(s0);
+  s1 = psc_warp_sum(s1);
+  s2 = psc_warp_sum(s2);
+  if (lane == 0 && c < k) {
+    const double wa = w[a];
+    proj[((long)a * 3 + 0) * k + c] = wa * s0;
+    proj[((long)a * 3 + 1) * k + c] = wa * s1;
+    proj[((long)a * 3 + 2) * k + c] = wa * s2;
   }
 }
 
-// One thread per (touched grid point, group of NL_SC columns): the entries
-// covering the point and their u values are read once and used for every
-// column of the group; each column's sum runs over the entries in atom
-// order (no atomics, so the result is bitwise reproducible).  The group's Y
-// values are all loaded before the sums and stored after them, so the
-// read-modify-writes of the NL_SC columns overlap instead of waiting on one
-// another.
+// Scatter (for launches whose stencil pass does not add the projector terms
+// itself): one thread per (touched grid point, group of NL_SC columns); the
+// entries covering the point and their u values are read once for every
+// column of the group, the group's Y values are loaded before the sums and
+// stored after them, and each column's sum runs over the entries in atom
+// order (no atomics, so the result is bitwise reproducible).
 constexpr int NL_SC = 8;
 template <typename T>
 __global__ void __launch_bounds__(256)
@@ -97,9 +92,8 @@ k_nl_scatter(T* __restrict__ Y, long ldy, int k, long ntouched, const int* __res
              const T* __restrict__ u, long npts, const double* __restrict__ proj, const double* __restrict__ coef,
              double ha) {
   const int ngrp = (k + NL_SC - 1) / NL_SC;
-  const long total = ntouched * (long)ngrp;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= total) return;
+  if (t >= ntouched * (long)ngrp) return;
   const double alpha = coef ? coef[0] : ha;
   const long pt = t % ntouched;
   const int c0 = (int)(t / ntouched) * NL_SC;
@@ -113,9 +107,8 @@ k_nl_scatter(T* __restrict__ Y, long ldy, int k, long ntouched, const int* __res
   for (int c = 0; c < NL_SC; ++c) s[c] = 0.0;
   for (int e = t_off[pt]; e < t_off[pt + 1]; ++e) {
     const int p = t_ent[e];
-    const int a = pt_atom[p];
     const double u0 = (double)u[p], u1 = (double)u[npts + p], u2 = (double)u[2 * npts + p];
-    const double* pr = proj + (long)a * 3 * k + c0;
+    const double* pr = proj + (long)pt_atom[p] * 3 * k + c0;
 #pragma unroll
     for (int c = 0; c < NL_SC; ++c)
       if (c < nc) s[c] += u0 * pr[c] + u1 * pr[k + c] + u2 * pr[2 * k + c];
@@ -140,11 +133,13 @@ int psc_nl_project(psc_ctx* ctx, int dtype, const void* X, long ldx, int k, cuda
   if (psc_ensure_proj(ctx, k)) return 1;
   dim3 grid(ctx->nl_atoms, (k + NL_KC - 1) / NL_KC);
   if (dtype == PSC_F64)
-    k_nl_project<double><<<grid, 128, 0, st>>>((const double*)X, ldx, k, ctx->nl_atom_off, ctx->nl_idx,
-                                                ctx->nl_u64, ctx->nl_points, ctx->nl_w, (double*)ctx->nl_proj);
+    k_nl_project<double><<<grid, NL_KC * 32, 0, st>>>((const double*)X, ldx, k, ctx->nl_atom_off, ctx->nl_idx,
+                                                       ctx->nl_u64, ctx->nl_points, ctx->nl_w,
+                                                       (double*)ctx->nl_proj);
   else
-    k_nl_project<float><<<grid, 128, 0, st>>>((const float*)X, ldx, k, ctx->nl_atom_off, ctx->nl_idx,
-                                               ctx->nl_u32, ctx->nl_points, ctx->nl_w, (double*)ctx->nl_proj);
+    k_nl_project<float><<<grid, NL_KC * 32, 0, st>>>((const float*)X, ldx, k, ctx->nl_atom_off, ctx->nl_idx,
+                                                      ctx->nl_u32, ctx->nl_points, ctx->nl_w,
+                                                      (double*)ctx->nl_proj);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }
@@ -154,7 +149,7 @@ int psc_nl_scatter(psc_ctx* ctx, int dtype, void* Y, long ldy, int k, const doub
   const long total = ctx->nl_touched * (long)((k + NL_SC - 1) / NL_SC);
   if (total == 0) return 0;
   PSC_REQUIRE(ctx, (total + 255) / 256 <= INT32_MAX, "nl_scatter: too many touched points x columns");
-  const int nb = (int)((total + 255) / 256);   // one (point, column group) per thread
+  const int nb = (int)((total + 255) / 256);   // one (touched point, column group) per thread
   if (dtype == PSC_F64)
     k_nl_scatter<double><<<nb, 256, 0, st>>>((double*)Y, ldy, k, ctx->nl_touched, ctx->nl_t_idx,
                                               ctx->nl_t_off, ctx->nl_t_ent, ctx->nl_point_atom, ctx->nl_u64,
@@ -170,6 +165,8 @@ int psc_nl_scatter(psc_ctx* ctx, int dtype, void* Y, long ldy, int k, const doub
 void psc_free_projectors(psc_ctx* ctx) {
   psc_dfree(ctx->nl_atom_off); psc_dfree(ctx->nl_idx); psc_dfree(ctx->nl_u64); psc_dfree(ctx->nl_u32);
   psc_dfree(ctx->nl_w); psc_dfree(ctx->nl_t_idx); psc_dfree(ctx->nl_t_off); psc_dfree(ctx->nl_t_ent);
+  psc_dfree(ctx->nl_tmap);
+  ctx->nl_tmap = nullptr;
   psc_dfree(ctx->nl_point_atom); psc_dfree(ctx->nl_proj);
   ctx->nl_atom_off = ctx->nl_idx = ctx->nl_t_idx = ctx->nl_t_off = ctx->nl_t_ent = ctx->nl_point_atom = nullptr;
   ctx->nl_u64 = nullptr; ctx->nl_u32 = nullptr; ctx->nl_w = nullptr; ctx->nl_proj = nullptr;
@@ -178,6 +175,13 @@ void psc_free_projectors(psc_ctx* ctx) {
 }
 
 int psc_nl_apply_mask(psc_ctx* ctx, cudaStream_t st);
+
+extern "C" int psc_set_projector_fusion(psc_ctx* ctx, int fused) {
+  if (!ctx) return 2;
+  PSC_REQUIRE(ctx, fused == 0 || fused == 1, "projector fusion must be 0 or 1");
+  ctx->nl_fuse = fused;
+  return 0;
+}
 
 // setup.cu
 int psc_nl_box_distances(psc_ctx* ctx, int nbox, const int* box_dev /* [nbox][8] */, const double* xyz_dev,
@@ -311,6 +315,12 @@ extern "C" int psc_projector_setup(psc_ctx* ctx, int natoms, const int* species,
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->nl_t_off, t_off.data(), t_off.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->nl_t_ent, t_ent.data(), t_ent.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(pt_orig_d, pt_orig.data(), npts * sizeof(int), cudaMemcpyHostToDevice, st));
+  // grid point -> touched index (-1 elsewhere), for the stencil pass that
+  // adds the projector terms in its epilogue
+  std::vector<int> tmap((size_t)ctx->n, -1);
+  for (size_t t = 0; t < t_idx.size(); ++t) tmap[(size_t)t_idx[t]] = (int)t;
+  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_tmap, tmap.size() * sizeof(int)));
+  PSC_CUDA(ctx, cudaMemcpyAsync(ctx->nl_tmap, tmap.data(), tmap.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   int rc = psc_nl_eval_u(ctx, npts, ctx->nl_idx, pt_orig_d, asp_d, xyz_d, radius, ctx->nl_u64, st);
   if (!rc) rc = psc_cast(ctx, PSC_F32, ctx->nl_u64, ctx->nl_u32, 3 * npts, st);
   if (!rc) rc = psc_nl_apply_mask(ctx, st);

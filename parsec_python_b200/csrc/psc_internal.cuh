@@ -78,6 +78,8 @@ struct psc_ctx {
   double* nl_w = nullptr;        // [nl_atoms] 1/xint = h^3 / Zvalue
   long nl_touched = 0;           // unique grid points covered by any ball
   int* nl_t_idx = nullptr;       // [nl_touched] grid index
+  int* nl_tmap = nullptr;        // [n] touched index of a grid point, -1 if no ball covers it
+  int nl_fuse = 1;               // 1: the TMA stencil pass adds the projector terms itself
   int* nl_t_off = nullptr;       // [nl_touched+1] offsets into nl_t_ent
   int* nl_t_ent = nullptr;       // [nl_points] ball-point ids (atom order)
   int* nl_point_atom = nullptr;  // [nl_points] owning atom of each ball point
@@ -105,6 +107,8 @@ struct psc_ctx {
   // tensor-core Gram pair (mixed precision)
   int gram_tc = 1;               // 1: FP32 Gram pairs on tcgen05 (3xTF32), 0: CUDA cores
   long gram_chunk = 0;           // rows per tensor-core Gram chunk (0: four waves of CTAs)
+  int* dm_pairs = nullptr;       // upper-triangle tile pairs of the DMMA Gram pair (int2)
+  int dm_pairs_cap = 0, dm_pairs_k = -1;
   float* tc_part = nullptr;      // per-chunk FP32 partial tiles
   size_t tc_part_floats = 0;
   void* tc_pairs = nullptr;      // int2 tile pairs (upper triangle)
@@ -317,6 +321,10 @@ int psc_random_impl(psc_ctx* ctx, int dtype, int dist, unsigned long long seed, 
 // zero the points outside the sphere mask in k columns (no-op without a mask)
 int psc_mask_block_impl(psc_ctx* ctx, int dtype, void* X, long ld, int k, cudaStream_t st);
 // FP32 block product W T on tensor cores; -1 when it does not apply
+int psc_gram_pair_dmma(psc_ctx* ctx, int dtype, const void* W, const void* V, long ld, int k, double* S, double* K,
+                       cudaStream_t st);
+int psc_gemm_tall_dmma(psc_ctx* ctx, int dtype, const void* W, long ldw, int k, const double* Tm, int kout, void* O,
+                       long ldo, cudaStream_t st);
 int psc_gemm_tall_tc(psc_ctx* ctx, const float* W, long ld, int k, const double* Tm, int kout, float* O, long ldo,
                      cudaStream_t st);
 // FP32 Gram pair on tensor cores; -1 when it does not apply

@@ -178,7 +178,9 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         return s.precision == "mixed" and (W is None or W.dtype == torch.float32)
 
     if s.precision == "mixed":
-        ctx.call("psc_set_gemm_impl", 1)   # the context may come from an earlier run's late phase
+        # the context may come from an earlier run's late phase
+        ctx.call("psc_set_gemm_impl", 1)
+        ctx.call("psc_set_gram_impl", 1)
     t_loop = time.perf_counter()
     def _done() -> bool:
         if err > s.tol:
@@ -196,14 +198,17 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
         H.set_potential(pot)
         if fp32_blocks():
             # mixed precision.  Late phase (error below mixed_switch): the
-            # block product W T leaves the tensor cores, whose truncating FP32
-            # accumulation holds the SCF error near 1e-6 and shakes the mixer,
-            # for the round-to-nearest path.  With mixed_finish = fp64 the
-            # blocks go to FP64 once the error is below mixed_fp64_at (or tol)
-            # or has not improved for three late iterations.
+            # Gram pair and the block product W T leave the tcgen05 tensor
+            # cores, whose FP32 accumulation rounds toward zero (it moves the
+            # FP32 fixed point: 2e-3 e of density at Si87H76), for the FP64
+            # tensor cores (exact products, FP64 sums).  With mixed_finish =
+            # fp64 the blocks go to FP64 once the error is below
+            # mixed_fp64_at (or tol) or has not improved for three late
+            # iterations.
             if err <= s.mixed_switch and not late:
                 late = True
                 ctx.call("psc_set_gemm_impl", 0)
+                ctx.call("psc_set_gram_impl", 0)
             if late:
                 stall = stall + 1 if err >= best_late else 0
                 best_late = min(best_late, err)

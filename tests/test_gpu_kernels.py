@@ -130,6 +130,38 @@ def test_hamiltonian_fp64_matches_reference_operator(h2o_box, golden_dir):
     assert np.abs(vnl - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("name", ["h2o", "si87h76"])
+def test_fused_projectors_equal_separate_pass(name):
+    """The projector terms added in the TMA stencil's epilogue against the
+    separate scatter pass on the same block: the same sums in the same order
+    (FP64 to 1e-15 of the largest entry, FP32 to its rounding), for a
+    Chebyshev-type step with P and for a plain H X."""
+    cfg = workloads.config_system(name)
+    dom = O.build_system(cfg["atoms"], h=cfg["h"], radius=cfg["radius"])
+    ctx = gpu.GridContext(dom, 8)
+    gpu.projector_setup(ctx, cfg["atoms"], ElementTable(), pseudo_tables())
+    n = ctx.n
+    g = torch.Generator(device="cuda").manual_seed(5)
+    gpu.Hamiltonian(ctx, torch.randn(n, dtype=torch.float64, device=DEV, generator=g))
+    k = 13
+    for dt, code, tol in ((torch.float64, F64, 1e-15), (torch.float32, F32, 1e-6)):
+        X = torch.randn(k, n, dtype=dt, device=DEV, generator=g)
+        P = torch.randn(k, n, dtype=dt, device=DEV, generator=g)
+        outs = []
+        for fused in (1, 0):
+            ctx.call("psc_set_projector_fusion", fused)
+            Y = P.clone()
+            ctx.call("psc_apply_h_axpby", code, gpu._p(X), n, gpu._p(Y), n, gpu._p(Y), n, k, 0.7, -0.2, -0.9,
+                     gpu._stream())
+            Z = torch.empty_like(X)
+            ctx.call("psc_apply_h", code, gpu._p(X), n, gpu._p(Z), n, k, gpu._stream())
+            outs.append((Y.double().cpu().numpy(), Z.double().cpu().numpy()))
+        ctx.call("psc_set_projector_fusion", 1)
+        for a, b in zip(outs[0], outs[1]):
+            assert rel(a, b) <= tol, (name, dt)
+    ctx.check_status()
+
+
 def test_hamiltonian_matches_reference_csr_on_h2o_grid(golden_dir):
     """H X on the H2O configuration's own grid (52^3, 0.2 A, O-H projectors)
     against the reference's assembled CSR B = 0.5 A + V_nl + diag(pot)
@@ -445,13 +477,18 @@ def _smooth_block(nx, ny, nz):
 
 @pytest.mark.parametrize("impl", [0, 2, 3, 4])
 def test_fp32_stencil_has_no_eigenvalue_offset(impl, capsys):
-    """The FP32 operator's Rayleigh quotients on smooth fields equal the
-    FP64 operator's to 5e-9 Ha with compensated weights (every occupied
-    eigenvalue of an FP32 SCF would otherwise move by the same constant,
-    which the band energy multiplies by the electron count).  With plain
-    FP32 weights the quotients move by the predicted sum-rule offset
-    dc0 + 6 sum_d dc_d (the weights' FP32 rounding errors), within 10 %.
-    Si87H76 grid (90^3, h = 0.4724 bohr), zero local potential."""
+    """Rayleigh quotients of smooth fields (the low spectrum, where the
+    occupied states live) under the FP32 operator against the FP64 one,
+    Si87H76 grid (90^3, h = 0.4724 bohr), zero local potential.  Plain FP32
+    weights move them by the sum-rule offset dc0 + 6 sum_d dc_d of the
+    weights' FP32 rounding errors (-6.1e-8 Ha here, a constant that the band
+    energy multiplies by the electron count); compensated weights remove
+    exactly that part (within 5 %).  What remains is the FP32 rounding of the
+    accumulation, which for the smoothest field cancels 2400-fold: 3e-8 Ha,
+    the value a CPU emulation of the kernel's operation order gives too.  Every
+    implementation computes the same operation order, so all four agree; the
+    bar of 4e-8 catches a weight-rounding offset or an accumulation whose
+    small terms are folded into a large sum (+2.3e-7)."""
     cfg = workloads.config_system("si87h76")
     dom = O.build_system(cfg["atoms"], h=cfg["h"], radius=cfg["radius"])
     ctx = gpu.GridContext(dom, 8)
@@ -479,8 +516,8 @@ def test_fp32_stencil_has_no_eigenvalue_offset(impl, capsys):
     with capsys.disabled():
         print(f"\nimpl {impl}: FP32 - FP64 Rayleigh quotients, compensated {out[1]}, plain {out[0]} "
               f"(predicted plain offset {pred:.3e} Ha)")
-    assert np.abs(out[1]).max() < 5e-9
-    assert np.abs(out[0] - pred).max() < 0.1 * abs(pred)
+    assert np.abs(out[1]).max() < 4e-8
+    assert np.abs((out[0] - out[1]) - pred).max() < 0.05 * abs(pred)
     ctx.check_status()
 
 
