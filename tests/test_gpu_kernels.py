@@ -310,8 +310,9 @@ def test_syev_edge_cases(k, kind):
                                      ((24, 24, 24), 143), ((21, 20, 19), 300)])
 def test_gram_pair_tensor_cores_match_fp64(shape, k):
     """FP32 Gram pair on tcgen05 (3xTF32, FP32 accumulation in tensor memory
-    per chunk of rows, FP64 across chunks) and on CUDA cores (FP64
-    accumulation), against FP64 products of the same FP32 values; odd n
+    per chunk of rows, FP64 across chunks) and on the FP64 tensor cores
+    (exact products, FP64 sums), against FP64 products of the same FP32
+    values; odd n
     exercises the scalar-load edge.  The tensor-core bound 2e-5 (relative to
     the largest entry) is the FP32 accumulation over a chunk of a few hundred
     rows; the products themselves are exact."""
@@ -331,18 +332,21 @@ def test_gram_pair_tensor_cores_match_fp64(shape, k):
         ctx.call("psc_gram_pair", F32, gpu._p(Wd), gpu._p(Vd), n, k, gpu._p(S), gpu._p(K), gpu._stream())
         out[impl] = (S.cpu().numpy().T, K.cpu().numpy().T)
     assert ctx.status()[5] == 0
-    # both paths return symmetric matrices: K = 0.5 (K + K^T), except that the
-    # tensor-core path forms off-diagonal 128-column tiles above the diagonal only
-    K_sym = 0.5 * (K_ref + K_ref.T)
-    K_tc = K_sym.copy()
-    t = np.arange(k) // 128
-    off = t[:, None] < t[None, :]
-    K_tc[off] = K_ref[off]
-    K_tc.T[off] = K_ref[off]
+    # both paths return symmetric matrices: K = 0.5 (K + K^T) inside the
+    # diagonal tiles, and the off-diagonal tiles formed above the diagonal
+    # only and mirrored (128-column tiles on tcgen05, 64-column tiles on the
+    # FP64 tensor cores); V here is not H W, so K itself is not symmetric
+    def tiled(width):
+        K_t = 0.5 * (K_ref + K_ref.T)
+        t = np.arange(k) // width
+        off = t[:, None] < t[None, :]
+        K_t[off] = K_ref[off]
+        K_t.T[off] = K_ref[off]
+        return K_t
     for impl, (S, K) in out.items():
         tol = 2e-5 if impl == 1 else 1e-12
         assert np.abs(S - S_ref).max() <= tol * np.abs(S_ref).max(), impl
-        assert np.abs(K - (K_tc if impl == 1 else K_sym)).max() <= tol * np.abs(K_ref).max(), impl
+        assert np.abs(K - tiled(128 if impl == 1 else 64)).max() <= tol * np.abs(K_ref).max(), impl
         assert np.array_equal(S, S.T) and np.array_equal(K, K.T)
         # the diagonals (column norms, Rayleigh quotients) are FP64 sums on
         # both paths: no bias from the tensor cores' FP32 accumulation
@@ -355,12 +359,12 @@ def test_gram_pair_tensor_cores_match_fp64(shape, k):
                                           ((16, 16, 16), 64, 30), ((12, 12, 12), 5, 3), ((33, 31, 29), 55, 40)])
 def test_block_product_tensor_cores_match_fp64(shape, k, kout):
     """FP32 block product Out = W T (the Rayleigh-Ritz W R^{-1} Y) on tcgen05
-    (3xTF32, FP32 accumulation over k) and on CUDA cores (FP64 arithmetic),
-    against the FP64 product of the same FP32 W and FP64 T.  kout > 256 uses
-    the second accumulator; an odd n (33 x 31 x 29) takes the CUDA-core path.
-    Bound 2e-5 of the largest entry for the tensor cores (the FP32
-    accumulation over k terms), FP32 rounding of the result for the CUDA
-    cores."""
+    (3xTF32, FP32 accumulation over k) and on the FP64 tensor cores (exact
+    products, FP64 sums, one rounding), against the FP64 product of the same
+    FP32 W and FP64 T.  kout > 256 uses the second accumulator; an odd n
+    (33 x 31 x 29) takes the FP64 tensor-core path.  Bound 2e-5 of the
+    largest entry for tcgen05 (the FP32 accumulation over k terms), FP32
+    rounding of the result for the FP64 tensor cores."""
     nx, ny, nz = shape
     ctx = gpu.GridContext({"nx": nx, "ny": ny, "nz": nz, "h": 0.4, "radius": 0.2 * (nx - 1)}, 8)
     n = ctx.n
