@@ -117,12 +117,6 @@ int psc_set_stencil_impl(psc_ctx* ctx, int impl);
  * rounding breaks the sum rule c0 + 6 sum c_d = 0 and shifts every
  * eigenvalue by a constant of order 1e-7 Ha. */
 int psc_set_stencil_weights(psc_ctx* ctx, int compensated);
-/* Kleinman-Bylander projector terms of H X: 1 (default) = added in the TMA
- * stencil pass's epilogue, at the points that balls cover, from the
- * projections taken before it (no separate read-modify-write of Y); 0 = a
- * separate scatter pass after the stencil (as the register-queue kernel
- * always does). */
-int psc_set_projector_fusion(psc_ctx* ctx, int fused);
 /* Sphere-masked Hamiltonian (no counterpart in the reference, which solves
  * on the whole cube): with radius > 0 (bohr) every H X returns zero at the
  * points farther than radius from the cube's centre, the projector tables

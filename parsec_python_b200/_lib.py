@@ -37,7 +37,6 @@ _SIGS = {
                           c_int),
     "psc_set_stencil_impl": ([_P, c_int], c_int),
     "psc_set_stencil_weights": ([_P, c_int], c_int),
-    "psc_set_projector_fusion": ([_P, c_int], c_int),
     "psc_laplacian_apply": ([_P, _P, _P, c_int, c_long, _P], c_int),
     "psc_cheb_filter": ([_P, c_int, c_int, c_int, _P, _P, _P, c_long, c_int, POINTER(c_int), _P], c_int),
     "psc_lanczos_bound": ([_P, c_int, c_ulonglong, _P, _P], c_int),

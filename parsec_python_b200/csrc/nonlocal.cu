@@ -5,10 +5,9 @@
 // w_a = 1/xint_a = h^3 / Zvalue_a, never forming the n_a x n_a blocks.
 //   project: one warp per (atom, column) reduces w_a * U_a^T X (3 values)
 //            over the ball with a fixed shuffle tree;
-//   scatter: adds, at every touched grid point, the sum over the balls
-//            covering it in atom order (no atomics, so the result is
-//            bitwise reproducible): inside the TMA stencil's epilogue where
-//            that pass runs, else one thread per (point, column group).
+//   scatter: one thread per (touched grid point, group of 8 columns) adds
+//            the sum over the balls covering that point, in atom order.  No
+//            atomics, so the result is bitwise reproducible.
 #include "psc_internal.cuh"
 #include "../../include/psc.h"
 
@@ -78,8 +77,7 @@ k_nl_project(const T* __restrict__ X, long ldx, int k, const int* __restrict__ a
   }
 }
 
-// Scatter (for launches whose stencil pass does not add the projector terms
-// itself): one thread per (touched grid point, group of NL_SC columns); the
+// Scatter: one thread per (touched grid point, group of NL_SC columns); the
 // entries covering the point and their u values are read once for every
 // column of the group, the group's Y values are loaded before the sums and
 // stored after them, and each column's sum runs over the entries in atom
@@ -165,8 +163,6 @@ int psc_nl_scatter(psc_ctx* ctx, int dtype, void* Y, long ldy, int k, const doub
 void psc_free_projectors(psc_ctx* ctx) {
   psc_dfree(ctx->nl_atom_off); psc_dfree(ctx->nl_idx); psc_dfree(ctx->nl_u64); psc_dfree(ctx->nl_u32);
   psc_dfree(ctx->nl_w); psc_dfree(ctx->nl_t_idx); psc_dfree(ctx->nl_t_off); psc_dfree(ctx->nl_t_ent);
-  psc_dfree(ctx->nl_tmap);
-  ctx->nl_tmap = nullptr;
   psc_dfree(ctx->nl_point_atom); psc_dfree(ctx->nl_proj);
   ctx->nl_atom_off = ctx->nl_idx = ctx->nl_t_idx = ctx->nl_t_off = ctx->nl_t_ent = ctx->nl_point_atom = nullptr;
   ctx->nl_u64 = nullptr; ctx->nl_u32 = nullptr; ctx->nl_w = nullptr; ctx->nl_proj = nullptr;
@@ -176,12 +172,6 @@ void psc_free_projectors(psc_ctx* ctx) {
 
 int psc_nl_apply_mask(psc_ctx* ctx, cudaStream_t st);
 
-extern "C" int psc_set_projector_fusion(psc_ctx* ctx, int fused) {
-  if (!ctx) return 2;
-  PSC_REQUIRE(ctx, fused == 0 || fused == 1, "projector fusion must be 0 or 1");
-  ctx->nl_fuse = fused;
-  return 0;
-}
 
 // setup.cu
 int psc_nl_box_distances(psc_ctx* ctx, int nbox, const int* box_dev /* [nbox][8] */, const double* xyz_dev,
@@ -315,12 +305,6 @@ extern "C" int psc_projector_setup(psc_ctx* ctx, int natoms, const int* species,
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->nl_t_off, t_off.data(), t_off.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->nl_t_ent, t_ent.data(), t_ent.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   PSC_CUDA(ctx, cudaMemcpyAsync(pt_orig_d, pt_orig.data(), npts * sizeof(int), cudaMemcpyHostToDevice, st));
-  // grid point -> touched index (-1 elsewhere), for the stencil pass that
-  // adds the projector terms in its epilogue
-  std::vector<int> tmap((size_t)ctx->n, -1);
-  for (size_t t = 0; t < t_idx.size(); ++t) tmap[(size_t)t_idx[t]] = (int)t;
-  PSC_CUDA(ctx, psc_dmalloc(&ctx->nl_tmap, tmap.size() * sizeof(int)));
-  PSC_CUDA(ctx, cudaMemcpyAsync(ctx->nl_tmap, tmap.data(), tmap.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   int rc = psc_nl_eval_u(ctx, npts, ctx->nl_idx, pt_orig_d, asp_d, xyz_d, radius, ctx->nl_u64, st);
   if (!rc) rc = psc_cast(ctx, PSC_F32, ctx->nl_u64, ctx->nl_u32, 3 * npts, st);
   if (!rc) rc = psc_nl_apply_mask(ctx, st);

@@ -78,8 +78,6 @@ struct psc_ctx {
   double* nl_w = nullptr;        // [nl_atoms] 1/xint = h^3 / Zvalue
   long nl_touched = 0;           // unique grid points covered by any ball
   int* nl_t_idx = nullptr;       // [nl_touched] grid index
-  int* nl_tmap = nullptr;        // [n] touched index of a grid point, -1 if no ball covers it
-  int nl_fuse = 1;               // 1: the TMA stencil pass adds the projector terms itself
   int* nl_t_off = nullptr;       // [nl_touched+1] offsets into nl_t_ent
   int* nl_t_ent = nullptr;       // [nl_points] ball-point ids (atom order)
   int* nl_point_atom = nullptr;  // [nl_points] owning atom of each ball point

@@ -166,7 +166,7 @@ static int launch_stencil_t(psc_ctx* ctx, const StencilPlan& p, const T* X, long
 
 template <typename T>
 int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy, const T* pot,
-                    const double* w, const double* coef, double a, double b, double g, bool masked, bool nl,
+                    const double* w, const double* coef, double a, double b, double g, bool masked,
                     cudaStream_t st);
 
 // Sphere mask: zero every point of k columns farther than sqrt(mask_r2)
@@ -200,20 +200,13 @@ int psc_mask_block_impl(psc_ctx* ctx, int dtype, void* X, long ld, int k, cudaSt
 template <typename T>
 static int launch_stencil(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy,
                           const T* pot, const double* c0c, const double* coef, double a, double b,
-                          double g, double* dot_partial, int* nblocks_out, cudaStream_t st, bool masked = false,
-                          bool* nl_fused = nullptr) {
+                          double g, double* dot_partial, int* nblocks_out, cudaStream_t st, bool masked = false) {
   // the TMA pipeline serves every launch that needs no fused dot product and
-  // meets the bulk-copy alignment rules (and then adds the projector terms
-  // itself when asked through nl_fused); the register-queue kernel the rest
+  // meets the bulk-copy alignment rules; the register-queue kernel the rest
   // (followed by a masking pass when the Hamiltonian is sphere-masked)
-  const bool nl = nl_fused && *nl_fused;
-  if (nl_fused) *nl_fused = false;
   if (!dot_partial && ctx->stencil_impl != 1) {
-    const int rc = psc_stencil_tma<T>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, c0c, coef, a, b, g, masked, nl, st);
-    if (rc >= 0) {
-      if (nl_fused) *nl_fused = nl;
-      return rc;
-    }
+    const int rc = psc_stencil_tma<T>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, c0c, coef, a, b, g, masked, st);
+    if (rc >= 0) return rc;
   }
   if (masked && ctx->mask_r2 > 0.0) {
     const int rc = launch_stencil<T>(ctx, k, X, ldx, P, ldp, Y, ldy, pot, c0c, coef, a, b, g, dot_partial,
@@ -270,17 +263,14 @@ int psc_apply_h_impl(psc_ctx* ctx, int dtype, const void* X, long ldx, void* Y, 
   }
   double w[5] = {ctx->ham_c0, ctx->ham_c[0], ctx->ham_c[1], ctx->ham_c[2], ctx->ham_c[3]};
   int rc;
-  // the projector terms: in the TMA stencil's epilogue where that pass runs
-  // (and fusion is on), else a separate scatter pass
-  bool fused = ctx->nl_atoms > 0 && ctx->nl_fuse && ctx->nl_tmap;
   if (dtype == PSC_F64)
     rc = launch_stencil<double>(ctx, k, (const double*)X, ldx, (const double*)P, ldp, (double*)Y, ldy,
-                                ctx->pot64, w, coef_dev, a, b, g, nullptr, nullptr, st, true, &fused);
+                                ctx->pot64, w, coef_dev, a, b, g, nullptr, nullptr, st, true);
   else
     rc = launch_stencil<float>(ctx, k, (const float*)X, ldx, (const float*)P, ldp, (float*)Y, ldy,
-                               ctx->pot32, w, coef_dev, a, b, g, nullptr, nullptr, st, true, &fused);
+                               ctx->pot32, w, coef_dev, a, b, g, nullptr, nullptr, st, true);
   if (rc) return rc;
-  if (ctx->nl_atoms > 0 && !fused) return psc_nl_scatter(ctx, dtype, Y, ldy, k, coef_dev, a, st);
+  if (ctx->nl_atoms > 0) return psc_nl_scatter(ctx, dtype, Y, ldy, k, coef_dev, a, st);
   return 0;
 }
 

@@ -207,21 +207,6 @@ struct TmaArgs {
   const T* pot;
   int nx, ny, nz;
   const int4* sched;  // per CTA: column, slab, first plane, end plane
-  // runs that cross or touch a row edge (only where VW does not divide nx):
-  // per slab, [number of interior runs, run of thread 0, ..., run of thread
-  // TNT-1], interior runs first, so that whole warps need no edge masks
-  const int* runs;
-  // projector terms added in the epilogue (tmap = NULL: a separate pass adds
-  // them): at a grid point covered by balls, alpha sum_e u_e . proj[atom_e]
-  // with alpha the step's H coefficient
-  const int* tmap;
-  const int* t_off;
-  const int* t_ent;
-  const int* pt_atom;
-  const T* nlu;
-  long npts;
-  const double* proj;
-  int kproj;
   T c0, c[4];
   T c0lo, clo[4];     // FP32: the coefficients' rounding errors (c + clo = the FP64 value to 2^-48)
   const double* coef;
@@ -335,16 +320,7 @@ k_stencil_tma(TmaArgs<T> A) {
   }
 
   // own run of VW points (it may cross a row boundary: every point has its own x)
-  // the thread's run: with a run table, warps whose runs are all interior
-  // (every x neighbour within the row) skip the per-point edge masks
-  int run = threadIdx.x;
-  bool fast_warp = false;
-  if (!(YA == VW) && A.runs) {
-    const int* rt = A.runs + (long)work.y * (TNT + 1);
-    run = rt[1 + threadIdx.x];
-    fast_warp = (int)(threadIdx.x | 31) < rt[0];
-  }
-  const int loc = VW * run;
+  const int loc = VW * threadIdx.x;
   const bool own = loc < seff;
   const int q = slab0 + loc;
   const int s_c = H + loc;  // window offset of the run
@@ -468,9 +444,7 @@ k_stencil_tma(TmaArgs<T> A) {
         }
       }
       const T* pl = ring + (size_t)((z - z0) % NBUF) * WS;
-      // MK: per-point edge masks on the x terms (runs that reach a row end)
-      auto compute = [&](auto MK) {
-        constexpr bool M = decltype(MK)::value;
+      if (own) {
         // x neighbours: the aligned vectors around the run (the run itself is
         // the queue's centre).  Row-aligned runs (EXACT) read the vectors
         // outside the row from the slot's zero pad; otherwise each point
@@ -485,8 +459,8 @@ k_stencil_tma(TmaArgs<T> A) {
             vload<VW>(pl + (EXACT ? xo[v] : s_c - OFF + v * VW), xs + v * VW);
           }
         }
-        auto xl = [&](int j, int d) -> T { return (!M || d <= el[j]) ? xs[OFF + j - d] : T(0); };
-        auto xr = [&](int j, int d) -> T { return (!M || d <= er[j]) ? xs[OFF + j + d] : T(0); };
+        auto xl = [&](int j, int d) -> T { return (EXACT || d <= el[j]) ? xs[OFF + j - d] : T(0); };
+        auto xr = [&](int j, int d) -> T { return (EXACT || d <= er[j]) ? xs[OFF + j + d] : T(0); };
         // per point: acc = c0 x + sum_d c_d (((y-d + y+d) + (z-d + z+d)) + (x-d + x+d)),
         // and with compensated weights the same sum over the weights'
         // rounding errors in its own (small) accumulator.  FP32 sums the
@@ -575,39 +549,6 @@ k_stencil_tma(TmaArgs<T> A) {
             if (Pc) o[j] += cg * pvv[j];
           }
         }
-        if (A.tmap) {
-          // Kleinman-Bylander terms of the points covered by balls: the
-          // sum over the covering entries in atom order, added as the
-          // separate scatter pass would add it to the stored value
-          int tm[VW];
-          const int* tp = A.tmap + (long)z * nxy + q;
-          if constexpr (VW == 4) {
-            const int4 v = *reinterpret_cast<const int4*>(tp);
-            tm[0] = v.x; tm[1] = v.y; tm[2] = v.z; tm[3] = v.w;
-          } else {
-#pragma unroll
-            for (int j = 0; j < VW; ++j) tm[j] = tp[j];
-          }
-          int hit = tm[0];
-#pragma unroll
-          for (int j = 1; j < VW; ++j) hit = max(hit, tm[j]);
-          if (hit >= 0) {
-            const double alpha = A.coef ? A.coef[0] : A.a;
-            const int kp = A.kproj;
-#pragma unroll
-            for (int j = 0; j < VW; ++j) {
-              if (tm[j] < 0) continue;
-              double sv = 0.0;
-              for (int e = A.t_off[tm[j]]; e < A.t_off[tm[j] + 1]; ++e) {
-                const int p = A.t_ent[e];
-                const double* pr = A.proj + (long)A.pt_atom[p] * 3 * kp + col;
-                sv += (double)A.nlu[p] * pr[0] + (double)A.nlu[A.npts + p] * pr[kp] +
-                      (double)A.nlu[2 * A.npts + p] * pr[2 * kp];
-              }
-              o[j] = (T)((double)o[j] + alpha * sv);
-            }
-          }
-        }
         if (masked) {
           const double zm = z * A.h - A.cz;
 #pragma unroll
@@ -615,12 +556,6 @@ k_stencil_tma(TmaArgs<T> A) {
             if (mxy[j] + zm * zm > A.mask_r2) o[j] = T(0);
         }
         vstore<VW>(Yc + (long)z * nxy + q, o);
-      };
-      if (own) {
-        if (EXACT || fast_warp)
-          compute(std::false_type{});
-        else
-          compute(std::true_type{});
       }
       // every SYNC_EVERY planes (and after the last): the slots of all
       // planes <= z are free, so the ring is topped up to plane z + NBUF.
@@ -792,50 +727,10 @@ static const int4* stencil_sched(psc_ctx* ctx, int nslab, int k, int fill, int s
   return reinterpret_cast<const int4*>(b.dev);
 }
 
-// Run table for VW-point runs when VW does not divide nx (cached per
-// context): per slab, thread t takes run table[1 + t]; interior runs (all
-// VW points at least R from both row ends, hence in one row) come first,
-// then the runs that reach a row end, then the runs past the plane's end;
-// table[0] counts the interior ones.
-static const int* stencil_runs(psc_ctx* ctx, int VW, int R, int nslab, cudaStream_t st) {
-  const long long key = -(1 + 64LL * VW + R);
-  for (auto& e : ctx->st_sched)
-    if (e.key == key) return e.dev;
-  const int nx = ctx->nx, nxy = ctx->nx * ctx->ny, ts = VW * TNT;
-  psc_ctx::StencilSched e;
-  e.key = key;
-  e.host.assign((size_t)nslab * (TNT + 1), 0);
-  for (int sl = 0; sl < nslab; ++sl) {
-    int* row = e.host.data() + (size_t)sl * (TNT + 1);
-    std::vector<int> inner, edge, past;
-    for (int r = 0; r < TNT; ++r) {
-      const long q = (long)sl * ts + (long)VW * r;
-      if (q >= nxy) {
-        past.push_back(r);
-        continue;
-      }
-      const int x0 = (int)(q % nx);
-      (x0 >= R && x0 + VW - 1 <= nx - 1 - R ? inner : edge).push_back(r);
-    }
-    row[0] = (int)inner.size();
-    int t = 1;
-    for (int r : inner) row[t++] = r;
-    for (int r : edge) row[t++] = r;
-    for (int r : past) row[t++] = r;
-  }
-  e.n = (int)e.host.size();
-  if (psc_dmalloc(&e.dev, e.host.size() * sizeof(int)) != cudaSuccess) return nullptr;
-  ctx->st_sched.push_back(std::move(e));
-  auto& b = ctx->st_sched.back();
-  if (cudaMemcpyAsync(b.dev, b.host.data(), b.host.size() * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return nullptr;
-  return b.dev;
-}
-
 template <typename T, int R, int VW, int MODE>
 static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy,
                         const T* pot, const double* w, const double* coef, double a, double b, double g,
-                        bool masked, bool nl, cudaStream_t st) {
+                        bool masked, cudaStream_t st) {
   const int nxy = ctx->nx * ctx->ny;
   constexpr int TS = slab_points<VW>();
   const int nslab = (nxy + TS - 1) / TS;
@@ -861,25 +756,6 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   TmaArgs<T> A;
   A.X = X; A.ldx = ldx; A.P = P; A.ldp = ldp; A.Y = Y; A.ldy = ldy; A.pot = pot;
   A.nx = ctx->nx; A.ny = ctx->ny; A.nz = ctx->nz; A.sched = sched;
-  A.tmap = nullptr;
-  if (nl) {
-    A.tmap = ctx->nl_tmap;
-    A.t_off = ctx->nl_t_off;
-    A.t_ent = ctx->nl_t_ent;
-    A.pt_atom = ctx->nl_point_atom;
-    if constexpr (sizeof(T) == 8)
-      A.nlu = ctx->nl_u64;
-    else
-      A.nlu = ctx->nl_u32;
-    A.npts = ctx->nl_points;
-    A.proj = (const double*)ctx->nl_proj;
-    A.kproj = k;
-  }
-  A.runs = nullptr;
-  if (ctx->nx % VW != 0) {
-    A.runs = stencil_runs(ctx, VW, R, nslab, st);
-    PSC_REQUIRE(ctx, A.runs != nullptr, "stencil: run table allocation failed");
-  }
   A.c0 = (T)w[0];
   A.c0lo = (T)(w[0] - (double)A.c0);
   for (int i = 0; i < 4; ++i) {
@@ -899,7 +775,7 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
 // Returns -1 if the TMA path does not apply (caller uses the register kernel).
 template <typename T>
 int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long ldp, T* Y, long ldy, const T* pot,
-                    const double* w, const double* coef, double a, double b, double g, bool masked, bool nl,
+                    const double* w, const double* coef, double a, double b, double g, bool masked,
                     cudaStream_t st) {
   if (!tma_ok<T>(ctx, X, ldx, P, ldp, Y, ldy)) return -1;
   // FP32 takes 4-point runs with the arithmetic on packed pairs (measured
@@ -911,7 +787,7 @@ int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long 
   const int impl = ctx->stencil_impl;
   const bool narrow = sizeof(T) == 4 && ctx->nx % 4 != 0 && ctx->nx % 2 == 0 && (impl == 2 || impl == 3);
   const int mode = (impl == 0 || impl == 2 ? 1 : 0) | (ctx->stencil_comp ? 2 : 0);
-#define PSC_TMA_ARGS ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, nl, st
+#define PSC_TMA_ARGS ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st
 #define PSC_TMA_MODES(VWW)                                                                                    \
   switch (mode) {                                                                                             \
     case 0: return launch_tma_t<T, RR, VWW, 0>(PSC_TMA_ARGS);                                                 \
@@ -944,7 +820,7 @@ int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long 
 
 template int psc_stencil_tma<double>(psc_ctx*, int, const double*, long, const double*, long, double*, long,
                                      const double*, const double*, const double*, double, double, double, bool,
-                                     bool, cudaStream_t);
+                                     cudaStream_t);
 template int psc_stencil_tma<float>(psc_ctx*, int, const float*, long, const float*, long, float*, long,
-                                    const float*, const double*, const double*, double, double, double, bool, bool,
+                                    const float*, const double*, const double*, double, double, double, bool,
                                     cudaStream_t);

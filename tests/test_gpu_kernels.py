@@ -130,38 +130,6 @@ def test_hamiltonian_fp64_matches_reference_operator(h2o_box, golden_dir):
     assert np.abs(vnl - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("name", ["h2o", "si87h76"])
-def test_fused_projectors_equal_separate_pass(name):
-    """The projector terms added in the TMA stencil's epilogue against the
-    separate scatter pass on the same block: the same sums in the same order
-    (FP64 to 1e-15 of the largest entry, FP32 to its rounding), for a
-    Chebyshev-type step with P and for a plain H X."""
-    cfg = workloads.config_system(name)
-    dom = O.build_system(cfg["atoms"], h=cfg["h"], radius=cfg["radius"])
-    ctx = gpu.GridContext(dom, 8)
-    gpu.projector_setup(ctx, cfg["atoms"], ElementTable(), pseudo_tables())
-    n = ctx.n
-    g = torch.Generator(device="cuda").manual_seed(5)
-    gpu.Hamiltonian(ctx, torch.randn(n, dtype=torch.float64, device=DEV, generator=g))
-    k = 13
-    for dt, code, tol in ((torch.float64, F64, 1e-15), (torch.float32, F32, 1e-6)):
-        X = torch.randn(k, n, dtype=dt, device=DEV, generator=g)
-        P = torch.randn(k, n, dtype=dt, device=DEV, generator=g)
-        outs = []
-        for fused in (1, 0):
-            ctx.call("psc_set_projector_fusion", fused)
-            Y = P.clone()
-            ctx.call("psc_apply_h_axpby", code, gpu._p(X), n, gpu._p(Y), n, gpu._p(Y), n, k, 0.7, -0.2, -0.9,
-                     gpu._stream())
-            Z = torch.empty_like(X)
-            ctx.call("psc_apply_h", code, gpu._p(X), n, gpu._p(Z), n, k, gpu._stream())
-            outs.append((Y.double().cpu().numpy(), Z.double().cpu().numpy()))
-        ctx.call("psc_set_projector_fusion", 1)
-        for a, b in zip(outs[0], outs[1]):
-            assert rel(a, b) <= tol, (name, dt)
-    ctx.check_status()
-
-
 def test_hamiltonian_matches_reference_csr_on_h2o_grid(golden_dir):
     """H X on the H2O configuration's own grid (52^3, 0.2 A, O-H projectors)
     against the reference's assembled CSR B = 0.5 A + V_nl + diag(pot)
