@@ -397,6 +397,26 @@ k_stencil_tma(TmaArgs<T> A) {
     el[j] = min(R, xj);
     er[j] = min(R, nx - 1 - xj);
   }
+  // Pair masks (FP32 4-point runs with packed arithmetic, nx = 2 mod 4):
+  // the run's 12-value x window is six aligned pairs, none of which crosses
+  // a row (nx is even), and the run itself splits into two pairs, A (points
+  // 0, 1) and B (points 2, 3), each in one row.  A window pair is a valid x
+  // neighbour of A's points iff it lies in A's row, likewise for B, so the
+  // edge masks are twelve loop-invariant 0/1 factors (instead of a compare
+  // and a select per point and distance in every plane).  mA[p], mB[p]:
+  // pair p of the window (flat q - 4 + 2p) for owner A, B.
+  constexpr bool PAIRM = (YA != VW) && PK && VW == 4 && YA == 2 && R <= 4;
+  float mA[6], mB[6];
+  if constexpr (PAIRM) {
+    const int x0 = own ? q % nx : 0;
+    const bool b_next = x0 + 2 > nx - 2;   // B starts the next row
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+      const int xp = x0 - 4 + 2 * p;       // x of the pair's first point, in A's row coordinates
+      mA[p] = (xp >= 0 && xp <= nx - 2) ? 1.f : 0.f;
+      mB[p] = b_next ? (xp >= nx ? 1.f : 0.f) : mA[p];
+    }
+  }
   const bool masked = A.mask_r2 > 0.0;
   double mxy[VW];   // (x^2 + y^2) of the run's points, for the sphere mask
 #pragma unroll
@@ -471,6 +491,16 @@ k_stencil_tma(TmaArgs<T> A) {
         T o[VW];
         if constexpr (PK) {
           constexpr int NP = VW / 2;
+          // the window masked for each owner pair (PAIRM): 16 multiplies
+          float xa[PAIRM ? NPV * VW : 1], xb[PAIRM ? NPV * VW : 1];
+          if constexpr (PAIRM) {
+#pragma unroll
+            for (int i = 0; i < NPV * VW; ++i) {
+              const int p = i >> 1;
+              xa[i] = p == 2 ? xs[i] : xs[i] * mA[p];
+              xb[i] = p == 3 ? xs[i] : xs[i] * mB[p];
+            }
+          }
           float2 acc[NP], alo[NP];
 #pragma unroll
           for (int h = 0; h < NP; ++h) {
@@ -491,7 +521,14 @@ k_stencil_tma(TmaArgs<T> A) {
               const int j = 2 * h;
               const float2 yy = __fadd2_rn(make_float2(ym[j], ym[j + 1]), make_float2(yp[j], yp[j + 1]));
               const float2 zz = __fadd2_rn(make_float2(zq[j][sm], zq[j + 1][sm]), make_float2(zq[j][sp], zq[j + 1][sp]));
-              const float2 xx = __fadd2_rn(make_float2(xl(j, d), xl(j + 1, d)), make_float2(xr(j, d), xr(j + 1, d)));
+              float2 xx;
+              if constexpr (PAIRM) {
+                const float* xw = h == 0 ? xa : xb;
+                xx = __fadd2_rn(make_float2(xw[OFF + j - d], xw[OFF + j + 1 - d]),
+                                make_float2(xw[OFF + j + d], xw[OFF + j + 1 + d]));
+              } else {
+                xx = __fadd2_rn(make_float2(xl(j, d), xl(j + 1, d)), make_float2(xr(j, d), xr(j + 1, d)));
+              }
               const float2 t = __fadd2_rn(__fadd2_rn(yy, zz), xx);
               acc[h] = __ffma2_rn(cd, t, acc[h]);
               if constexpr (COMP) alo[h] = __ffma2_rn(make_float2(A.clo[d - 1], A.clo[d - 1]), t, alo[h]);
