@@ -303,7 +303,7 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
     time per step over `reps` steps, inputs larger than L2.  impls: stencil
     implementations to time (0 default, 2 two-point FP32 runs, 3 / 4 scalar
     FP32 arithmetic with two- / four-point runs); weights: FP32 stencil
-    weights (1 compensated, the default; 0 plain FP32)."""
+    weights (1 with the sum-rule correction, the default; 0 plain FP32)."""
     import torch
 
     from parsec_python_b200 import gpu
@@ -769,7 +769,7 @@ def main():
     ap.add_argument("--hx-masks", default="cube,sphere", help="masks of --hx")
     ap.add_argument("--hx-dtypes", default="f64,f32", help="block types of --hx")
     ap.add_argument("--hx-nl", default="0,1", help="--hx without (0) and with (1) the projectors")
-    ap.add_argument("--hx-weights", default="1", help="FP32 stencil weights of --hx (1 compensated, 0 plain)")
+    ap.add_argument("--hx-weights", default="1", help="FP32 stencil weights of --hx (1 sum-rule corrected, 0 plain)")
     ap.add_argument("--syev", nargs="?", const="55_rand,55_near,143_near,307_near", default=None,
                     help="only time the k x k symmetric eigensolver (comma-separated <k>_<rand|near> cases)")
     args = ap.parse_args()

@@ -111,11 +111,10 @@ int psc_apply_h_axpby(psc_ctx* ctx, int dtype, const void* X, long ldx, const vo
  * everywhere, 2 = the TMA pipeline with 2-point FP32 runs when nx is even but
  * not a multiple of 4, 3 / 4 = as 2 / 0 with scalar FP32 arithmetic. */
 int psc_set_stencil_impl(psc_ctx* ctx, int impl);
-/* FP32 weights of the TMA stencil: 1 (default) = each weight applied as its
- * FP32 value plus its FP32 rounding error, so the FP32 operator is the FP64
- * one up to unbiased arithmetic rounding; 0 = plain FP32 weights, whose
- * rounding breaks the sum rule c0 + 6 sum c_d = 0 and shifts every
- * eigenvalue by a constant of order 1e-7 Ha. */
+/* FP32 weights of the TMA stencil: 1 (default) = FP32 weights plus one
+ * correction term for their sum rule (c0 + 6 sum c_d = 0, which the weights'
+ * rounding breaks by a constant of order 1e-7 Ha that every eigenvalue would
+ * carry); 0 = plain FP32 weights. */
 int psc_set_stencil_weights(psc_ctx* ctx, int compensated);
 /* Sphere-masked Hamiltonian (no counterpart in the reference, which solves
  * on the whole cube): with radius > 0 (bohr) every H X returns zero at the

@@ -208,7 +208,7 @@ struct TmaArgs {
   int nx, ny, nz;
   const int4* sched;  // per CTA: column, slab, first plane, end plane
   T c0, c[4];
-  T c0lo, clo[4];     // FP32: the coefficients' rounding errors (c + clo = the FP64 value to 2^-48)
+  T csr;              // FP32 weights: minus their sum-rule residual, (c0 + 6 sum_d c_d) in FP32 - in FP64
   const double* coef;
   double a, b, g;
   long wait_limit;    // polls of each mbarrier wait before the CTA gives up
@@ -222,12 +222,13 @@ struct TmaArgs {
 
 // YA: alignment (in elements) of the y-neighbour rows, the largest of VW, 2, 1
 // that divides nx; their loads are split to match.  MODE (FP32 only):
-// bit 0 = the arithmetic on packed pairs of points, bit 1 =
-// compensated coefficients: every weight is applied as c + clo, the FP32
-// value and its rounding error, so the operator is the FP64 one up to the
-// rounding of the arithmetic (which is unbiased).  With plain FP32 weights
-// the sum rule c0 + 6 sum_d c_d = 0 fails by a few 1e-8 Ha, a constant shift
-// of every eigenvalue that the band energy multiplies by the electron count.
+// bit 0 = the arithmetic on packed pairs of points, bit 1 = sum-rule
+// correction: with the weights rounded to FP32 the sum rule c0 + 6 sum_d c_d
+// = 0 fails by their rounding errors (-6.1e-8 Ha at h = 0.47 bohr), a
+// constant shift of every eigenvalue that the band energy multiplies by the
+// electron count; one more term, -(that residual) x, removes it.  (Applying
+// every weight as its FP32 value plus its rounding error moved the
+// Rayleigh quotients of smooth fields by no more than this one term does.)
 template <typename T, int R, int YA, int VW, int MODE>
 __global__ void __launch_bounds__(TNT)
 k_stencil_tma(TmaArgs<T> A) {
@@ -501,12 +502,11 @@ k_stencil_tma(TmaArgs<T> A) {
               xb[i] = p == 3 ? xs[i] : xs[i] * mB[p];
             }
           }
-          float2 acc[NP], alo[NP];
+          float2 acc[NP];
 #pragma unroll
           for (int h = 0; h < NP; ++h) {
             const float2 xc = make_float2(xs[OFF + 2 * h], xs[OFF + 2 * h + 1]);
             acc[h] = REV ? make_float2(0.f, 0.f) : __fmul2_rn(make_float2(c0, c0), xc);
-            alo[h] = (COMP && !REV) ? __fmul2_rn(make_float2(A.c0lo, A.c0lo), xc) : make_float2(0.f, 0.f);
           }
 #pragma unroll
           for (int dd = 0; dd < R; ++dd) {
@@ -531,7 +531,6 @@ k_stencil_tma(TmaArgs<T> A) {
               }
               const float2 t = __fadd2_rn(__fadd2_rn(yy, zz), xx);
               acc[h] = __ffma2_rn(cd, t, acc[h]);
-              if constexpr (COMP) alo[h] = __ffma2_rn(make_float2(A.clo[d - 1], A.clo[d - 1]), t, alo[h]);
             }
           }
 #pragma unroll
@@ -539,11 +538,8 @@ k_stencil_tma(TmaArgs<T> A) {
             const int j = 2 * h;
             const float2 xc = make_float2(xs[OFF + j], xs[OFF + j + 1]);
             float2 a = acc[h];
-            if constexpr (REV) {
-              a = __ffma2_rn(make_float2(c0, c0), xc, a);
-              if constexpr (COMP) alo[h] = __ffma2_rn(make_float2(A.c0lo, A.c0lo), xc, alo[h]);
-            }
-            if constexpr (COMP) a = __fadd2_rn(a, alo[h]);
+            if constexpr (REV) a = __ffma2_rn(make_float2(c0, c0), xc, a);
+            if constexpr (COMP) a = __ffma2_rn(make_float2(A.csr, A.csr), xc, a);
             if (has_pot) a = __ffma2_rn(make_float2(pov[j], pov[j + 1]), xc, a);
             float2 r = __ffma2_rn(make_float2(ca, ca), a, __fmul2_rn(make_float2(cb, cb), xc));
             if (Pc) r = __ffma2_rn(make_float2(cg, cg), make_float2(pvv[j], pvv[j + 1]), r);
@@ -551,12 +547,9 @@ k_stencil_tma(TmaArgs<T> A) {
             o[j + 1] = r.y;
           }
         } else {
-          T acc[VW], alo[VW];
+          T acc[VW];
 #pragma unroll
-          for (int j = 0; j < VW; ++j) {
-            acc[j] = REV ? T(0) : c0 * xs[OFF + j];
-            alo[j] = (COMP && !REV) ? A.c0lo * xs[OFF + j] : T(0);
-          }
+          for (int j = 0; j < VW; ++j) acc[j] = REV ? T(0) : c0 * xs[OFF + j];
 #pragma unroll
           for (int dd = 0; dd < R; ++dd) {
             const int d = REV ? R - dd : dd + 1;
@@ -569,18 +562,14 @@ k_stencil_tma(TmaArgs<T> A) {
               const T t = ((ym[j] + yp[j]) + (zq[j][(u + R - d) % Q] + zq[j][(u + R + d) % Q])) +
                           (xl(j, d) + xr(j, d));
               acc[j] += cd * t;
-              if constexpr (COMP) alo[j] += A.clo[d - 1] * t;
             }
           }
 #pragma unroll
           for (int j = 0; j < VW; ++j) {
             const T xc = xs[OFF + j];
             T a = acc[j];
-            if constexpr (REV) {
-              a += c0 * xc;
-              if constexpr (COMP) alo[j] += A.c0lo * xc;
-            }
-            if constexpr (COMP) a += alo[j];
+            if constexpr (REV) a += c0 * xc;
+            if constexpr (COMP) a += A.csr * xc;
             if (has_pot) a += pov[j] * xc;
             o[j] = ca * a + cb * xc;
             if (Pc) o[j] += cg * pvv[j];
@@ -794,11 +783,15 @@ static int launch_tma_t(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, l
   A.X = X; A.ldx = ldx; A.P = P; A.ldp = ldp; A.Y = Y; A.ldy = ldy; A.pot = pot;
   A.nx = ctx->nx; A.ny = ctx->ny; A.nz = ctx->nz; A.sched = sched;
   A.c0 = (T)w[0];
-  A.c0lo = (T)(w[0] - (double)A.c0);
+  // the sum rule c0 + 6 sum_d c_d = 0 holds for the FP64 weights; in the
+  // stored type it is off by the weights' rounding errors, which the
+  // correction term removes (FP32 only, MODE bit 1)
+  double rs = (double)A.c0 - w[0];
   for (int i = 0; i < 4; ++i) {
     A.c[i] = (T)w[1 + i];
-    A.clo[i] = (T)(w[1 + i] - (double)A.c[i]);
+    rs += 6.0 * ((double)A.c[i] - w[1 + i]);
   }
+  A.csr = (T)(-rs);
   A.coef = coef; A.a = a; A.b = b; A.g = g; A.status = ctx->dev_status;
   A.wait_limit = ctx->wait_limit;
   A.mask_r2 = masked ? ctx->mask_r2 : 0.0;

@@ -454,13 +454,14 @@ def test_fp32_stencil_has_no_eigenvalue_offset(impl, capsys):
     Si87H76 grid (90^3, h = 0.4724 bohr), zero local potential.  Plain FP32
     weights move them by the sum-rule offset dc0 + 6 sum_d dc_d of the
     weights' FP32 rounding errors (-6.1e-8 Ha here, a constant that the band
-    energy multiplies by the electron count); compensated weights remove
+    energy multiplies by the electron count); the sum-rule correction removes
     exactly that part (within 5 %).  What remains is the FP32 rounding of the
     accumulation, which for the smoothest field cancels 2400-fold: 3e-8 Ha,
     the value a CPU emulation of the kernel's operation order gives too.  Every
     implementation computes the same operation order, so all four agree; the
     bar of 4e-8 catches a weight-rounding offset or an accumulation whose
-    small terms are folded into a large sum (+2.3e-7)."""
+    small terms are folded into a large sum (+2.3e-7).  "compensated" below
+    is weights mode 1."""
     cfg = workloads.config_system("si87h76")
     dom = O.build_system(cfg["atoms"], h=cfg["h"], radius=cfg["radius"])
     ctx = gpu.GridContext(dom, 8)
