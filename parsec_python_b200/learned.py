@@ -263,10 +263,22 @@ def _bias_mask() -> np.ndarray:
     return np.concatenate(mask)
 
 
+_W_CACHE: dict = {}
+
+
 def load_weights(path: Path | str = DEFAULT_WEIGHTS) -> dict | None:
+    """The trained parameters in a file, read once per process (and again if
+    the file changes): the same dict for every SCF, so the network built from
+    it (cached_net) is reused instead of rebuilt with fresh device buffers
+    for every solve."""
     p = Path(path)
     if not p.exists():
         return None
+    st = p.stat()
+    key = (str(p.resolve()), st.st_mtime_ns, st.st_size)
+    hit = _W_CACHE.get(key)
+    if hit is not None:
+        return hit
     z = np.load(p, allow_pickle=False)
     if "wb16" in z.files:
         # BF16 -> FP32 is exact: the bit pattern is the upper half of the FP32 word
@@ -274,8 +286,10 @@ def load_weights(path: Path | str = DEFAULT_WEIGHTS) -> dict | None:
         w[_bias_mask()] = z["bias"]
     else:
         w = z["w"]
-    return {"w": w, "a0": float(z["a0"]), "a1": float(z["a1"]), "at": float(z["at"]),
-            "meta": json.loads(str(z["meta"]))}
+    params = {"w": w, "a0": float(z["a0"]), "a1": float(z["a1"]), "at": float(z["at"]),
+              "meta": json.loads(str(z["meta"]))}
+    _W_CACHE[key] = params
+    return params
 
 
 # Networks built for a grid shape, reused by later SCFs on the same grid: the
