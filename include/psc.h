@@ -308,6 +308,10 @@ int psc_gram_pair(psc_ctx* ctx, int dtype, const void* W, const void* V, long ld
  * grid ceil(n / stride)), ksize 3 (padding 1) or 1. */
 int psc_conv3d_fwd(psc_ctx* ctx, const int* geom, const void* A, const void* S, const void* W, const float* bias,
                    int act, void* out, float* out32, void* stream);
+/* Forward implementation: 1 (default) tcgen05 implicit GEMM (BF16 operands,
+ * FP32 accumulation in tensor memory; activations 16-byte aligned), 0 the
+ * CUDA-core kernel.  The backward always runs on the CUDA cores. */
+int psc_set_conv_impl(psc_ctx* ctx, int tensor_cores);
 /* act: 0 identity, 1 ReLU, 2 leaky ReLU (slope 1/16 below zero).
  * Backward of one convolution.  gout: dL/d(out) FP32 [nvo][Cout]; out: the
  * forward's BF16 output (needed when act != 0);

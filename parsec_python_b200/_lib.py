@@ -69,6 +69,7 @@ _SIGS = {
     "psc_mask_block": ([_P, c_int, _P, c_long, c_int, _P], c_int),
     "psc_gram_pair": ([_P, c_int, _P, _P, c_long, c_int, _P, _P, _P], c_int),
     "psc_conv3d_fwd": ([_P, _P, _P, _P, _P, _P, c_int, _P, _P, _P], c_int),
+    "psc_set_conv_impl": ([_P, c_int], c_int),
     "psc_conv3d_bwd": ([_P, _P, _P, _P, _P, _P, _P, c_int, _P, _P, _P, c_int, _P, c_int, _P, _P, _P, c_long, _P],
                        c_int),
     "psc_mse_loss": ([_P, _P, c_int, _P, c_long, _P, _P, _P], c_int),

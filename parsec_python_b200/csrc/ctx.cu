@@ -114,6 +114,7 @@ extern "C" int psc_ctx_destroy(psc_ctx* ctx) {
   psc_dfree(ctx->tc_part); psc_dfree(ctx->tc_pairs); psc_dfree(ctx->tri_work); psc_dfree(ctx->col_norm_part); psc_dfree(ctx->tsplit);
   for (auto& e : ctx->st_sched) psc_dfree(e.dev);
   psc_dfree(ctx->dm_pairs);
+  psc_dfree(ctx->conv_wt);
   for (int a = 0; a < 3; ++a) { psc_dfree(ctx->spec_S[a]); psc_dfree(ctx->spec_lam[a]); }
   psc_dfree(ctx->spec_tmp); psc_dfree(ctx->lz_basis);
   if (ctx->cg_exec) cudaGraphExecDestroy(ctx->cg_exec);

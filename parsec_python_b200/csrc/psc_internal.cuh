@@ -115,11 +115,15 @@ struct psc_ctx {
   int gemm_tc = 1;               // 1: FP32 W T on tcgen05 (3xTF32), 0: CUDA cores
   float* tsplit = nullptr;       // T split into TF32 hi/lo B tiles
   size_t tsplit_floats = 0;
+  // learned-start convolution forward: 1 tcgen05 implicit GEMM, 0 CUDA cores
+  int conv_tc = 1;
+  void* conv_wt = nullptr;       // BF16 weights transposed to [Cout rounded to 16][K rounded to 64]
+  size_t conv_wt_bytes = 0;
   // sphere mask of the Hamiltonian (0: the whole cube): H X is zero at
   // points farther than sqrt(mask_r2) from mask_c (the cube's centre)
   double mask_r2 = 0.0;
   double mask_c[3] = {0.0, 0.0, 0.0};
-  // polls of every bounded device-side wait before it gives up (status words 3-6)
+  // polls of every bounded device-side wait before it gives up (status words 3-7)
   long wait_limit = PSC_WAIT_DEFAULT;
   // exact squared column norms of FP32 blocks (density normalisation)
   double* col_norm_part = nullptr;  // [cap][PSC_NORM_CHUNKS]

@@ -19,16 +19,9 @@
 
 #include <cuda_bf16.h>
 
-namespace {
+#include "conv_geom.cuh"
 
-struct ConvGeom {
-  int nxi, nyi, nzi;   // virtual input grid
-  int nxa, nya, nza;   // grid of A (the virtual grid halved when up)
-  int up;
-  int Ca, Cs, Cin;
-  int nxo, nyo, nzo;   // output grid
-  int stride, ksize, Cout;
-};
+namespace {
 
 __device__ __forceinline__ void unpack8(const uint4 u, float* f) {
   const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
@@ -38,19 +31,6 @@ __device__ __forceinline__ void unpack8(const uint4 u, float* f) {
     f[2 * i] = t.x;
     f[2 * i + 1] = t.y;
   }
-}
-
-// 8 channels [c0, c0+8) of the virtual input at voxel (x, y, z) (inside the grid)
-__device__ __forceinline__ uint4 vin8(const __nv_bfloat16* A, const __nv_bfloat16* S, const ConvGeom& g, int x,
-                                      int y, int z, int c0) {
-  if (c0 < g.Ca) {
-    long va;
-    if (g.up) va = (x >> 1) + (long)g.nxa * ((y >> 1) + (long)g.nya * (z >> 1));
-    else va = x + (long)g.nxa * (y + (long)g.nya * z);
-    return *reinterpret_cast<const uint4*>(A + va * g.Ca + c0);
-  }
-  const long vs = x + (long)g.nxi * (y + (long)g.nyi * z);
-  return *reinterpret_cast<const uint4*>(S + vs * g.Cs + (c0 - g.Ca));
 }
 
 constexpr int FWD_NT = 128;
@@ -105,7 +85,7 @@ k_conv_fwd(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict_
       if (xi < 0 || yi < 0 || zi < 0 || xi >= g.nxi || yi >= g.nyi || zi >= g.nzi) continue;
       for (int c8 = 0; c8 < cn; c8 += 8) {
         float x[8];
-        unpack8(vin8(A, S, g, xi, yi, zi, cc + c8), x);
+        unpack8(conv_vin8(A, S, g, xi, yi, zi, cc + c8), x);
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const float* wr = ws + (tap * CIN_CHUNK + c8 + j) * COT;
@@ -243,7 +223,7 @@ k_conv_bwd_w(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restric
         const int yo = (int)(r % g.nyo), zo = (int)(r / g.nyo);
         const int xi = xo * g.stride + dx - pad, yi = yo * g.stride + dy - pad, zi = zo * g.stride + dz - pad;
         if (xi >= 0 && yi >= 0 && zi >= 0 && xi < g.nxi && yi < g.nyi && zi < g.nzi)
-          unpack8(vin8(A, S, g, xi, yi, zi, c0), x);
+          unpack8(conv_vin8(A, S, g, xi, yi, zi, c0), x);
       }
 #pragma unroll
       for (int i = 0; i < 8; ++i) xs[j][8 * half + i] = x[i];
@@ -447,6 +427,7 @@ extern "C" int psc_conv3d_fwd(psc_ctx* ctx, const int* geom, const void* A, cons
   const auto* s = static_cast<const __nv_bfloat16*>(S);
   const auto* w = static_cast<const __nv_bfloat16*>(W);
   auto* o = static_cast<__nv_bfloat16*>(out);
+  if (ctx->conv_tc) return psc_conv_tc_forward(ctx, g, a, s, w, bias, act, o, out32, st);
   if (g.Cout % 16 == 0) {
     dim3 grid(psc_div_up(nvo, FWD_NT), g.Cout / 16);
     k_conv_fwd<16><<<grid, FWD_NT, 0, st>>>(a, s, w, bias, g, act, o, out32);

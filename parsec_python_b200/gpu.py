@@ -148,6 +148,8 @@ class GridContext:
             raise PscError("tensor-core Gram pipeline wait timed out")
         if f[6]:
             raise PscError("tensor-core block product pipeline wait timed out")
+        if f[7]:
+            raise PscError("tensor-core conv3d pipeline wait timed out")
 
     def info(self) -> dict:
         out = (c_long * 8)()

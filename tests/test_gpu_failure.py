@@ -1,7 +1,7 @@
 """Failure detection on the GPU path, in forms that fault, trap or hang no GPU.
 
-Device side: every bounded wait (stencil bulk-copy pipeline, tensor-core Gram
-and block-product pipelines, the persistent CG's grid barrier) takes its poll
+Device side: every bounded wait (stencil bulk-copy pipeline, tensor-core Gram,
+block-product and convolution pipelines, the persistent CG's grid barrier) takes its poll
 limit from the context.  With the limit set to 0 each wait runs out at its
 first unsatisfied poll; the kernels must then record their status word,
 drain what they issued and return, and the context must stay usable: the
@@ -12,6 +12,8 @@ Host side: the errors the reference raises or reports on bad input
 maxits, rsdft_solver.py:397-413), a NaN potential, and the learned start's
 fallback to SAD on a non-finite prediction.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -45,7 +47,19 @@ def test_wait_limit_zero_reports_every_pipeline_and_context_recovers():
     zero = torch.zeros(n, dtype=torch.float64, device=DEV)
     A = gpu.Laplacian(ctx)
     st = gpu._stream()
+    # one 3x3x3 convolution of the learned start: 8 -> 16 channels on an 8^3 grid
+    geom = (ctypes.c_int * 15)(8, 8, 8, 8, 8, 8, 0, 8, 0, 8, 8, 8, 1, 3, 16)
+    cx = torch.from_numpy(rng.standard_normal((512, 8)).astype(np.float32)).to(torch.bfloat16).to(DEV)
+    cw = torch.from_numpy((rng.standard_normal(27 * 8 * 16) / 15).astype(np.float32)).to(torch.bfloat16).to(DEV)
+    cb = torch.zeros(16, dtype=torch.float32, device=DEV)
     ctx.status(clear=True)
+
+    def conv(impl):
+        ctx.call("psc_set_conv_impl", impl)
+        y = torch.empty(512, 16, dtype=torch.bfloat16, device=DEV)
+        y32 = torch.full((512, 16), float("nan"), dtype=torch.float32, device=DEV)
+        ctx.call("psc_conv3d_fwd", geom, gpu._p(cx), None, gpu._p(cw), gpu._p(cb), 0, gpu._p(y), gpu._p(y32), st)
+        return y32
 
     def run_all():
         Y = H @ X64
@@ -53,8 +67,9 @@ def test_wait_limit_zero_reports_every_pipeline_and_context_recovers():
         ctx.call("psc_gram_pair", F32, gpu._p(W32), gpu._p(W32), n, 40, gpu._p(S), gpu._p(K), st)
         O32 = torch.empty_like(W32)
         ctx.call("psc_gemm_nn", F32, gpu._p(W32), n, 40, gpu._p(T), 40, gpu._p(O32), n, st)
+        C = conv(1)
         torch.cuda.synchronize()
-        return Y, S, O32
+        return Y, S, O32, C
 
     ctx.call("psc_set_wait_limit", 0)
     run_all()
@@ -62,6 +77,7 @@ def test_wait_limit_zero_reports_every_pipeline_and_context_recovers():
     assert flags[3] == 1, "stencil pipeline wait did not report"
     assert flags[5] == 1, "tensor-core Gram wait did not report"
     assert flags[6] == 1, "tensor-core block product wait did not report"
+    assert flags[7] == 1, "tensor-core convolution wait did not report"
     with pytest.raises(PscError, match="grid barrier timed out"):
         gpu.pcg(A, rhs, zero, 20, 1e-5)
     assert ctx.status(clear=True)[4] == 1
@@ -71,7 +87,7 @@ def test_wait_limit_zero_reports_every_pipeline_and_context_recovers():
     # default limit: the same calls are correct and report nothing
     ctx.call("psc_set_wait_limit", -1)
     ctx.status(clear=True)
-    Y, S, O32 = run_all()
+    Y, S, O32, C = run_all()
     x, its = gpu.pcg(A, rhs, zero, 20, 1e-5)
     assert ctx.status(clear=True) == [0] * 8
     dom = {"nx": 24, "ny": 24, "nz": 24, "h": 0.4, "radius": 0.2 * 23}
@@ -82,6 +98,9 @@ def test_wait_limit_zero_reports_every_pipeline_and_context_recovers():
     assert np.abs(S.cpu().numpy().T - W64 @ W64.T).max() < 2e-5 * np.abs(W64 @ W64.T).max()
     Oref = W64.T @ T.cpu().numpy().T
     assert np.abs(O32.double().cpu().numpy().T - Oref).max() < 2e-5 * np.abs(Oref).max()
+    C0 = conv(0)
+    assert ctx.status(clear=True) == [0] * 8
+    assert (C - C0).abs().max().item() < 2e-5 * max(1.0, C0.abs().max().item())
     xo, its_o = O.pcg(O.laplacian(dom, 8), rhs.cpu().numpy(), np.zeros(n), 20, 1e-5)
     assert its == its_o and np.abs(x.cpu().numpy() - xo).max() < 1e-8 * np.abs(xo).max()
 
