@@ -365,6 +365,40 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
     return out
 
 
+def unet_timing(nx: int = 90, reps: int = 10) -> dict:
+    """The learned start's network forward (11 convolutions, psc_conv3d_fwd)
+    on an nx^3 grid with random weights and input, on the tensor cores
+    (tcgen05 implicit GEMM) and on the CUDA cores: median CUDA-event time of
+    one forward after 3 warm-up passes, and the largest difference of the
+    two outputs."""
+    import torch
+
+    from parsec_python_b200 import gpu, learned
+
+    ctx = gpu.GridContext({"nx": nx, "ny": nx, "nz": nx, "h": 0.4724, "radius": 0.2 * (nx - 1)}, 8)
+    net = learned.UNet3D(ctx, seed=1)
+    x = torch.randn(nx ** 3, 8, device="cuda").to(torch.bfloat16)
+    res, outs = {}, {}
+    for impl, key in ((1, "tcgen05"), (0, "cuda_cores")):
+        ctx.call("psc_set_conv_impl", impl)
+        for _ in range(3):
+            net.forward(x)
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            y = net.forward(x)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        res[key + "_ms"] = float(np.median(ts))
+        outs[key] = y.clone()
+    ctx.call("psc_set_conv_impl", 1)
+    ctx.check_status()
+    return {"nx": nx, **res, "max_abs_diff": (outs["tcgen05"] - outs["cuda_cores"]).abs().max().item(),
+            "max_abs_out": outs["cuda_cores"].abs().max().item()}
+
+
 def syev_timing(cases: str = "55_rand,55_near,143_near,307_near", reps: int = 20) -> dict:
     """The FP64 symmetric eigensolver of the Rayleigh-Ritz step (psc_syev:
     Householder tridiagonalisation, bisection, inverse iteration,
@@ -777,6 +811,8 @@ def main():
     ap.add_argument("--hx-dtypes", default="f64,f32", help="block types of --hx")
     ap.add_argument("--hx-nl", default="0,1", help="--hx without (0) and with (1) the projectors")
     ap.add_argument("--hx-weights", default="1", help="FP32 stencil weights of --hx (1 sum-rule corrected, 0 plain)")
+    ap.add_argument("--unet", type=int, default=None, metavar="NX",
+                    help="only time the learned start's network forward on an NX^3 grid (both conv implementations)")
     ap.add_argument("--syev", nargs="?", const="55_rand,55_near,143_near,307_near", default=None,
                     help="only time the k x k symmetric eigensolver (comma-separated <k>_<rand|near> cases)")
     args = ap.parse_args()
@@ -806,6 +842,9 @@ def main():
         return
     if args.syev:
         print(json.dumps(syev_timing(args.syev)))
+        return
+    if args.unet:
+        print(json.dumps(unet_timing(args.unet, reps=max(1, args.steps) * 2)))
         return
     if args.hx:
         widths = tuple(int(x) for x in args.hx_widths.split(","))

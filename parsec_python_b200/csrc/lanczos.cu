@@ -291,11 +291,75 @@ __device__ __forceinline__ double warp_dot_col(const double* x, const double* y,
   return psc_warp_sum(s);
 }
 
-// work per cluster start: rdiag, du, du2, dl, piv (5k doubles)
+// LU with partial pivoting of T - lam I (one thread; sequential by nature):
+// rd = inverted diagonal of U, du / du2 its two superdiagonals, dl the
+// multipliers, piv 1 where rows i and i+1 were interchanged
+__device__ __forceinline__ void tri_lu(const double* __restrict__ a, const double* __restrict__ e, int k, double lam,
+                                       double tiny, double* __restrict__ rd, double* __restrict__ du,
+                                       double* __restrict__ du2, double* __restrict__ dl, double* __restrict__ piv) {
+  double dc = a[0] - lam;
+  double uc = k > 1 ? e[0] : 0.0;
+  for (int i = 0; i + 1 < k; ++i) {
+    const double sub = e[i];
+    const double dn = a[i + 1] - lam;
+    const double un = i + 2 < k ? e[i + 1] : 0.0;
+    if (fabs(dc) >= fabs(sub)) {
+      const double d = fabs(dc) < tiny ? (dc < 0.0 ? -tiny : tiny) : dc;
+      const double r = 1.0 / d;
+      const double m = sub * r;
+      rd[i] = r; du[i] = uc; du2[i] = 0.0; dl[i] = m; piv[i] = 0.0;
+      dc = dn - m * uc;
+      uc = un;
+    } else {
+      const double r = 1.0 / sub;
+      const double m = dc * r;
+      rd[i] = r; du[i] = dn; du2[i] = un; dl[i] = m; piv[i] = 1.0;
+      dc = uc - m * dn;
+      uc = -m * un;
+    }
+  }
+  const double d = fabs(dc) < tiny ? (dc < 0.0 ? -tiny : tiny) : dc;
+  rd[k - 1] = 1.0 / d;
+}
+
+// x <- (T - lam I)^{-1} x from the factors of tri_lu (one thread)
+__device__ __forceinline__ void tri_lu_solve(double* __restrict__ x, int k, const double* __restrict__ rd,
+                                             const double* __restrict__ du, const double* __restrict__ du2,
+                                             const double* __restrict__ dl, const double* __restrict__ piv) {
+  // forward: apply the row interchanges and multipliers
+  double xi = x[0];
+  for (int i = 0; i + 1 < k; ++i) {
+    const double xn = x[i + 1];
+    if (piv[i] == 0.0) {
+      x[i] = xi;
+      xi = xn - dl[i] * xi;
+    } else {
+      x[i] = xn;
+      xi = xi - dl[i] * xn;
+    }
+  }
+  x[k - 1] = xi;
+  // backward with U (diagonal stored inverted)
+  double x1 = x[k - 1] * rd[k - 1], x2 = 0.0;
+  x[k - 1] = x1;
+  for (int i = k - 2; i >= 0; --i) {
+    const double v = (x[i] - du[i] * x1 - du2[i] * x2) * rd[i];
+    x[i] = v;
+    x2 = x1;
+    x1 = v;
+  }
+}
+
+// Eigenvectors of the tridiagonal T by inverse iteration, one warp per
+// cluster of close eigenvalues (the members are orthogonalised against the
+// earlier ones).  With one warp per CTA (NT = 32) the LU factors and the
+// iterate live in shared memory (8k doubles with T); with NT = 128 the
+// factors go to `work` (5k doubles per cluster start) and the iterate to Z.
 template <int NT>
 __global__ void __launch_bounds__(NT)
 k_tri_invit(const double* __restrict__ ab, int k, const double* __restrict__ evals, int nvec, double* __restrict__ Z,
             long ldz, double crel, double* __restrict__ work) {
+  constexpr bool SMEM = NT == 32;
   extern __shared__ double tri_sm[];
   __shared__ double red[64];
   __shared__ double s_lo, s_hi;
@@ -313,7 +377,7 @@ k_tri_invit(const double* __restrict__ ab, int k, const double* __restrict__ eva
   while (s1 < nvec && evals[s1] - evals[s1 - 1] <= ctol) ++s1;
   const double tiny = fmax(DBL_EPSILON * tnorm, DBL_MIN);
   const double pertol = 10.0 * DBL_EPSILON * tnorm;
-  double* rd = work + (long)s0 * 5 * k;
+  double* rd = SMEM ? tri_sm + 2 * k : work + (long)s0 * 5 * k;
   double* du = rd + k;
   double* du2 = du + k;
   double* dl = du2 + k;
@@ -323,31 +387,9 @@ k_tri_invit(const double* __restrict__ ab, int k, const double* __restrict__ eva
     double lam = evals[j];
     if (j > s0) lam = fmax(lam, lam_prev + pertol);
     lam_prev = lam;
-    double* x = Z + (long)j * ldz;
-    // LU with partial pivoting of T - lam I (lane 0; sequential by nature)
-    if (lane == 0) {
-      double dc = a[0] - lam;
-      double uc = k > 1 ? e[0] : 0.0;
-      for (int i = 0; i + 1 < k; ++i) {
-        const double sub = e[i];
-        const double dn = a[i + 1] - lam;
-        const double un = i + 2 < k ? e[i + 1] : 0.0;
-        if (fabs(dc) >= fabs(sub)) {
-          const double d = fabs(dc) < tiny ? (dc < 0.0 ? -tiny : tiny) : dc;
-          const double m = sub / d;
-          rd[i] = 1.0 / d; du[i] = uc; du2[i] = 0.0; dl[i] = m; piv[i] = 0.0;
-          dc = dn - m * uc;
-          uc = un;
-        } else {
-          const double m = dc / sub;
-          rd[i] = 1.0 / sub; du[i] = dn; du2[i] = un; dl[i] = m; piv[i] = 1.0;
-          dc = uc - m * dn;
-          uc = -m * un;
-        }
-      }
-      const double d = fabs(dc) < tiny ? (dc < 0.0 ? -tiny : tiny) : dc;
-      rd[k - 1] = 1.0 / d;
-    }
+    double* z = Z + (long)j * ldz;
+    double* x = SMEM ? piv + k : z;
+    if (lane == 0) tri_lu(a, e, k, lam, tiny, rd, du, du2, dl, piv);
     for (int i = lane; i < k; i += 32) x[i] = tri_hash_unit(j, i);
     __syncwarp();
     for (int it = 0; it < 3; ++it) {
@@ -355,30 +397,7 @@ k_tri_invit(const double* __restrict__ ab, int k, const double* __restrict__ eva
       const double sc = nrm > 0.0 ? 1.0 / nrm : 1.0;
       for (int i = lane; i < k; i += 32) x[i] *= sc;
       __syncwarp();
-      if (lane == 0) {
-        // forward: apply the row interchanges and multipliers
-        double xi = x[0];
-        for (int i = 0; i + 1 < k; ++i) {
-          const double xn = x[i + 1];
-          if (piv[i] == 0.0) {
-            x[i] = xi;
-            xi = xn - dl[i] * xi;
-          } else {
-            x[i] = xn;
-            xi = xi - dl[i] * xn;
-          }
-        }
-        x[k - 1] = xi;
-        // backward with U (diagonal stored inverted)
-        double x1 = x[k - 1] * rd[k - 1], x2 = 0.0;
-        x[k - 1] = x1;
-        for (int i = k - 2; i >= 0; --i) {
-          const double v = (x[i] - du[i] * x1 - du2[i] * x2) * rd[i];
-          x[i] = v;
-          x2 = x1;
-          x1 = v;
-        }
-      }
+      if (lane == 0) tri_lu_solve(x, k, rd, du, du2, dl, piv);
       __syncwarp();
       for (int p = s0; p < j; ++p) {
         const double* zp = Z + (long)p * ldz;
@@ -398,7 +417,7 @@ k_tri_invit(const double* __restrict__ ab, int k, const double* __restrict__ eva
       if (fabs(other) > fabs(best) || (fabs(other) == fabs(best) && other > best)) best = other;
     }
     const double sc = (best < 0.0 ? -1.0 : 1.0) / nrm;
-    for (int i = lane; i < k; i += 32) x[i] *= sc;
+    for (int i = lane; i < k; i += 32) z[i] = x[i] * sc;
     __syncwarp();
   }
 }
@@ -434,8 +453,9 @@ int psc_tridiag_eig_impl(psc_ctx* ctx, const double* ab, int k, int nvec, double
     ctx->tri_work_doubles = need;
   }
   if (solo) {
-    if (tri_smem(ctx, (const void*)k_tri_invit<32>, smem)) return 1;
-    k_tri_invit<32><<<nvec, 32, smem, st>>>(ab, k, evals, nvec, Z, ldz, crel, ctx->tri_work);
+    const size_t smem_iv = 8 * (size_t)k * sizeof(double);   // T, the LU factors and the iterate
+    if (tri_smem(ctx, (const void*)k_tri_invit<32>, smem_iv)) return 1;
+    k_tri_invit<32><<<nvec, 32, smem_iv, st>>>(ab, k, evals, nvec, Z, ldz, crel, ctx->tri_work);
   } else {
     if (tri_smem(ctx, (const void*)k_tri_invit<128>, smem)) return 1;
     k_tri_invit<128><<<psc_div_up(nvec, 4), 128, smem, st>>>(ab, k, evals, nvec, Z, ldz, crel, ctx->tri_work);
