@@ -40,6 +40,7 @@ from __future__ import annotations
 
 import argparse
 import gc
+import gc
 import json
 import os
 import statistics
@@ -367,10 +368,10 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
 
 def unet_timing(nx: int = 90, reps: int = 10) -> dict:
     """The learned start's network forward (11 convolutions, psc_conv3d_fwd)
-    on an nx^3 grid with random weights and input, on the tensor cores
-    (tcgen05 implicit GEMM) and on the CUDA cores: median CUDA-event time of
-    one forward after 3 warm-up passes, and the largest difference of the
-    two outputs."""
+    on an nx^3 grid with random weights and input: every layer on the tensor
+    cores (tcgen05 implicit GEMM), every layer on the CUDA cores, and the
+    default choice by layer; median CUDA-event time of one forward after 3
+    warm-up passes, and the largest difference of the first two outputs."""
     import torch
 
     from parsec_python_b200 import gpu, learned
@@ -379,7 +380,7 @@ def unet_timing(nx: int = 90, reps: int = 10) -> dict:
     net = learned.UNet3D(ctx, seed=1)
     x = torch.randn(nx ** 3, 8, device="cuda").to(torch.bfloat16)
     res, outs = {}, {}
-    for impl, key in ((1, "tcgen05"), (0, "cuda_cores")):
+    for impl, key in ((2, "tcgen05"), (0, "cuda_cores"), (1, "by_layer")):
         ctx.call("psc_set_conv_impl", impl)
         for _ in range(3):
             net.forward(x)
@@ -555,6 +556,9 @@ def e2e_once(form: str, workdir: Path, name: str = CFG_NAME) -> tuple[float, int
     inp = workdir / f"{name}.in"
     inp.write_text(E2E_INPUT.format(atoms=lines, h=cfg["h"], radius=cfg["radius"], tol=cfg["tol"],
                                     poldeg=cfg["poldeg"], nev=cfg["nev"], **f))
+    # the previous call's context and blocks are released before the clock
+    # starts, so their device frees cannot land inside this call
+    gc.collect()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     res = cli.main([str(inp)])

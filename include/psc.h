@@ -259,6 +259,26 @@ int psc_mixer_reset(psc_ctx* ctx, int capacity);
 int psc_mixer_step(psc_ctx* ctx, const double* x1, const double* f1, double mix, double restart_factor,
                    double* x_new, int* m_used, void* stream);
 int psc_mixer_history(psc_ctx* ctx, int* m_out);
+/* Type-II multisecant mixer (Mixer/msecant2.py:24-93; Anderson mixing with
+ * group size 0): its control flow runs on the host, these are its operations
+ * on the FP64 n-vectors of the history (n = the context's grid size, columns
+ * lda apart, lda >= n):
+ *   psc_mix2_diff:  df = f1 - df, dx = (x1 - dx) + mix df (msecant2.py:58-60)
+ *   psc_mix2_store: dx = x1, df = f1
+ *   psc_block_dots: out_dev[i] = A_i . x for the r columns of A
+ *   psc_block_combine: y = base + mix f - sum_i A_i c_i (f may be NULL, y may
+ *     be base)
+ *   psc_block_absrow_max: out_dev[0] = max over rows of sum_i |A_i| (the
+ *     infinity norm Mixer/qinv.py:27 scales its rank tolerance by).
+ * The Gram matrix of a group and the product DF C use psc_gram and
+ * psc_gemm_nn. */
+int psc_mix2_diff(psc_ctx* ctx, const double* x1, const double* f1, double* dx, double* df, double mix,
+                  void* stream);
+int psc_mix2_store(psc_ctx* ctx, const double* x1, const double* f1, double* dx, double* df, void* stream);
+int psc_block_dots(psc_ctx* ctx, const double* A, long lda, int r, const double* x, double* out_dev, void* stream);
+int psc_block_combine(psc_ctx* ctx, double* y, const double* base, const double* f, double mix, const double* A,
+                      long lda, int r, const double* c_dev, void* stream);
+int psc_block_absrow_max(psc_ctx* ctx, const double* A, long lda, int r, double* out_dev, void* stream);
 
 /* ---- utilities ---------------------------------------------------------- */
 /* Counter-based random block: dist 0 uniform [0,1) (np.random.rand in
@@ -308,10 +328,11 @@ int psc_gram_pair(psc_ctx* ctx, int dtype, const void* W, const void* V, long ld
  * grid ceil(n / stride)), ksize 3 (padding 1) or 1. */
 int psc_conv3d_fwd(psc_ctx* ctx, const int* geom, const void* A, const void* S, const void* W, const float* bias,
                    int act, void* out, float* out32, void* stream);
-/* Forward implementation: 1 (default) tcgen05 implicit GEMM (BF16 operands,
- * FP32 accumulation in tensor memory; activations 16-byte aligned), 0 the
- * CUDA-core kernel.  The backward always runs on the CUDA cores. */
-int psc_set_conv_impl(psc_ctx* ctx, int tensor_cores);
+/* Forward implementation: 2 the tcgen05 implicit GEMM (BF16 operands, FP32
+ * accumulation in tensor memory; activations 16-byte aligned), 0 the
+ * CUDA-core kernel, 1 (default) by layer: tcgen05 from 32 output channels.
+ * The backward always runs on the CUDA cores. */
+int psc_set_conv_impl(psc_ctx* ctx, int impl);
 /* act: 0 identity, 1 ReLU, 2 leaky ReLU (slope 1/16 below zero).
  * Backward of one convolution.  gout: dL/d(out) FP32 [nvo][Cout]; out: the
  * forward's BF16 output (needed when act != 0);

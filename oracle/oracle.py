@@ -866,7 +866,7 @@ def spectral_preconditioner(domain: dict, order: int):
 
 
 # ----------------------------------------------------------------------------
-# mixer (Mixer/msecant1.py with Mixer/includemix.py parameters)
+# mixers (Mixer/msecant1.py, Mixer/msecant2.py with Mixer/includemix.py parameters)
 # ----------------------------------------------------------------------------
 def qinv(A, tol=np.finfo(float).eps):
     """Quasi-inverse by pivoted QR, Mixer/qinv.py:5-62."""
@@ -952,6 +952,71 @@ class MSecant1:
             x_new = x_new - self.DX[:, m - res:m] @ ((C @ self.N[:, :res].T) @ f1)
         self.DX = np.hstack([self.DX, x1[:, None]])
         self.DF = np.hstack([self.DF, f1[:, None]])
+        return x_new, m
+
+
+class MSecant2:
+    """Multisecant Type-II update, Mixer/msecant2.py:6-100 with the parameters
+    of Mixer/includemix.py:21-49 (mix 0.5, restart factor 0.1, EN_like 0);
+    group_size 0 takes all iterates as one group: Anderson mixing.  A restart
+    sets the EN stage to 2 whatever EN_like is (msecant2.py:45-51), after
+    which the stage alternates 2 -> 1 -> 2: on stage-1 calls the newest
+    difference is not formed and, with a full last group, the stored DF C is
+    used as it is; on stage-2 calls the new iterate is not appended."""
+
+    def __init__(self, mix=0.5, group_size=0, restart_factor=0.1, en_like=0):
+        self.mix, self.gs, self.rf, self.en_like = mix, group_size, restart_factor, en_like
+        self.tol = np.finfo(float).eps
+        self.DX = None
+        self.DF = None
+        self.en = None
+
+    def __call__(self, x1, f1):
+        mix = self.mix
+        x1 = np.asarray(x1, dtype=np.float64).ravel()
+        f1 = np.asarray(f1, dtype=np.float64).ravel()
+        if self.DX is None:
+            self.DX = x1[:, None].copy()
+            self.DF = f1[:, None].copy()
+            self.en = 0 if self.en_like == 0 else 2
+            return x1 + mix * f1, 0
+        m = self.DX.shape[1]
+        sz = m + 1 if self.gs == 0 else self.gs
+        if self.en != 1 and m >= 2 and np.linalg.norm(self.DF[:, -1], 2) < self.rf * np.linalg.norm(f1, 2):
+            self.DX = x1[:, None].copy()
+            self.DF = f1[:, None].copy()
+            self.en = 2
+            return x1 + mix * f1, 0
+        res = (m + sz - 1) % sz + 1
+        ngroup = (m - res) // sz
+        if self.en != 1:
+            self.DX[:, m - 1] = x1 - self.DX[:, m - 1]
+            self.DF[:, m - 1] = f1 - self.DF[:, m - 1]
+            self.DX[:, m - 1] += mix * self.DF[:, m - 1]
+            for i in range(ngroup):
+                s, e = i * sz, (i + 1) * sz
+                self.DX[:, m - 1] -= self.DX[:, s:e] @ (self.DF[:, s:e].T @ self.DF[:, m - 1])
+        x_new = x1 + mix * f1
+        for i in range(ngroup):
+            s, e = i * sz, (i + 1) * sz
+            x_new -= self.DX[:, s:e] @ (self.DF[:, s:e].T @ f1)
+        if self.en == 1 and res == sz:
+            x_new -= self.DX[:, ngroup * sz:m] @ (self.DF[:, ngroup * sz:m].T @ f1)
+        else:
+            C2 = qinv(self.DF[:, m - res:m], self.tol)
+            C = C2 @ C2.T
+            if res == sz:
+                self.DF[:, m - sz:m] = self.DF[:, m - sz:m] @ C
+                x_new -= self.DX[:, m - res:m] @ (self.DF[:, m - res:m].T @ f1)
+            else:
+                x_new -= self.DX[:, m - res:m] @ ((self.DF[:, m - res:m] @ C).T @ f1)
+        if self.en != 2:
+            self.DX = np.hstack([self.DX, x1[:, None]])
+            self.DF = np.hstack([self.DF, f1[:, None]])
+        if self.en == 1:
+            self.en = 2
+        elif self.en == 2:
+            self.en = 1
         return x_new, m
 
 

@@ -81,6 +81,11 @@ _SIGS = {
     "psc_mixer_reset": ([_P, c_int], c_int),
     "psc_mixer_step": ([_P, _P, _P, c_double, c_double, _P, POINTER(c_int), _P], c_int),
     "psc_mixer_history": ([_P, POINTER(c_int)], c_int),
+    "psc_mix2_diff": ([_P, _P, _P, _P, _P, c_double, _P], c_int),
+    "psc_mix2_store": ([_P, _P, _P, _P, _P, _P], c_int),
+    "psc_block_dots": ([_P, _P, c_long, c_int, _P, _P, _P], c_int),
+    "psc_block_combine": ([_P, _P, _P, _P, c_double, _P, c_long, c_int, _P, _P], c_int),
+    "psc_block_absrow_max": ([_P, _P, c_long, c_int, _P, _P], c_int),
     "psc_random": ([_P, c_int, c_int, c_ulonglong, _P, c_long, c_long, c_int, _P], c_int),
     "psc_cast": ([_P, c_int, _P, _P, c_long, _P], c_int),
     "psc_dot": ([_P, _P, _P, c_long, _P, _P], c_int),

@@ -287,8 +287,9 @@ int psc_conv_tc_forward(psc_ctx* ctx, const ConvGeom& g, const __nv_bfloat16* a,
   return 0;
 }
 
-extern "C" int psc_set_conv_impl(psc_ctx* ctx, int tensor_cores) {
+extern "C" int psc_set_conv_impl(psc_ctx* ctx, int impl) {
   if (!ctx) return 2;
-  ctx->conv_tc = tensor_cores ? 1 : 0;
+  PSC_REQUIRE(ctx, impl >= 0 && impl <= 2, "conv_impl: 0 (CUDA cores), 1 (by layer) or 2 (tensor cores)");
+  ctx->conv_tc = impl;
   return 0;
 }

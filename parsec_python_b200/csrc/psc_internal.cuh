@@ -115,7 +115,8 @@ struct psc_ctx {
   int gemm_tc = 1;               // 1: FP32 W T on tcgen05 (3xTF32), 0: CUDA cores
   float* tsplit = nullptr;       // T split into TF32 hi/lo B tiles
   size_t tsplit_floats = 0;
-  // learned-start convolution forward: 1 tcgen05 implicit GEMM, 0 CUDA cores
+  // learned-start convolution forward: 2 tcgen05 implicit GEMM, 0 CUDA cores,
+  // 1 by layer (tcgen05 from 32 output channels)
   int conv_tc = 1;
   void* conv_wt = nullptr;       // BF16 weights transposed to [Cout rounded to 16][K rounded to 64]
   size_t conv_wt_bytes = 0;

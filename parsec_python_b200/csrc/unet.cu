@@ -427,7 +427,11 @@ extern "C" int psc_conv3d_fwd(psc_ctx* ctx, const int* geom, const void* A, cons
   const auto* s = static_cast<const __nv_bfloat16*>(S);
   const auto* w = static_cast<const __nv_bfloat16*>(W);
   auto* o = static_cast<__nv_bfloat16*>(out);
-  if (ctx->conv_tc) return psc_conv_tc_forward(ctx, g, a, s, w, bias, act, o, out32, st);
+  // the tensor cores where a layer has 32 or more output channels; the
+  // full-grid layers with 8 (N padded to 16) are gather-bound and faster on
+  // the CUDA cores (90^3: 636 against 779 us for the widest of them)
+  if (ctx->conv_tc == 2 || (ctx->conv_tc == 1 && g.Cout >= 32))
+    return psc_conv_tc_forward(ctx, g, a, s, w, bias, act, o, out32, st);
   if (g.Cout % 16 == 0) {
     dim3 grid(psc_div_up(nvo, FWD_NT), g.Cout / 16);
     k_conv_fwd<16><<<grid, FWD_NT, 0, st>>>(a, s, w, bias, g, act, o, out32);

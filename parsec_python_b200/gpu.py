@@ -529,6 +529,144 @@ class Mixer:
         return out, m.value
 
 
+def qinv_from_gram(G: np.ndarray, tol: float) -> np.ndarray:
+    """C = qinv(A) qinv(A)^T of Mixer/qinv.py:5-62 from G = A^T A (r x r) and
+    tol = eps ||A||_inf.  qinv pivots A's columns by their remaining norms
+    and cuts the rank at the first |R_ii| < tol; the pivoted Cholesky of G
+    makes the same choices (its remaining diagonal is the squared remaining
+    column norm, ties to the first column as LAPACK's) and gives the same
+    |R_ii|.  C = P (S S^T) P^T with S = R11^{-1}, whatever the signs of R's
+    rows.  The Gram matrix resolves a column's remaining norm only down to
+    about sqrt(eps) of that column's own norm; a column whose remaining norm
+    is below 8 sqrt(eps) of its norm is rounding noise of a dependent column
+    and is cut there as well (the QR resolves down to tol itself; between
+    the two the reference's coefficients are 1 / |R_ii|^2 amplifications of
+    its own rounding).  Columns that are merely small are kept: late in an
+    SCF the newest residual differences are many decades below the first."""
+    G = 0.5 * (G + G.T)
+    r = G.shape[0]
+    norm0 = np.sqrt(np.maximum(np.diag(G), 0.0))
+    floor = 8.0 * np.sqrt(np.finfo(float).eps)
+    piv = np.arange(r)
+    R = np.zeros((r, r))
+    rank = r
+    for j in range(r):
+        p = j + int(np.argmax(np.diag(G)[j:]))
+        if p != j:
+            G[[j, p], :] = G[[p, j], :]
+            G[:, [j, p]] = G[:, [p, j]]
+            R[:j, [j, p]] = R[:j, [p, j]]
+            piv[[j, p]] = piv[[p, j]]
+        d = np.sqrt(max(G[j, j], 0.0))
+        if d < tol or d <= floor * norm0[piv[j]]:
+            rank = j
+            break
+        R[j, j] = d
+        R[j, j + 1:] = G[j, j + 1:] / d
+        G[j + 1:, j + 1:] -= np.outer(R[j, j + 1:], R[j, j + 1:])
+    C = np.zeros((r, r))
+    if rank:
+        S = np.linalg.solve(R[:rank, :rank], np.eye(rank))   # R11 upper triangular: back substitution
+        C[np.ix_(piv[:rank], piv[:rank])] = S @ S.T
+    return C
+
+
+class Mixer2:
+    """Type-II multisecant mixer, Mixer/msecant2.py:24-93 with the parameters
+    of Mixer/includemix.py:21-49; group_size 0 takes all iterates as one
+    group (Anderson mixing).  The history (one FP64 n-vector pair per
+    iterate) stays in device memory and every n-vector operation is a libpsc
+    kernel (psc_mix2_*, psc_block_*, psc_gram, psc_gemm_nn); the host follows
+    the reference's control flow: the restart test, the EN stages (a restart
+    sets stage 2, after which the stages alternate, msecant2.py:45-93), the
+    groups, and the quasi-inverse of the last group from its Gram matrix
+    (qinv_from_gram)."""
+
+    def __init__(self, ctx: GridContext, capacity: int, mix: float = 0.5, group_size: int = 0,
+                 restart_factor: float = 0.1, en_like: int = 0):
+        self.ctx, self.mix, self.gs, self.rf, self.en_like = ctx, mix, int(group_size), restart_factor, en_like
+        self.cap = int(capacity) + 1
+        self.DX = ctx.empty(self.cap, ctx.n)
+        self.DF = ctx.empty(self.cap, ctx.n)
+        self.coef = ctx.empty(self.cap)
+        self.scal = ctx.empty(4)
+        self.m = 0
+        self.en = None
+
+    def _dots(self, A: torch.Tensor, i0: int, r: int, x: torch.Tensor) -> torch.Tensor:
+        self.ctx.call("psc_block_dots", _p(A[i0]), self.ctx.n, r, _p(x), _p(self.coef), _stream())
+        return self.coef[:r]
+
+    def _combine(self, y, base, f, mix, A=None, i0=0, r=0, c=None):
+        self.ctx.call("psc_block_combine", _p(y), _p(base), _p(f), float(mix), _p(A[i0]) if r else None,
+                      self.ctx.n, r, _p(c) if r else None, _stream())
+
+    def __call__(self, x1: torch.Tensor, f1: torch.Tensor):
+        ctx, mix, n = self.ctx, self.mix, self.ctx.n
+        out = torch.empty_like(x1)
+        if self.m == 0:
+            ctx.call("psc_mix2_store", _p(x1), _p(f1), _p(self.DX[0]), _p(self.DF[0]), _stream())
+            self._combine(out, x1, f1, mix)
+            self.m, self.en = 1, (0 if self.en_like == 0 else 2)
+            return out, 0
+        m = self.m
+        sz = m + 1 if self.gs == 0 else self.gs
+        if self.en != 1 and m >= 2:
+            ctx.call("psc_dot", _p(self.DF[m - 1]), _p(self.DF[m - 1]), n, _p(self.scal[0:1]), _stream())
+            ctx.call("psc_dot", _p(f1), _p(f1), n, _p(self.scal[1:2]), _stream())
+            nd, nf = np.sqrt(self.scal[:2].cpu().numpy())
+            if nd < self.rf * nf:
+                ctx.call("psc_mix2_store", _p(x1), _p(f1), _p(self.DX[0]), _p(self.DF[0]), _stream())
+                self._combine(out, x1, f1, mix)
+                self.m, self.en = 1, 2
+                return out, 0
+        if m + 1 > self.cap:
+            raise PscError("mixer: history capacity exceeded")
+        res = (m + sz - 1) % sz + 1
+        ngroup = (m - res) // sz
+        g = ngroup * sz
+        if self.en != 1:
+            ctx.call("psc_mix2_diff", _p(x1), _p(f1), _p(self.DX[m - 1]), _p(self.DF[m - 1]), float(mix),
+                     _stream())
+            if g:
+                c = self._dots(self.DF, 0, g, self.DF[m - 1])
+                self._combine(self.DX[m - 1], self.DX[m - 1], None, 0.0, self.DX, 0, g, c)
+        if g:
+            c = self._dots(self.DF, 0, g, f1)
+            self._combine(out, x1, f1, mix, self.DX, 0, g, c)
+        else:
+            self._combine(out, x1, f1, mix)
+        if self.en == 1 and res == sz:
+            c = self._dots(self.DF, g, m - g, f1)
+            self._combine(out, out, None, 0.0, self.DX, g, m - g, c)
+        else:
+            i0 = m - res
+            G = ctx.empty(res, res)
+            ctx.call("psc_gram", F64, _p(self.DF[i0]), n, _p(self.DF[i0]), n, res, 0, _p(G), _stream())
+            ctx.call("psc_block_absrow_max", _p(self.DF[i0]), n, res, _p(self.scal[2:3]), _stream())
+            Gh = G.cpu().numpy().reshape(res, res).T.copy()
+            tol = np.finfo(float).eps * float(self.scal[2].item())
+            C = qinv_from_gram(Gh, tol)
+            if res == sz:
+                Cd = torch.from_numpy(np.asfortranarray(C).ravel(order="F").copy()).to(ctx.device)
+                tmp = torch.empty(res, n, dtype=torch.float64, device=ctx.device)
+                ctx.call("psc_gemm_nn", F64, _p(self.DF[i0]), n, res, _p(Cd), res, _p(tmp), n, _stream())
+                self.DF[i0:m].copy_(tmp)
+                c = self._dots(self.DF, i0, res, f1)
+            else:
+                d = self._dots(self.DF, i0, res, f1).cpu().numpy()
+                c = torch.from_numpy(C @ d).to(ctx.device)
+            self._combine(out, out, None, 0.0, self.DX, i0, res, c)
+        if self.en != 2:
+            ctx.call("psc_mix2_store", _p(x1), _p(f1), _p(self.DX[m]), _p(self.DF[m]), _stream())
+            self.m = m + 1
+        if self.en == 1:
+            self.en = 2
+        elif self.en == 2:
+            self.en = 1
+        return out, m
+
+
 def sad_setup(ctx: GridContext, atoms, elem, tables, ml_grid: bool = False):
     """SAD density, local and SAD Hartree potentials (V_ion/pseudoDiag.py).
     ml_grid: grid point i at i h instead of i h - radius, as

@@ -60,6 +60,8 @@ class SolverSettings:
     mask: str = "cube"           # cube (the reference's domain) | sphere (H zero outside the inscribed sphere)
     first_tol: float = 0.08      # first_filt: stop when the Ritz trace moves by <= this fraction (first_filt.py:14)
     first_rounds: int = 0        # first_filt: most filter rounds; 0 = the reference's max(min(60 / polm, 5), 3)
+    mixer: str = "msecant1"      # msecant1 (the reference's default) | msecant2 (Type-II) | anderson (msecant2, groups of all iterates)
+    mix_group_size: int = 0      # msecant2: iterates per group (0 = all of them: Anderson mixing)
 
     _KEYS = {
         "fd_order": ("fd_order", int), "maxits": ("maxits", int), "tol": ("tol", _parse_tol),
@@ -72,6 +74,7 @@ class SolverSettings:
         "init": ("init", str), "seed": ("seed", int), "mixed_switch": ("mixed_switch", float),
         "mixed_finish": ("mixed_finish", str), "mixed_fp64_at": ("mixed_fp64_at", float),
         "mask": ("mask", str), "first_tol": ("first_tol", float), "first_rounds": ("first_rounds", int),
+        "mixer": ("mixer", str), "mix_group_size": ("mix_group_size", int),
     }
 
     def normalize(self) -> None:
@@ -95,6 +98,12 @@ class SolverSettings:
         if self.init not in ("sad", "learned"):
             self.init = "sad"
         self.mixed_switch = float(self.mixed_switch)
+        self.mixer = str(self.mixer).lower()
+        if self.mixer == "anderson":
+            self.mixer, self.mix_group_size = "msecant2", 0
+        if self.mixer not in ("msecant1", "msecant2"):
+            self.mixer = "msecant1"
+        self.mix_group_size = max(0, int(self.mix_group_size))
         self.mixed_finish = str(self.mixed_finish).lower()
         if self.mixed_finish not in ("fp32", "fp64"):
             self.mixed_finish = "fp64"

@@ -153,7 +153,10 @@ def run_rsdft_calculation(problem: PreparedSystem, elem, n_elements, backend: So
     timings["setup_total"] = time.perf_counter() - t_start
 
     nelec = gpu.nelectrons(atoms, elem) - problem.input_data.z_charge
-    mixer = gpu.Mixer(ctx, capacity=s.maxits + 2)
+    if s.mixer == "msecant2":
+        mixer = gpu.Mixer2(ctx, capacity=s.maxits + 2, group_size=s.mix_group_size)
+    else:
+        mixer = gpu.Mixer(ctx, capacity=s.maxits + 2)
     H = gpu.Hamiltonian(ctx, pot)
     if s.adaptive_scheme != 0 and sum(problem.input_data.n_atom) <= 2:
         deg_mod, m_mod = 0.75, 0.95

@@ -67,7 +67,7 @@ def test_wait_limit_zero_reports_every_pipeline_and_context_recovers():
         ctx.call("psc_gram_pair", F32, gpu._p(W32), gpu._p(W32), n, 40, gpu._p(S), gpu._p(K), st)
         O32 = torch.empty_like(W32)
         ctx.call("psc_gemm_nn", F32, gpu._p(W32), n, 40, gpu._p(T), 40, gpu._p(O32), n, st)
-        C = conv(1)
+        C = conv(2)
         torch.cuda.synchronize()
         return Y, S, O32, C
 

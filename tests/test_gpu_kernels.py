@@ -384,6 +384,22 @@ def test_mixer_matches_reference_including_restart(golden_dir):
         assert rel(out.cpu().numpy(), mx["out"][i]) < 1e-11, i
 
 
+@pytest.mark.parametrize("name,group_size", [("anderson", 0), ("group2", 2)])
+def test_mixer2_matches_reference_including_restart(golden_dir, name, group_size):
+    """Type-II multisecant mixer on the device (history in HBM, libpsc
+    kernels; Anderson for group size 0) against the reference's msecant2
+    outputs, through the restart and the alternating EN stages after it."""
+    g = np.load(golden_dir / "ref_mixer2.npz")
+    n = g[f"{name}_x"].shape[1]
+    ctx = gpu.GridContext({"nx": n, "ny": 1, "nz": 1, "h": 1.0, "radius": 1.0}, 8)
+    m = gpu.Mixer2(ctx, capacity=20, group_size=group_size)
+    for i in range(len(g[f"{name}_x"])):
+        out, used = m(torch.from_numpy(g[f"{name}_x"][i]).to(DEV), torch.from_numpy(g[f"{name}_f"][i]).to(DEV))
+        assert used == int(g[f"{name}_m"][i]), i
+        assert rel(out.cpu().numpy(), g[f"{name}_out"][i]) < 1e-10, i
+    ctx.check_status()
+
+
 def test_pcg_matches_reference(golden_dir):
     pc = np.load(golden_dir / "ref_pcg.npz")
     ctx = gpu.GridContext({"nx": 10, "ny": 10, "nz": 10, "h": 0.4, "radius": 1.8}, 8)

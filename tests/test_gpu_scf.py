@@ -98,6 +98,26 @@ def test_benchmark_config_matches_reference(golden_dir, name, tag):
     check(prob, res, ref, cfg["nev"])
 
 
+@pytest.mark.parametrize("group_size", [0, 2], ids=["anderson", "groups-of-2"])
+def test_scf_with_type2_mixer_lands_on_the_reference(golden_dir, group_size):
+    """The Type-II multisecant mixer (Mixer/msecant2.py; group size 0 is the
+    Anderson mixing the H2O configuration names) on the H2O configuration:
+    the converged fixed point does not depend on the mixer, so the same
+    energy, eigenvalue and density bars hold against the reference's SCF."""
+    meta = json.loads((golden_dir / "ref_h2o.json").read_text())
+    ref = np.load(golden_dir / "ref_h2o.npz")
+    cfg = workloads.config_system("h2o")
+    s = SolverSettings(tol=meta["tol"], poldeg=cfg["poldeg"], maxits=80, mixer="msecant2",
+                       mix_group_size=group_size)
+    s.normalize()
+    elem = ElementTable()
+    prob = system_from_atoms(cfg["atoms"], h=cfg["h"], radius=cfg["radius"], nev=cfg["nev"], settings=s, elem=elem)
+    res = run_rsdft_calculation(prob, elem, len(elem), select_solver_backend(s), verbose=False)
+    print(f"msecant2 group size {group_size}: {res.iterations} iterations (reference msecant1: "
+          f"{meta.get('iterations')})")
+    check(prob, res, ref, cfg["nev"])
+
+
 def _mixed_vs_reference(golden_dir, name, tag, switch):
     f = golden_dir / f"ref_{tag}.npz"
     if not f.exists():

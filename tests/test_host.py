@@ -190,3 +190,48 @@ def test_wfn_dat_round_trip(tmp_path):
     f.write_bytes(f.read_bytes() + b"x")
     with pytest.raises(ValueError, match="trailing"):
         output.load_wavefunction(str(f))
+
+
+@pytest.mark.parametrize("kind", ["random", "graded", "steep", "dependent", "zero"])
+def test_quasi_inverse_from_gram_matches_pivoted_qr(kind):
+    """The Type-II mixer's quasi-inverse product C = qinv(A) qinv(A)^T
+    (Mixer/qinv.py:5-62, pivoted QR of the n x r history block) computed from
+    the r x r Gram matrix by a pivoted Cholesky, as the GPU mixer does: the
+    same rank cut and C to 1e-10 on well-conditioned and graded blocks
+    (column norms over six and over eighteen decades, as the newest residual
+    differences of a converging SCF are: small columns are kept), and an
+    exactly dependent or zero column dropped as the QR drops it."""
+    from parsec_python_b200 import gpu
+
+    rng = np.random.default_rng({"random": 1, "graded": 2, "steep": 5, "dependent": 3, "zero": 4}[kind])
+    A = rng.standard_normal((300, 7))
+    if kind == "graded":
+        A *= 10.0 ** -np.arange(7)
+    elif kind == "steep":
+        A *= 10.0 ** (-3 * np.arange(7))
+    elif kind == "dependent":
+        A[:, 4] = A[:, 1]
+    elif kind == "zero":
+        A[:, 2] = 0.0
+    B = O.qinv(A)
+    ref = B @ B.T
+    got = gpu.qinv_from_gram(A.T @ A, np.finfo(float).eps * np.linalg.norm(A, np.inf))
+    # each entry against the scale of its columns (C_ij ~ 1 / (|a_i| |a_j|))
+    cn = np.linalg.norm(A, axis=0)
+    sc = np.where(np.outer(cn, cn) > 0, 1.0 / np.maximum(np.outer(cn, cn), 1e-300), 0.0)
+    assert (np.abs(got - ref) <= 1e-9 * sc + 1e-12 * np.abs(ref).max()).all()
+    assert ((got != 0) == (ref != 0)).all()
+
+
+def test_settings_select_the_anderson_mixer():
+    s = SolverSettings()
+    assert s.mixer == "msecant1"
+    s.apply_overrides({"mixer": "anderson"})
+    s.normalize()
+    assert (s.mixer, s.mix_group_size) == ("msecant2", 0)
+    s.apply_overrides({"mixer": "msecant2", "mix_group_size": "3"})
+    s.normalize()
+    assert (s.mixer, s.mix_group_size) == ("msecant2", 3)
+    s.apply_overrides({"mixer": "nonsense"})
+    s.normalize()
+    assert s.mixer == "msecant1"

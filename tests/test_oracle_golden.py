@@ -129,6 +129,19 @@ def test_mixer_bit_exact_including_restart(golden_dir):
     assert restarted
 
 
+@pytest.mark.parametrize("name,group_size", [("anderson", 0), ("group2", 2)])
+def test_mixer2_bit_exact_including_restart(golden_dir, name, group_size):
+    """Type-II multisecant mixer (Anderson for group_size 0) against the
+    reference's own msecant2 outputs, through the restart at step 9 and the
+    alternating EN stages after it (tests/golden/make_golden_mixer2.py)."""
+    g = np.load(golden_dir / "ref_mixer2.npz")
+    m = O.MSecant2(group_size=group_size)
+    for i in range(len(g[f"{name}_x"])):
+        out, used = m(g[f"{name}_x"][i], g[f"{name}_f"][i])
+        assert used == int(g[f"{name}_m"][i])
+        np.testing.assert_array_equal(out, g[f"{name}_out"][i])
+
+
 def test_occupations_bit_exact(golden_dir):
     oc = np.load(golden_dir / "ref_occupations.npz")
     for i in range(4):
