@@ -242,7 +242,7 @@ constexpr int CB = 64;
 __global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int k, int j0, double* __restrict__ D,
                                                     int* status) {
   __shared__ double a[CB][CB + 1];   // a[c][r] = A[j0 + r, j0 + c]
-  __shared__ double u[CB], dg[CB];
+  __shared__ double u[CB], dg[CB], dgi[CB];   // dgi = 1 / dg
   const int nb = min(CB, k - j0);
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   for (int e = tid; e < nb * nb; e += 256) {
@@ -253,12 +253,14 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int 
   for (int j = 0; j < nb; ++j) {
     const double d = a[j][j];
     const double rjj = d > 0.0 ? sqrt(d) : 1.0;
+    const double rinv = 1.0 / rjj;
     if (tid == 0) {
       dg[j] = rjj;
+      dgi[j] = rinv;
       if (!(d > 0.0) && status[1] == 0) status[1] = j0 + j + 1;   // not positive definite
     }
     for (int c = j + 1 + tid; c < nb; c += 256) {
-      const double v = a[c][j] / rjj;
+      const double v = a[c][j] * rinv;
       u[c] = v;
       a[c][j] = v;
     }
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ A, int 
     for (int r = lane; r < nb; r += 32) b[w][r] = r == j ? 1.0 : 0.0;
     __syncwarp();
     for (int i = j; i >= 0; --i) {
-      const double xi = b[w][i] / dg[i];
+      const double xi = b[w][i] * dgi[i];
       for (int r = lane; r < i; r += 32) b[w][r] -= a[i][r] * xi;
       if (lane == 0) b[w][i] = xi;
       __syncwarp();
@@ -361,26 +363,46 @@ __global__ void k_tril_zero(double* A, int k) {
     if ((int)(e % k) > (int)(e / k)) A[e] = 0.0;
 }
 
-// X = R^{-1}, one warp per column: b = e_j, then for i = j .. 0: x_i = b_i / r_ii,
-// b_r -= R[r, i] x_i (r < i); columns of R come from global memory
-__global__ void __launch_bounds__(256) k_trtri_warp(const double* __restrict__ R, int k, double* __restrict__ X) {
-  extern __shared__ double bs[];   // [8][k]
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+// X = R^{-1}, one warp per column j (8 per CTA): b = e_j, then for i = j .. 0:
+// x_i = b_i / r_ii, b_r -= R[r, i] x_i (r < i).  Every step depends on the
+// one before, so R's columns are not read from global memory inside the
+// steps: the CTA stages the columns it needs (i <= its largest j) in shared
+// memory, `ch` at a time from the highest down, rows 0..i of each, with the
+// reciprocals of their diagonals.
+__global__ void __launch_bounds__(256) k_trtri_warp(const double* __restrict__ R, int k, int ch,
+                                                    double* __restrict__ X) {
+  extern __shared__ double bs[];   // [8][k] b vectors, [ch][k] staged columns, [ch] 1 / r_ii
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int j = blockIdx.x * 8 + w;
-  if (j >= k) return;
+  const int jmax = min(k - 1, blockIdx.x * 8 + 7);
   double* b = bs + (long)w * k;
+  double* rs = bs + 8L * k;
+  double* rinv = rs + (long)ch * k;
   double* xj = X + (long)j * k;
-  for (int r = lane; r < k; r += 32) {
-    if (r <= j) b[r] = r == j ? 1.0 : 0.0;
-    else xj[r] = 0.0;
-  }
-  __syncwarp();
-  for (int i = j; i >= 0; --i) {
-    const double* ri = R + (long)i * k;
-    const double xi = b[i] / ri[i];
-    for (int r = lane; r < i; r += 32) b[r] -= ri[r] * xi;
-    if (lane == 0) xj[i] = xi;
-    __syncwarp();
+  if (j < k)
+    for (int r = lane; r < k; r += 32) {
+      if (r <= j) b[r] = r == j ? 1.0 : 0.0;
+      else xj[r] = 0.0;
+    }
+  for (int c_hi = jmax; c_hi >= 0; c_hi -= ch) {
+    const int c_lo = max(0, c_hi - ch + 1);
+    const int nr = c_hi + 1;   // rows 0..c_hi cover every staged column's rows 0..i
+    __syncthreads();           // the previous chunk has been used by every warp
+    for (int e = tid; e < (c_hi - c_lo + 1) * nr; e += 256) {
+      const int cc = e / nr, r = e % nr, c = c_lo + cc;
+      if (r < c) rs[(long)cc * k + r] = R[r + (long)c * k];
+      else if (r == c) rinv[cc] = 1.0 / R[c + (long)c * k];
+    }
+    __syncthreads();
+    if (j < k) {
+      for (int i = min(j, c_hi); i >= c_lo; --i) {
+        const double* ri = rs + (long)(i - c_lo) * k;
+        const double xi = b[i] * rinv[i - c_lo];
+        for (int r = lane; r < i; r += 32) b[r] -= ri[r] * xi;
+        if (lane == 0) xj[i] = xi;
+        __syncwarp();
+      }
+    }
   }
 }
 
@@ -413,10 +435,14 @@ int psc_chol_inv_dev(psc_ctx* ctx, double* S, int k, double* X, cudaStream_t st)
   }
   k_tril_zero<<<std::max(1, std::min(592, psc_div_up((long)k * k, 256))), 256, 0, st>>>(S, k);
   PSC_LAUNCH_CHECK(ctx);
-  const size_t tdyn = 8 * (size_t)k * sizeof(double);
+  // staged columns per chunk: 16, fewer when 8 b vectors + 16 columns of k
+  // rows exceed 200 KB of shared memory
+  const int ch = (int)std::max<long>(1, std::min<long>(16, ((200L * 1024 / 8) - 8L * k) / (k + 1)));
+  const size_t tdyn = ((size_t)(8 + ch) * k + ch) * sizeof(double);
+  PSC_REQUIRE(ctx, tdyn <= 227 * 1024, "chol_inv: k too large for the triangular inverse");
   if (tdyn > 48 * 1024)
     PSC_CUDA(ctx, cudaFuncSetAttribute(k_trtri_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tdyn));
-  k_trtri_warp<<<psc_div_up(k, 8), 256, tdyn, st>>>(S, k, X);
+  k_trtri_warp<<<psc_div_up(k, 8), 256, tdyn, st>>>(S, k, ch, X);
   PSC_LAUNCH_CHECK(ctx);
   return 0;
 }

@@ -400,6 +400,35 @@ def test_mixer2_matches_reference_including_restart(golden_dir, name, group_size
     ctx.check_status()
 
 
+@pytest.mark.parametrize("group_size", [0, 3])
+def test_mixer2_long_history_matches_oracle(group_size):
+    """The device Type-II mixer against the oracle's msecant2 (pinned to the
+    reference) over 30 steps of a contracting fixed-point map on 5,000
+    points: histories past 16 columns (the dot products run in chunks of 16),
+    slowly shrinking residual differences, groups of 3."""
+    n = 5000
+    rng = np.random.default_rng(40 + group_size)
+    q = np.linalg.qr(rng.standard_normal((n, 24)))[0]
+    lam = np.linspace(0.2, 0.97, 24)
+    b = rng.standard_normal(n)
+
+    def g(x):   # x -> b + Q diag(lam) Q^T x + 0.05 tanh(x): residual f = g(x) - x
+        return b + q @ (lam * (q.T @ x)) + 0.05 * np.tanh(x)
+
+    ctx = gpu.GridContext({"nx": n, "ny": 1, "nz": 1, "h": 1.0, "radius": 1.0}, 8)
+    dev = gpu.Mixer2(ctx, capacity=40, group_size=group_size)
+    ora = O.MSecant2(group_size=group_size)
+    x = rng.standard_normal(n)
+    for i in range(30):
+        f = g(x) - x
+        xo, mo = ora(x, f)
+        xd, md = dev(torch.from_numpy(x).to(DEV), torch.from_numpy(f).to(DEV))
+        assert md == mo, i
+        assert rel(xd.cpu().numpy(), xo) < 1e-8, i
+        x = xo
+    ctx.check_status()
+
+
 def test_pcg_matches_reference(golden_dir):
     pc = np.load(golden_dir / "ref_pcg.npz")
     ctx = gpu.GridContext({"nx": 10, "ny": 10, "nz": 10, "h": 0.4, "radius": 1.8}, 8)

@@ -114,7 +114,7 @@ def test_scf_with_type2_mixer_lands_on_the_reference(golden_dir, group_size):
     prob = system_from_atoms(cfg["atoms"], h=cfg["h"], radius=cfg["radius"], nev=cfg["nev"], settings=s, elem=elem)
     res = run_rsdft_calculation(prob, elem, len(elem), select_solver_backend(s), verbose=False)
     print(f"msecant2 group size {group_size}: {res.iterations} iterations (reference msecant1: "
-          f"{meta.get('iterations')})")
+          f"{meta.get('iterations')}); errors", " ".join(f"{r['err']:.1e}" for r in res.history))
     check(prob, res, ref, cfg["nev"])
 
 
