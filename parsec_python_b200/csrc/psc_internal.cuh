@@ -115,6 +115,17 @@ struct psc_ctx {
   int gemm_tc = 1;               // 1: FP32 W T on tcgen05 (3xTF32), 0: CUDA cores
   float* tsplit = nullptr;       // T split into TF32 hi/lo B tiles
   size_t tsplit_floats = 0;
+  // NumPy-order pairwise sum: leaf ranges and the tree above them for length pw_n
+  long pw_n = 0;
+  void* pw_buf = nullptr;
+  long* pw_lo = nullptr;
+  long* pw_len = nullptr;
+  double* pw_vals = nullptr;
+  int2* pw_kids = nullptr;
+  int* pw_order = nullptr;
+  int* pw_level_off = nullptr;
+  long pw_nleaf = 0;
+  int pw_nlevel = 0;
   // learned-start convolution forward: 2 tcgen05 implicit GEMM, 0 CUDA cores,
   // 1 by layer (tcgen05 from 32 output channels)
   int conv_tc = 1;

@@ -69,16 +69,32 @@ __global__ void k_scale_div(double* x, long n, const double* num_scalar, double 
 // NumPy's pairwise summation (the order np.sum uses for a contiguous float64
 // vector): blocks of <= 128 elements summed with 8 interleaved accumulators,
 // blocks of < 8 summed sequentially, larger ranges split at n/2 rounded down
-// to a multiple of 8.  Leaves are summed in parallel, then one thread replays
-// the recursion consuming the leaf sums in order.
+// to a multiple of 8.  Leaves are summed in parallel; the recursion above
+// them is a fixed binary tree, built on the host once per length and
+// evaluated level by level in one CTA (each node the sum of its left and
+// right child, so every addition is the one np.sum makes).
 // ---------------------------------------------------------------------------
-static void pw_leaves(long off, long n, std::vector<long>& lo, std::vector<long>& len) {
-  if (n <= 128) { lo.push_back(off); len.push_back(n); return; }
+namespace {
+// the node of range [off, off + n): -(leaf index + 1) for a leaf, else the
+// index of an internal node; appends the leaves and the internal nodes below
+// it, with each internal node's height above the leaves
+int pw_build(long off, long n, std::vector<long>& lo, std::vector<long>& len, std::vector<int2>& kids,
+             std::vector<int>& height) {
+  if (n <= 128) {
+    lo.push_back(off);
+    len.push_back(n);
+    return -(int)lo.size();
+  }
   long n2 = n / 2;
   n2 -= n2 % 8;
-  pw_leaves(off, n2, lo, len);
-  pw_leaves(off + n2, n - n2, lo, len);
+  const int a = pw_build(off, n2, lo, len, kids, height);
+  const int b = pw_build(off + n2, n - n2, lo, len, kids, height);
+  kids.push_back(make_int2(a, b));
+  const int ha = a < 0 ? 0 : height[a], hb = b < 0 ? 0 : height[b];
+  height.push_back(1 + std::max(ha, hb));
+  return (int)kids.size() - 1;
 }
+}  // namespace
 
 __global__ void k_pw_leaf(const double* __restrict__ a, const long* __restrict__ lo, const long* __restrict__ len,
                           long nleaf, double* __restrict__ out) {
@@ -102,42 +118,74 @@ __global__ void k_pw_leaf(const double* __restrict__ a, const long* __restrict__
   }
 }
 
-__device__ double pw_combine(long n, const double* leaf, long* cursor) {
-  if (n <= 128) return leaf[(*cursor)++];
-  long n2 = n / 2;
-  n2 -= n2 % 8;
-  const double left = pw_combine(n2, leaf, cursor);
-  const double right = pw_combine(n - n2, leaf, cursor);
-  return left + right;
-}
-
-__global__ void k_pw_root(long n, const double* leaf, double* out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    long cursor = 0;
-    *out = pw_combine(n, leaf, &cursor);
+// vals[0, nleaf) = leaf sums; internal node i lands in vals[nleaf + i].
+// order[] lists the internal nodes level by level (level_off[h] .. level_off[h+1]).
+__global__ void __launch_bounds__(1024) k_pw_tree(const int2* __restrict__ kids, const int* __restrict__ order,
+                                                   const int* __restrict__ level_off, int nlevel, int nleaf,
+                                                   double* vals, double* out) {
+  for (int h = 0; h < nlevel; ++h) {
+    for (int t = level_off[h] + threadIdx.x; t < level_off[h + 1]; t += blockDim.x) {
+      const int i = order[t];
+      const int2 c = kids[i];
+      const double a = vals[c.x < 0 ? -c.x - 1 : nleaf + c.x];
+      const double b = vals[c.y < 0 ? -c.y - 1 : nleaf + c.y];
+      vals[nleaf + i] = a + b;
+    }
+    __syncthreads();
   }
+  if (threadIdx.x == 0) *out = nlevel ? vals[nleaf + order[level_off[nlevel] - 1]] : vals[0];
 }
 
 extern "C" int psc_numpy_sum(psc_ctx* ctx, const double* x, long n, double* out_dev, void* stream) {
   if (!ctx) return 2;
   PSC_REQUIRE(ctx, n >= 1, "numpy_sum: n < 1");
   cudaStream_t st = (cudaStream_t)stream;
-  std::vector<long> lo, len;
-  pw_leaves(0, n, lo, len);
-  const long nl = (long)lo.size();
-  long *lo_d = nullptr, *len_d = nullptr;
-  double* leaf_d = nullptr;
-  PSC_CUDA(ctx, psc_dmalloc(&lo_d, nl * sizeof(long)));
-  PSC_CUDA(ctx, psc_dmalloc(&len_d, nl * sizeof(long)));
-  PSC_CUDA(ctx, psc_dmalloc(&leaf_d, nl * sizeof(double)));
-  PSC_CUDA(ctx, cudaMemcpyAsync(lo_d, lo.data(), nl * sizeof(long), cudaMemcpyHostToDevice, st));
-  PSC_CUDA(ctx, cudaMemcpyAsync(len_d, len.data(), nl * sizeof(long), cudaMemcpyHostToDevice, st));
-  k_pw_leaf<<<std::max(1, (int)std::min<long>(1184, (nl + 127) / 128)), 128, 0, st>>>(x, lo_d, len_d, nl, leaf_d);
+  if (ctx->pw_n != n) {
+    std::vector<long> lo, len;
+    std::vector<int2> kids;
+    std::vector<int> height;
+    pw_build(0, n, lo, len, kids, height);
+    const int nl = (int)lo.size(), ni = (int)kids.size();
+    int nlevel = 0;
+    for (int hgt : height) nlevel = std::max(nlevel, hgt);
+    // internal nodes ordered by height: those of height h + 1 at off[h] .. off[h + 1]
+    std::vector<int> cnt(nlevel + 1, 0), off(nlevel + 1, 0), order(std::max(ni, 1));
+    for (int hgt : height) ++cnt[hgt];
+    for (int h = 1; h <= nlevel; ++h) off[h] = off[h - 1] + cnt[h];
+    std::vector<int> fill(off.begin(), off.end());
+    for (int i = 0; i < ni; ++i) order[fill[height[i] - 1]++] = i;
+    psc_dfree(ctx->pw_buf);
+    ctx->pw_buf = nullptr;
+    ctx->pw_n = 0;
+    // one allocation: lo, len (long), leaf + node sums (double), kids (int2), order, level offsets (int)
+    const size_t bytes = (size_t)nl * 8 * 2 + (size_t)(nl + ni) * 8 + (size_t)std::max(ni, 1) * 8 +
+                         (size_t)std::max(ni, 1) * 4 + (size_t)(nlevel + 1) * 4 + 64;
+    PSC_CUDA(ctx, psc_dmalloc(&ctx->pw_buf, bytes));
+    char* b = static_cast<char*>(ctx->pw_buf);
+    ctx->pw_lo = reinterpret_cast<long*>(b);
+    ctx->pw_len = ctx->pw_lo + nl;
+    ctx->pw_vals = reinterpret_cast<double*>(ctx->pw_len + nl);
+    ctx->pw_kids = reinterpret_cast<int2*>(ctx->pw_vals + nl + ni);
+    ctx->pw_order = reinterpret_cast<int*>(ctx->pw_kids + std::max(ni, 1));
+    ctx->pw_level_off = ctx->pw_order + std::max(ni, 1);
+    PSC_CUDA(ctx, cudaMemcpy(ctx->pw_lo, lo.data(), nl * sizeof(long), cudaMemcpyHostToDevice));
+    PSC_CUDA(ctx, cudaMemcpy(ctx->pw_len, len.data(), nl * sizeof(long), cudaMemcpyHostToDevice));
+    if (ni) {
+      PSC_CUDA(ctx, cudaMemcpy(ctx->pw_kids, kids.data(), ni * sizeof(int2), cudaMemcpyHostToDevice));
+      PSC_CUDA(ctx, cudaMemcpy(ctx->pw_order, order.data(), ni * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    PSC_CUDA(ctx, cudaMemcpy(ctx->pw_level_off, off.data(), (nlevel + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    ctx->pw_nleaf = nl;
+    ctx->pw_nlevel = nlevel;
+    ctx->pw_n = n;
+  }
+  const long nl = ctx->pw_nleaf;
+  k_pw_leaf<<<std::max(1, (int)std::min<long>(1184, (nl + 127) / 128)), 128, 0, st>>>(x, ctx->pw_lo, ctx->pw_len,
+                                                                                   nl, ctx->pw_vals);
   PSC_LAUNCH_CHECK(ctx);
-  k_pw_root<<<1, 32, 0, st>>>(n, leaf_d, out_dev);
+  k_pw_tree<<<1, 1024, 0, st>>>(ctx->pw_kids, ctx->pw_order, ctx->pw_level_off, ctx->pw_nlevel, (int)nl,
+                                ctx->pw_vals, out_dev);
   PSC_LAUNCH_CHECK(ctx);
-  PSC_CUDA(ctx, cudaStreamSynchronize(st));
-  psc_dfree(lo_d); psc_dfree(len_d); psc_dfree(leaf_d);
   return 0;
 }
 

@@ -8,7 +8,8 @@ through the C ABI twice in a row, on different densities, and compares each
 result with the context-based psc_lda_xc at the tolerance of the other XC
 test (1e-13 relative on v_xc, 1e-12 on E_xc); it also checks the entry point
 against the reference's own exc_nspn fixture and that a call leaves the
-device's free memory unchanged.  The file name sorts last so
+device's free memory unchanged, and that a call made during a CUDA graph
+capture replays correctly.  The file name sorts last so
 that a run stopping at the first failure has already run every other test.
 """
 import ctypes
@@ -103,6 +104,40 @@ def test_noalloc_xc_allocates_nothing_and_propagates_nan():
     torch.cuda.synchronize()
     for o in (out.cpu().numpy(), out_b.cpu().numpy()):
         assert np.isnan(o[1]) and np.isnan(o[2])
+
+
+def test_noalloc_xc_runs_inside_a_cuda_graph_capture():
+    """The case the entry point exists for: after one call outside (which
+    looks up its scratch), a call made while a stream is being captured into
+    a CUDA graph records its launches; replaying the graph on a new density
+    gives the context path's result for that density."""
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    n = 20_000
+    rho = torch.from_numpy(_densities(n, 4)).to(dev)
+    vxc = torch.empty_like(rho)
+    out = torch.empty(3, dtype=torch.float64, device=dev)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert lib.psc_lda_xc_noalloc(_p(rho), _p(vxc), n, 1.0, _p(out), st) == 0
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        cap = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = lib.psc_lda_xc_noalloc(_p(rho), _p(vxc), n, 1.0, _p(out), cap)
+    assert rc == 0, lib.psc_last_error(None)
+    rho.copy_(torch.from_numpy(_densities(n, 5)).to(dev))
+    vxc.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    ctx = gpu.GridContext({"nx": n, "ny": 1, "nz": 1, "h": 1.0, "radius": 1.0}, 8)
+    vxc_b, out_b = gpu.lda_xc(ctx, rho)
+    torch.cuda.synchronize()
+    va, vb = vxc.cpu().numpy(), vxc_b.cpu().numpy()
+    assert np.abs(va - vb).max() <= 1e-13 * np.abs(vb).max()
+    oa, ob = out.cpu().numpy(), out_b.cpu().numpy()
+    assert abs(oa[0] - ob[0]) <= 1e-12 * abs(ob[0])
+    assert oa[1] == ob[1] and oa[2] == ob[2]
+    del g
 
 
 def test_noalloc_xc_rejects_sizes_beyond_its_scratch():
