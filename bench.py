@@ -293,7 +293,7 @@ def stencil_roofline(reps: int = 40, dtype: str = "f32", name: str = CFG_NAME, k
 
 
 def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 20,
-             masks=("cube", "sphere"), impls=(0,), dtypes=("f64", "f32"), nl=(False, True), weights=(1,)) -> list:
+             masks=("cube", "sphere"), impls=(0,), dtypes=("f64", "f32"), nl=(False, True), weights=(2,)) -> list:
     """H.X microbenchmark on the real grids of C10H8 (78^3) and Si87H76 (90^3):
     one Chebyshev step Out = a H In + b In + g Prev on k random columns, FP64
     and FP32, first with the stencil and local potential alone (one kernel),
@@ -305,7 +305,8 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
     time per step over `reps` steps, inputs larger than L2.  impls: stencil
     implementations to time (0 default, 2 two-point FP32 runs, 3 / 4 scalar
     FP32 arithmetic with two- / four-point runs); weights: FP32 stencil
-    weights (1 with the sum-rule correction, the default; 0 plain FP32)."""
+    weights (2, the default: the sum-rule correction carried by the FP32
+    potential; 1: as a term in the kernel; 0: plain FP32)."""
     import torch
 
     from parsec_python_b200 import gpu
@@ -333,7 +334,7 @@ def hx_sweep(names=("c10h8", "si87h76"), widths=(27, 55, 143, 307), reps: int = 
                     ctx.call("psc_set_stencil_weights", wmode)
                     for k in widths:
                         for dtype in dtypes:
-                            if (impl >= 2 or wmode != 1) and dtype == "f64":   # FP32-only variants
+                            if (impl >= 2 or wmode != 2) and dtype == "f64":   # FP32-only variants
                                 continue
                             tdt, code, size = (torch.float64, F64, 8) if dtype == "f64" else (torch.float32, F32, 4)
                             X = ctx.mask_block(torch.randn(k, n, dtype=tdt, device="cuda"))
@@ -814,7 +815,8 @@ def main():
     ap.add_argument("--hx-masks", default="cube,sphere", help="masks of --hx")
     ap.add_argument("--hx-dtypes", default="f64,f32", help="block types of --hx")
     ap.add_argument("--hx-nl", default="0,1", help="--hx without (0) and with (1) the projectors")
-    ap.add_argument("--hx-weights", default="1", help="FP32 stencil weights of --hx (1 sum-rule corrected, 0 plain)")
+    ap.add_argument("--hx-weights", default="2",
+                    help="FP32 stencil weights of --hx (2 correction in the FP32 potential, 1 as a kernel term, 0 none)")
     ap.add_argument("--unet", type=int, default=None, metavar="NX",
                     help="only time the learned start's network forward on an NX^3 grid (both conv implementations)")
     ap.add_argument("--syev", nargs="?", const="55_rand,55_near,143_near,307_near", default=None,

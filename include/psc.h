@@ -111,11 +111,13 @@ int psc_apply_h_axpby(psc_ctx* ctx, int dtype, const void* X, long ldx, const vo
  * everywhere, 2 = the TMA pipeline with 2-point FP32 runs when nx is even but
  * not a multiple of 4, 3 / 4 = as 2 / 0 with scalar FP32 arithmetic. */
 int psc_set_stencil_impl(psc_ctx* ctx, int impl);
-/* FP32 weights of the TMA stencil: 1 (default) = FP32 weights plus one
- * correction term for their sum rule (c0 + 6 sum c_d = 0, which the weights'
- * rounding breaks by a constant of order 1e-7 Ha that every eigenvalue would
- * carry); 0 = plain FP32 weights. */
-int psc_set_stencil_weights(psc_ctx* ctx, int compensated);
+/* FP32 stencil weights.  Rounded to FP32 they break the sum rule
+ * c0 + 6 sum c_d = 0 by a constant of order 1e-7 Ha that every eigenvalue
+ * would carry.  2 (default) = the correction added to the FP32 potential
+ * (pot32 = fl(pot + correction); a call with another potential, or none,
+ * takes the term inside the TMA kernel); 1 = the correction as one more term
+ * in the TMA kernel; 0 = plain FP32 weights.  Recasts the FP32 potential. */
+int psc_set_stencil_weights(psc_ctx* ctx, int mode);
 /* Sphere-masked Hamiltonian (no counterpart in the reference, which solves
  * on the whole cube): with radius > 0 (bohr) every H X returns zero at the
  * points farther than radius from the cube's centre, the projector tables

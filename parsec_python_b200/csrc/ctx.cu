@@ -60,6 +60,12 @@ extern "C" int psc_ctx_create(int nx, int ny, int nz, double h, int fd_order, ps
     ctx->lap_c[i] = c[i] * ih2;
     ctx->ham_c[i] = 0.5 * (c[i] * ih2);
   }
+  {
+    // the weights' FP32 rounding errors break the sum rule c0 + 6 sum_d c_d = 0
+    double rs = (double)(float)ctx->ham_c0 - ctx->ham_c0;
+    for (int i = 0; i < 4; ++i) rs += 6.0 * ((double)(float)ctx->ham_c[i] - ctx->ham_c[i]);
+    ctx->sumrule32 = -rs;
+  }
   ctx->species.resize(32);
   auto fail = [&](cudaError_t e, const char* what) {
     psc_set_error(nullptr, std::string("psc_ctx_create: ") + what + ": " + cudaGetErrorString(e));
@@ -364,13 +370,27 @@ extern "C" int psc_cast(psc_ctx* ctx, int to_dtype, const void* src, void* dst, 
   return 0;
 }
 
+__global__ void k_cast_d2f_shift(const double* a, float* b, long n, double shift) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    b[i] = (float)(a[i] + shift);
+}
+
+// pot32 = fl(pot64 + shift): with weights mode 2 the FP32 weights' sum-rule
+// correction rides on the FP32 potential (the stencil's pot x term), so the
+// FP32 kernel needs no term of its own.  Each point's rounding error is as
+// random as fl(pot64)'s own, and the systematic shift survives it.
+int psc_recast_pot32(psc_ctx* ctx, cudaStream_t st) {
+  ctx->pot32_shift = ctx->stencil_comp == 2 ? ctx->sumrule32 : 0.0;
+  k_cast_d2f_shift<<<148 * 8, 256, 0, st>>>(ctx->pot64, ctx->pot32, ctx->n, ctx->pot32_shift);
+  PSC_LAUNCH_CHECK(ctx);
+  return 0;
+}
+
 extern "C" int psc_set_potential(psc_ctx* ctx, const double* pot, void* stream) {
   if (!ctx || !pot) return 2;
   cudaStream_t st = (cudaStream_t)stream;
   PSC_CUDA(ctx, cudaMemcpyAsync(ctx->pot64, pot, ctx->n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  k_cast_d2f<<<148 * 8, 256, 0, st>>>(ctx->pot64, ctx->pot32, ctx->n);
-  PSC_LAUNCH_CHECK(ctx);
-  return 0;
+  return psc_recast_pot32(ctx, st);
 }
 
 extern "C" int psc_status(psc_ctx* ctx, int* host_flags /* [8] */, int clear, void* stream) {

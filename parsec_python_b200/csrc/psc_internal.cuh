@@ -53,7 +53,13 @@ struct psc_ctx {
   double h = 0.0;
   int fd_order = 8;
   int radius = 4;            // stencil half-width (fd_order/2, capped at 4)
-  int stencil_comp = 1;      // FP32 TMA stencil: weights applied as FP32 value + rounding error
+  // FP32 stencil weights: 0 plain FP32 weights; 1 plus a correction term for
+  // their sum-rule residual in the TMA kernel; 2 that correction folded into
+  // the FP32 potential pot32 (calls with another potential, or none, take the
+  // term in the kernel)
+  int stencil_comp = 2;
+  double sumrule32 = 0.0;    // -(c0 + 6 sum_d c_d) of the Hamiltonian weights rounded to FP32, in FP64
+  double pot32_shift = 0.0;  // the shift pot32 = fl(pot64 + shift) currently carries
   int stencil_impl = 0;      // 0: TMA pipeline where it applies, 1: register-queue kernel only,
                              // 2: TMA with 2-point FP32 runs, 3 / 4: as 2 / 0 with scalar FP32 arithmetic
   double lap_c0 = 0.0;       // centre weight of A = -Lap_h (1/h^2 folded in)

@@ -406,10 +406,16 @@ extern "C" int psc_mask_block(psc_ctx* ctx, int dtype, void* X, long ld, int k, 
   return psc_mask_block_impl(ctx, dtype, X, ld, k, (cudaStream_t)stream);
 }
 
-extern "C" int psc_set_stencil_weights(psc_ctx* ctx, int compensated) {
+int psc_recast_pot32(psc_ctx* ctx, cudaStream_t st);
+
+extern "C" int psc_set_stencil_weights(psc_ctx* ctx, int mode) {
   if (!ctx) return 2;
-  PSC_REQUIRE(ctx, compensated == 0 || compensated == 1, "stencil weights mode must be 0 or 1");
-  ctx->stencil_comp = compensated;
+  PSC_REQUIRE(ctx, mode >= 0 && mode <= 2, "stencil weights mode must be 0, 1 or 2");
+  ctx->stencil_comp = mode;
+  // pot32 follows the mode (it carries the correction in mode 2 only); the
+  // legacy default stream orders this after work queued on blocking streams
+  if (int rc = psc_recast_pot32(ctx, nullptr)) return rc;
+  PSC_CUDA(ctx, cudaStreamSynchronize(nullptr));
   return 0;
 }
 

@@ -813,10 +813,14 @@ int psc_stencil_tma(psc_ctx* ctx, int k, const T* X, long ldx, const T* P, long 
   // edge masks: 818 us per step at 90^3, k = 307, against 995-1055 us for
   // 2-point runs and 894 us for scalar arithmetic); impl 2 / 3 ask for
   // 2-point runs when nx is even but not a multiple of 4, impl 3 / 4 for
-  // scalar arithmetic; compensated weights unless the context turned them off
+  // scalar arithmetic
   const int impl = ctx->stencil_impl;
   const bool narrow = sizeof(T) == 4 && ctx->nx % 4 != 0 && ctx->nx % 2 == 0 && (impl == 2 || impl == 3);
-  const int mode = (impl == 0 || impl == 2 ? 1 : 0) | (ctx->stencil_comp ? 2 : 0);
+  // the correction term in the kernel: weights mode 1, or mode 2 when this
+  // call's potential is not the FP32 potential that carries it
+  const bool comp = ctx->stencil_comp == 1 ||
+                    (ctx->stencil_comp == 2 && (const void*)pot != (const void*)ctx->pot32);
+  const int mode = (impl == 0 || impl == 2 ? 1 : 0) | (comp ? 2 : 0);
 #define PSC_TMA_ARGS ctx, k, X, ldx, P, ldp, Y, ldy, pot, w, coef, a, b, g, masked, st
 #define PSC_TMA_MODES(VWW)                                                                                    \
   switch (mode) {                                                                                             \

@@ -506,7 +506,10 @@ def test_fp32_stencil_has_no_eigenvalue_offset(impl, capsys):
     implementation computes the same operation order, so all four agree; the
     bar of 4e-8 catches a weight-rounding offset or an accumulation whose
     small terms are folded into a large sum (+2.3e-7).  "compensated" below
-    is weights mode 1."""
+    is weights mode 1 (the correction as a kernel term); mode 2 (the default)
+    carries it in the FP32 potential and must agree with mode 1, also under a
+    smooth nonzero potential, where fl(pot + correction) and fl(pot) +
+    correction round differently at every point but alike on average."""
     cfg = workloads.config_system("si87h76")
     dom = O.build_system(cfg["atoms"], h=cfg["h"], radius=cfg["radius"])
     ctx = gpu.GridContext(dom, 8)
@@ -515,27 +518,40 @@ def test_fp32_stencil_has_no_eigenvalue_offset(impl, capsys):
     k = W.shape[1]
     Wd = block(W)
     ctx.call("psc_set_stencil_impl", impl)
-    Y64 = torch.empty_like(Wd)
-    ctx.call("psc_apply_h", F64, gpu._p(Wd), ctx.n, gpu._p(Y64), ctx.n, k, gpu._stream())
-    q64 = np.einsum("nk,nk->k", W, host(Y64)) / np.einsum("nk,nk->k", W, W)
     W32 = Wd.float()
-    out = {}
-    for comp in (1, 0):
-        ctx.call("psc_set_stencil_weights", comp)
-        Y32 = torch.empty_like(W32)
-        ctx.call("psc_apply_h", F32, gpu._p(W32), ctx.n, gpu._p(Y32), ctx.n, k, gpu._stream())
-        out[comp] = np.einsum("nk,nk->k", W, host(Y32).astype(np.float64)) / np.einsum("nk,nk->k", W, W) - q64
-    ctx.call("psc_set_stencil_weights", 1)
+
+    def offsets(modes):
+        y64 = torch.empty_like(Wd)
+        ctx.call("psc_apply_h", F64, gpu._p(Wd), ctx.n, gpu._p(y64), ctx.n, k, gpu._stream())
+        r64 = np.einsum("nk,nk->k", W, host(y64)) / np.einsum("nk,nk->k", W, W)
+        res = {}
+        for comp in modes:
+            ctx.call("psc_set_stencil_weights", comp)
+            Y32 = torch.empty_like(W32)
+            ctx.call("psc_apply_h", F32, gpu._p(W32), ctx.n, gpu._p(Y32), ctx.n, k, gpu._stream())
+            res[comp] = np.einsum("nk,nk->k", W, host(Y32).astype(np.float64)) / np.einsum("nk,nk->k", W, W) - r64
+        return res
+
+    out = offsets((2, 1, 0))
+    # a smooth well of a few Ha (the scale of the local potential)
+    x = (np.arange(ctx.nx) - 0.5 * (ctx.nx - 1)) * dom["h"]
+    r2 = x[None, None, :] ** 2 + x[None, :, None] ** 2 + x[:, None, None] ** 2
+    gpu.Hamiltonian(ctx, torch.from_numpy((-3.0 * np.exp(-r2 / 40.0)).ravel()).to(DEV))
+    well = offsets((2, 1))
+    ctx.call("psc_set_stencil_weights", 2)
     ctx.call("psc_set_stencil_impl", 0)
     h = dom["h"]
     c0, c = 205.0 / 24.0, np.array([-8.0 / 5.0, 1.0 / 5.0, -8.0 / 315.0, 1.0 / 560.0])
     w0, wd = 0.5 * (c0 / h ** 2), 0.5 * (c / h ** 2)
     pred = (float(np.float32(w0)) - w0) + 6.0 * sum(float(np.float32(x)) - x for x in wd)
     with capsys.disabled():
-        print(f"\nimpl {impl}: FP32 - FP64 Rayleigh quotients, compensated {out[1]}, plain {out[0]} "
-              f"(predicted plain offset {pred:.3e} Ha)")
-    assert np.abs(out[1]).max() < 4e-8
+        print(f"\nimpl {impl}: FP32 - FP64 Rayleigh quotients, in the potential {out[2]}, compensated {out[1]}, "
+              f"plain {out[0]} (predicted plain offset {pred:.3e} Ha); under a well: in the potential "
+              f"{well[2]}, compensated {well[1]}")
+    assert np.abs(out[1]).max() < 4e-8 and np.abs(out[2]).max() < 4e-8
     assert np.abs((out[0] - out[1]) - pred).max() < 0.05 * abs(pred)
+    assert np.abs((out[0] - out[2]) - pred).max() < 0.05 * abs(pred)
+    assert np.abs(well[2] - well[1]).max() < 5e-9 and np.abs(well[2]).max() < 6e-8
     ctx.check_status()
 
 
