@@ -45,10 +45,11 @@ int psc_ctx_info(const psc_ctx* ctx, long* out);
 /* host flags[8] of device-side checks: [0] filter bounds inverted, [1]
  * Cholesky pivot <= 0 at column flags[1]-1, [3] TMA stencil wait timed out,
  * [4] persistent CG grid barrier timed out, [5] tensor-core Gram pipeline
- * wait timed out, [6] tensor-core block product pipeline wait timed out;
- * [2] reserved.  clear != 0 resets */
+ * wait timed out, [6] tensor-core block product pipeline wait timed out,
+ * [7] tensor-core convolution pipeline wait timed out; [2] reserved.
+ * clear != 0 resets */
 int psc_status(psc_ctx* ctx, int* host_flags, int clear, void* stream);
-/* Polls of every bounded device-side wait (status words 3-6) before the CTA
+/* Polls of every bounded device-side wait (status words 3-7) before the CTA
  * gives up, records its status word and returns; polls < 0 restores the
  * default (2^24; the CG grid barrier waits 4x as long).  0 makes every wait
  * run out at once (failure-path tests).  No counterpart in the reference. */

@@ -403,7 +403,7 @@ extern "C" int psc_status(psc_ctx* ctx, int* host_flags /* [8] */, int clear, vo
 }
 
 // Polls of every bounded device-side wait (stencil bulk-copy pipeline,
-// tensor-core Gram and block-product pipelines; the CG grid barrier waits 4x
+// tensor-core Gram, block-product and convolution pipelines; the CG grid barrier waits 4x
 // as long) before the CTA gives up and records its status word.  polls < 0
 // restores the default.  A test can set 0 to make every wait run out at once
 // and check that the failure is reported and the context stays usable.
