@@ -122,6 +122,7 @@ extern "C" int psc_ctx_destroy(psc_ctx* ctx) {
   psc_dfree(ctx->dm_pairs);
   psc_dfree(ctx->conv_wt);
   psc_dfree(ctx->pw_buf);
+  psc_dfree(ctx->dens_w);
   for (int a = 0; a < 3; ++a) { psc_dfree(ctx->spec_S[a]); psc_dfree(ctx->spec_lam[a]); }
   psc_dfree(ctx->spec_tmp); psc_dfree(ctx->lz_basis);
   if (ctx->cg_exec) cudaGraphExecDestroy(ctx->cg_exec);

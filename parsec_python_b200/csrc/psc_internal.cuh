@@ -121,6 +121,7 @@ struct psc_ctx {
   int gemm_tc = 1;               // 1: FP32 W T on tcgen05 (3xTF32), 0: CUDA cores
   float* tsplit = nullptr;       // T split into TF32 hi/lo B tiles
   size_t tsplit_floats = 0;
+  double* dens_w = nullptr;      // [1024] density weight per state (k_density_weights)
   // NumPy-order pairwise sum: leaf ranges and the tree above them for length pw_n
   long pw_n = 0;
   void* pw_buf = nullptr;

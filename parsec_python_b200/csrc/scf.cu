@@ -257,19 +257,11 @@ extern "C" int psc_occupations(psc_ctx* ctx, const double* lam_dev, int n, doubl
 // hrhs = 4pi/h^3 (rho_raw - rho0), rho = rho_raw / h^3 (rsdft_solver.py:327-328)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_density(const T* __restrict__ W, long ld, int nev, const double* __restrict__ occ,
-                          const double* __restrict__ norm_part, const double* __restrict__ rho0,
-                          double* __restrict__ rho, double* __restrict__ hrhs, long n, double fourpi_h3, double h3) {
+__global__ void k_density(const T* __restrict__ W, long ld, int nev, const double* __restrict__ wgt,
+                          const double* __restrict__ rho0, double* __restrict__ rho, double* __restrict__ hrhs, long n,
+                          double fourpi_h3, double h3) {
   __shared__ double f2[1024];
-  for (int i = threadIdx.x; i < nev; i += blockDim.x) {
-    double w = 2 * occ[i];
-    if (norm_part) {
-      double nn = 0.0;
-      for (int c = 0; c < PSC_NORM_CHUNKS; ++c) nn += norm_part[(long)i * PSC_NORM_CHUNKS + c];
-      w /= nn;
-    }
-    f2[i] = w;
-  }
+  for (int i = threadIdx.x; i < nev; i += blockDim.x) f2[i] = wgt[i];
   __syncthreads();
   for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     double s = 0.0;
@@ -279,6 +271,22 @@ __global__ void k_density(const T* __restrict__ W, long ld, int nev, const doubl
     }
     if (hrhs) hrhs[p] = fourpi_h3 * (s - rho0[p]);
     rho[p] = s / h3;
+  }
+}
+
+// the density weight of each state, 2 occ_i, divided for FP32 blocks by the
+// state's exact squared norm (its PSC_NORM_CHUNKS partials summed in order);
+// formed once per call instead of in every block of k_density
+__global__ void k_density_weights(const double* __restrict__ occ, const double* __restrict__ norm_part, int nev,
+                                  double* __restrict__ wgt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nev; i += gridDim.x * blockDim.x) {
+    double w = 2 * occ[i];
+    if (norm_part) {
+      double nn = 0.0;
+      for (int c = 0; c < PSC_NORM_CHUNKS; ++c) nn += norm_part[(long)i * PSC_NORM_CHUNKS + c];
+      w /= nn;
+    }
+    wgt[i] = w;
   }
 }
 
@@ -312,8 +320,11 @@ extern "C" int psc_density(psc_ctx* ctx, int dtype, const void* W, long ld, int 
   PSC_REQUIRE(ctx, W && occ_dev && rho && ld >= ctx->n && (!hrhs || rho0), "density: bad arguments");
   cudaStream_t st = (cudaStream_t)stream;
   const int nb = 148 * 8;
+  if (!ctx->dens_w) PSC_CUDA(ctx, psc_dmalloc(&ctx->dens_w, 1024 * sizeof(double)));
   if (dtype == PSC_F64) {
-    k_density<double><<<nb, 256, 0, st>>>((const double*)W, ld, nev, occ_dev, nullptr, rho0, rho, hrhs, ctx->n,
+    k_density_weights<<<1, 1024, 0, st>>>(occ_dev, nullptr, nev, ctx->dens_w);
+    PSC_LAUNCH_CHECK(ctx);
+    k_density<double><<<nb, 256, 0, st>>>((const double*)W, ld, nev, ctx->dens_w, rho0, rho, hrhs, ctx->n,
                                           fourpi_h3, h3);
   } else {
     if (ctx->col_norm_cap < nev) {
@@ -327,8 +338,10 @@ extern "C" int psc_density(psc_ctx* ctx, int dtype, const void* W, long ld, int 
     k_colnorm_part<<<dim3(PSC_NORM_CHUNKS, nev), 256, 0, st>>>((const float*)W, ld, ctx->n, chunk,
                                                                ctx->col_norm_part);
     PSC_LAUNCH_CHECK(ctx);
-    k_density<float><<<nb, 256, 0, st>>>((const float*)W, ld, nev, occ_dev, ctx->col_norm_part, rho0, rho, hrhs,
-                                         ctx->n, fourpi_h3, h3);
+    k_density_weights<<<1, 1024, 0, st>>>(occ_dev, ctx->col_norm_part, nev, ctx->dens_w);
+    PSC_LAUNCH_CHECK(ctx);
+    k_density<float><<<nb, 256, 0, st>>>((const float*)W, ld, nev, ctx->dens_w, rho0, rho, hrhs, ctx->n,
+                                         fourpi_h3, h3);
   }
   PSC_LAUNCH_CHECK(ctx);
   return 0;
