@@ -223,6 +223,19 @@ def test_quasi_inverse_from_gram_matches_pivoted_qr(kind):
     assert ((got != 0) == (ref != 0)).all()
 
 
+def test_input_file_selects_the_anderson_mixer(tmp_path):
+    """`mixer = anderson` in the settings block of an .in file (a key of this
+    library; the reference has no mixer key) reaches the solver settings."""
+    f = tmp_path / "h2o_anderson.in"
+    f.write_text(SAMPLE_IN.replace("diagmeth = 3", "diagmeth = 3\nmixer = anderson"))
+    assert "mixer = anderson" in f.read_text()
+    s = SolverSettings()
+    data = prepare_input_data(s, str(f))
+    s.apply_overrides(data.settings_overrides)
+    s.normalize()
+    assert (s.mixer, s.mix_group_size) == ("msecant2", 0)
+
+
 def test_settings_select_the_anderson_mixer():
     s = SolverSettings()
     assert s.mixer == "msecant1"
